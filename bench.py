@@ -1,0 +1,350 @@
+"""Ant env-steps/s on B200: the batched FP64 Newton substep behind Physics.
+
+Workload (one bench step = one substep of every env, fresh controls):
+  Ant (nq=15, nv=14, nu=8, 57 candidate pairs, plane floor), dt 0.01,
+  Newton with tolerance 1e-10 and a 30-iteration cap, 4096 envs per GPU,
+  qpos = qpos0 + U[-0.1, 0.1], qvel ~ N(0, 0.1^2), ctrl ~ U[-1, 1] each step,
+  from seeded generators (synthetic; no dataset).
+
+Output: one JSON line (rank 0). `value` times pg_step_device with the
+controls already in HBM (L2 flushed between timed steps by writing a 256 MB
+buffer outside the timed events); `e2e` times the C-ABI path with host
+buffers (pinned controls in, qpos out) every step. `--impl reference` times
+the CPU restatement of the reference engine (oracle/) on all host cores on
+the same workload. Multi-GPU: one process per GPU, envs sharded (weak
+scaling, no data-path collective), max time over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+TOL = 1e-10
+ITERS = 30
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--envs", type=int, default=4096, help="envs per GPU")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    return ap.parse_args()
+
+
+def workload(envs):
+    return {"workload": f"ant: {envs} envs/GPU, dt 0.01, Newton tol 1e-10 cap {ITERS}, "
+                        "qpos0+U[-0.1,0.1], qvel N(0,0.1^2), ctrl U[-1,1] per step",
+            "model": "ant (nq 15, nv 14, nu 8)", "envs_per_gpu": envs, "substeps_per_step": 1,
+            "l2": "flushed between timed steps (256 MB write)"}
+
+
+def initial_state(m, n, seed):
+    rng = np.random.default_rng(seed)
+    q = np.tile(np.array(m.qpos0), (n, 1)) + rng.uniform(-0.1, 0.1, (n, m.nq))
+    v = rng.normal(0.0, 0.1, (n, m.nv))
+    return q, v, rng
+
+
+def dist_setup(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+# ------------------------------------------------------------------ CPU legs
+def cpu_rollout_rate(blob, m, envs, seconds, fast=True):
+    """Oracle rollout (batch.rs:46-59 shape) on all host threads, repeated
+    until `seconds` of work; returns (env-steps/s, threads, sample text)."""
+    from oracle.oracle import QPOS, QVEL, Oracle
+    o = Oracle(blob, envs, threads=0, fast=fast)
+    o.set_solver(tolerance=TOL, iterations=ITERS)
+    q, v, rng = initial_state(m, envs, 1)
+    o.set(QPOS, q)
+    o.set(QVEL, v)
+    nstep = 200
+    done, t0, reps = 0, time.perf_counter(), 0
+    while True:
+        ctrl = rng.uniform(-1, 1, (envs, nstep, m.nu))
+        o.rollout(ctrl, record=False)
+        done += envs * nstep
+        reps += 1
+        el = time.perf_counter() - t0
+        if el >= seconds or reps >= 50:
+            break
+    return done / el, o.threads, f"Ant {envs} envs x {nstep} steps rollout x {reps} (oracle, {o.threads} threads)"
+
+
+def algorithmic_flops(blob, m, envs=256, steps=120):
+    """FP64 operations per Ant env-step of the reference algorithm as written
+    (the oracle's per-stage counters, averaged over a seeded trajectory)."""
+    from oracle.oracle import QPOS, QVEL, Oracle
+    o = Oracle(blob, envs, threads=0, fast=False)
+    o.set_solver(tolerance=TOL, iterations=ITERS)
+    q, v, rng = initial_state(m, envs, 2)
+    o.set(QPOS, q)
+    o.set(QVEL, v)
+    o.flops(reset=True)
+    o.rollout(rng.uniform(-1, 1, (envs, steps, m.nu)), record=False)
+    f = o.flops()
+    return sum(f.values()) / (envs * steps), {k: v / (envs * steps) for k, v in f.items()}
+
+
+def run_reference(args):
+    """--impl reference: the oracle on the host cores, same workload."""
+    ws, rank, _ = dist_setup(args)
+    if rank != 0:
+        return
+    from oracle.oracle import CTRL, QPOS, QVEL, Oracle
+    from pippin_b200 import mjcf, scenes
+    xml = scenes.ant_xml()
+    m = mjcf.load_string(xml)
+    blob = mjcf.to_blob(m)
+    n = args.envs * max(args.gpus, 1)
+    o = Oracle(blob, n, threads=0, fast=True)
+    o.set_solver(tolerance=TOL, iterations=ITERS)
+    q, v, rng = initial_state(m, n, 1)
+    o.set(QPOS, q)
+    o.set(QVEL, v)
+    ctrls = [rng.uniform(-1, 1, (n, m.nu)) for _ in range(args.warmup + args.steps)]
+    for k in range(args.warmup):
+        o.set(CTRL, ctrls[k])
+        o.step(0, n, 1)
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        o.set(CTRL, ctrls[args.warmup + k])
+        o.step(0, n, 1)
+    el = time.perf_counter() - t0
+    value = n * args.steps / el
+    line = {"metric": "Ant env-steps/s", "value": value, "unit": "env-steps/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict(workload(args.envs), parallelism=f"{o.threads} host threads"), "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": "env-steps/s", "cores": o.threads, "kind": "port",
+                             "sample": f"Ant {n} envs x {args.steps} steps (Physics::step shape, per-step ctrl)"},
+            "e2e": {"value": value, "unit": "env-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax = float(p[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, p[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ our arm
+def run_ours(args):
+    import torch
+
+    from pippin_b200 import CudaPhysics, Field, mjcf, scenes
+    from pippin_b200.physics import WarmStart, fp64_peak
+
+    ws, rank, local = dist_setup(args)
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    xml = scenes.ant_xml(tolerance=TOL, iterations=ITERS)
+    m = mjcf.load_string(xml)
+    blob = mjcf.to_blob(m)
+    n = args.envs
+    phys = CudaPhysics(blob, n, device=local)
+    q, v, rng = initial_state(m, n, 1000 + rank)
+    phys.set(Field.QPOS, range(n), q)
+    phys.set(Field.QVEL, range(n), v)
+    phys.autotune(nstep=1)
+    # restore the start state the autotuner trialled from (it restores itself)
+    lanes, per_block, blocks = phys.launch()
+
+    K, W = args.steps, args.warmup
+    ctrl_all = torch.from_numpy(rng.uniform(-1, 1, (W + K, n, m.nu))).to(dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.ExternalStream(phys.stream(), device=dev)
+
+    def barrier():
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def timed_device_loop(ctrl, steps, warm):
+        phys.set_solver(warm=int(warm))
+        for k in range(W):
+            phys.step_device(range(n), 1, ctrl[k].data_ptr())
+        phys.synchronize()
+        barrier()
+        total_ms = 0.0
+        for k in range(steps):
+            flush.fill_(float(k))
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            phys.step_device(range(n), 1, ctrl[W + k].data_ptr())
+            e1.record(stream)
+            e1.synchronize()
+            total_ms += e0.elapsed_time(e1)
+        barrier()
+        return total_ms
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms_ref = timed_device_loop(ctrl_all, K, WarmStart.REF_PREV_QACC)
+    clock_info = clocks.stop()
+    st = phys.stats()
+    # cold-start Newton on the same trajectory distribution (fresh state)
+    phys.set(Field.QPOS, range(n), q)
+    phys.set(Field.QVEL, range(n), v)
+    ms_cold = timed_device_loop(ctrl_all, K, WarmStart.COLD)
+    st_cold = phys.stats()
+    phys.set_solver(warm=int(WarmStart.REF_PREV_QACC))
+
+    # end to end through the C-ABI with host buffers
+    pin_ctrl = torch.empty((n, m.nu), dtype=torch.float64, pin_memory=True).numpy()
+    pin_q = torch.empty((n, m.nq), dtype=torch.float64, pin_memory=True).numpy()
+    ctrl_host = ctrl_all.cpu().numpy()
+    phys.set(Field.QPOS, range(n), q)
+    phys.set(Field.QVEL, range(n), v)
+    for k in range(W):
+        pin_ctrl[:] = ctrl_host[k]
+        phys.set(Field.CTRL, range(n), pin_ctrl)
+        phys.step(range(n), 1)
+        phys.get(Field.QPOS, range(n), out=pin_q)
+    barrier()
+    e2e_ms = 0.0
+    for k in range(K):
+        pin_ctrl[:] = ctrl_host[W + k]
+        flush.fill_(float(k))
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        phys.set(Field.CTRL, range(n), pin_ctrl)
+        phys.step(range(n), 1)
+        phys.get(Field.QPOS, range(n), out=pin_q)
+        e1.record(stream)
+        e1.synchronize()
+        e2e_ms += e0.elapsed_time(e1)
+    barrier()
+
+    times = torch.tensor([ms_ref, ms_cold, e2e_ms], dtype=torch.float64, device=dev)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.all_reduce(times, op=dist.ReduceOp.MAX)
+    ms_ref, ms_cold, e2e_ms = (float(x) for x in times.cpu())
+    total_env_steps = n * ws * K
+    value = total_env_steps / (ms_ref * 1e-3)
+    value_cold = total_env_steps / (ms_cold * 1e-3)
+    e2e = total_env_steps / (e2e_ms * 1e-3)
+
+    if rank == 0:
+        peak = fp64_peak(local)
+        flops_step, per_stage = algorithmic_flops(blob, m)
+        per_launch_ms = ms_ref / K
+        achieved = flops_step * n / (per_launch_ms * 1e-3) / 1e12
+        bytes_step = (m.nq + m.nv + m.nv + m.nu) * 8 + (m.nq + m.nv + m.nv) * 8
+        line = {
+            "metric": "Ant env-steps/s", "value": value, "unit": "env-steps/s", "n_gpus": ws, "steps": K,
+            "warmup": W, "ms_per_step": ms_ref / K, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict(workload(n), parallelism=f"env-sharded x{ws} (no collective)",
+                           launch={"lanes_per_env": lanes, "envs_per_block": per_block, "blocks": blocks}),
+            "e2e": {"value": e2e, "unit": "env-steps/s", "h2d_bytes_per_step": n * m.nu * 8,
+                    "d2h_bytes_per_step": n * m.nq * 8},
+            "gpu_launches": K,
+            "variants": {"newton_ref_prev_qacc": value, "newton_cold": value_cold,
+                         "mean_iters_ref": float(st["iters"].mean()), "mean_iters_cold": float(st_cold["iters"].mean()),
+                         "p99_iters_ref": float(np.percentile(st["iters"], 99)),
+                         "mean_ncon": float(st["ncon"].mean()), "mean_rows": float(st["nrows"].mean())},
+            "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "note": f"{flops_step:.0f} algorithmic FP64 ops per env-step (oracle counters) x {n} envs "
+                                 "per launch / step-kernel time; peak = live DFMA microbenchmark (pg_fp64_peak)",
+                         "hbm_achieved_gbs": bytes_step * n / (per_launch_ms * 1e-3) / 1e9},
+            "clocks": clock_info,
+        }
+        if ws == 1 and not args.no_cpu_baseline:
+            rate, cores, sample = cpu_rollout_rate(blob, m, 1024, args.cpu_seconds)
+            line["cpu_baseline"] = {"value": rate, "unit": "env-steps/s", "cores": cores, "kind": "port",
+                                    "sample": sample}
+        print(json.dumps(line), flush=True)
+    phys.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

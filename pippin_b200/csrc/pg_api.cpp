@@ -1,0 +1,1527 @@
+// Host side of the C-ABI (include/pippin_b200.h): model blob parsing, the
+// derived device model (tree levels, children lists, dof-chain masks, work
+// caps), per-env parameter blocks and state in HBM, launch configuration,
+// CUDA-graph replay of the step, and the Physics-trait entry points.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/pippin_b200.h"
+#include "pg_kernels.h"
+#include "pg_model.h"
+
+using namespace pg;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+int cuda_fail(cudaError_t e, const char* what) {
+  g_err = std::string(what) + ": " + cudaGetErrorString(e);
+  return PG_ERR_CUDA;
+}
+#define CK(call)                                  \
+  do {                                            \
+    cudaError_t _e = (call);                      \
+    if (_e != cudaSuccess) return cuda_fail(_e, #call); \
+  } while (0)
+
+// ---------------------------------------------------------------- blob
+struct BlobArr {
+  uint32_t dtype = 0;
+  uint64_t count = 0;
+  const uint8_t* data = nullptr;
+};
+
+struct Blob {
+  std::map<std::string, BlobArr> a;
+  bool parse(const void* p, size_t bytes, std::string* err) {
+    const uint8_t* b = (const uint8_t*)p;
+    if (!p || bytes < 16 || std::memcmp(b, "PGBLOB01", 8) != 0) {
+      *err = "model blob: bad magic";
+      return false;
+    }
+    uint32_t ver, n;
+    std::memcpy(&ver, b + 8, 4);
+    std::memcpy(&n, b + 12, 4);
+    if (ver != 1) {
+      *err = "model blob: unsupported version";
+      return false;
+    }
+    if (16 + 64ull * n > bytes) {
+      *err = "model blob: truncated directory";
+      return false;
+    }
+    for (uint32_t i = 0; i < n; i++) {
+      const uint8_t* e = b + 16 + 64ull * i;
+      char name[41];
+      std::memcpy(name, e, 40);
+      name[40] = 0;
+      BlobArr x;
+      uint64_t off;
+      std::memcpy(&x.dtype, e + 40, 4);
+      std::memcpy(&x.count, e + 48, 8);
+      std::memcpy(&off, e + 56, 8);
+      uint64_t es = x.dtype == 3 ? 1 : 8;
+      if (x.dtype < 1 || x.dtype > 3 || off % 8 || x.count > bytes || off + x.count * es > bytes) {
+        *err = std::string("model blob: bad entry ") + name;
+        return false;
+      }
+      x.data = b + off;
+      a[name] = x;
+    }
+    return true;
+  }
+  template <class T>
+  bool get(const char* name, uint32_t dtype, std::vector<T>& out, long expect, std::string* err) {
+    auto it = a.find(name);
+    if (it == a.end() || it->second.dtype != dtype || (expect >= 0 && (long)it->second.count != expect)) {
+      *err = std::string("model blob: missing or mis-sized array ") + name;
+      return false;
+    }
+    out.resize(it->second.count);
+    if (dtype == 1) {
+      std::vector<double> tmp(it->second.count);
+      std::memcpy(tmp.data(), it->second.data, 8 * tmp.size());
+      for (size_t k = 0; k < tmp.size(); k++) out[k] = (T)tmp[k];
+    } else if (dtype == 2) {
+      std::vector<int64_t> tmp(it->second.count);
+      std::memcpy(tmp.data(), it->second.data, 8 * tmp.size());
+      for (size_t k = 0; k < tmp.size(); k++) out[k] = (T)tmp[k];
+    } else {
+      for (size_t k = 0; k < it->second.count; k++) out[k] = (T)it->second.data[k];
+    }
+    return true;
+  }
+  std::vector<std::string> names(const char* name) {
+    std::vector<std::string> out;
+    auto it = a.find(name);
+    if (it == a.end()) return out;
+    std::string cur;
+    for (uint64_t k = 0; k < it->second.count; k++) {
+      char c = (char)it->second.data[k];
+      if (c == 0) {
+        out.push_back(cur);
+        cur.clear();
+      } else {
+        cur.push_back(c);
+      }
+    }
+    return out;
+  }
+};
+
+// ---------------------------------------------------------------- host model
+struct HostModel {
+  int nq = 0, nv = 0, nu = 0, nbody = 0, njnt = 0, ngeom = 0, ncam = 0, neq = 0, nmesh = 0;
+  double timestep = 0, gravity[3] = {0, 0, 0};
+  int integrator = 0, solver = 0, iterations = 0;
+  double tolerance = 0, margin = 0, solref[2] = {0, 0}, solimp[5] = {0, 0, 0, 0, 0}, impratio = 0, hertz = 0,
+         dampratio = 0, slop = 0;
+  std::vector<int> body_parent, body_jntadr, body_jntnum, body_dofadr, body_dofnum, body_lastdof, body_weldid;
+  std::vector<double> body_pos, body_quat, body_mass, body_ipos, body_inertia;
+  std::vector<int> jnt_type, jnt_body, jnt_qposadr, jnt_dofadr, jnt_limited;
+  std::vector<double> jnt_pos, jnt_axis, jnt_range, jnt_stiffness, jnt_springref;
+  std::vector<int> dof_body, dof_jnt, dof_parent;
+  std::vector<double> dof_damping, dof_armature;
+  std::vector<int> geom_type, geom_body, geom_dataid, geom_group, geom_contype, geom_conaffinity;
+  std::vector<double> geom_pos, geom_quat, geom_size, geom_friction, geom_rgba;
+  std::vector<int> cam_body;
+  std::vector<double> cam_pos, cam_quat, cam_fovy;
+  std::vector<int> act_joint, act_ctrllimited, act_forcelimited, act_moment_adr, act_moment_num, moment_jnt;
+  std::vector<double> act_gear, act_gain, act_bias, act_ctrlrange, act_forcerange, moment_coef;
+  std::vector<int> eq_j1, eq_j2;
+  std::vector<double> eq_poly, eq_solref, eq_solimp;
+  std::vector<int> dof_blocks, pairs;
+  std::vector<double> qpos0, qpos_reset;
+  std::vector<int> hull_vadr, hull_vnum, hull_tadr, hull_tnum, hull_tri;
+  std::vector<double> hull_vert;
+  std::vector<int> mesh_vadr, mesh_vnum, mesh_tadr, mesh_tnum, mesh_tri;
+  std::vector<double> mesh_vert;
+  std::vector<std::string> names[6];  // body, geom, camera, mesh, joint, actuator
+};
+
+bool load_model(const void* blob, size_t bytes, HostModel& m, std::string* err) {
+  Blob b;
+  if (!b.parse(blob, bytes, err)) return false;
+  std::vector<double> f;
+  std::vector<int> i;
+#define F1(name, dst)                                  \
+  if (!b.get(name, 1, f, 1, err)) return false;        \
+  dst = f[0];
+#define I1(name, dst)                                  \
+  if (!b.get(name, 2, i, 1, err)) return false;        \
+  dst = i[0];
+  F1("timestep", m.timestep);
+  if (!b.get("gravity", 1, f, 3, err)) return false;
+  for (int k = 0; k < 3; k++) m.gravity[k] = f[k];
+  I1("integrator", m.integrator);
+  I1("opt_solver", m.solver);
+  I1("opt_iterations", m.iterations);
+  F1("opt_tolerance", m.tolerance);
+  F1("opt_margin", m.margin);
+  if (!b.get("opt_solref", 1, f, 2, err)) return false;
+  m.solref[0] = f[0];
+  m.solref[1] = f[1];
+  if (!b.get("opt_solimp", 1, f, 5, err)) return false;
+  for (int k = 0; k < 5; k++) m.solimp[k] = f[k];
+  F1("opt_impratio", m.impratio);
+  F1("opt_hertz", m.hertz);
+  F1("opt_dampratio", m.dampratio);
+  F1("opt_slop", m.slop);
+#undef F1
+#undef I1
+  std::vector<long> dims;
+  if (!b.get("dims", 2, dims, 9, err)) return false;
+  m.nq = (int)dims[0];
+  m.nv = (int)dims[1];
+  m.nu = (int)dims[2];
+  m.nbody = (int)dims[3];
+  m.njnt = (int)dims[4];
+  m.ngeom = (int)dims[5];
+  m.ncam = (int)dims[6];
+  m.neq = (int)dims[7];
+  m.nmesh = (int)dims[8];
+  long nb = m.nbody, nj = m.njnt, nv = m.nv, ng = m.ngeom, nc = m.ncam, nu = m.nu, ne = m.neq, nm = m.nmesh;
+  bool ok = b.get("body_parent", 2, m.body_parent, nb, err) && b.get("body_jntadr", 2, m.body_jntadr, nb, err) &&
+            b.get("body_jntnum", 2, m.body_jntnum, nb, err) && b.get("body_dofadr", 2, m.body_dofadr, nb, err) &&
+            b.get("body_dofnum", 2, m.body_dofnum, nb, err) && b.get("body_lastdof", 2, m.body_lastdof, nb, err) &&
+            b.get("body_weldid", 2, m.body_weldid, nb, err) && b.get("body_pos", 1, m.body_pos, 3 * nb, err) &&
+            b.get("body_quat", 1, m.body_quat, 4 * nb, err) && b.get("body_mass", 1, m.body_mass, nb, err) &&
+            b.get("body_ipos", 1, m.body_ipos, 3 * nb, err) && b.get("body_inertia", 1, m.body_inertia, 9 * nb, err) &&
+            b.get("jnt_type", 2, m.jnt_type, nj, err) && b.get("jnt_body", 2, m.jnt_body, nj, err) &&
+            b.get("jnt_qposadr", 2, m.jnt_qposadr, nj, err) && b.get("jnt_dofadr", 2, m.jnt_dofadr, nj, err) &&
+            b.get("jnt_limited", 2, m.jnt_limited, nj, err) && b.get("jnt_pos", 1, m.jnt_pos, 3 * nj, err) &&
+            b.get("jnt_axis", 1, m.jnt_axis, 3 * nj, err) && b.get("jnt_range", 1, m.jnt_range, 2 * nj, err) &&
+            b.get("jnt_stiffness", 1, m.jnt_stiffness, nj, err) && b.get("jnt_springref", 1, m.jnt_springref, nj, err) &&
+            b.get("dof_body", 2, m.dof_body, nv, err) && b.get("dof_jnt", 2, m.dof_jnt, nv, err) &&
+            b.get("dof_parent", 2, m.dof_parent, nv, err) && b.get("dof_damping", 1, m.dof_damping, nv, err) &&
+            b.get("dof_armature", 1, m.dof_armature, nv, err) && b.get("geom_type", 2, m.geom_type, ng, err) &&
+            b.get("geom_body", 2, m.geom_body, ng, err) && b.get("geom_dataid", 2, m.geom_dataid, ng, err) &&
+            b.get("geom_group", 2, m.geom_group, ng, err) && b.get("geom_contype", 2, m.geom_contype, ng, err) &&
+            b.get("geom_conaffinity", 2, m.geom_conaffinity, ng, err) && b.get("geom_pos", 1, m.geom_pos, 3 * ng, err) &&
+            b.get("geom_quat", 1, m.geom_quat, 4 * ng, err) && b.get("geom_size", 1, m.geom_size, 3 * ng, err) &&
+            b.get("geom_friction", 1, m.geom_friction, ng, err) && b.get("geom_rgba", 1, m.geom_rgba, 4 * ng, err) &&
+            b.get("cam_body", 2, m.cam_body, nc, err) && b.get("cam_pos", 1, m.cam_pos, 3 * nc, err) &&
+            b.get("cam_quat", 1, m.cam_quat, 4 * nc, err) && b.get("cam_fovy", 1, m.cam_fovy, nc, err) &&
+            b.get("actuator_joint", 2, m.act_joint, nu, err) &&
+            b.get("actuator_ctrllimited", 2, m.act_ctrllimited, nu, err) &&
+            b.get("actuator_forcelimited", 2, m.act_forcelimited, nu, err) &&
+            b.get("actuator_gear", 1, m.act_gear, nu, err) && b.get("actuator_gain", 1, m.act_gain, nu, err) &&
+            b.get("actuator_bias", 1, m.act_bias, 3 * nu, err) &&
+            b.get("actuator_ctrlrange", 1, m.act_ctrlrange, 2 * nu, err) &&
+            b.get("actuator_forcerange", 1, m.act_forcerange, 2 * nu, err) &&
+            b.get("actuator_moment_adr", 2, m.act_moment_adr, nu, err) &&
+            b.get("actuator_moment_num", 2, m.act_moment_num, nu, err) && b.get("moment_jnt", 2, m.moment_jnt, -1, err) &&
+            b.get("moment_coef", 1, m.moment_coef, (long)m.moment_jnt.size(), err) &&
+            b.get("eq_joint1", 2, m.eq_j1, ne, err) && b.get("eq_joint2", 2, m.eq_j2, ne, err) &&
+            b.get("eq_polycoef", 1, m.eq_poly, 5 * ne, err) && b.get("eq_solref", 1, m.eq_solref, 2 * ne, err) &&
+            b.get("eq_solimp", 1, m.eq_solimp, 5 * ne, err) && b.get("dof_blocks", 2, m.dof_blocks, -1, err) &&
+            b.get("pair_candidates", 2, m.pairs, -1, err) && b.get("qpos0", 1, m.qpos0, m.nq, err) &&
+            b.get("qpos_reset", 1, m.qpos_reset, m.nq, err) && b.get("hull_vert_adr", 2, m.hull_vadr, nm, err) &&
+            b.get("hull_vert_num", 2, m.hull_vnum, nm, err) && b.get("hull_vert", 1, m.hull_vert, -1, err) &&
+            b.get("hull_tri_adr", 2, m.hull_tadr, nm, err) && b.get("hull_tri_num", 2, m.hull_tnum, nm, err) &&
+            b.get("hull_tri", 2, m.hull_tri, -1, err) && b.get("mesh_vert_adr", 2, m.mesh_vadr, nm, err) &&
+            b.get("mesh_vert_num", 2, m.mesh_vnum, nm, err) && b.get("mesh_vert", 1, m.mesh_vert, -1, err) &&
+            b.get("mesh_tri_adr", 2, m.mesh_tadr, nm, err) && b.get("mesh_tri_num", 2, m.mesh_tnum, nm, err) &&
+            b.get("mesh_tri", 2, m.mesh_tri, -1, err);
+  if (!ok) return false;
+  const char* tables[6] = {"names_body", "names_geom", "names_cam", "names_mesh", "names_jnt", "names_actuator"};
+  for (int t = 0; t < 6; t++) m.names[t] = b.names(tables[t]);
+  // structural checks the kernels rely on
+  if (m.nv > NV_MAX) {
+    *err = "model has more than 64 degrees of freedom (dof-chain masks are 64-bit)";
+    return false;
+  }
+  if (m.dof_blocks.size() / 2 > 64) {
+    *err = "model has more than 64 independent trees";
+    return false;
+  }
+  for (int b2 = 1; b2 < m.nbody; b2++)
+    if (m.body_parent[b2] < 0 || m.body_parent[b2] >= b2) {
+      *err = "model blob: bodies must follow their parents";
+      return false;
+    }
+  for (int g = 0; g < m.ngeom; g++)
+    if (m.geom_body[g] < 0 || m.geom_body[g] >= m.nbody) {
+      *err = "model blob: geom_body out of range";
+      return false;
+    }
+  for (size_t k = 0; k < m.pairs.size(); k++)
+    if (m.pairs[k] < 0 || m.pairs[k] >= m.ngeom) {
+      *err = "model blob: pair_candidates out of range";
+      return false;
+    }
+  // every index a kernel follows must stay in range, and every parent chain
+  // must end: a corrupt blob is rejected here instead of reaching the GPU
+  auto bad = [&](const char* what) {
+    *err = std::string("model blob: ") + what + " out of range";
+    return false;
+  };
+  for (int k = 0; k < m.nv; k++) {
+    if (m.dof_parent[k] < -1 || m.dof_parent[k] >= k) return bad("dof_parent");
+    if (m.dof_body[k] < 1 || m.dof_body[k] >= m.nbody) return bad("dof_body");
+  }
+  for (int b = 0; b < m.nbody; b++) {
+    if (m.body_lastdof[b] < -1 || m.body_lastdof[b] >= m.nv) return bad("body_lastdof");
+    if (m.body_jntadr[b] < 0 || m.body_jntnum[b] < 0 || m.body_jntadr[b] + m.body_jntnum[b] > m.njnt)
+      return bad("body joints");
+    if (m.body_dofadr[b] < 0 || m.body_dofnum[b] < 0 || m.body_dofadr[b] + m.body_dofnum[b] > m.nv)
+      return bad("body dofs");
+  }
+  for (int j = 0; j < m.njnt; j++) {
+    int t = m.jnt_type[j];
+    int nqj = t == JNT_FREE ? 7 : (t == JNT_BALL ? 4 : 1), nvj = t == JNT_FREE ? 6 : (t == JNT_BALL ? 3 : 1);
+    if (t < 0 || t > 3) return bad("jnt_type");
+    if (m.jnt_qposadr[j] < 0 || m.jnt_qposadr[j] + nqj > m.nq) return bad("jnt_qposadr");
+    if (m.jnt_dofadr[j] < 0 || m.jnt_dofadr[j] + nvj > m.nv) return bad("jnt_dofadr");
+  }
+  for (int g = 0; g < m.ngeom; g++) {
+    if (m.geom_type[g] < 0 || m.geom_type[g] > 5) return bad("geom_type");
+    if (m.geom_type[g] == GEOM_MESH && (m.geom_dataid[g] < 0 || m.geom_dataid[g] >= m.nmesh)) return bad("geom_dataid");
+  }
+  long nhv = (long)m.hull_vert.size() / 3, nht = (long)m.hull_tri.size() / 3;
+  for (int i = 0; i < m.nmesh; i++) {
+    if (m.hull_vadr[i] < 0 || m.hull_vnum[i] < 1 || m.hull_vadr[i] + m.hull_vnum[i] > nhv) return bad("hull vertices");
+    if (m.hull_tadr[i] < 0 || m.hull_tnum[i] < 0 || m.hull_tadr[i] + m.hull_tnum[i] > nht) return bad("hull triangles");
+    for (int t = 0; t < 3 * m.hull_tnum[i]; t++) {
+      int v = m.hull_tri[3 * m.hull_tadr[i] + t];
+      if (v < 0 || v >= m.hull_vnum[i]) return bad("hull triangle vertex");
+    }
+    long nmv = (long)m.mesh_vert.size() / 3, nmt = (long)m.mesh_tri.size() / 3;
+    if (m.mesh_vadr[i] < 0 || m.mesh_vnum[i] < 0 || m.mesh_vadr[i] + m.mesh_vnum[i] > nmv) return bad("mesh vertices");
+    if (m.mesh_tadr[i] < 0 || m.mesh_tnum[i] < 0 || m.mesh_tadr[i] + m.mesh_tnum[i] > nmt) return bad("mesh triangles");
+  }
+  for (int c = 0; c < m.ncam; c++)
+    if (m.cam_body[c] < 0 || m.cam_body[c] >= m.nbody) return bad("cam_body");
+  for (int u = 0; u < m.nu; u++) {
+    if (m.act_moment_adr[u] < 0 || m.act_moment_num[u] < 1 ||
+        m.act_moment_adr[u] + m.act_moment_num[u] > (int)m.moment_jnt.size())
+      return bad("actuator_moment");
+  }
+  for (int j : m.moment_jnt)
+    if (j < 0 || j >= m.njnt || (m.jnt_type[j] != JNT_HINGE && m.jnt_type[j] != JNT_SLIDE)) return bad("moment_jnt");
+  for (int e = 0; e < m.neq; e++) {
+    if (m.eq_j1[e] < 0 || m.eq_j1[e] >= m.njnt) return bad("eq_joint1");
+    if (m.eq_j2[e] < -1 || m.eq_j2[e] >= m.njnt) return bad("eq_joint2");
+  }
+  if (m.dof_blocks.size() % 2 || m.pairs.size() % 2) return bad("dof_blocks/pairs layout");
+  {
+    int expect = 0;
+    for (size_t k = 0; k + 1 < m.dof_blocks.size(); k += 2) {
+      if (m.dof_blocks[k] != expect || m.dof_blocks[k + 1] <= m.dof_blocks[k]) return bad("dof_blocks");
+      expect = m.dof_blocks[k + 1];
+    }
+    if (expect != m.nv) return bad("dof_blocks");
+  }
+  if (!(m.timestep > 0.0) || !std::isfinite(m.timestep)) return bad("timestep");
+  if (m.hertz <= 0.0) m.hertz = 0.25 / m.timestep;
+  return true;
+}
+
+// Largest contact count a pair can produce (collision.rs routines).
+int max_hits(int a, int b) {
+  if (a > b) std::swap(a, b);
+  if (a == GEOM_PLANE) {
+    if (b == GEOM_SPHERE) return 1;
+    if (b == GEOM_CAPSULE) return 2;
+    return 4;  // box, cylinder, mesh
+  }
+  if (a == GEOM_SPHERE && b <= GEOM_BOX) return 1;
+  if (a == GEOM_CAPSULE && (b == GEOM_CAPSULE || b == GEOM_BOX)) return 3;
+  return 4;
+}
+
+// ---------------------------------------------------------------- device model
+struct DevArena {
+  std::vector<uint8_t> host;
+  size_t add(const void* p, size_t bytes) {
+    size_t off = (host.size() + 15) & ~size_t(15);
+    host.resize(off + std::max<size_t>(bytes, 8));
+    if (bytes) std::memcpy(host.data() + off, p, bytes);
+    return off;
+  }
+};
+
+struct Handle {
+  HostModel hm;
+  DModel dm{};
+  WsLayout w{};
+  ScrLayout s{};
+  int64_t n = 0;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  void* d_model = nullptr;
+  double *qpos = nullptr, *qvel = nullptr, *ctrl = nullptr, *qacc = nullptr, *applied = nullptr, *params = nullptr;
+  int32_t *iters = nullptr, *ncon = nullptr, *nrows = nullptr, *status = nullptr;
+  double* scratch = nullptr;
+  size_t scratch_tiles = 0;
+  int* queue = nullptr;
+  std::vector<double> base_params;
+  int warm_mode = WARM_REF_PREV_QACC;
+  LaunchCfg cfg{32, 4, 0};
+  int sm_count = 0;
+  size_t smem_optin = 0;
+  // growable device buffers
+  struct Buf {
+    void* p = nullptr;
+    size_t bytes = 0;
+  };
+  Buf b_ctrl, b_qout, b_poses_g, b_poses_c, b_dbg, b_vals, b_ids;
+  // graph cache for pg_step
+  std::map<std::tuple<int64_t, int64_t, int64_t>, cudaGraphExec_t> graphs;
+  uint64_t version = 1, graph_version = 0;
+  std::string name = "pippin-cuda";
+};
+
+}  // namespace
+
+struct pg_handle : Handle {};
+
+namespace {
+
+int grow(Handle* h, Handle::Buf& b, size_t bytes) {
+  if (b.bytes >= bytes) return PG_OK;
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.bytes = 0;
+  size_t want = std::max<size_t>(bytes, 256);
+  cudaError_t e = cudaMalloc(&b.p, want);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc");
+  b.bytes = want;
+  (void)h;
+  return PG_OK;
+}
+
+void clear_graphs(Handle* h) {
+  for (auto& kv : h->graphs) cudaGraphExecDestroy(kv.second);
+  h->graphs.clear();
+}
+
+StepArgs make_args(Handle* h) {
+  StepArgs a{};
+  a.m = h->dm;
+  a.w = h->w;
+  a.s = h->s;
+  a.st.qpos = h->qpos;
+  a.st.qvel = h->qvel;
+  a.st.ctrl = h->ctrl;
+  a.st.qacc = h->qacc;
+  a.st.applied = h->applied;
+  a.st.params = h->params;
+  a.st.iters = h->iters;
+  a.st.ncon = h->ncon;
+  a.st.nrows = h->nrows;
+  a.st.status = h->status;
+  a.st.prev_con = nullptr;
+  a.st.prev_ncon = nullptr;
+  a.scratch = h->scratch;
+  a.queue = h->queue;
+  a.warm_mode = h->warm_mode;
+  return a;
+}
+
+// workspace and scratch layouts from the model dims
+void layouts(const HostModel& m, int maxcon, int maxrows, WsLayout* w, ScrLayout* s) {
+  int off = 0;
+  auto take = [&](int n) {
+    int o = off;
+    off += (n + 1) & ~1;  // keep 16-byte alignment
+    return o;
+  };
+  int nb = m.nbody, nv = m.nv, ng = m.ngeom, nu = m.nu;
+  w->qpos = take(m.nq);
+  w->qvel = take(nv);
+  w->ctrl = take(nu);
+  w->qacc = take(nv);
+  w->applied = take(nv);
+  w->xpos = take(3 * nb);
+  w->xquat = take(4 * nb);
+  w->xmat = take(9 * nb);
+  w->xipos = take(3 * nb);
+  w->cinert = take(13 * nb);
+  w->crb = take(13 * nb);
+  w->cvel = take(6 * nb);
+  w->cacc = take(6 * nb);
+  w->cfrc = take(6 * nb);
+  w->cdof = take(6 * nv);
+  w->cdof_dot = take(6 * nv);
+  w->gxpos = take(3 * ng);
+  w->gxmat = take(9 * ng);
+  w->gaabb = take(6 * ng);
+  w->qm = take(nv * nv);
+  w->fac = take(nv * nv);
+  w->bias = take(nv);
+  w->passive = take(nv);
+  w->actf = take(nv);
+  w->smooth = take(nv);
+  w->acc = take(nv);
+  w->qfrc_c = take(nv);
+  w->a0 = take(nv);
+  w->grad = take(nv);
+  w->p = take(nv);
+  w->tmp = take(nv);
+  w->tmp2 = take(nv);
+  w->mp = take(nv);
+  w->vel = take(nv);
+  w->warm = take(nv);
+  w->actforce = take(nu);
+  w->actclamped = take(nu);
+  w->misc = take(8);
+  w->stride = off;
+
+  off = 0;
+  int rhs = nv + 6 * nb + 32;  // set_const right-hand sides + per-lane row copies
+  s->contacts = take(maxcon * C_STRIDE);
+  s->jac = take(std::max(maxrows * nv, rhs * nv));
+  s->rows = take(std::max(maxrows * R_STRIDE, rhs));
+  int multi = m.dof_blocks.size() / 2 > 1;
+  s->sub_m = take(multi ? nv * nv : 0);
+  s->sub_j = take(multi ? maxrows * nv : 0);
+  s->sub_rows = take(multi ? maxrows * R_STRIDE : 0);
+  s->isl_dof = take(nv + 2);
+  s->isl_row = take(maxrows + (nv + maxrows + 1) / 2 + 2);
+  s->isl_of_row = take(maxrows / 2 + 2);
+  s->minv_jt = take(0);
+  s->lambda = take(0);
+  s->stride = off;
+}
+
+int choose_grid(Handle* h, const LaunchCfg& want, LaunchCfg* out) {
+  LaunchCfg c = want;
+  size_t smem = (size_t)c.tiles_per_block * h->w.stride * sizeof(double);
+  if (smem > h->smem_optin) return fail(PG_ERR_INVALID, "launch shape needs more shared memory than a block has");
+  int threads = c.tiles_per_block * c.G;
+  if (threads > 256 || threads < 32) return fail(PG_ERR_INVALID, "launch shape: 32..256 threads per block");
+  int per_sm = 0;
+  for (int k : {K_STEP, K_FORWARD, K_SET_CONST, K_POSES}) {
+    const void* fn = tile_kernel(k, c.G);
+    if (!fn) return fail(PG_ERR_INVALID, "lanes per env must be 8, 16 or 32");
+    CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int nb = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, threads, smem));
+    if (k == K_STEP) per_sm = nb;
+    else if (nb == 0) return fail(PG_ERR_INVALID, "launch shape does not fit on an SM");
+  }
+  if (per_sm < 1) return fail(PG_ERR_INVALID, "launch shape does not fit on an SM");
+  c.blocks = per_sm * h->sm_count;
+  *out = c;
+  return PG_OK;
+}
+
+int ensure_scratch(Handle* h, const LaunchCfg& c) {
+  size_t tiles = (size_t)c.blocks * c.tiles_per_block;
+  if (tiles <= h->scratch_tiles) return PG_OK;
+  if (h->scratch) cudaFree(h->scratch);
+  h->scratch = nullptr;
+  CK(cudaMalloc(&h->scratch, tiles * h->s.stride * sizeof(double) + 64));
+  h->scratch_tiles = tiles;
+  return PG_OK;
+}
+
+int apply_cfg(Handle* h, const LaunchCfg& want) {
+  LaunchCfg c;
+  int rc = choose_grid(h, want, &c);
+  if (rc) return rc;
+  rc = ensure_scratch(h, c);
+  if (rc) return rc;
+  h->cfg = c;
+  h->version++;
+  return PG_OK;
+}
+
+LaunchCfg grid_for(Handle* h, int64_t count) {
+  LaunchCfg c = h->cfg;
+  int64_t need = (count + c.tiles_per_block - 1) / c.tiles_per_block;
+  if (need < c.blocks) c.blocks = (int)std::max<int64_t>(need, 1);
+  return c;
+}
+
+int run_tile_kernel(Handle* h, int which, StepArgs& a, int64_t count, const int* envs = nullptr, float* g = nullptr,
+                    float* cm = nullptr, double* dbg = nullptr, int dbg_stride = 0, int maxcon_out = 0) {
+  LaunchCfg c = grid_for(h, count);
+  CK(cudaMemsetAsync(h->queue, 0, sizeof(int), h->stream));
+  cudaError_t e = cudaSuccess;
+  switch (which) {
+    case K_STEP: e = launch_step(a, c, h->stream); break;
+    case K_FORWARD: e = launch_forward(a, c, dbg, dbg_stride, maxcon_out, h->stream); break;
+    case K_SET_CONST: e = launch_set_const(a, c, envs, (int)count, h->stream); break;
+    case K_POSES: e = launch_poses(a, c, g, cm, h->stream); break;
+  }
+  if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
+  return PG_OK;
+}
+
+int set_const_range(Handle* h, int64_t start, int64_t end) {
+  if (end <= start) return PG_OK;
+  StepArgs a = make_args(h);
+  a.start = (int)start;
+  a.count = (int)(end - start);
+  return run_tile_kernel(h, K_SET_CONST, a, end - start);
+}
+
+int check_range(Handle* h, int64_t start, int64_t end) {
+  if (start < 0 || end < start || end > h->n)
+    return fail(PG_ERR_INVALID, "env range [" + std::to_string(start) + ", " + std::to_string(end) + ") out of bounds (have " +
+                                    std::to_string(h->n) + ")");
+  return PG_OK;
+}
+
+int field_width(const HostModel& m, int f) {
+  switch (f) {
+    case PG_FIELD_QPOS: return m.nq;
+    case PG_FIELD_QVEL: return m.nv;
+    case PG_FIELD_CTRL: return m.nu;
+    case PG_FIELD_QACC: return m.nv;
+    case PG_FIELD_QFRC_APPLIED: return m.nv;
+  }
+  return -1;
+}
+double* field_ptr(Handle* h, int f) {
+  switch (f) {
+    case PG_FIELD_QPOS: return h->qpos;
+    case PG_FIELD_QVEL: return h->qvel;
+    case PG_FIELD_CTRL: return h->ctrl;
+    case PG_FIELD_QACC: return h->qacc;
+    case PG_FIELD_QFRC_APPLIED: return h->applied;
+  }
+  return nullptr;
+}
+
+// params.rs:61-83
+int param_width(const HostModel& m, int p) {
+  switch (p) {
+    case PG_PARAM_GEOM_SIZE: case PG_PARAM_ACTUATOR_BIAS: case PG_PARAM_BODY_INERTIA: case PG_PARAM_BODY_IPOS: return 3;
+    case PG_PARAM_GEOM_RGBA: return 4;
+    case PG_PARAM_QPOS0: return m.nq;
+    default: return 1;
+  }
+}
+int param_count(const HostModel& m, int p) {
+  switch (p) {
+    case PG_PARAM_GEOM_FRICTION: case PG_PARAM_GEOM_SIZE: case PG_PARAM_GEOM_RGBA: case PG_PARAM_GEOM_CONTYPE:
+    case PG_PARAM_GEOM_CONAFFINITY: return m.ngeom;
+    case PG_PARAM_BODY_MASS: case PG_PARAM_BODY_INERTIA: case PG_PARAM_BODY_IPOS: return m.nbody;
+    case PG_PARAM_QPOS0: return 1;
+    case PG_PARAM_DOF_DAMPING: return m.nv;
+    case PG_PARAM_ACTUATOR_GAIN: case PG_PARAM_ACTUATOR_BIAS: return m.nu;
+  }
+  return 0;
+}
+const char* param_name(int p) {
+  static const char* n[] = {"GeomFriction", "GeomSize", "GeomRgba", "GeomContype", "GeomConaffinity", "BodyMass",
+                            "DofDamping", "ActuatorGain", "ActuatorBias", "BodyInertia", "BodyIpos", "Qpos0"};
+  return (p >= 0 && p < 12) ? n[p] : "?";
+}
+
+// params.rs:111-177 validation (values of one env)
+bool validate_param(const HostModel& m, int p, int64_t id, const double* v, std::string* err) {
+  int w = param_width(m, p);
+  for (int k = 0; k < w; k++)
+    if (!std::isfinite(v[k])) {
+      *err = std::string(param_name(p)) + ": values must be finite";
+      return false;
+    }
+  switch (p) {
+    case PG_PARAM_GEOM_SIZE:
+      if (m.geom_type[id] == GEOM_MESH || m.geom_type[id] == GEOM_PLANE) {
+        *err = "geom_size applies to sphere, capsule, box, and cylinder geoms";
+        return false;
+      }
+      for (int k = 0; k < 3; k++)
+        if (v[k] < 0.0) {
+          *err = "geom_size must be non-negative";
+          return false;
+        }
+      break;
+    case PG_PARAM_BODY_MASS:
+      if (id == 0) {
+        *err = "the world body has no mass";
+        return false;
+      }
+      if (v[0] <= 0.0 && m.body_jntnum[id] > 0) {
+        *err = "moving bodies need positive mass";
+        return false;
+      }
+      break;
+    case PG_PARAM_BODY_INERTIA:
+      if (id == 0 || v[0] < 0.0 || v[1] < 0.0 || v[2] < 0.0) {
+        *err = "body_inertia needs a non-world body and non-negative moments";
+        return false;
+      }
+      break;
+    case PG_PARAM_BODY_IPOS:
+      if (id == 0) {
+        *err = "the world body has no center of mass";
+        return false;
+      }
+      break;
+  }
+  return true;
+}
+
+// apply one env's new values to its parameter block (params.rs:121-176)
+void apply_param(const DModel& d, double* prm, int p, int64_t id, const double* v, int nq) {
+  switch (p) {
+    case PG_PARAM_GEOM_FRICTION: prm[d.p_friction + id] = std::fmax(v[0], 0.0); break;
+    case PG_PARAM_GEOM_SIZE: for (int k = 0; k < 3; k++) prm[d.p_size + 3 * id + k] = v[k]; break;
+    case PG_PARAM_GEOM_RGBA: for (int k = 0; k < 4; k++) prm[d.p_rgba + 4 * id + k] = (double)(float)v[k]; break;
+    case PG_PARAM_GEOM_CONTYPE:
+    case PG_PARAM_GEOM_CONAFFINITY: {
+      double bits = std::floor(std::fmin(std::fmax(v[0], 0.0), 4294967295.0));
+      prm[(p == PG_PARAM_GEOM_CONTYPE ? d.p_contype : d.p_conaff) + id] = bits;
+      break;
+    }
+    case PG_PARAM_BODY_MASS: {
+      double old = prm[d.p_mass + id];
+      double scale = old > 0.0 ? v[0] / old : 1.0;
+      prm[d.p_mass + id] = v[0];
+      for (int k = 0; k < 9; k++) prm[d.p_inertia + 9 * id + k] *= scale;
+      break;
+    }
+    case PG_PARAM_DOF_DAMPING: prm[d.p_damping + id] = std::fmax(v[0], 0.0); break;
+    case PG_PARAM_ACTUATOR_GAIN: prm[d.p_gain + id] = v[0]; break;
+    case PG_PARAM_ACTUATOR_BIAS: for (int k = 0; k < 3; k++) prm[d.p_bias + 3 * id + k] = v[k]; break;
+    case PG_PARAM_BODY_INERTIA:
+      for (int k = 0; k < 9; k++) prm[d.p_inertia + 9 * id + k] = 0.0;
+      for (int k = 0; k < 3; k++) prm[d.p_inertia + 9 * id + 4 * k] = v[k];
+      break;
+    case PG_PARAM_BODY_IPOS: for (int k = 0; k < 3; k++) prm[d.p_ipos + 3 * id + k] = v[k]; break;
+    case PG_PARAM_QPOS0: for (int k = 0; k < nq; k++) prm[d.p_qpos_reset + k] = v[k]; break;
+  }
+}
+
+void read_param(const DModel& d, const double* prm, int p, int64_t id, double* o, int nq) {
+  switch (p) {
+    case PG_PARAM_GEOM_FRICTION: o[0] = prm[d.p_friction + id]; break;
+    case PG_PARAM_GEOM_SIZE: for (int k = 0; k < 3; k++) o[k] = prm[d.p_size + 3 * id + k]; break;
+    case PG_PARAM_GEOM_RGBA: for (int k = 0; k < 4; k++) o[k] = prm[d.p_rgba + 4 * id + k]; break;
+    case PG_PARAM_GEOM_CONTYPE: o[0] = prm[d.p_contype + id]; break;
+    case PG_PARAM_GEOM_CONAFFINITY: o[0] = prm[d.p_conaff + id]; break;
+    case PG_PARAM_BODY_MASS: o[0] = prm[d.p_mass + id]; break;
+    case PG_PARAM_DOF_DAMPING: o[0] = prm[d.p_damping + id]; break;
+    case PG_PARAM_ACTUATOR_GAIN: o[0] = prm[d.p_gain + id]; break;
+    case PG_PARAM_ACTUATOR_BIAS: for (int k = 0; k < 3; k++) o[k] = prm[d.p_bias + 3 * id + k]; break;
+    case PG_PARAM_BODY_INERTIA: for (int k = 0; k < 3; k++) o[k] = prm[d.p_inertia + 9 * id + 4 * k]; break;
+    case PG_PARAM_BODY_IPOS: for (int k = 0; k < 3; k++) o[k] = prm[d.p_ipos + 3 * id + k]; break;
+    case PG_PARAM_QPOS0: for (int k = 0; k < nq; k++) o[k] = prm[d.p_qpos_reset + k]; break;
+  }
+}
+
+int build_device_model(Handle* h) {
+  HostModel& m = h->hm;
+  DModel& d = h->dm;
+  DevArena ar;
+  int nb = m.nbody, nv = m.nv;
+  // tree levels (world at level 0) and children in decreasing id
+  std::vector<int> depth(nb, 0);
+  int nlevel = 1;
+  for (int b = 1; b < nb; b++) {
+    depth[b] = depth[m.body_parent[b]] + 1;
+    nlevel = std::max(nlevel, depth[b] + 1);
+  }
+  std::vector<int> level_adr(nlevel + 1, 0), level_body;
+  for (int L = 0; L < nlevel; L++) {
+    level_adr[L] = (int)level_body.size();
+    for (int b = 0; b < nb; b++)
+      if (depth[b] == L) level_body.push_back(b);
+  }
+  level_adr[nlevel] = (int)level_body.size();
+  std::vector<int> child_adr(nb + 1, 0), child_list;
+  for (int b = 0; b < nb; b++) {
+    child_adr[b] = (int)child_list.size();
+    for (int c = nb - 1; c > b; c--)
+      if (m.body_parent[c] == b) child_list.push_back(c);
+  }
+  child_adr[nb] = (int)child_list.size();
+  std::vector<unsigned long long> dofmask(nb, 0);
+  for (int b = 0; b < nb; b++)
+    for (int k = m.body_lastdof[b]; k != -1; k = m.dof_parent[k]) dofmask[b] |= 1ull << k;
+  int nblock = (int)m.dof_blocks.size() / 2;
+  std::vector<int> dof_block(std::max(nv, 1), 0);
+  for (int b = 0; b < nblock; b++)
+    for (int k = m.dof_blocks[2 * b]; k < m.dof_blocks[2 * b + 1]; k++) dof_block[k] = b;
+  // actuator contributions per dof, in (actuator, moment entry) order
+  std::vector<std::vector<std::pair<int, double>>> per(nv);
+  for (int u = 0; u < m.nu; u++)
+    for (int k = 0; k < m.act_moment_num[u]; k++) {
+      int j = m.moment_jnt[m.act_moment_adr[u] + k];
+      per[m.jnt_dofadr[j]].push_back({u, m.moment_coef[m.act_moment_adr[u] + k]});
+    }
+  std::vector<int> dofact_adr(nv + 1, 0), dofact_u;
+  std::vector<double> dofact_coef;
+  for (int k = 0; k < nv; k++) {
+    dofact_adr[k] = (int)dofact_u.size();
+    for (auto& pc : per[k]) {
+      dofact_u.push_back(pc.first);
+      dofact_coef.push_back(pc.second);
+    }
+  }
+  dofact_adr[nv] = (int)dofact_u.size();
+  // work caps: every candidate pair at its largest manifold
+  int maxcon = 0;
+  for (size_t k = 0; k + 1 < m.pairs.size(); k += 2) maxcon += max_hits(m.geom_type[m.pairs[k]], m.geom_type[m.pairs[k + 1]]);
+  int nlim = 0;
+  for (int j = 0; j < m.njnt; j++)
+    if (m.jnt_limited[j] && (m.jnt_type[j] == JNT_HINGE || m.jnt_type[j] == JNT_SLIDE)) nlim++;
+  int maxrows = 4 * maxcon + 2 * nlim + m.neq;
+  // hull faces (outward normal, offset) from the triangles, for mesh geoms
+  std::vector<int> hull_fadr(std::max(m.nmesh, 1), 0), hull_fnum(std::max(m.nmesh, 1), 0);
+  std::vector<double> hull_face;
+  for (int i = 0; i < m.nmesh; i++) {
+    hull_fadr[i] = (int)hull_face.size() / 4;
+    for (int t = 0; t < m.hull_tnum[i]; t++) {
+      const int* tri = &m.hull_tri[3 * (m.hull_tadr[i] + t)];
+      const double* va = &m.hull_vert[3 * (m.hull_vadr[i] + tri[0])];
+      const double* vb = &m.hull_vert[3 * (m.hull_vadr[i] + tri[1])];
+      const double* vc = &m.hull_vert[3 * (m.hull_vadr[i] + tri[2])];
+      double e1[3] = {vb[0] - va[0], vb[1] - va[1], vb[2] - va[2]};
+      double e2[3] = {vc[0] - va[0], vc[1] - va[1], vc[2] - va[2]};
+      double n[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+      double l = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+      if (l <= 0) continue;
+      for (int k = 0; k < 3; k++) n[k] /= l;
+      hull_face.insert(hull_face.end(), {n[0], n[1], n[2], n[0] * va[0] + n[1] * va[1] + n[2] * va[2]});
+      hull_fnum[i]++;
+    }
+  }
+
+  d.nq = m.nq;
+  d.nv = nv;
+  d.nu = m.nu;
+  d.nbody = nb;
+  d.njnt = m.njnt;
+  d.ngeom = m.ngeom;
+  d.ncam = m.ncam;
+  d.neq = m.neq;
+  d.npair = (int)m.pairs.size() / 2;
+  d.nblock = nblock;
+  d.nlevel = nlevel;
+  d.nmesh = m.nmesh;
+  d.maxcon = maxcon;
+  d.maxrows = maxrows;
+  d.timestep = m.timestep;
+  for (int k = 0; k < 3; k++) d.gravity[k] = m.gravity[k];
+  d.integrator = m.integrator;
+  d.solver = m.solver;
+  d.iterations = m.iterations;
+  d.tolerance = m.tolerance;
+  d.margin = m.margin;
+  d.solref[0] = m.solref[0];
+  d.solref[1] = m.solref[1];
+  for (int k = 0; k < 5; k++) d.solimp[k] = m.solimp[k];
+  d.impratio = m.impratio;
+  d.hertz = m.hertz;
+  d.dampratio = m.dampratio;
+  d.slop = m.slop;
+
+  struct Fix {
+    const void** slot;
+    size_t off;
+  };
+  std::vector<Fix> fix;
+  auto addv = [&](const void** slot, const void* p, size_t bytes) { fix.push_back({slot, ar.add(p, bytes)}); };
+#define ADDI(field, vec) addv((const void**)&d.field, vec.data(), vec.size() * sizeof(int))
+#define ADDD(field, vec) addv((const void**)&d.field, vec.data(), vec.size() * sizeof(double))
+  ADDI(body_parent, m.body_parent);
+  ADDI(body_jntadr, m.body_jntadr);
+  ADDI(body_jntnum, m.body_jntnum);
+  ADDI(body_dofadr, m.body_dofadr);
+  ADDI(body_dofnum, m.body_dofnum);
+  ADDI(body_lastdof, m.body_lastdof);
+  addv((const void**)&d.body_dofmask, dofmask.data(), dofmask.size() * 8);
+  ADDD(body_pos, m.body_pos);
+  ADDD(body_quat, m.body_quat);
+  ADDI(level_adr, level_adr);
+  ADDI(level_body, level_body);
+  ADDI(child_adr, child_adr);
+  ADDI(child_list, child_list);
+  ADDI(jnt_type, m.jnt_type);
+  ADDI(jnt_qposadr, m.jnt_qposadr);
+  ADDI(jnt_dofadr, m.jnt_dofadr);
+  ADDI(jnt_limited, m.jnt_limited);
+  ADDD(jnt_pos, m.jnt_pos);
+  ADDD(jnt_axis, m.jnt_axis);
+  ADDD(jnt_range, m.jnt_range);
+  ADDD(jnt_stiffness, m.jnt_stiffness);
+  ADDD(jnt_springref, m.jnt_springref);
+  ADDI(dof_body, m.dof_body);
+  ADDI(dof_parent, m.dof_parent);
+  ADDD(dof_armature, m.dof_armature);
+  ADDI(dof_block, dof_block);
+  ADDI(block_adr, m.dof_blocks);
+  ADDI(dofact_adr, dofact_adr);
+  ADDI(dofact_u, dofact_u);
+  ADDD(dofact_coef, dofact_coef);
+  ADDI(geom_type, m.geom_type);
+  ADDI(geom_body, m.geom_body);
+  ADDI(geom_dataid, m.geom_dataid);
+  ADDD(geom_pos, m.geom_pos);
+  ADDD(geom_quat, m.geom_quat);
+  ADDI(pair_g, m.pairs);
+  ADDI(cam_body, m.cam_body);
+  ADDD(cam_pos, m.cam_pos);
+  ADDD(cam_quat, m.cam_quat);
+  ADDD(act_gear, m.act_gear);
+  ADDI(act_ctrllimited, m.act_ctrllimited);
+  ADDD(act_ctrlrange, m.act_ctrlrange);
+  ADDI(act_forcelimited, m.act_forcelimited);
+  ADDD(act_forcerange, m.act_forcerange);
+  ADDI(act_moment_adr, m.act_moment_adr);
+  ADDI(act_moment_num, m.act_moment_num);
+  ADDI(moment_jnt, m.moment_jnt);
+  ADDD(moment_coef, m.moment_coef);
+  ADDI(eq_j1, m.eq_j1);
+  ADDI(eq_j2, m.eq_j2);
+  ADDD(eq_poly, m.eq_poly);
+  ADDD(eq_solref, m.eq_solref);
+  ADDD(eq_solimp, m.eq_solimp);
+  ADDD(qpos0, m.qpos0);
+  ADDI(hull_vadr, m.hull_vadr);
+  ADDI(hull_vnum, m.hull_vnum);
+  ADDD(hull_vert, m.hull_vert);
+  ADDI(hull_fadr, hull_fadr);
+  ADDI(hull_fnum, hull_fnum);
+  ADDD(hull_face, hull_face);
+#undef ADDI
+#undef ADDD
+  CK(cudaMalloc(&h->d_model, ar.host.size()));
+  CK(cudaMemcpy(h->d_model, ar.host.data(), ar.host.size(), cudaMemcpyHostToDevice));
+  for (auto& f : fix) *f.slot = (const uint8_t*)h->d_model + f.off;
+
+  // per-env parameter block
+  int off = 0;
+  auto take = [&](int n) {
+    int o = off;
+    off += n;
+    return o;
+  };
+  int ng = m.ngeom;
+  d.p_friction = take(ng);
+  d.p_size = take(3 * ng);
+  d.p_contype = take(ng);
+  d.p_conaff = take(ng);
+  d.p_mass = take(nb);
+  d.p_inertia = take(9 * nb);
+  d.p_ipos = take(3 * nb);
+  d.p_damping = take(nv);
+  d.p_gain = take(m.nu);
+  d.p_bias = take(3 * m.nu);
+  d.p_qpos_reset = take(m.nq);
+  d.p_body_invw = take(2 * nb);
+  d.p_dof_invw = take(nv);
+  d.p_rgba = take(4 * ng);
+  d.pstride = (off + 3) & ~3;
+  std::vector<double>& bp = h->base_params;
+  bp.assign(d.pstride, 0.0);
+  for (int g = 0; g < ng; g++) {
+    bp[d.p_friction + g] = m.geom_friction[g];
+    for (int k = 0; k < 3; k++) bp[d.p_size + 3 * g + k] = m.geom_size[3 * g + k];
+    bp[d.p_contype + g] = m.geom_contype[g];
+    bp[d.p_conaff + g] = m.geom_conaffinity[g];
+    for (int k = 0; k < 4; k++) bp[d.p_rgba + 4 * g + k] = m.geom_rgba[4 * g + k];
+  }
+  for (int b = 0; b < nb; b++) {
+    bp[d.p_mass + b] = m.body_mass[b];
+    for (int k = 0; k < 9; k++) bp[d.p_inertia + 9 * b + k] = m.body_inertia[9 * b + k];
+    for (int k = 0; k < 3; k++) bp[d.p_ipos + 3 * b + k] = m.body_ipos[3 * b + k];
+  }
+  for (int k = 0; k < nv; k++) bp[d.p_damping + k] = m.dof_damping[k];
+  for (int u = 0; u < m.nu; u++) {
+    bp[d.p_gain + u] = m.act_gain[u];
+    for (int k = 0; k < 3; k++) bp[d.p_bias + 3 * u + k] = m.act_bias[3 * u + k];
+  }
+  for (int k = 0; k < m.nq; k++) bp[d.p_qpos_reset + k] = m.qpos_reset[k];
+  layouts(m, maxcon, maxrows, &h->w, &h->s);
+  return PG_OK;
+}
+
+void destroy(pg_handle* h) {
+  if (!h) return;
+  cudaSetDevice(h->device);
+  clear_graphs(h);
+  void* ptrs[] = {h->d_model, h->qpos, h->qvel, h->ctrl, h->qacc, h->applied, h->params, h->iters, h->ncon,
+                  h->nrows, h->status, h->scratch, h->queue, h->b_ctrl.p, h->b_qout.p, h->b_poses_g.p,
+                  h->b_poses_c.p, h->b_dbg.p, h->b_vals.p, h->b_ids.p};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+}
+
+int copy_rows_d2h(Handle* h, double* dst, const double* src, int64_t start, int64_t end, int width) {
+  if (end <= start || width == 0) return PG_OK;
+  CK(cudaMemcpyAsync(dst, src + start * width, sizeof(double) * (end - start) * width, cudaMemcpyDeviceToHost,
+                     h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return PG_OK;
+}
+
+// read the parameter blocks of [start, end) to the host
+int read_params(Handle* h, int64_t start, int64_t end, std::vector<double>& out) {
+  out.resize((size_t)(end - start) * h->dm.pstride);
+  return copy_rows_d2h(h, out.data(), h->params, start, end, h->dm.pstride);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* pg_last_error(void) { return g_err.c_str(); }
+
+int pg_create(const void* blob, size_t bytes, int64_t n_envs, int device, pg_handle** out) {
+  g_err.clear();
+  if (!out) return fail(PG_ERR_INVALID, "out is NULL");
+  *out = nullptr;
+  if (n_envs < 0 || n_envs > (1ll << 30)) return fail(PG_ERR_INVALID, "n_envs out of range");
+  std::unique_ptr<pg_handle, void (*)(pg_handle*)> h(new pg_handle, [](pg_handle* p) { destroy(p); });
+  std::string err;
+  if (!load_model(blob, bytes, h->hm, &err)) return fail(PG_ERR_INVALID, err);
+  int ndev = 0;
+  CK(cudaGetDeviceCount(&ndev));
+  if (device < 0 || device >= ndev) return fail(PG_ERR_INVALID, "no such CUDA device");
+  h->device = device;
+  CK(cudaSetDevice(device));
+  cudaDeviceProp prop;
+  CK(cudaGetDeviceProperties(&prop, device));
+  if (prop.major < 10) return fail(PG_ERR_UNSUPPORTED, "this library is built for sm_100a (B200)");
+  h->sm_count = prop.multiProcessorCount;
+  h->smem_optin = prop.sharedMemPerBlockOptin;
+  CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  int rc = build_device_model(h.get());
+  if (rc) return rc;
+  h->n = n_envs;
+  const HostModel& m = h->hm;
+  size_t n = (size_t)std::max<int64_t>(n_envs, 1);
+  CK(cudaMalloc(&h->qpos, sizeof(double) * n * std::max(m.nq, 1)));
+  CK(cudaMalloc(&h->qvel, sizeof(double) * n * std::max(m.nv, 1)));
+  CK(cudaMalloc(&h->ctrl, sizeof(double) * n * std::max(m.nu, 1)));
+  CK(cudaMalloc(&h->qacc, sizeof(double) * n * std::max(m.nv, 1)));
+  CK(cudaMalloc(&h->applied, sizeof(double) * n * std::max(m.nv, 1)));
+  CK(cudaMalloc(&h->params, sizeof(double) * n * h->dm.pstride));
+  CK(cudaMalloc(&h->iters, sizeof(int32_t) * n));
+  CK(cudaMalloc(&h->ncon, sizeof(int32_t) * n));
+  CK(cudaMalloc(&h->nrows, sizeof(int32_t) * n));
+  CK(cudaMalloc(&h->status, sizeof(int32_t) * n));
+  CK(cudaMalloc(&h->queue, sizeof(int) * 4));
+  CK(cudaMemsetAsync(h->qvel, 0, sizeof(double) * n * std::max(m.nv, 1), h->stream));
+  CK(cudaMemsetAsync(h->ctrl, 0, sizeof(double) * n * std::max(m.nu, 1), h->stream));
+  CK(cudaMemsetAsync(h->qacc, 0, sizeof(double) * n * std::max(m.nv, 1), h->stream));
+  CK(cudaMemsetAsync(h->applied, 0, sizeof(double) * n * std::max(m.nv, 1), h->stream));
+  CK(cudaMemsetAsync(h->iters, 0, sizeof(int32_t) * n, h->stream));
+  CK(cudaMemsetAsync(h->ncon, 0, sizeof(int32_t) * n, h->stream));
+  CK(cudaMemsetAsync(h->nrows, 0, sizeof(int32_t) * n, h->stream));
+  CK(cudaMemsetAsync(h->status, 0, sizeof(int32_t) * n, h->stream));
+  {
+    std::vector<double> hq((size_t)n_envs * m.nq), hp((size_t)n_envs * h->dm.pstride);
+    for (int64_t e = 0; e < n_envs; e++) {
+      std::copy(m.qpos_reset.begin(), m.qpos_reset.end(), hq.begin() + e * m.nq);
+      std::copy(h->base_params.begin(), h->base_params.end(), hp.begin() + e * h->dm.pstride);
+    }
+    if (n_envs > 0) {
+      if (m.nq) CK(cudaMemcpyAsync(h->qpos, hq.data(), sizeof(double) * hq.size(), cudaMemcpyHostToDevice, h->stream));
+      CK(cudaMemcpyAsync(h->params, hp.data(), sizeof(double) * hp.size(), cudaMemcpyHostToDevice, h->stream));
+    }
+    CK(cudaStreamSynchronize(h->stream));
+  }
+  LaunchCfg want{m.nv > 16 ? 32 : 16, 4, 0};
+  rc = apply_cfg(h.get(), want);
+  if (rc) return rc;
+  rc = set_const_range(h.get(), 0, n_envs);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(h->stream));
+  *out = h.release();
+  return PG_OK;
+}
+
+int pg_destroy(pg_handle* h) {
+  destroy(h);
+  return PG_OK;
+}
+
+const char* pg_name(const pg_handle* h) { return h ? h->name.c_str() : ""; }
+int64_t pg_num_envs(const pg_handle* h) { return h ? h->n : 0; }
+
+int pg_dims(const pg_handle* h, pg_model_dims* out) {
+  if (!h || !out) return fail(PG_ERR_INVALID, "NULL argument");
+  out->nq = h->hm.nq;
+  out->nv = h->hm.nv;
+  out->nu = h->hm.nu;
+  out->ngeom = h->hm.ngeom;
+  out->ncam = h->hm.ncam;
+  out->nbody = h->hm.nbody;
+  out->njnt = h->hm.njnt;
+  return PG_OK;
+}
+
+int pg_step(pg_handle* h, int64_t start, int64_t end, int64_t nstep) {
+  if (!h) return fail(PG_ERR_INVALID, "NULL handle");
+  int rc = check_range(h, start, end);
+  if (rc) return rc;
+  if (nstep < 0 || nstep > (1 << 30)) return fail(PG_ERR_INVALID, "nstep out of range");
+  if (end == start || nstep == 0) return PG_OK;
+  CK(cudaSetDevice(h->device));
+  if (h->graph_version != h->version) {
+    clear_graphs(h);
+    h->graph_version = h->version;
+  }
+  auto key = std::make_tuple(start, end, nstep);
+  auto it = h->graphs.find(key);
+  if (it == h->graphs.end()) {
+    if (h->graphs.size() >= 32) clear_graphs(h);
+    StepArgs a = make_args(h);
+    a.start = (int)start;
+    a.count = (int)(end - start);
+    a.nstep = (int)nstep;
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    int rc2 = run_tile_kernel(h, K_STEP, a, end - start);
+    cudaError_t ce = cudaStreamEndCapture(h->stream, &g);
+    if (rc2) return rc2;
+    if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamEndCapture");
+    cudaGraphExec_t ex;
+    ce = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    if (ce != cudaSuccess) return cuda_fail(ce, "cudaGraphInstantiate");
+    it = h->graphs.emplace(key, ex).first;
+  }
+  CK(cudaGraphLaunch(it->second, h->stream));
+  return PG_OK;
+}
+
+int pg_step_device(pg_handle* h, int64_t start, int64_t end, int64_t nstep, const double* ctrl_dev) {
+  if (!h) return fail(PG_ERR_INVALID, "NULL handle");
+  int rc = check_range(h, start, end);
+  if (rc) return rc;
+  if (end > start && h->hm.nu > 0) {
+    if (!ctrl_dev) return fail(PG_ERR_INVALID, "ctrl_dev is NULL");
+    CK(cudaSetDevice(h->device));
+    CK(cudaMemcpyAsync(h->ctrl + start * h->hm.nu, ctrl_dev, sizeof(double) * (end - start) * h->hm.nu,
+                       cudaMemcpyDeviceToDevice, h->stream));
+  }
+  return pg_step(h, start, end, nstep);
+}
+
+int pg_rollout(pg_handle* h, int64_t start, int64_t end, int64_t nstep, const double* ctrl, double* qpos_out) {
+  if (!h) return fail(PG_ERR_INVALID, "NULL handle");
+  int rc = check_range(h, start, end);
+  if (rc) return rc;
+  if (nstep < 0) return fail(PG_ERR_INVALID, "nstep out of range");
+  int64_t cnt = end - start;
+  if (cnt == 0 || nstep == 0) return PG_OK;
+  const HostModel& m = h->hm;
+  if (!ctrl && m.nu > 0) return fail(PG_ERR_INVALID, "ctrl is NULL");
+  CK(cudaSetDevice(h->device));
+  size_t cb = sizeof(double) * cnt * nstep * std::max(m.nu, 1), qb = sizeof(double) * cnt * nstep * m.nq;
+  if ((rc = grow(h, h->b_ctrl, cb))) return rc;
+  if (qpos_out && (rc = grow(h, h->b_qout, qb))) return rc;
+  if (m.nu) CK(cudaMemcpyAsync(h->b_ctrl.p, ctrl, sizeof(double) * cnt * nstep * m.nu, cudaMemcpyHostToDevice, h->stream));
+  StepArgs a = make_args(h);
+  a.start = (int)start;
+  a.count = (int)cnt;
+  a.nstep = (int)nstep;
+  a.ctrl_seq = m.nu ? (const double*)h->b_ctrl.p : nullptr;
+  a.qpos_out = qpos_out ? (double*)h->b_qout.p : nullptr;
+  if ((rc = run_tile_kernel(h, K_STEP, a, cnt))) return rc;
+  if (qpos_out) CK(cudaMemcpyAsync(qpos_out, h->b_qout.p, qb, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return PG_OK;
+}
+
+int pg_reset(pg_handle* h, const int64_t* envs, int64_t n) {
+  if (!h) return fail(PG_ERR_INVALID, "NULL handle");
+  if (n < 0 || (n > 0 && !envs)) return fail(PG_ERR_INVALID, "bad env list");
+  for (int64_t k = 0; k < n; k++)
+    if (envs[k] < 0 || envs[k] >= h->n) return fail(PG_ERR_INVALID, "env id " + std::to_string(envs[k]) + " out of range");
+  if (n == 0) return PG_OK;
+  CK(cudaSetDevice(h->device));
+  int rc = grow(h, h->b_ids, sizeof(int64_t) * n);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(h->b_ids.p, envs, sizeof(int64_t) * n, cudaMemcpyHostToDevice, h->stream));
+  StepArgs a = make_args(h);
+  CK(launch_reset(a, (const int64_t*)h->b_ids.p, (int)n, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return PG_OK;
+}
+
+int pg_get(pg_handle* h, int field, int64_t start, int64_t end, double* out, size_t len) {
+  if (!h) return fail(PG_ERR_INVALID, "NULL handle");
+  int w = field_width(h->hm, field);
+  if (w < 0) return fail(PG_ERR_INVALID, "unknown field");
+  int rc = check_range(h, start, end);
+  if (rc) return rc;
+  if (len != (size_t)(end - start) * w)
+    return fail(PG_ERR_LENGTH, "get: buffer has " + std::to_string(len) + " elements, expected " +
+                                   std::to_string(end - start) + " x " + std::to_string(w));
+  CK(cudaSetDevice(h->device));
+  return copy_rows_d2h(h, out, field_ptr(h, field), start, end, w);
+}
+
+int pg_set(pg_handle* h, int field, int64_t start, int64_t end, const double* src, size_t len) {
+  if (!h) return fail(PG_ERR_INVALID, "NULL handle");
+  int w = field_width(h->hm, field);
+  if (w < 0) return fail(PG_ERR_INVALID, "unknown field");
+  int rc = check_range(h, start, end);
+  if (rc) return rc;
+  if (len != (size_t)(end - start) * w)
+    return fail(PG_ERR_LENGTH, "set: buffer has " + std::to_string(len) + " elements, expected " +
+                                   std::to_string(end - start) + " x " + std::to_string(w));
+  if (end == start || w == 0) return PG_OK;
+  CK(cudaSetDevice(h->device));
+  CK(cudaMemcpyAsync(field_ptr(h, field) + start * w, src, sizeof(double) * len, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return PG_OK;
+}
+
+int pg_poses(pg_handle* h, int64_t start, int64_t end, pg_pose* geoms, size_t ngeoms_len, pg_pose* cams,
+             size_t ncams_len) {
+  if (!h) return fail(PG_ERR_INVALID, "NULL handle");
+  int rc = check_range(h, start, end);
+  if (rc) return rc;
+  int64_t cnt = end - start;
+  const HostModel& m = h->hm;
+  if (ngeoms_len != (size_t)cnt * m.ngeom)
+    return fail(PG_ERR_LENGTH, "poses(geoms): buffer has " + std::to_string(ngeoms_len) + " elements, expected " +
+                                   std::to_string(cnt) + " x " + std::to_string(m.ngeom));
+  if (ncams_len != (size_t)cnt * m.ncam)
+    return fail(PG_ERR_LENGTH, "poses(cams): buffer has " + std::to_string(ncams_len) + " elements, expected " +
+                                   std::to_string(cnt) + " x " + std::to_string(m.ncam));
+  if (cnt == 0) return PG_OK;
+  CK(cudaSetDevice(h->device));
+  if ((rc = grow(h, h->b_poses_g, sizeof(pg_pose) * cnt * std::max(m.ngeom, 1)))) return rc;
+  if ((rc = grow(h, h->b_poses_c, sizeof(pg_pose) * cnt * std::max(m.ncam, 1)))) return rc;
+  StepArgs a = make_args(h);
+  a.start = (int)start;
+  a.count = (int)cnt;
+  if ((rc = run_tile_kernel(h, K_POSES, a, cnt, nullptr, (float*)h->b_poses_g.p, (float*)h->b_poses_c.p))) return rc;
+  if (m.ngeom) CK(cudaMemcpyAsync(geoms, h->b_poses_g.p, sizeof(pg_pose) * cnt * m.ngeom, cudaMemcpyDeviceToHost, h->stream));
+  if (m.ncam) CK(cudaMemcpyAsync(cams, h->b_poses_c.p, sizeof(pg_pose) * cnt * m.ncam, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return PG_OK;
+}
+
+int pg_param_width(const pg_handle* h, int param) {
+  if (!h || param < 0 || param > PG_PARAM_QPOS0) return -1;
+  return param_width(h->hm, param);
+}
+
+int pg_set_param(pg_handle* h, int param, int64_t id, int64_t start, int64_t end, const double* values, size_t len) {
+  if (!h) return fail(PG_ERR_INVALID, "NULL handle");
+  if (param < 0 || param > PG_PARAM_QPOS0) return fail(PG_ERR_INVALID, "unknown parameter");
+  int rc = check_range(h, start, end);
+  if (rc) return rc;
+  const HostModel& m = h->hm;
+  int w = param_width(m, param);
+  if (len != (size_t)(end - start) * w)
+    return fail(PG_ERR_LENGTH, "set_param: buffer has " + std::to_string(len) + " elements, expected " +
+                                   std::to_string(end - start) + " x " + std::to_string(w));
+  if (id < 0 || id >= param_count(m, param))
+    return fail(PG_ERR_INVALID, std::string(param_name(param)) + ": id " + std::to_string(id) +
+                                    " out of range (have " + std::to_string(param_count(m, param)) + ")");
+  std::string err;
+  for (int64_t k = 0; k < end - start; k++)
+    if (!validate_param(m, param, id, values + k * w, &err)) return fail(PG_ERR_INVALID, err);
+  if (end == start) return PG_OK;
+  CK(cudaSetDevice(h->device));
+  std::vector<double> blk;
+  if ((rc = read_params(h, start, end, blk))) return rc;
+  for (int64_t k = 0; k < end - start; k++) apply_param(h->dm, blk.data() + k * h->dm.pstride, param, id, values + k * w, m.nq);
+  CK(cudaMemcpyAsync(h->params + start * h->dm.pstride, blk.data(), sizeof(double) * blk.size(), cudaMemcpyHostToDevice,
+                     h->stream));
+  if (param == PG_PARAM_BODY_MASS || param == PG_PARAM_BODY_INERTIA || param == PG_PARAM_BODY_IPOS) {
+    if ((rc = set_const_range(h, start, end))) return rc;
+  }
+  CK(cudaStreamSynchronize(h->stream));
+  return PG_OK;
+}
+
+int pg_get_param(pg_handle* h, int param, int64_t id, int64_t start, int64_t end, double* out, size_t len) {
+  if (!h) return fail(PG_ERR_INVALID, "NULL handle");
+  if (param < 0 || param > PG_PARAM_QPOS0) return fail(PG_ERR_INVALID, "unknown parameter");
+  int rc = check_range(h, start, end);
+  if (rc) return rc;
+  const HostModel& m = h->hm;
+  int w = param_width(m, param);
+  if (len != (size_t)(end - start) * w)
+    return fail(PG_ERR_LENGTH, "get_param: buffer has " + std::to_string(len) + " elements, expected " +
+                                   std::to_string(end - start) + " x " + std::to_string(w));
+  if (id < 0 || id >= param_count(m, param))
+    return fail(PG_ERR_INVALID, std::string(param_name(param)) + ": id " + std::to_string(id) + " out of range");
+  if (end == start) return PG_OK;
+  CK(cudaSetDevice(h->device));
+  std::vector<double> blk;
+  if ((rc = read_params(h, start, end, blk))) return rc;
+  for (int64_t k = 0; k < end - start; k++) read_param(h->dm, blk.data() + k * h->dm.pstride, param, id, out + k * w, m.nq);
+  return PG_OK;
+}
+
+int pg_appearance(pg_handle* h, int64_t start, int64_t end, pg_geom_appearance* out, size_t len) {
+  if (!h) return fail(PG_ERR_INVALID, "NULL handle");
+  int rc = check_range(h, start, end);
+  if (rc) return rc;
+  const HostModel& m = h->hm;
+  if (len != (size_t)(end - start) * m.ngeom)
+    return fail(PG_ERR_LENGTH, "appearance: buffer has " + std::to_string(len) + " elements, expected " +
+                                   std::to_string(end - start) + " x " + std::to_string(m.ngeom));
+  if (end == start) return PG_OK;
+  CK(cudaSetDevice(h->device));
+  std::vector<double> blk;
+  if ((rc = read_params(h, start, end, blk))) return rc;
+  const DModel& d = h->dm;
+  for (int64_t k = 0; k < end - start; k++) {
+    const double* prm = blk.data() + k * d.pstride;
+    for (int g = 0; g < m.ngeom; g++) {
+      pg_geom_appearance& a = out[k * m.ngeom + g];
+      for (int c = 0; c < 4; c++) a.rgba[c] = (float)prm[d.p_rgba + 4 * g + c];
+      for (int c = 0; c < 3; c++) {
+        double base = m.geom_size[3 * g + c];
+        a.scale[c] = base > 0.0 ? (float)(prm[d.p_size + 3 * g + c] / base) : 1.0f;
+      }
+      a.pad = 0.0f;
+    }
+  }
+  return PG_OK;
+}
+
+int pg_scene_counts(const pg_handle* h, int64_t* nbody, int64_t* ngeom, int64_t* nmesh, int64_t* ncam) {
+  if (!h) return fail(PG_ERR_INVALID, "NULL handle");
+  if (nbody) *nbody = h->hm.nbody;
+  if (ngeom) *ngeom = h->hm.ngeom;
+  if (nmesh) *nmesh = h->hm.nmesh;
+  if (ncam) *ncam = h->hm.ncam;
+  return PG_OK;
+}
+
+int pg_scene_geoms(const pg_handle* h, pg_geom_visual* out, size_t len) {
+  if (!h) return fail(PG_ERR_INVALID, "NULL handle");
+  const HostModel& m = h->hm;
+  if (len != (size_t)m.ngeom) return fail(PG_ERR_LENGTH, "scene geoms: buffer must hold ngeom entries");
+  for (int g = 0; g < m.ngeom; g++) {
+    pg_geom_visual& v = out[g];
+    v.shape = m.geom_type[g];
+    v.mesh = m.geom_type[g] == GEOM_MESH ? m.geom_dataid[g] : -1;
+    for (int k = 0; k < 3; k++) v.size[k] = (float)m.geom_size[3 * g + k];
+    for (int k = 0; k < 4; k++) v.rgba[k] = (float)m.geom_rgba[4 * g + k];
+    v.body = m.geom_body[g];
+    v.group = m.geom_group[g];
+  }
+  return PG_OK;
+}
+
+int pg_scene_mesh(const pg_handle* h, int64_t mesh, float* vertices, size_t nvert_len, uint32_t* triangles,
+                  size_t ntri_len, int64_t* nvert, int64_t* ntri) {
+  if (!h) return fail(PG_ERR_INVALID, "NULL handle");
+  const HostModel& m = h->hm;
+  if (mesh < 0 || mesh >= m.nmesh) return fail(PG_ERR_INVALID, "mesh id out of range");
+  int nv = m.mesh_vnum[mesh], nt = m.mesh_tnum[mesh];
+  if (nvert) *nvert = nv;
+  if (ntri) *ntri = nt;
+  if (vertices) {
+    if (nvert_len != (size_t)nv * 3) return fail(PG_ERR_LENGTH, "mesh vertices: buffer must hold 3 x nvert floats");
+    for (int k = 0; k < 3 * nv; k++) vertices[k] = (float)m.mesh_vert[3 * m.mesh_vadr[mesh] + k];
+  }
+  if (triangles) {
+    if (ntri_len != (size_t)nt * 3) return fail(PG_ERR_LENGTH, "mesh triangles: buffer must hold 3 x ntri indices");
+    for (int k = 0; k < 3 * nt; k++) triangles[k] = (uint32_t)m.mesh_tri[3 * m.mesh_tadr[mesh] + k];
+  }
+  return PG_OK;
+}
+
+int pg_camera_fovy(const pg_handle* h, int64_t cam, float* fovy) {
+  if (!h || !fovy) return fail(PG_ERR_INVALID, "NULL argument");
+  if (cam < 0 || cam >= h->hm.ncam) return fail(PG_ERR_INVALID, "camera id out of range");
+  *fovy = (float)h->hm.cam_fovy[cam];
+  return PG_OK;
+}
+
+int pg_name_of(const pg_handle* h, int table, int64_t id, char* buf, size_t len) {
+  if (!h || !buf || len == 0) return fail(PG_ERR_INVALID, "NULL argument");
+  if (table < 0 || table > 5) return fail(PG_ERR_INVALID, "unknown name table");
+  const auto& t = h->hm.names[table];
+  if (id < 0 || id >= (int64_t)t.size()) return fail(PG_ERR_INVALID, "name id out of range");
+  size_t n = std::min(t[id].size(), len - 1);
+  std::memcpy(buf, t[id].data(), n);
+  buf[n] = 0;
+  return PG_OK;
+}
+
+int pg_set_solver(pg_handle* h, int kind, int max_iter, double tolerance, int warm_mode) {
+  if (!h) return fail(PG_ERR_INVALID, "NULL handle");
+  if (kind > 1 || warm_mode > 2) return fail(PG_ERR_INVALID, "unknown solver or warm-start mode");
+  if (kind == PG_SOLVER_PGS) return fail(PG_ERR_UNSUPPORTED, "PGS is not available in this build");
+  if (warm_mode == PG_WARM_LEARNED) return fail(PG_ERR_UNSUPPORTED, "no learned warm start is loaded");
+  if (kind >= 0) h->dm.solver = kind;
+  if (max_iter >= 0) h->dm.iterations = max_iter;
+  if (tolerance >= 0) h->dm.tolerance = tolerance;
+  if (warm_mode >= 0) h->warm_mode = warm_mode;
+  h->version++;
+  return PG_OK;
+}
+
+int pg_stats(pg_handle* h, int64_t start, int64_t end, int32_t* iters, int32_t* ncon, int32_t* nrows, int32_t* status) {
+  if (!h) return fail(PG_ERR_INVALID, "NULL handle");
+  int rc = check_range(h, start, end);
+  if (rc) return rc;
+  if (end == start) return PG_OK;
+  CK(cudaSetDevice(h->device));
+  size_t b = sizeof(int32_t) * (end - start);
+  if (iters) CK(cudaMemcpyAsync(iters, h->iters + start, b, cudaMemcpyDeviceToHost, h->stream));
+  if (ncon) CK(cudaMemcpyAsync(ncon, h->ncon + start, b, cudaMemcpyDeviceToHost, h->stream));
+  if (nrows) CK(cudaMemcpyAsync(nrows, h->nrows + start, b, cudaMemcpyDeviceToHost, h->stream));
+  if (status) CK(cudaMemcpyAsync(status, h->status + start, b, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return PG_OK;
+}
+
+int pg_debug_forward(pg_handle* h, int64_t env, double* qm, double* qfrc_bias, double* contacts, int64_t maxcon,
+                     int64_t* ncon) {
+  if (!h) return fail(PG_ERR_INVALID, "NULL handle");
+  if (env < 0 || env >= h->n) return fail(PG_ERR_INVALID, "env out of range");
+  if (maxcon < 0) return fail(PG_ERR_INVALID, "maxcon must be non-negative");
+  CK(cudaSetDevice(h->device));
+  int nv = h->hm.nv;
+  int stride = nv * nv + nv + 1 + 13 * (int)std::min<int64_t>(maxcon, h->dm.maxcon);
+  int rc = grow(h, h->b_dbg, sizeof(double) * stride);
+  if (rc) return rc;
+  StepArgs a = make_args(h);
+  a.start = (int)env;
+  a.count = 1;
+  if ((rc = run_tile_kernel(h, K_FORWARD, a, 1, nullptr, nullptr, nullptr, (double*)h->b_dbg.p, stride,
+                            (int)std::min<int64_t>(maxcon, h->dm.maxcon))))
+    return rc;
+  std::vector<double> out(stride);
+  CK(cudaMemcpyAsync(out.data(), h->b_dbg.p, sizeof(double) * stride, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  if (qm) std::memcpy(qm, out.data(), sizeof(double) * nv * nv);
+  if (qfrc_bias) std::memcpy(qfrc_bias, out.data() + nv * nv, sizeof(double) * nv);
+  int64_t n = (int64_t)out[nv * nv + nv];
+  if (ncon) *ncon = n;
+  if (contacts) std::memcpy(contacts, out.data() + nv * nv + nv + 1, sizeof(double) * 13 * std::min(n, maxcon));
+  return PG_OK;
+}
+
+int pg_invweight(pg_handle* h, int64_t env, double* body, double* dof) {
+  if (!h) return fail(PG_ERR_INVALID, "NULL handle");
+  if (env < 0 || env >= h->n) return fail(PG_ERR_INVALID, "env out of range");
+  std::vector<double> blk;
+  int rc = read_params(h, env, env + 1, blk);
+  if (rc) return rc;
+  if (body) std::memcpy(body, blk.data() + h->dm.p_body_invw, sizeof(double) * 2 * h->hm.nbody);
+  if (dof) std::memcpy(dof, blk.data() + h->dm.p_dof_invw, sizeof(double) * h->hm.nv);
+  return PG_OK;
+}
+
+int pg_set_launch(pg_handle* h, int lanes_per_env, int envs_per_block) {
+  if (!h) return fail(PG_ERR_INVALID, "NULL handle");
+  LaunchCfg c = h->cfg;
+  if (lanes_per_env > 0) c.G = lanes_per_env;
+  if (envs_per_block > 0) c.tiles_per_block = envs_per_block;
+  CK(cudaSetDevice(h->device));
+  return apply_cfg(h, c);
+}
+
+int pg_get_launch(const pg_handle* h, int* lanes_per_env, int* envs_per_block, int* blocks) {
+  if (!h) return fail(PG_ERR_INVALID, "NULL handle");
+  if (lanes_per_env) *lanes_per_env = h->cfg.G;
+  if (envs_per_block) *envs_per_block = h->cfg.tiles_per_block;
+  if (blocks) *blocks = h->cfg.blocks;
+  return PG_OK;
+}
+
+int pg_autotune(pg_handle* h, int64_t nstep) {
+  if (!h) return fail(PG_ERR_INVALID, "NULL handle");
+  if (h->n == 0) return PG_OK;
+  if (nstep < 1) nstep = 1;
+  CK(cudaSetDevice(h->device));
+  const HostModel& m = h->hm;
+  size_t n = h->n;
+  // save the state the trial steps will overwrite
+  std::vector<double*> fields = {h->qpos, h->qvel, h->ctrl, h->qacc, h->applied};
+  std::vector<size_t> widths = {(size_t)m.nq, (size_t)m.nv, (size_t)m.nu, (size_t)m.nv, (size_t)m.nv};
+  std::vector<void*> saved;
+  for (size_t k = 0; k < fields.size(); k++) {
+    void* p = nullptr;
+    CK(cudaMalloc(&p, sizeof(double) * n * std::max<size_t>(widths[k], 1)));
+    CK(cudaMemcpyAsync(p, fields[k], sizeof(double) * n * widths[k], cudaMemcpyDeviceToDevice, h->stream));
+    saved.push_back(p);
+  }
+  auto restore = [&]() {
+    for (size_t k = 0; k < fields.size(); k++)
+      cudaMemcpyAsync(fields[k], saved[k], sizeof(double) * n * widths[k], cudaMemcpyDeviceToDevice, h->stream);
+  };
+  LaunchCfg best = h->cfg;
+  float best_ms = 1e30f;
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  int rc = PG_OK;
+  for (int G : {8, 16, 32}) {
+    for (int tpb : {1, 2, 4, 8, 16}) {
+      LaunchCfg want{G, tpb, 0}, c;
+      if (tpb * G < 32 || tpb * G > 256) continue;
+      if (choose_grid(h, want, &c) != PG_OK) continue;
+      if (ensure_scratch(h, c) != PG_OK) continue;
+      h->cfg = c;
+      StepArgs a = make_args(h);
+      a.start = 0;
+      a.count = (int)n;
+      a.nstep = (int)nstep;
+      restore();
+      run_tile_kernel(h, K_STEP, a, n);  // warm-up
+      restore();
+      cudaEventRecord(e0, h->stream);
+      run_tile_kernel(h, K_STEP, a, n);
+      cudaEventRecord(e1, h->stream);
+      if (cudaEventSynchronize(e1) != cudaSuccess) {
+        rc = cuda_fail(cudaGetLastError(), "autotune trial");
+        break;
+      }
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (ms < best_ms) {
+        best_ms = ms;
+        best = c;
+      }
+    }
+    if (rc) break;
+  }
+  restore();
+  cudaStreamSynchronize(h->stream);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  for (void* p : saved) cudaFree(p);
+  g_err.clear();
+  h->cfg = best;
+  h->version++;
+  return rc;
+}
+
+int pg_synchronize(pg_handle* h) {
+  if (!h) return fail(PG_ERR_INVALID, "NULL handle");
+  CK(cudaSetDevice(h->device));
+  CK(cudaStreamSynchronize(h->stream));
+  return PG_OK;
+}
+
+int pg_field_device_ptr(pg_handle* h, int field, double** dev_ptr) {
+  if (!h || !dev_ptr) return fail(PG_ERR_INVALID, "NULL argument");
+  double* p = field_ptr(h, field);
+  if (!p) return fail(PG_ERR_INVALID, "unknown field");
+  *dev_ptr = p;
+  return PG_OK;
+}
+
+void* pg_stream(pg_handle* h) { return h ? (void*)h->stream : nullptr; }
+
+}  // extern "C"

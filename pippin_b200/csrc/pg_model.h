@@ -1,0 +1,180 @@
+// Device-resident model, per-env parameter blocks, per-env state and the
+// per-tile workspace layout of the batched substep.
+//
+// HBM layout (all FP64 unless noted):
+//   model constants   one copy, read through L1 by every tile
+//   env parameters    [env][pstride]: the per-env copy of every parameter
+//                     the reference can change per environment
+//                     (crates/pippin/src/params.rs:10-39) plus derived
+//                     invweight0 (forward.rs:275-333)
+//   env state         qpos[env][nq], qvel[env][nv], ctrl[env][nu],
+//                     qacc[env][nv] (Newton warm start), qfrc_applied[env][nv]
+//   tile scratch      [tile][sstride]: contacts, constraint rows and island
+//                     buffers of the env a tile is working on
+//   shared memory     [tile][wstride]: kinematics, inertia, M and its factor
+#pragma once
+#include <cstdint>
+
+namespace pg {
+
+enum { JNT_FREE = 0, JNT_BALL = 1, JNT_SLIDE = 2, JNT_HINGE = 3 };
+enum { GEOM_PLANE = 0, GEOM_SPHERE = 1, GEOM_CAPSULE = 2, GEOM_BOX = 3, GEOM_CYLINDER = 4, GEOM_MESH = 5 };
+enum { SOLVER_NEWTON = 0, SOLVER_PGS = 1 };
+enum { WARM_REF_PREV_QACC = 0, WARM_COLD = 1, WARM_LEARNED = 2 };
+
+// per-env status bits
+enum { ST_OK = 0, ST_CAP_EXCEEDED = 1, ST_NOT_SPD = 2, ST_UNSUPPORTED_PAIR = 4 };
+
+// contact record in tile scratch (doubles)
+enum { C_POS = 0, C_NORMAL = 3, C_TANGENT = 6, C_DEPTH = 9, C_G1 = 10, C_G2 = 11, C_FEATURE = 12, C_T1 = 13,
+       C_T2 = 16, C_ROW = 19, C_STRIDE = 20 };
+// constraint row record in tile scratch (doubles)
+enum { R_AREF = 0, R_D = 1, R_JAR = 2, R_JP = 3, R_POS = 4, R_DIAG = 5, R_FLAGS = 6, R_ACT = 7, R_STRIDE = 8 };
+
+constexpr int NV_MAX = 64;  // dof-chain masks are 64-bit
+
+struct DModel {
+  // ---- dims
+  int nq, nv, nu, nbody, njnt, ngeom, ncam, neq, npair, nblock, nlevel, nmesh;
+  int maxcon, maxrows;
+  // ---- options (model.rs:60-100)
+  double timestep, gravity[3];
+  int integrator, solver, iterations;
+  double tolerance, margin, solref[2], solimp[5], impratio, hertz, dampratio, slop;
+
+  // ---- bodies
+  const int* body_parent;
+  const int* body_jntadr;
+  const int* body_jntnum;
+  const int* body_dofadr;
+  const int* body_dofnum;
+  const int* body_lastdof;
+  const unsigned long long* body_dofmask;  // bit k: dof k on the body's chain to the world
+  const double* body_pos;                  // [nb][3]
+  const double* body_quat;                 // [nb][4]
+  const int* level_adr;                    // [nlevel+1] into level_body (bodies by depth)
+  const int* level_body;
+  const int* child_adr;                    // [nb+1] into child_list (children, decreasing id)
+  const int* child_list;
+  // ---- joints
+  const int* jnt_type;
+  const int* jnt_qposadr;
+  const int* jnt_dofadr;
+  const int* jnt_limited;
+  const double* jnt_pos;  // [nj][3]
+  const double* jnt_axis;
+  const double* jnt_range;  // [nj][2]
+  const double* jnt_stiffness;
+  const double* jnt_springref;
+  // ---- dofs
+  const int* dof_body;
+  const int* dof_parent;
+  const double* dof_armature;
+  const int* dof_block;       // block id of each dof
+  const int* block_adr;       // [nblock][2] = [start, end)
+  const int* dofact_adr;      // [nv+1] actuator contributions per dof, in actuator order
+  const int* dofact_u;
+  const double* dofact_coef;
+  // ---- geoms
+  const int* geom_type;
+  const int* geom_body;
+  const int* geom_dataid;
+  const double* geom_pos;   // [ng][3]
+  const double* geom_quat;  // [ng][4]
+  const int* pair_g;        // [npair][2] candidate pairs (static filter; masks per env)
+  // ---- cameras
+  const int* cam_body;
+  const double* cam_pos;
+  const double* cam_quat;
+  // ---- actuators
+  const double* act_gear;
+  const int* act_ctrllimited;
+  const double* act_ctrlrange;  // [nu][2]
+  const int* act_forcelimited;
+  const double* act_forcerange;
+  const int* act_moment_adr;
+  const int* act_moment_num;
+  const int* moment_jnt;
+  const double* moment_coef;
+  // ---- joint equality
+  const int* eq_j1;
+  const int* eq_j2;
+  const double* eq_poly;    // [neq][5]
+  const double* eq_solref;  // [neq][2]
+  const double* eq_solimp;  // [neq][5]
+  // ---- reference configuration
+  const double* qpos0;
+  // ---- convex hulls (for mesh geoms)
+  const int* hull_vadr;
+  const int* hull_vnum;
+  const double* hull_vert;  // [*][3]
+  const int* hull_fadr;
+  const int* hull_fnum;
+  const double* hull_face;  // [*][4]: outward unit normal, offset (n.x <= d)
+
+  // ---- per-env parameter block offsets (doubles) and stride
+  int p_friction, p_size, p_contype, p_conaff, p_mass, p_inertia, p_ipos, p_damping, p_gain, p_bias, p_qpos_reset,
+      p_body_invw, p_dof_invw, p_rgba;
+  int pstride;
+};
+
+// Per-tile shared-memory workspace (offsets in doubles).
+struct WsLayout {
+  int qpos, qvel, ctrl, qacc, applied;
+  int xpos, xquat, xmat, xipos, cinert, crb, cvel, cacc, cfrc;
+  int cdof, cdof_dot;
+  int gxpos, gxmat, gaabb;
+  int qm, fac;
+  int bias, passive, actf, smooth, acc, qfrc_c, a0, grad, p, tmp, tmp2, mp, vel, warm;
+  int actforce, actclamped;
+  int misc;  // small scalars
+  int stride;
+};
+
+// Per-tile global scratch layout (offsets in doubles).
+struct ScrLayout {
+  int contacts;  // maxcon * C_STRIDE
+  int jac;       // maxrows * nv
+  int rows;      // maxrows * R_STRIDE
+  int sub_m;     // nv * nv   (island gather)
+  int sub_j;     // maxrows * nv
+  int sub_rows;  // maxrows * R_STRIDE
+  int isl_dof;   // nv ints stored as doubles
+  int isl_row;   // maxrows
+  int isl_of_row;
+  int minv_jt;   // PGS: maxrows * nv
+  int lambda;    // PGS: maxrows
+  int stride;
+};
+
+struct EnvState {
+  double* qpos;
+  double* qvel;
+  double* ctrl;
+  double* qacc;
+  double* applied;
+  double* params;  // [env][pstride]
+  int32_t* iters;
+  int32_t* ncon;
+  int32_t* nrows;
+  int32_t* status;
+  // PGS warm start carried between steps (solver.rs:254-289)
+  double* prev_con;   // [env][maxcon][C_PREV]
+  int32_t* prev_ncon;
+};
+enum { P_POS = 0, P_NORMAL = 3, P_TANGENT = 6, P_G1 = 9, P_G2 = 10, P_LAMBDA = 11, P_STRIDE = 14 };
+
+struct StepArgs {
+  DModel m;
+  WsLayout w;
+  ScrLayout s;
+  EnvState st;
+  double* scratch;        // [tiles][s.stride]
+  int* queue;             // work counter (reset to 0 before each launch)
+  int start, count, nstep;
+  int warm_mode;
+  const double* ctrl_seq;  // optional (count, nstep, nu): per-substep controls
+  double* qpos_out;        // optional (count, nstep, nq): qpos after each substep
+};
+
+}  // namespace pg

@@ -1,0 +1,680 @@
+// Contacts, constraint rows and the primal Newton solver of one environment
+// on a tile of G lanes. Restates crates/pippin/src/forward.rs:214-260
+// (broad + narrow phase), crates/pippin/src/newton.rs:113-473 (pyramidal
+// contact rows, joint-limit and joint-equality rows with soft-constraint
+// constants, islands over dof blocks, dense Newton with exact line search
+// and the cost-gated warm start) and forward.rs:336-480 (substep driver,
+// implicit damping, integration).
+#pragma once
+#include "pg_collide.cuh"
+#include "pg_dynamics.cuh"
+#include "pg_linalg.cuh"
+
+namespace pg {
+
+// ---------------------------------------------------------------- collide
+// Local bounding box of a geom (model.rs:365-382) from the per-env size.
+__device__ inline void local_aabb(const DModel& m, const double* prm, int g, V3* c, V3* h) {
+  V3 s = ld3(prm + m.p_size + 3 * g);
+  *c = V3{0, 0, 0};
+  switch (m.geom_type[g]) {
+    case GEOM_PLANE: *h = V3{INFINITY, INFINITY, INFINITY}; break;
+    case GEOM_SPHERE: *h = V3{s.x, s.x, s.x}; break;
+    case GEOM_CAPSULE: *h = V3{s.x, s.x, s.x + s.y}; break;
+    case GEOM_BOX: *h = s; break;
+    case GEOM_CYLINDER: *h = V3{s.x, s.x, s.y}; break;
+    default: {  // mesh: bounds of the hull vertices
+      int id = m.geom_dataid[g];
+      V3 lo{INFINITY, INFINITY, INFINITY}, hi{-INFINITY, -INFINITY, -INFINITY};
+      for (int k = 0; k < m.hull_vnum[id]; k++) {
+        V3 v = ld3(m.hull_vert + 3 * (m.hull_vadr[id] + k));
+        lo = V3{fmin(lo.x, v.x), fmin(lo.y, v.y), fmin(lo.z, v.z)};
+        hi = vmax(hi, v);
+      }
+      *c = (lo + hi) * 0.5;
+      *h = (hi - lo) * 0.5;
+    }
+  }
+}
+
+// Returns the contact count; contacts land in scratch in pair order (and
+// hit order within a pair), as in the reference's sequential pair loop.
+template <int G>
+__device__ int collide(const Tile<G>& T, const DModel& m, const WsLayout& w, const ScrLayout& s, const EnvCtx& e,
+                       int* status) {
+  int lane = T.lane();
+  double* ws = e.ws;
+  const double* prm = e.prm;
+  double* gaabb = ws + w.gaabb;
+  for (int g = lane; g < m.ngeom; g += G) {
+    V3 c, h;
+    local_aabb(m, prm, g, &c, &h);
+    if (!isfinite(h.x)) {
+      st3(gaabb + 6 * g, V3{0, 0, 0});
+      st3(gaabb + 6 * g + 3, h);
+      continue;
+    }
+    M3 r = ld9(ws + w.gxmat + 9 * g);
+    V3 center = ld3(ws + w.gxpos + 3 * g) + mv(r, c);
+    V3 half{fabs(r.m[0]) * h.x + fabs(r.m[1]) * h.y + fabs(r.m[2]) * h.z,
+            fabs(r.m[3]) * h.x + fabs(r.m[4]) * h.y + fabs(r.m[5]) * h.z,
+            fabs(r.m[6]) * h.x + fabs(r.m[7]) * h.y + fabs(r.m[8]) * h.z};
+    st3(gaabb + 6 * g, center);
+    st3(gaabb + 6 * g + 3, half);
+  }
+  T.sync();
+  double* con = e.scr + s.contacts;
+  int ncon = 0;
+  int st = 0;
+  for (int base = 0; base < m.npair; base += G) {
+    int p = base + lane;
+    Hits hits;
+    hits.n = 0;
+    int g1 = 0, g2 = 0;
+    if (p < m.npair) {
+      g1 = m.pair_g[2 * p];
+      g2 = m.pair_g[2 * p + 1];
+      unsigned t1 = (unsigned)prm[m.p_contype + g1], a1 = (unsigned)prm[m.p_conaff + g1];
+      unsigned t2 = (unsigned)prm[m.p_contype + g2], a2 = (unsigned)prm[m.p_conaff + g2];
+      bool masks = (t1 & a2) != 0 || (t2 & a1) != 0;
+      if (masks) {
+        V3 c1 = ld3(gaabb + 6 * g1), h1 = ld3(gaabb + 6 * g1 + 3);
+        V3 c2 = ld3(gaabb + 6 * g2), h2 = ld3(gaabb + 6 * g2 + 3);
+        bool sep = fabs(c1.x - c2.x) > h1.x + h2.x + m.margin || fabs(c1.y - c2.y) > h1.y + h2.y + m.margin ||
+                   fabs(c1.z - c2.z) > h1.z + h2.z + m.margin;
+        if (!sep) {
+          GPose a{m.geom_type[g1], ld3(ws + w.gxpos + 3 * g1), ld9(ws + w.gxmat + 9 * g1), ld3(prm + m.p_size + 3 * g1)};
+          GPose b{m.geom_type[g2], ld3(ws + w.gxpos + 3 * g2), ld9(ws + w.gxmat + 9 * g2), ld3(prm + m.p_size + 3 * g2)};
+          if (needs_general(a.type, b.type)) st |= ST_UNSUPPORTED_PAIR;
+          else collide_primitive(a, b, m.margin, hits);
+        }
+      }
+    }
+    int nh = hits.n < MAX_HITS ? hits.n : MAX_HITS;
+    int tot;
+    int off = T.excl_scan(nh, &tot);
+    for (int k = 0; k < nh; k++) {
+      int c = ncon + off + k;
+      if (c >= m.maxcon) {
+        st |= ST_CAP_EXCEEDED;
+        break;
+      }
+      double* r = con + C_STRIDE * c;
+      const Hit& h = hits.h[k];
+      st3(r + C_POS, h.pos);
+      st3(r + C_NORMAL, h.normal);
+      st3(r + C_TANGENT, h.tangent);
+      r[C_DEPTH] = h.depth;
+      r[C_G1] = g1;
+      r[C_G2] = g2;
+      r[C_FEATURE] = k;
+      V3 t1, t2;
+      contact_frame(h.normal, h.tangent, &t1, &t2);
+      st3(r + C_T1, t1);
+      st3(r + C_T2, t2);
+    }
+    ncon += tot;
+  }
+  if (ncon > m.maxcon) ncon = m.maxcon;
+  *status |= T.ior(st);
+  T.sync();
+  return ncon;
+}
+
+// ---------------------------------------------------------------- rows
+// newton.rs:52-66
+__device__ inline double impedance(const double* solimp, double pos) {
+  double dmin = solimp[0], dmax = solimp[1], width = solimp[2], mid = solimp[3], power = solimp[4];
+  double x = fmin(fabs(pos) / fmax(width, 1e-12), 1.0);
+  if (x >= 1.0 || dmin == dmax) return dmax;
+  auto pw = [](double b, double ex) { return ex == 2.0 ? b * b : (ex == 1.0 ? b : pow(b, ex)); };
+  double y = x <= mid ? pw(x, power) / pw(mid, power - 1.0) : 1.0 - pw(1.0 - x, power) / pw(1.0 - mid, power - 1.0);
+  return clampd(dmin + y * (dmax - dmin), 1e-4, 0.9999);
+}
+
+// Jacobian entry k of a world point on the pair (b1, b2) along `dir`
+// (solver.rs:53-59 applied to b2 with +1, then b1 with -1).
+__device__ inline double pair_jac(const DModel& m, const double* cdof, int b1, int b2, V3 p, V3 dir, int k) {
+  double v = 0.0;
+  unsigned long long bit = 1ull << k;
+  if (m.body_dofmask[b2] & bit) v += dot(dir, point_vel(ld6(cdof + 6 * k), p));
+  if (m.body_dofmask[b1] & bit) v += -1.0 * dot(dir, point_vel(ld6(cdof + 6 * k), p));
+  return v;
+}
+
+// newton.rs:113-218. Returns the row count. Row order: 4 pyramid rows per
+// touching contact (contact order), violated joint limits (joint order,
+// lower side first), joint equalities.
+template <int G>
+__device__ int build_rows(const Tile<G>& T, const DModel& m, const WsLayout& w, const ScrLayout& s, const EnvCtx& e,
+                          int ncon, int* status) {
+  int lane = T.lane(), nv = m.nv;
+  const double* ws = e.ws;
+  const double* prm = e.prm;
+  double* con = e.scr + s.contacts;
+  double* J = e.scr + s.jac;
+  double* R = e.scr + s.rows;
+  const double* cdof = ws + w.cdof;
+  // touching contacts get 4 rows each; C_ROW records the first one
+  int nt = 0;
+  for (int base = 0; base < ncon; base += G) {
+    int c = base + lane;
+    bool touch = c < ncon && con[C_STRIDE * c + C_DEPTH] > 0.0;
+    int tot;
+    int off = T.excl_scan(touch ? 1 : 0, &tot);
+    if (c < ncon) {
+      double* r = con + C_STRIDE * c;
+      int row = touch ? 4 * (nt + off) : -1;
+      if (row + 4 > m.maxrows) row = -1;
+      r[C_ROW] = row;
+      if (row >= 0) {
+        int g1 = (int)r[C_G1], g2 = (int)r[C_G2];
+        int b1 = m.geom_body[g1], b2 = m.geom_body[g2];
+        double mu = fmax(prm[m.p_friction + g1], prm[m.p_friction + g2]);
+        double tran = prm[m.p_body_invw + 2 * b1] + prm[m.p_body_invw + 2 * b2];
+        double dpyr = 2.0 * mu * mu * (1.0 + mu * mu) * tran / m.impratio;
+        for (int q = 0; q < 4; q++) {
+          double* rr = R + R_STRIDE * (row + q);
+          rr[R_POS] = -r[C_DEPTH];
+          rr[R_DIAG] = dpyr;
+          rr[R_FLAGS] = 0.0;
+        }
+      }
+    }
+    nt += tot;
+  }
+  int ncrow = 4 * nt;
+  if (ncrow > m.maxrows) {
+    *status |= ST_CAP_EXCEEDED;
+    ncrow = m.maxrows & ~3;
+  }
+  T.sync();
+  // Jacobian entries: one item per (contact, dof)
+  for (int it = lane; it < ncon * nv; it += G) {
+    int c = it / nv, k = it % nv;
+    const double* r = con + C_STRIDE * c;
+    int row = (int)r[C_ROW];
+    if (row < 0) continue;
+    int g1 = (int)r[C_G1], g2 = (int)r[C_G2];
+    int b1 = m.geom_body[g1], b2 = m.geom_body[g2];
+    double mu = fmax(prm[m.p_friction + g1], prm[m.p_friction + g2]);
+    V3 p = ld3(r + C_POS);
+    double jn = pair_jac(m, cdof, b1, b2, p, ld3(r + C_NORMAL), k);
+    double jt1 = pair_jac(m, cdof, b1, b2, p, ld3(r + C_T1), k);
+    double jt2 = pair_jac(m, cdof, b1, b2, p, ld3(r + C_T2), k);
+    J[(row + 0) * nv + k] = jn + mu * jt1;
+    J[(row + 1) * nv + k] = jn + (-mu) * jt1;
+    J[(row + 2) * nv + k] = jn + mu * jt2;
+    J[(row + 3) * nv + k] = jn + (-mu) * jt2;
+  }
+  // joint limits: count violated sides per joint, then place
+  int nl = 0;
+  for (int base = 0; base < m.njnt; base += G) {
+    int j = base + lane;
+    int cnt = 0;
+    double sep[2] = {0.0, 0.0};
+    int da = 0;
+    if (j < m.njnt && m.jnt_limited[j] && (m.jnt_type[j] == JNT_HINGE || m.jnt_type[j] == JNT_SLIDE)) {
+      double q = ws[w.qpos + m.jnt_qposadr[j]];
+      da = m.jnt_dofadr[j];
+      sep[0] = q - m.jnt_range[2 * j];
+      sep[1] = m.jnt_range[2 * j + 1] - q;
+      cnt = (sep[0] < 0.0 ? 1 : 0) + (sep[1] < 0.0 ? 1 : 0);
+    }
+    int tot;
+    int off = T.excl_scan(cnt, &tot);
+    int row = ncrow + nl + off;
+    for (int t = 0; t < 2; t++) {
+      if (!(sep[t] < 0.0) || cnt == 0) continue;
+      if (row < m.maxrows) {
+        double* jr = J + row * nv;
+        for (int k = 0; k < nv; k++) jr[k] = 0.0;
+        jr[da] = t == 0 ? 1.0 : -1.0;
+        double* rr = R + R_STRIDE * row;
+        rr[R_POS] = sep[t];
+        rr[R_DIAG] = prm[m.p_dof_invw + da];
+        rr[R_FLAGS] = 0.0;
+      }
+      row++;
+    }
+    nl += tot;
+  }
+  int nineq = ncrow + nl;
+  // joint equality rows (bilateral)
+  for (int q = lane; q < m.neq; q += G) {
+    int row = nineq + q;
+    if (row >= m.maxrows) continue;
+    int j1 = m.eq_j1[q], j2 = m.eq_j2[q];
+    const double* c = m.eq_poly + 5 * q;
+    double q1 = ws[w.qpos + m.jnt_qposadr[j1]] - m.qpos0[m.jnt_qposadr[j1]];
+    double poly = c[0], dpoly = 0.0;
+    if (j2 != -1) {
+      double x = ws[w.qpos + m.jnt_qposadr[j2]] - m.qpos0[m.jnt_qposadr[j2]];
+      poly = c[0] + x * (c[1] + x * (c[2] + x * (c[3] + x * c[4])));
+      dpoly = c[1] + x * (2.0 * c[2] + x * (3.0 * c[3] + x * 4.0 * c[4]));
+    }
+    double* jr = J + row * nv;
+    for (int k = 0; k < nv; k++) jr[k] = 0.0;
+    jr[m.jnt_dofadr[j1]] += 1.0;
+    double dg = prm[m.p_dof_invw + m.jnt_dofadr[j1]];
+    if (j2 != -1) {
+      jr[m.jnt_dofadr[j2]] -= dpoly;
+      dg += prm[m.p_dof_invw + m.jnt_dofadr[j2]];
+    }
+    double* rr = R + R_STRIDE * row;
+    rr[R_POS] = q1 - poly;
+    rr[R_DIAG] = dg;
+    rr[R_FLAGS] = 1.0;
+  }
+  int nr = nineq + m.neq;
+  if (nr > m.maxrows) {
+    *status |= ST_CAP_EXCEEDED;
+    nr = m.maxrows;
+  }
+  T.sync();
+  // reference acceleration and regularisation per row
+  const double* qvel = ws + w.qvel;
+  for (int r = lane; r < nr; r += G) {
+    double* rr = R + R_STRIDE * r;
+    bool bil = rr[R_FLAGS] != 0.0;
+    const double* solref = m.solref;
+    const double* solimp = m.solimp;
+    if (bil) {
+      int q = r - nineq;
+      solref = m.eq_solref + 2 * q;
+      solimp = m.eq_solimp + 5 * q;
+    }
+    double tc = fmax(solref[0], 2.0 * m.timestep), dr = solref[1];
+    double dmax = solimp[1];
+    double b = 2.0 / (dmax * tc);
+    double kk = 1.0 / (dmax * dmax * tc * tc * dr * dr);
+    const double* jr = J + r * nv;
+    double vel = 0.0;
+    for (int i = 0; i < nv; i++) vel += jr[i] * qvel[i];
+    double imp = impedance(solimp, rr[R_POS]);
+    double reg = fmax((1.0 - imp) / imp * rr[R_DIAG], 1e-15);
+    rr[R_AREF] = -b * vel - kk * imp * rr[R_POS];
+    rr[R_D] = 1.0 / reg;
+  }
+  T.sync();
+  return nr;
+}
+
+// ---------------------------------------------------------------- dense Newton
+struct NewtonBufs {
+  double *a0, *grad, *p, *tmp, *tmp2, *mp, *hess;
+};
+
+__device__ inline bool row_active(const double* rr, double v) { return rr[R_FLAGS] != 0.0 || v < 0.0; }
+
+// y = M x (newton.rs:75-81; the damping term there is zero)
+template <int G>
+__device__ inline void mul_m(const Tile<G>& T, const double* M, int k, const double* x, double* y) {
+  for (int i = T.lane(); i < k; i += G) y[i] = dot_ref(M + i * k, 1, x, 1, k);
+  T.sync();
+}
+
+// newton.rs:96-110: total cost at aa (fills R_JAR)
+template <int G>
+__device__ double cost(const Tile<G>& T, int k, int nr, const double* J, double* R, const double* M, const double* aa,
+                       const double* a0, double* tmp, double* tmp2) {
+  int lane = T.lane();
+  for (int i = lane; i < k; i += G) tmp[i] = aa[i] - a0[i];
+  T.sync();
+  mul_m(T, M, k, tmp, tmp2);
+  double s = 0.0;
+  for (int i = lane; i < k; i += G) s += tmp[i] * tmp2[i];
+  double c = 0.5 * T.sum(s);
+  double cr = 0.0;
+  for (int r = lane; r < nr; r += G) {
+    double* rr = R + R_STRIDE * r;
+    double jar = dot_ref(J + r * k, 1, aa, 1, k) - rr[R_AREF];
+    rr[R_JAR] = jar;
+    if (row_active(rr, jar)) cr += 0.5 * rr[R_D] * jar * jar;
+  }
+  T.sync();
+  return c + T.sum(cr);
+}
+
+// newton.rs:224-358: `a` holds the unconstrained acceleration on entry and
+// the constrained one on exit. Returns the iteration count.
+template <int G>
+__device__ int newton_dense(const Tile<G>& T, int k, int nr, const double* J, double* R, const double* M, double* a,
+                            const double* warm, int max_iters, double tol, const NewtonBufs& B) {
+  int lane = T.lane();
+  double *a0 = B.a0, *grad = B.grad, *p = B.p, *tmp = B.tmp, *tmp2 = B.tmp2, *mp = B.mp, *H = B.hess;
+  for (int i = lane; i < k; i += G) a0[i] = a[i];
+  T.sync();
+  if (warm) {
+    double c0 = cost(T, k, nr, J, R, M, a0, a0, tmp, tmp2);
+    double c1 = cost(T, k, nr, J, R, M, warm, a0, tmp, tmp2);
+    if (c1 < c0)
+      for (int i = lane; i < k; i += G) a[i] = warm[i];
+    T.sync();
+  }
+  mul_m(T, M, k, a0, tmp);
+  double ss = 0.0;
+  for (int i = lane; i < k; i += G) ss += tmp[i] * tmp[i];
+  double scale = 1.0 + sqrt(T.sum(ss));
+  int iters = 0;
+  int maxit = max_iters > 1 ? max_iters : 1;
+  while (iters < maxit) {
+    iters++;
+    for (int i = lane; i < k; i += G) tmp[i] = a[i] - a0[i];
+    T.sync();
+    mul_m(T, M, k, tmp, grad);
+    // residuals, active set; R_ACT keeps the previous iteration's set
+    bool same = true;
+    for (int r = lane; r < nr; r += G) {
+      double* rr = R + R_STRIDE * r;
+      double jar = dot_ref(J + r * k, 1, a, 1, k) - rr[R_AREF];
+      rr[R_JAR] = jar;
+      double act = row_active(rr, jar) ? 1.0 : 0.0;
+      if (act != rr[R_ACT]) same = false;
+      rr[R_ACT] = act;
+    }
+    T.sync();
+    for (int i = lane; i < k; i += G) {
+      double g = grad[i];
+      for (int r = 0; r < nr; r++) {
+        const double* rr = R + R_STRIDE * r;
+        if (rr[R_ACT] != 0.0) g += (rr[R_D] * rr[R_JAR]) * J[r * k + i];
+      }
+      grad[i] = g;
+    }
+    T.sync();
+    double gs = 0.0;
+    for (int i = lane; i < k; i += G) gs += grad[i] * grad[i];
+    double gnorm = sqrt(T.sum(gs));
+    bool unchanged = T.all(same);
+    if (gnorm < tol * scale || (nr <= 128 && unchanged && iters > 1)) break;
+    // H = M + J_A' D J_A (lower triangle)
+    for (int t = lane; t < k * (k + 1) / 2; t += G) {
+      int i = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+      while ((i + 1) * (i + 2) / 2 <= t) i++;
+      while (i * (i + 1) / 2 > t) i--;
+      int j = t - i * (i + 1) / 2;
+      double h = M[i * k + j];
+      for (int r = 0; r < nr; r++) {
+        const double* rr = R + R_STRIDE * r;
+        if (rr[R_ACT] == 0.0) continue;
+        double ji = J[r * k + i];
+        if (ji == 0.0) continue;
+        h += (rr[R_D] * ji) * J[r * k + j];
+      }
+      H[i * k + j] = h;
+    }
+    T.sync();
+    if (!chol_blocks(T, H, k, k, 1, nullptr, nullptr, k)) break;
+    for (int i = lane; i < k; i += G) p[i] = -grad[i];
+    T.sync();
+    solve_blocks(T, H, k, k, 1, nullptr, p);
+    // exact line search on the piecewise quadratic along p
+    mul_m(T, M, k, p, mp);
+    double s1 = 0.0, s2 = 0.0;
+    for (int i = lane; i < k; i += G) {
+      s1 += p[i] * mp[i];
+      s2 += tmp[i] * mp[i];
+    }
+    double mpp = T.sum(s1), mpg = T.sum(s2);
+    for (int r = lane; r < nr; r += G) {
+      double* rr = R + R_STRIDE * r;
+      rr[R_JP] = dot_ref(J + r * k, 1, p, 1, k);
+    }
+    T.sync();
+    auto deriv = [&](double al, double* d1o, double* d2o) {
+      double d1 = 0.0, d2 = 0.0;
+      for (int r = lane; r < nr; r += G) {
+        const double* rr = R + R_STRIDE * r;
+        double v = rr[R_JAR] + al * rr[R_JP];
+        if (row_active(rr, v)) {
+          double dq = rr[R_D] * rr[R_JP];
+          d1 += dq * v;
+          d2 += dq * rr[R_JP];
+        }
+      }
+      *d1o = (al * mpp + mpg) + T.sum(d1);
+      *d2o = mpp + T.sum(d2);
+    };
+    double lo = 0.0, hi = INFINITY, al = 1.0;
+    double d10, d20;
+    deriv(0.0, &d10, &d20);
+    double ltol = 1e-12 * fmax(fabs(d10), 1e-30);
+    for (int it = 0; it < 50; it++) {
+      double d1, d2;
+      deriv(al, &d1, &d2);
+      if (fabs(d1) <= ltol) break;
+      if (d1 < 0.0) lo = al;
+      else hi = al;
+      double next = al - d1 / fmax(d2, 1e-30);
+      if (next <= lo || next >= hi) next = isfinite(hi) ? 0.5 * (lo + hi) : 2.0 * fmax(al, lo);
+      if (fabs(next - al) <= 1e-14 * fmax(fabs(al), 1.0)) {
+        al = next;
+        break;
+      }
+      al = next;
+    }
+    for (int i = lane; i < k; i += G) a[i] += al * p[i];
+    T.sync();
+  }
+  return iters;
+}
+
+// newton.rs:361-371: qfrc[idx[i]] += -J' D (J a - aref) over active rows
+template <int G>
+__device__ void add_constraint_force(const Tile<G>& T, int k, int nr, const double* J, double* R, const double* a,
+                                     const int* idx, double* qfrc) {
+  int lane = T.lane();
+  for (int r = lane; r < nr; r += G) {
+    double* rr = R + R_STRIDE * r;
+    double v = dot_ref(J + r * k, 1, a, 1, k) - rr[R_AREF];
+    rr[R_JAR] = row_active(rr, v) ? -rr[R_D] * v : 0.0;
+    rr[R_ACT] = row_active(rr, v) ? 1.0 : 0.0;
+  }
+  T.sync();
+  for (int i = lane; i < k; i += G) {
+    int o = idx ? idx[i] : i;
+    double q = qfrc[o];
+    for (int r = 0; r < nr; r++) {
+      const double* rr = R + R_STRIDE * r;
+      if (rr[R_ACT] != 0.0) q += rr[R_JAR] * J[r * k + i];
+    }
+    qfrc[o] = q;
+  }
+  T.sync();
+}
+
+// newton.rs:378-473: islands over dof blocks, each a dense subproblem.
+template <int G>
+__device__ int newton_solve(const Tile<G>& T, const DModel& m, const WsLayout& w, const ScrLayout& s,
+                            const EnvCtx& e, int nr, double* a, const double* warm) {
+  int lane = T.lane(), nv = m.nv;
+  double* ws = e.ws;
+  double* qfrc = ws + w.qfrc_c;
+  for (int i = lane; i < nv; i += G) qfrc[i] = 0.0;
+  T.sync();
+  if (nr == 0) return 0;
+  double* J = e.scr + s.jac;
+  double* R = e.scr + s.rows;
+  for (int r = lane; r < nr; r += G) R[R_STRIDE * r + R_ACT] = -1.0;  // no previous active set
+  T.sync();
+  NewtonBufs B{ws + w.a0, ws + w.grad, ws + w.p, ws + w.tmp, ws + w.tmp2, ws + w.mp, ws + w.fac};
+  int max_iters = m.iterations;
+  double tol = m.tolerance;
+  if (m.nblock == 1) {
+    // one tree: the rows either touch it (one island spanning everything)
+    // or none has a nonzero entry (no island: nothing is solved)
+    bool nz = false;
+    for (int t = lane; t < nr * nv; t += G) nz |= J[t] != 0.0;
+    if (!T.any(nz)) return 0;
+    int it = newton_dense(T, nv, nr, J, R, ws + w.qm, a, warm, max_iters, tol, B);
+    add_constraint_force(T, nv, nr, J, R, a, (const int*)nullptr, qfrc);
+    return it;
+  }
+  // rows -> touched blocks (bit mask), then union-find on lane 0
+  int* iscr = (int*)(e.scr + s.isl_of_row);       // [maxrows] island of each row (-1 none)
+  int* blk_isl = (int*)(e.scr + s.isl_dof);       // [nblock] island id (min block of component)
+  unsigned long long* rmask = (unsigned long long*)(e.scr + s.isl_row);  // [maxrows]
+  for (int r = lane; r < nr; r += G) {
+    unsigned long long mk = 0;
+    for (int k = 0; k < nv; k++)
+      if (J[r * nv + k] != 0.0) mk |= 1ull << m.dof_block[k];
+    rmask[r] = mk;
+  }
+  T.sync();
+  if (lane == 0) {
+    int par[64];
+    for (int b = 0; b < m.nblock; b++) par[b] = b;
+    auto find = [&](int x) {
+      while (par[x] != x) {
+        par[x] = par[par[x]];
+        x = par[x];
+      }
+      return x;
+    };
+    for (int r = 0; r < nr; r++) {
+      unsigned long long mk = rmask[r];
+      if (!mk) continue;
+      int first = __ffsll((long long)mk) - 1;
+      mk &= mk - 1;
+      while (mk) {
+        int b = __ffsll((long long)mk) - 1;
+        mk &= mk - 1;
+        int x = find(first), y = find(b);
+        if (x != y) par[x > y ? x : y] = x < y ? x : y;
+      }
+    }
+    for (int b = 0; b < m.nblock; b++) blk_isl[b] = find(b);
+    for (int r = 0; r < nr; r++) iscr[r] = rmask[r] ? blk_isl[__ffsll((long long)rmask[r]) - 1] : -1;
+  }
+  T.sync();
+  // islands in increasing id order; single island spanning all blocks -> in place
+  int n_isl = 0, only = -1;
+  bool all_one = true;
+  for (int isl = 0; isl < m.nblock; isl++) {
+    bool has = false;
+    for (int r = lane; r < nr; r += G) has |= iscr[r] == isl;
+    if (T.any(has)) {
+      n_isl++;
+      only = isl;
+    }
+  }
+  for (int b = 0; b < m.nblock; b++) all_one &= blk_isl[b] == only;
+  if (n_isl == 1 && all_one) {
+    int it = newton_dense(T, nv, nr, J, R, ws + w.qm, a, warm, max_iters, tol, B);
+    add_constraint_force(T, nv, nr, J, R, a, (const int*)nullptr, qfrc);
+    return it;
+  }
+  int iters = 0;
+  double* subM = e.scr + s.sub_m;
+  double* subJ = e.scr + s.sub_j;
+  double* subR = e.scr + s.sub_rows;
+  int* idx = (int*)(e.scr + s.isl_row) + 2 * m.maxrows;  // after rmask words
+  double* suba = ws + w.vel;   // free until the solve returns
+  double* wsub = ws + w.warm;  // gathered warm start
+  for (int isl = 0; isl < m.nblock; isl++) {
+    bool has = false;
+    for (int r = lane; r < nr; r += G) has |= iscr[r] == isl;
+    if (!T.any(has)) continue;
+    // dofs of the island's blocks, in block order
+    int kk = 0;
+    for (int b = 0; b < m.nblock; b++) {
+      if (blk_isl[b] != isl) continue;
+      int s0 = m.block_adr[2 * b], s1 = m.block_adr[2 * b + 1];
+      for (int i = s0 + lane; i < s1; i += G) idx[kk + (i - s0)] = i;
+      kk += s1 - s0;
+    }
+    // rows of the island, in row order
+    int nri = 0;
+    for (int base = 0; base < nr; base += G) {
+      int r = base + lane;
+      bool in = r < nr && iscr[r] == isl;
+      int tot;
+      int off = T.excl_scan(in ? 1 : 0, &tot);
+      if (in) idx[nv + nri + off] = r;
+      nri += tot;
+    }
+    T.sync();
+    for (int t = lane; t < kk * kk; t += G) subM[t] = ws[w.qm + idx[t / kk] * nv + idx[t % kk]];
+    for (int t = lane; t < nri * kk; t += G) subJ[t] = J[idx[nv + t / kk] * nv + idx[t % kk]];
+    for (int t = lane; t < nri * R_STRIDE; t += G) subR[t] = R[R_STRIDE * idx[nv + t / R_STRIDE] + t % R_STRIDE];
+    for (int i = lane; i < kk; i += G) {
+      suba[i] = a[idx[i]];
+      wsub[i] = warm ? warm[idx[i]] : 0.0;
+    }
+    T.sync();
+    int it = newton_dense(T, kk, nri, subJ, subR, subM, suba, warm ? wsub : nullptr, max_iters, tol, B);
+    iters = it > iters ? it : iters;
+    for (int i = lane; i < kk; i += G) a[idx[i]] = suba[i];
+    T.sync();
+    add_constraint_force(T, kk, nri, subJ, subR, suba, idx, qfrc);
+  }
+  return iters;
+}
+
+// forward.rs:407-431,392-401: factor M + h D per dof block into ws fac
+template <int G>
+__device__ bool factor_mass(const Tile<G>& T, const DModel& m, const WsLayout& w, const EnvCtx& e, double h) {
+  int lane = T.lane(), nv = m.nv;
+  double* ws = e.ws;
+  double* F = ws + w.fac;
+  const double* qm = ws + w.qm;
+  for (int t = lane; t < nv * nv; t += G) F[t] = qm[t];
+  T.sync();
+  for (int k = lane; k < nv; k += G) F[k * nv + k] += h * e.prm[m.p_damping + k];
+  T.sync();
+  if (m.integrator == 1 && lane == 0) {  // implicitfast actuator terms (rare path)
+    for (int u = 0; u < m.nu; u++) {
+      double kv = -e.prm[m.p_bias + 3 * u + 2] * m.act_gear[u] * m.act_gear[u];
+      if (kv == 0.0 || ws[w.actclamped + u] != 0.0) continue;
+      int a0 = m.act_moment_adr[u], an = m.act_moment_num[u];
+      for (int x = 0; x < an; x++)
+        for (int y = 0; y < an; y++) {
+          int da = m.jnt_dofadr[m.moment_jnt[a0 + x]], db = m.jnt_dofadr[m.moment_jnt[a0 + y]];
+          bool rel = da == db;
+          for (int q = m.dof_parent[db]; q != -1 && !rel; q = m.dof_parent[q]) rel = q == da;
+          for (int q = m.dof_parent[da]; q != -1 && !rel; q = m.dof_parent[q]) rel = q == db;
+          if (rel) F[da * nv + db] += h * kv * m.moment_coef[a0 + x] * m.moment_coef[a0 + y];
+        }
+    }
+  }
+  T.sync();
+  int maxbs = 0;
+  for (int b = 0; b < m.nblock; b++) {
+    int sz = m.block_adr[2 * b + 1] - m.block_adr[2 * b];
+    maxbs = sz > maxbs ? sz : maxbs;
+  }
+  return chol_blocks(T, F, nv, nv, m.nblock, m.block_adr, m.dof_block, maxbs);
+}
+
+// forward.rs:454-456
+__device__ inline bool has_implicit_terms(const DModel& m, const double* prm) {
+  for (int k = 0; k < m.nv; k++)
+    if (prm[m.p_damping + k] != 0.0) return true;
+  if (m.integrator == 1)
+    for (int u = 0; u < m.nu; u++)
+      if (prm[m.p_bias + 3 * u + 2] != 0.0) return true;
+  return false;
+}
+
+// forward.rs:459-480
+template <int G>
+__device__ void integrate_pos(const Tile<G>& T, const DModel& m, double* qpos, const double* v, double h) {
+  for (int j = T.lane(); j < m.njnt; j += G) {
+    int qa = m.jnt_qposadr[j], da = m.jnt_dofadr[j];
+    int type = m.jnt_type[j];
+    if (type == JNT_FREE) {
+      for (int k = 0; k < 3; k++) qpos[qa + k] += h * v[da + k];
+      Q4 q = q_integrate_local(ld4(qpos + qa + 3), ld3(v + da + 3), h);
+      st4(qpos + qa + 3, q);
+    } else if (type == JNT_BALL) {
+      Q4 q = q_integrate_local(ld4(qpos + qa), ld3(v + da), h);
+      st4(qpos + qa, q);
+    } else {
+      qpos[qa] += h * v[da];
+    }
+  }
+  T.sync();
+}
+
+}  // namespace pg

@@ -1,0 +1,50 @@
+// A tile of G lanes (G = 8, 16 or 32) that cooperates on one environment.
+// Reductions are butterfly (xor) all-reduces, so every lane ends with the
+// bit-identical value and control flow that depends on it stays uniform.
+#pragma once
+#include <cooperative_groups.h>
+
+namespace pg {
+namespace cg = cooperative_groups;
+
+template <int G>
+struct Tile {
+  cg::thread_block_tile<G> t;
+  __device__ explicit Tile(cg::thread_block_tile<G> tt) : t(tt) {}
+  __device__ int lane() const { return (int)t.thread_rank(); }
+  __device__ void sync() const { t.sync(); }
+  template <class T>
+  __device__ T bcast(T v, int src) const {
+    return t.shfl(v, src);
+  }
+  __device__ double sum(double v) const {
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) v += t.shfl_xor(v, o);
+    return v;
+  }
+  __device__ int isum(int v) const {
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) v += t.shfl_xor(v, o);
+    return v;
+  }
+  __device__ int ior(int v) const {
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) v |= t.shfl_xor(v, o);
+    return v;
+  }
+  __device__ bool all(bool b) const { return t.all(b ? 1 : 0) != 0; }
+  __device__ bool any(bool b) const { return t.any(b ? 1 : 0) != 0; }
+  // exclusive prefix sum over lanes; *total gets the sum over the tile
+  __device__ int excl_scan(int v, int* total) const {
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < G; o <<= 1) {
+      int y = t.shfl_up(x, o);
+      if (lane() >= o) x += y;
+    }
+    *total = t.shfl(x, G - 1);
+    return x - v;
+  }
+};
+
+}  // namespace pg

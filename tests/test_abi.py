@@ -1,0 +1,50 @@
+"""The C-ABI library loads and exports every function include/pippin_b200.h
+declares; the Python bindings cover the same set. No GPU needed (nothing
+here calls into CUDA)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from pippin_b200 import _native
+
+INCLUDE = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include")
+
+
+def declared_functions():
+    names = set()
+    for h in sorted(os.listdir(INCLUDE)):
+        if h.endswith(".h"):
+            text = re.sub(r"/\*.*?\*/", "", open(os.path.join(INCLUDE, h)).read(), flags=re.S)
+            names |= set(re.findall(r"^[a-z_][\w\s\*]*?\b(pg_\w+)\s*\(", text, flags=re.M))
+    return sorted(names)
+
+
+def test_header_declares_the_api():
+    names = declared_functions()
+    for must in ["pg_create", "pg_destroy", "pg_step", "pg_reset", "pg_get", "pg_set", "pg_poses", "pg_set_param",
+                 "pg_get_param", "pg_appearance", "pg_scene_geoms", "pg_last_error", "pg_stats"]:
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol():
+    from pippin_b200 import build
+    build.build()
+    lib = ctypes.CDLL(_native.LIB_PATH)
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_bindings_match_header():
+    bound = {name for name, _, _ in _native.SIGNATURES}
+    assert bound == set(declared_functions())
+
+
+def test_missing_library_fails_loudly(tmp_path):
+    with pytest.raises(_native.NativeLibraryError):
+        _native._lib = None
+        try:
+            _native.load(str(tmp_path / "nope.so"))
+        finally:
+            _native._lib = None

@@ -1,0 +1,300 @@
+"""CUDA backend vs the oracle (C++ restatement of the reference CPU engine).
+
+Tolerances (relative to the quantity's scale, max(|ref|_inf, 1)):
+  M(q), c(q, qdot)                 1e-12
+  contact pos / normal / depth     1e-12 (same count, pairs and order)
+  per-step qacc, qvel, qpos        1e-10 (identical input states each step)
+  contact-free 1 s trajectories    1e-8
+"""
+import numpy as np
+import pytest
+
+from oracle.oracle import CTRL, QACC, QPOS, QVEL, Oracle
+from pippin_b200 import CudaPhysics, Field, Param, PhysicsError, mjcf, scenes
+from tests import scenarios as S
+
+pytestmark = pytest.mark.gpu
+
+TOL_MC = 1e-12
+TOL_STEP = 1e-10
+TOL_TRAJ = 1e-8
+
+
+def rel(a, b):
+    a, b = np.asarray(a, float), np.asarray(b, float)
+    if a.size == 0:
+        return 0.0
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1.0))
+
+
+def random_state(m, n, rng, qnoise=0.1, vscale=0.1):
+    q = np.tile(np.array(m.qpos0), (n, 1)) + rng.uniform(-qnoise, qnoise, (n, m.nq))
+    v = rng.normal(0, vscale, (n, m.nv))
+    return q, v
+
+
+def pair(xml, n, tolerance=None):
+    m = mjcf.load_string(xml)
+    blob = mjcf.to_blob(m)
+    g = CudaPhysics(blob, n)
+    o = Oracle(blob, n, threads=4)
+    if tolerance is not None:
+        g.set_solver(tolerance=tolerance)
+        o.set_solver(tolerance=tolerance)
+    return m, g, o
+
+
+MODELS = {
+    "ant": scenes.ant_xml,
+    "cartpole": scenes.cartpole_xml,
+    "arm3d": scenes.arm3d_xml,
+    "arm3hinge": scenes.arm3hinge_xml,
+    "box_drop": scenes.box_drop_xml,
+    "shapes_on_box": lambda: S.ON_BOX,
+    "box_stack": lambda: S.box_stack_xml(),
+}
+
+
+@pytest.mark.parametrize("name", list(MODELS))
+def test_forward_parity(name):
+    """M, bias forces and contact sets on random states (forward.rs:263-271)."""
+    n = 32
+    m, g, o = pair(MODELS[name](), n)
+    rng = np.random.default_rng(1)
+    q, v = random_state(m, n, rng, qnoise=0.3, vscale=1.0)
+    for sim in (g, o):
+        sim.set(QPOS if sim is o else Field.QPOS, q) if sim is o else sim.set(Field.QPOS, range(n), q)
+    o.set(QVEL, v)
+    g.set(Field.QVEL, range(n), v)
+    o.forward()
+    for e in range(n):
+        dg = g.debug_forward(e)
+        do = o.debug(e)
+        assert rel(dg["qm"], do["qm"]) < TOL_MC, (e, rel(dg["qm"], do["qm"]))
+        assert rel(dg["qfrc_bias"], do["qfrc_bias"]) < TOL_MC, e
+        assert dg["ncon"] == do["ncon"], (e, dg["ncon"], do["ncon"])
+        if do["ncon"]:
+            cg, co = dg["contacts"], do["contacts"]
+            np.testing.assert_array_equal(cg[:, 10:13], co[:, 10:13])
+            assert rel(cg[:, :10], co[:, :10]) < TOL_MC, e
+
+
+def _copy_state(src_g, dst_o, n):
+    for fg, fo in ((Field.QPOS, QPOS), (Field.QVEL, QVEL), (Field.QACC, QACC), (Field.CTRL, CTRL)):
+        dst_o.set(fo, src_g.get(fg, range(n)))
+
+
+def test_ant_step_parity_on_identical_states():
+    """Per-step Newton output on identical input states (config 1 setup,
+    tolerance 1e-10), through falls, ground contact and joint limits."""
+    n, T = 64, 120
+    m, g, o = pair(scenes.ant_xml(), n, tolerance=1e-10)
+    rng = np.random.default_rng(0)
+    q, v = random_state(m, n, rng)
+    g.set(Field.QPOS, range(n), q)
+    g.set(Field.QVEL, range(n), v)
+    worst = {"qacc": 0.0, "qvel": 0.0, "qpos": 0.0}
+    contacts_seen = 0
+    for t in range(T):
+        g.set(Field.CTRL, range(n), rng.uniform(-1, 1, (n, m.nu)))
+        _copy_state(g, o, n)
+        g.step(range(n), 1)
+        o.step(0, n, 1)
+        sg, so = g.stats(), o.stats()
+        np.testing.assert_array_equal(sg["ncon"], so["ncon"])
+        np.testing.assert_array_equal(sg["nrows"], so["nrows"])
+        assert not sg["status"].any()
+        contacts_seen += int(so["ncon"].sum())
+        for fg, fo, key in ((Field.QACC, QACC, "qacc"), (Field.QVEL, QVEL, "qvel"), (Field.QPOS, QPOS, "qpos")):
+            a, b = g.get(fg, range(n)), o.get(fo)
+            for e in range(n):
+                worst[key] = max(worst[key], rel(a[e], b[e]))
+    assert contacts_seen > 0
+    assert worst["qacc"] < TOL_STEP, worst
+    assert worst["qvel"] < TOL_STEP, worst
+    assert worst["qpos"] < TOL_STEP, worst
+
+
+@pytest.mark.parametrize("name", ["cartpole", "arm3d", "arm3hinge"])
+def test_contact_free_trajectories(name):
+    """Config 2: random states, per-env masses x U[0.5, 2], 1 s of motion."""
+    n = 64
+    m, g, o = pair(MODELS[name](), n)
+    rng = np.random.default_rng(2)
+    q = np.tile(np.array(m.qpos0), (n, 1))
+    for j in range(m.njnt):
+        qa = m.jnt_qposadr[j]
+        if m.jnt_type[j] == mjcf.JNT_HINGE:
+            q[:, qa] = rng.uniform(-np.pi, np.pi, n)
+        elif m.jnt_type[j] == mjcf.JNT_SLIDE:
+            q[:, qa] = rng.uniform(-0.5, 0.5, n)
+        elif m.jnt_type[j] == mjcf.JNT_BALL:
+            w = rng.normal(size=(n, 4))
+            q[:, qa:qa + 4] = w / np.linalg.norm(w, axis=1, keepdims=True)
+    v = rng.normal(0, 1, (n, m.nv))
+    for b in range(1, m.nbody):
+        scale = rng.uniform(0.5, 2.0, n)
+        vals = (np.array(m.body_mass[b]) * scale).reshape(n, 1)
+        g.set_param(Param.BODY_MASS, b, range(n), vals)
+        o.set_param(5, b, vals)
+    for e in range(0, n, 7):
+        bg, dg = g.invweight(e)
+        bo, do = o.invweight(e)
+        assert rel(bg, bo) < TOL_MC and rel(dg, do) < TOL_MC
+    g.set(Field.QPOS, range(n), q)
+    g.set(Field.QVEL, range(n), v)
+    o.set(QPOS, q)
+    o.set(QVEL, v)
+    steps = int(round(1.0 / m.timestep))
+    ctrl = rng.uniform(-1, 1, (n, steps, max(m.nu, 0)))
+    og = g.rollout(ctrl)
+    oo = o.rollout(ctrl)
+    assert rel(og[:, -1], oo[:, -1]) < TOL_TRAJ, rel(og[:, -1], oo[:, -1])
+
+
+def test_set_const_matches_oracle():
+    n = 8
+    m, g, o = pair(scenes.ant_xml(), n)
+    for e in range(n):
+        bg, dg = g.invweight(e)
+        bo, do = o.invweight(e)
+        assert rel(bg, bo) < TOL_MC and rel(dg, do) < TOL_MC
+    g.set_param(Param.BODY_IPOS, 2, range(2, 5), np.full((3, 3), 0.01))
+    o.set_param(10, 2, np.full((3, 3), 0.01), 2, 5)
+    g.set_param(Param.BODY_INERTIA, 3, range(1, 3), [[0.1, 0.2, 0.3], [0.2, 0.2, 0.2]])
+    o.set_param(9, 3, [[0.1, 0.2, 0.3], [0.2, 0.2, 0.2]], 1, 3)
+    for e in range(n):
+        bg, dg = g.invweight(e)
+        bo, do = o.invweight(e)
+        assert rel(bg, bo) < TOL_MC and rel(dg, do) < TOL_MC, e
+
+
+@pytest.mark.parametrize("check", S.CONTACT_CHECKS, ids=lambda f: f.__name__)
+def test_contact_behaviour_newton(check):
+    check(S.CudaSim, S.NEWTON)
+
+
+@pytest.mark.parametrize("check", S.PARAM_CHECKS, ids=lambda f: f.__name__)
+def test_param_behaviour(check):
+    check(S.CudaSim)
+
+
+def test_invalid_params_rejected():
+    S.check_invalid_params_rejected(S.CudaSim, PhysicsError)
+
+
+def test_poses_and_appearance_match_oracle():
+    n = 16
+    m, g, o = pair(scenes.ant_xml(), n)
+    rng = np.random.default_rng(3)
+    q, v = random_state(m, n, rng)
+    g.set(Field.QPOS, range(n), q)
+    g.set(Field.QVEL, range(n), v)
+    o.set(QPOS, q)
+    o.set(QVEL, v)
+    g.step(range(n), 5)
+    o.step(0, n, 5)
+    gg, gc = g.poses(range(n))
+    og, oc = o.poses()
+    np.testing.assert_allclose(gg, og, rtol=0, atol=1e-6)
+    g.set_param(Param.GEOM_SIZE, 1, range(0, 2), [[0.3, 0, 0], [0.2, 0, 0]])
+    o.set_param(1, 1, [[0.3, 0, 0], [0.2, 0, 0]], 0, 2)
+    np.testing.assert_array_equal(g.appearance(range(n)), o.appearance())
+
+
+def test_reset_keeps_qacc_and_restores_state():
+    n = 4
+    m, g, o = pair(scenes.ant_xml(), n)
+    g.set(Field.CTRL, range(n), np.ones((n, m.nu)))
+    g.step(range(n), 30)
+    qacc = g.get(Field.QACC, range(n))
+    g.set_param(Param.QPOS0, 0, range(1, 2), [np.array(m.qpos0) + 0.01])
+    g.reset([1, 3])
+    q = g.get(Field.QPOS, range(n))
+    np.testing.assert_array_equal(q[1], np.array(m.qpos0) + 0.01)
+    np.testing.assert_array_equal(q[3], np.array(m.qpos0))
+    assert not g.get(Field.QVEL, range(n))[[1, 3]].any()
+    assert not g.get(Field.CTRL, range(n))[[1, 3]].any()
+    np.testing.assert_array_equal(g.get(Field.QACC, range(n)), qacc)
+
+
+def test_subranges_step_like_the_whole():
+    """Stepping halves separately equals stepping all envs (the async
+    pipeline steps groups, backends_agree.rs:12-14)."""
+    n = 32
+    m = mjcf.load_string(scenes.ant_xml())
+    blob = mjcf.to_blob(m)
+    a, b = CudaPhysics(blob, n), CudaPhysics(blob, n)
+    rng = np.random.default_rng(4)
+    q, v = random_state(m, n, rng)
+    for p in (a, b):
+        p.set(Field.QPOS, range(n), q)
+        p.set(Field.QVEL, range(n), v)
+    a.step(range(n), 40)
+    b.step(range(0, 13), 40)
+    b.step(range(13, n), 40)
+    np.testing.assert_array_equal(a.get(Field.QPOS, range(n)), b.get(Field.QPOS, range(n)))
+
+
+def test_rollout_matches_step_loop():
+    n, t = 8, 30
+    m = mjcf.load_string(scenes.ant_xml())
+    blob = mjcf.to_blob(m)
+    a, b = CudaPhysics(blob, n), CudaPhysics(blob, n)
+    ctrl = np.sin(np.arange(n * t * m.nu) * 0.37).reshape(n, t, m.nu)
+    out = a.rollout(ctrl)
+    for k in range(t):
+        b.set(Field.CTRL, range(n), ctrl[:, k])
+        b.step(range(n), 1)
+    np.testing.assert_array_equal(out[:, -1], b.get(Field.QPOS, range(n)))
+
+
+def test_errors_are_reported():
+    g = CudaPhysics(scenes.ant_xml(), 4)
+    with pytest.raises(PhysicsError):
+        g.step(range(2, 9), 1)
+    with pytest.raises(PhysicsError):
+        g.get(Field.QPOS, range(4), out=np.zeros((4, 3)))
+    with pytest.raises(PhysicsError):
+        g.set(Field.CTRL, range(4), np.zeros(5))
+    with pytest.raises(PhysicsError):
+        g.reset([7])
+    with pytest.raises(PhysicsError):
+        CudaPhysics(b"not a model blob", 1)
+    g.step(range(2, 2), 5)  # empty range is a no-op
+    assert g.name() == "pippin-cuda"
+    sc = g.scene()
+    assert len(sc.geoms) == 14 and sc.geoms[0].name == "floor"
+
+
+def test_zero_envs():
+    g = CudaPhysics(scenes.ant_xml(), 0)
+    g.step(range(0, 0), 3)
+    assert g.get(Field.QPOS, range(0, 0)).shape == (0, 15)
+
+
+def test_full_size_ant_properties():
+    """Config 1 at full size (4096 envs x 200 steps, tol 1e-10): finite
+    state, no status flags, unit free-joint quaternions, contacts present,
+    and per-step parity on a sample of envs at the last step."""
+    n, T = 4096, 200
+    m, g, o = pair(scenes.ant_xml(), n, tolerance=1e-10)
+    rng = np.random.default_rng(5)
+    q, v = random_state(m, n, rng)
+    g.set(Field.QPOS, range(n), q)
+    g.set(Field.QVEL, range(n), v)
+    ctrl = rng.uniform(-1, 1, (n, T, m.nu))
+    traj = g.rollout(ctrl)
+    assert np.isfinite(traj).all()
+    st = g.stats()
+    assert not st["status"].any()
+    quat = traj[:, -1, 3:7]
+    np.testing.assert_allclose(np.linalg.norm(quat, axis=1), 1.0, atol=1e-12)
+    sample = rng.choice(n, 64, replace=False)
+    og = Oracle(mjcf.compile_string(scenes.ant_xml()), 64, threads=4)
+    og.set_solver(tolerance=1e-10)
+    for fg, fo in ((Field.QPOS, QPOS), (Field.QVEL, QVEL), (Field.QACC, QACC), (Field.CTRL, CTRL)):
+        og.set(fo, g.get(fg, range(n))[sample])
+    g.step(range(n), 1)
+    og.step(0, 64, 1)
+    assert rel(g.get(Field.QACC, range(n))[sample], og.get(QACC)) < TOL_STEP
