@@ -266,14 +266,17 @@ __device__ inline void capsule_box(const GPose& a, const GPose& b, double margin
   for (int i = 0; i < nt; i++) sphere_box(p0 + d * ts[i], r, b, margin, out);
 }
 
-// collision.rs:496-511: Sutherland-Hodgman against pn.p <= off
+// collision.rs:496-511: Sutherland-Hodgman against pn.p <= off. A convex
+// polygon gains at most one vertex per clip; `cap` bounds the output even
+// if rounding produced more sign changes than that.
+constexpr int CLIP_CAP = 16;
 __device__ inline int clip_poly(const V3* in, int n, V3 pn, double off, V3* out) {
   int k = 0;
   for (int i = 0; i < n; i++) {
     V3 a = in[i], b = in[(i + 1) % n];
     double da = dot(pn, a) - off, db = dot(pn, b) - off;
-    if (da <= 0.0) out[k++] = a;
-    if ((da < 0.0) != (db < 0.0) && fabs(da - db) > 1e-15) out[k++] = a + (b - a) * (da / (da - db));
+    if (da <= 0.0 && k < CLIP_CAP) out[k++] = a;
+    if ((da < 0.0) != (db < 0.0) && fabs(da - db) > 1e-15 && k < CLIP_CAP) out[k++] = a + (b - a) * (da / (da - db));
   }
   return k;
 }
@@ -406,7 +409,7 @@ __device__ inline void box_box(const GPose& a, const GPose& b, double margin, Hi
   V3 ic = inc.pos + iaxes[j] * (s * comp(inc.size, j));
   int ku = (j + 1) % 3, kv = (j + 2) % 3;
   V3 eu = iaxes[ku] * comp(inc.size, ku), ev = iaxes[kv] * comp(inc.size, kv);
-  V3 bufa[16], bufb[16];
+  V3 bufa[CLIP_CAP], bufb[CLIP_CAP];
   bufa[0] = ic + eu + ev;
   bufa[1] = ic - eu + ev;
   bufa[2] = ic - eu - ev;
@@ -427,7 +430,7 @@ __device__ inline void box_box(const GPose& a, const GPose& b, double margin, Hi
       if (np == 0) return;
     }
   }
-  DP pts[16];
+  DP pts[CLIP_CAP];
   int k2 = 0;
   for (int i = 0; i < np; i++) {
     double sep = dot(cur[i] - ref_center, nref);
