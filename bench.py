@@ -36,11 +36,14 @@ ITERS = 30
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--envs", type=int, default=4096, help="envs per GPU")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shape")
+    ap.add_argument("--lanes", type=int, default=0, help="force lanes per env (8, 16, 32)")
+    ap.add_argument("--per-block", type=int, default=0, help="force envs per block")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     return ap.parse_args()
 
@@ -218,9 +221,13 @@ def run_ours(args):
     q, v, rng = initial_state(m, n, 1000 + rank)
     phys.set(Field.QPOS, range(n), q)
     phys.set(Field.QVEL, range(n), v)
-    phys.autotune(nstep=1)
-    # restore the start state the autotuner trialled from (it restores itself)
+    if args.lanes or args.per_block:
+        phys.set_launch(args.lanes, args.per_block)
+    elif not args.no_autotune:
+        phys.autotune(nstep=1)  # trial steps run on a saved copy of the state
     lanes, per_block, blocks = phys.launch()
+    clocks = ClockSampler(local)
+    clocks.start()
 
     K, W = args.steps, args.warmup
     ctrl_all = torch.from_numpy(rng.uniform(-1, 1, (W + K, n, m.nu))).to(dev)
@@ -252,10 +259,7 @@ def run_ours(args):
         barrier()
         return total_ms
 
-    clocks = ClockSampler(local)
-    clocks.start()
     ms_ref = timed_device_loop(ctrl_all, K, WarmStart.REF_PREV_QACC)
-    clock_info = clocks.stop()
     st = phys.stats()
     # cold-start Newton on the same trajectory distribution (fresh state)
     phys.set(Field.QPOS, range(n), q)
@@ -290,6 +294,7 @@ def run_ours(args):
         e1.synchronize()
         e2e_ms += e0.elapsed_time(e1)
     barrier()
+    clock_info = clocks.stop()
 
     times = torch.tensor([ms_ref, ms_cold, e2e_ms], dtype=torch.float64, device=dev)
     if ws > 1:

@@ -409,6 +409,10 @@ void clear_graphs(Handle* h) {
   h->graphs.clear();
 }
 
+// largest arena staged into shared memory (bigger models read it from L1/L2)
+constexpr int STAGE_LIMIT = 48 * 1024;
+std::vector<int> dmodel_pointer_fields();
+
 StepArgs make_args(Handle* h) {
   StepArgs a{};
   a.m = h->dm;
@@ -429,6 +433,10 @@ StepArgs make_args(Handle* h) {
   a.scratch = h->scratch;
   a.queue = h->queue;
   a.warm_mode = h->warm_mode;
+  a.stage_model = h->dm.arena_bytes <= STAGE_LIMIT ? 1 : 0;
+  std::vector<int> po = dmodel_pointer_fields();
+  a.n_ptr = (int)std::min<size_t>(po.size(), MAX_PTR_FIELDS);
+  for (int k = 0; k < a.n_ptr; k++) a.ptr_off[k] = po[k];
   return a;
 }
 
@@ -441,33 +449,37 @@ void layouts(const HostModel& m, int maxcon, int maxrows, WsLayout* w, ScrLayout
     return o;
   };
   int nb = m.nbody, nv = m.nv, ng = m.ngeom, nu = m.nu;
+  // live for the whole substep
   w->qpos = take(m.nq);
   w->qvel = take(nv);
   w->ctrl = take(nu);
   w->qacc = take(nv);
   w->applied = take(nv);
+  w->qm = take(nv * nv);
+  w->cdof = take(6 * nv);
+  w->smooth = take(nv);
+  w->qfrc_c = take(nv);
+  w->acc = take(nv);
+  w->rinv = take(nv);
+  w->actforce = take(nu);
+  w->actclamped = take(nu);
+  w->misc = take(8);
+  int region = off;
+  // tree walks and passive/actuator forces
   w->xpos = take(3 * nb);
   w->xquat = take(4 * nb);
   w->xmat = take(9 * nb);
-  w->xipos = take(3 * nb);
   w->cinert = take(13 * nb);
-  w->crb = take(13 * nb);
   w->cvel = take(6 * nb);
   w->cacc = take(6 * nb);
   w->cfrc = take(6 * nb);
-  w->cdof = take(6 * nv);
-  w->cdof_dot = take(6 * nv);
-  w->gxpos = take(3 * ng);
-  w->gxmat = take(9 * ng);
-  w->gaabb = take(6 * ng);
-  w->qm = take(nv * nv);
-  w->fac = take(nv * nv);
   w->bias = take(nv);
   w->passive = take(nv);
   w->actf = take(nv);
-  w->smooth = take(nv);
-  w->acc = take(nv);
-  w->qfrc_c = take(nv);
+  int tree_end = off;
+  // factorisations and Newton reuse the same region
+  off = region;
+  w->fac = take(nv * nv);
   w->a0 = take(nv);
   w->grad = take(nv);
   w->p = take(nv);
@@ -476,16 +488,15 @@ void layouts(const HostModel& m, int maxcon, int maxrows, WsLayout* w, ScrLayout
   w->mp = take(nv);
   w->vel = take(nv);
   w->warm = take(nv);
-  w->actforce = take(nu);
-  w->actclamped = take(nu);
-  w->misc = take(8);
-  w->stride = off;
+  w->stride = std::max(off, tree_end);
 
   off = 0;
   int rhs = nv + 6 * nb + 32;  // set_const right-hand sides + per-lane row copies
+  s->geoms = take(ng * G_STRIDE);
   s->contacts = take(maxcon * C_STRIDE);
   s->jac = take(std::max(maxrows * nv, rhs * nv));
   s->rows = take(std::max(maxrows * R_STRIDE, rhs));
+  s->chol = take(nv * nv);
   int multi = m.dof_blocks.size() / 2 > 1;
   s->sub_m = take(multi ? nv * nv : 0);
   s->sub_j = take(multi ? maxrows * nv : 0);
@@ -493,14 +504,36 @@ void layouts(const HostModel& m, int maxcon, int maxrows, WsLayout* w, ScrLayout
   s->isl_dof = take(nv + 2);
   s->isl_row = take(maxrows + (nv + maxrows + 1) / 2 + 2);
   s->isl_of_row = take(maxrows / 2 + 2);
-  s->minv_jt = take(0);
-  s->lambda = take(0);
   s->stride = off;
+}
+
+// Model staging: the byte offset of every pointer field of DModel (the
+// kernels rebase them onto the block's shared copy of the arena).
+std::vector<int> dmodel_pointer_fields() {
+  std::vector<int> o;
+#define PF(f) o.push_back((int)offsetof(DModel, f))
+  PF(body_parent); PF(body_jntadr); PF(body_jntnum); PF(body_dofadr); PF(body_dofnum); PF(body_lastdof);
+  PF(body_dofmask); PF(body_pos); PF(body_quat); PF(level_adr); PF(level_body); PF(child_adr); PF(child_list);
+  PF(jnt_type); PF(jnt_qposadr); PF(jnt_dofadr); PF(jnt_limited); PF(jnt_pos); PF(jnt_axis); PF(jnt_range);
+  PF(jnt_stiffness); PF(jnt_springref); PF(dof_body); PF(dof_parent); PF(dof_armature); PF(dof_block);
+  PF(block_adr); PF(dofact_adr); PF(dofact_u); PF(dofact_coef); PF(geom_type); PF(geom_body); PF(geom_dataid);
+  PF(geom_pos); PF(geom_quat); PF(pair_g); PF(cam_body); PF(cam_pos); PF(cam_quat); PF(act_gear);
+  PF(act_ctrllimited); PF(act_ctrlrange); PF(act_forcelimited); PF(act_forcerange); PF(act_moment_adr);
+  PF(act_moment_num); PF(moment_jnt); PF(moment_coef); PF(eq_j1); PF(eq_j2); PF(eq_poly); PF(eq_solref);
+  PF(eq_solimp); PF(qpos0); PF(hull_vadr); PF(hull_vnum); PF(hull_vert); PF(hull_fadr); PF(hull_fnum);
+  PF(hull_face);
+#undef PF
+  return o;
+}
+
+size_t block_smem_bytes(const Handle* h, const LaunchCfg& c) {
+  size_t staged = h->dm.arena_bytes <= STAGE_LIMIT ? (size_t)staged_model_bytes(h->dm.arena_bytes) : 0;
+  return staged + (size_t)c.tiles_per_block * h->w.stride * sizeof(double);
 }
 
 int choose_grid(Handle* h, const LaunchCfg& want, LaunchCfg* out) {
   LaunchCfg c = want;
-  size_t smem = (size_t)c.tiles_per_block * h->w.stride * sizeof(double);
+  size_t smem = block_smem_bytes(h, c);
   if (smem > h->smem_optin) return fail(PG_ERR_INVALID, "launch shape needs more shared memory than a block has");
   int threads = c.tiles_per_block * c.G;
   if (threads > 256 || threads < 32) return fail(PG_ERR_INVALID, "launch shape: 32..256 threads per block");
@@ -811,6 +844,8 @@ int build_device_model(Handle* h) {
   d.nmesh = m.nmesh;
   d.maxcon = maxcon;
   d.maxrows = maxrows;
+  d.maxbs = 0;
+  for (int b = 0; b < nblock; b++) d.maxbs = std::max(d.maxbs, m.dof_blocks[2 * b + 1] - m.dof_blocks[2 * b]);
   d.timestep = m.timestep;
   for (int k = 0; k < 3; k++) d.gravity[k] = m.gravity[k];
   d.integrator = m.integrator;
@@ -896,9 +931,12 @@ int build_device_model(Handle* h) {
   ADDD(hull_face, hull_face);
 #undef ADDI
 #undef ADDD
+  ar.host.resize((ar.host.size() + 15) & ~size_t(15));  // staged in 16-byte chunks
   CK(cudaMalloc(&h->d_model, ar.host.size()));
   CK(cudaMemcpy(h->d_model, ar.host.data(), ar.host.size(), cudaMemcpyHostToDevice));
   for (auto& f : fix) *f.slot = (const uint8_t*)h->d_model + f.off;
+  d.arena = (const unsigned char*)h->d_model;
+  d.arena_bytes = (int)ar.host.size();
 
   // per-env parameter block
   int off = 0;

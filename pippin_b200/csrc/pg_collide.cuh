@@ -110,7 +110,9 @@ __device__ inline void sort_dp(DP* a, int n) {
 }
 
 // collision.rs:214-236
-__device__ inline void plane_box(const GPose& pl, const GPose& b, double margin, Hits& out) {
+// The larger routines below stay out of line: one copy each keeps the
+// step kernel's hot path small enough for the instruction cache.
+__device__ __noinline__ void plane_box(const GPose& pl, const GPose& b, double margin, Hits& out) {
   V3 n = col(pl.mat, 2);
   DP hits[8];
   int k = 0;
@@ -125,7 +127,7 @@ __device__ inline void plane_box(const GPose& pl, const GPose& b, double margin,
 }
 
 // collision.rs:238-267
-__device__ inline void plane_cylinder(const GPose& pl, const GPose& c, double margin, Hits& out) {
+__device__ __noinline__ void plane_cylinder(const GPose& pl, const GPose& c, double margin, Hits& out) {
   V3 n = col(pl.mat, 2);
   V3 axis = col(c.mat, 2);
   double r = c.size.x, h = c.size.y;
@@ -169,7 +171,7 @@ __device__ inline void sphere_sphere(V3 c1, double r1, V3 c2, double r2, double 
 }
 
 // collision.rs:282-316 (normal from sphere to box)
-__device__ inline void sphere_box(V3 c, double r, const GPose& b, double margin, Hits& out) {
+__device__ __noinline__ void sphere_box(V3 c, double r, const GPose& b, double margin, Hits& out) {
   V3 local = mtv(b.mat, c - b.pos);
   V3 h = b.size;
   V3 cl{clampd(local.x, -h.x, h.x), clampd(local.y, -h.y, h.y), clampd(local.z, -h.z, h.z)};
@@ -203,7 +205,7 @@ __device__ inline void sphere_box(V3 c, double r, const GPose& b, double margin,
 }
 
 // collision.rs:318-335
-__device__ inline void capsule_capsule(const GPose& a, const GPose& b, double margin, Hits& out) {
+__device__ __noinline__ void capsule_capsule(const GPose& a, const GPose& b, double margin, Hits& out) {
   V3 p0, p1, q0, q1;
   segment(a, &p0, &p1);
   segment(b, &q0, &q1);
@@ -231,7 +233,7 @@ __device__ inline double box_sdf(const GPose& b, V3 p) {
 }
 
 // collision.rs:346-380: golden-section minimum of the box SDF along the segment
-__device__ inline void capsule_box(const GPose& a, const GPose& b, double margin, Hits& out) {
+__device__ __noinline__ void capsule_box(const GPose& a, const GPose& b, double margin, Hits& out) {
   V3 p0, p1;
   segment(a, &p0, &p1);
   double r = a.size.x;
@@ -329,7 +331,7 @@ __device__ inline int reduce_to_four(DP* pts, int n) {
 }
 
 // collision.rs:383-493: separating axes, face clipping or edge-edge point
-__device__ inline void box_box(const GPose& a, const GPose& b, double margin, Hits& out) {
+__device__ __noinline__ void box_box(const GPose& a, const GPose& b, double margin, Hits& out) {
   V3 d = b.pos - a.pos;
   V3 ax[3] = {col(a.mat, 0), col(a.mat, 1), col(a.mat, 2)};
   V3 bx[3] = {col(b.mat, 0), col(b.mat, 1), col(b.mat, 2)};
@@ -447,7 +449,7 @@ __device__ inline bool needs_general(int a, int b) {
 }
 
 // collision.rs:59-96: order by type, flip the normals of a swapped call
-__device__ inline void collide_primitive(const GPose& a0, const GPose& b0, double margin, Hits& out) {
+__device__ __noinline__ void collide_primitive(const GPose& a0, const GPose& b0, double margin, Hits& out) {
   bool swap = a0.type > b0.type;
   const GPose& a = swap ? b0 : a0;
   const GPose& b = swap ? a0 : b0;

@@ -2,16 +2,19 @@
 // per-tile workspace layout of the batched substep.
 //
 // HBM layout (all FP64 unless noted):
-//   model constants   one copy, read through L1 by every tile
+//   model arena       one copy of the model constants; each block stages it
+//                     into its shared memory when it fits (model_bytes)
 //   env parameters    [env][pstride]: the per-env copy of every parameter
 //                     the reference can change per environment
 //                     (crates/pippin/src/params.rs:10-39) plus derived
 //                     invweight0 (forward.rs:275-333)
 //   env state         qpos[env][nq], qvel[env][nv], ctrl[env][nu],
 //                     qacc[env][nv] (Newton warm start), qfrc_applied[env][nv]
-//   tile scratch      [tile][sstride]: contacts, constraint rows and island
-//                     buffers of the env a tile is working on
-//   shared memory     [tile][wstride]: kinematics, inertia, M and its factor
+//   tile scratch      [tile][sstride]: geom poses, contacts, constraint rows
+//                     and island buffers of the env a tile is working on
+//   shared memory     per block: staged model, then [tile][wstride]
+//                     workspaces (state, M, cdof, and one region used first
+//                     by the tree walks, then by the factorisations/Newton)
 #pragma once
 #include <cstdint>
 
@@ -30,13 +33,15 @@ enum { C_POS = 0, C_NORMAL = 3, C_TANGENT = 6, C_DEPTH = 9, C_G1 = 10, C_G2 = 11
        C_T2 = 16, C_ROW = 19, C_STRIDE = 20 };
 // constraint row record in tile scratch (doubles)
 enum { R_AREF = 0, R_D = 1, R_JAR = 2, R_JP = 3, R_POS = 4, R_DIAG = 5, R_FLAGS = 6, R_ACT = 7, R_STRIDE = 8 };
+// geom record in tile scratch (doubles): world pose and world bounding box
+enum { G_POS = 0, G_MAT = 3, G_AABB = 12, G_STRIDE = 18 };
 
 constexpr int NV_MAX = 64;  // dof-chain masks are 64-bit
 
 struct DModel {
   // ---- dims
   int nq, nv, nu, nbody, njnt, ngeom, ncam, neq, npair, nblock, nlevel, nmesh;
-  int maxcon, maxrows;
+  int maxcon, maxrows, maxbs;
   // ---- options (model.rs:60-100)
   double timestep, gravity[3];
   int integrator, solver, iterations;
@@ -116,34 +121,38 @@ struct DModel {
   int p_friction, p_size, p_contype, p_conaff, p_mass, p_inertia, p_ipos, p_damping, p_gain, p_bias, p_qpos_reset,
       p_body_invw, p_dof_invw, p_rgba;
   int pstride;
+
+  // ---- the arena all pointers above point into
+  const unsigned char* arena;
+  int arena_bytes;
 };
 
-// Per-tile shared-memory workspace (offsets in doubles).
+// Per-tile shared-memory workspace (offsets in doubles). The `tree` region
+// (poses, inertias, velocities, forces) is dead once the contacts are built
+// and is reused by the factorisations and Newton (`fac` .. `warm`).
 struct WsLayout {
-  int qpos, qvel, ctrl, qacc, applied;
-  int xpos, xquat, xmat, xipos, cinert, crb, cvel, cacc, cfrc;
-  int cdof, cdof_dot;
-  int gxpos, gxmat, gaabb;
-  int qm, fac;
-  int bias, passive, actf, smooth, acc, qfrc_c, a0, grad, p, tmp, tmp2, mp, vel, warm;
-  int actforce, actclamped;
-  int misc;  // small scalars
+  // live for the whole substep
+  int qpos, qvel, ctrl, qacc, applied, qm, cdof, smooth, qfrc_c, acc, rinv, actforce, actclamped, misc;
+  // tree walks, passive/actuator forces
+  int xpos, xquat, xmat, cinert, cvel, cacc, cfrc, bias, passive, actf;
+  // factorisations and Newton (alias the tree region)
+  int fac, a0, grad, p, tmp, tmp2, mp, vel, warm;
   int stride;
 };
 
 // Per-tile global scratch layout (offsets in doubles).
 struct ScrLayout {
+  int geoms;     // ngeom * G_STRIDE
   int contacts;  // maxcon * C_STRIDE
   int jac;       // maxrows * nv
   int rows;      // maxrows * R_STRIDE
+  int chol;      // nv * nv   (set_const factor)
   int sub_m;     // nv * nv   (island gather)
   int sub_j;     // maxrows * nv
   int sub_rows;  // maxrows * R_STRIDE
   int isl_dof;   // nv ints stored as doubles
   int isl_row;   // maxrows
   int isl_of_row;
-  int minv_jt;   // PGS: maxrows * nv
-  int lambda;    // PGS: maxrows
   int stride;
 };
 
@@ -159,22 +168,37 @@ struct EnvState {
   int32_t* nrows;
   int32_t* status;
   // PGS warm start carried between steps (solver.rs:254-289)
-  double* prev_con;   // [env][maxcon][C_PREV]
+  double* prev_con;  // [env][maxcon][P_STRIDE]
   int32_t* prev_ncon;
 };
 enum { P_POS = 0, P_NORMAL = 3, P_TANGENT = 6, P_G1 = 9, P_G2 = 10, P_LAMBDA = 11, P_STRIDE = 14 };
+
+constexpr int MAX_PTR_FIELDS = 80;
 
 struct StepArgs {
   DModel m;
   WsLayout w;
   ScrLayout s;
   EnvState st;
-  double* scratch;        // [tiles][s.stride]
-  int* queue;             // work counter (reset to 0 before each launch)
+  double* scratch;   // [tiles][s.stride]
+  int* queue;        // work counter (reset to 0 before each launch)
   int start, count, nstep;
   int warm_mode;
   const double* ctrl_seq;  // optional (count, nstep, nu): per-substep controls
   double* qpos_out;        // optional (count, nstep, nq): qpos after each substep
+  // model staging: byte offsets of the pointer fields of DModel, and
+  // whether the arena is copied into shared memory
+  int stage_model;
+  int n_ptr;
+  int ptr_off[MAX_PTR_FIELDS];
 };
+
+// shared bytes a block reserves for the staged model (DModel copy + arena)
+#ifdef __CUDACC__
+__host__ __device__
+#endif
+inline int staged_model_bytes(int arena_bytes) {
+  return ((int)sizeof(DModel) + 15) / 16 * 16 + (arena_bytes + 15) / 16 * 16;
+}
 
 }  // namespace pg

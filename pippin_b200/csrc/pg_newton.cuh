@@ -13,56 +13,14 @@
 namespace pg {
 
 // ---------------------------------------------------------------- collide
-// Local bounding box of a geom (model.rs:365-382) from the per-env size.
-__device__ inline void local_aabb(const DModel& m, const double* prm, int g, V3* c, V3* h) {
-  V3 s = ld3(prm + m.p_size + 3 * g);
-  *c = V3{0, 0, 0};
-  switch (m.geom_type[g]) {
-    case GEOM_PLANE: *h = V3{INFINITY, INFINITY, INFINITY}; break;
-    case GEOM_SPHERE: *h = V3{s.x, s.x, s.x}; break;
-    case GEOM_CAPSULE: *h = V3{s.x, s.x, s.x + s.y}; break;
-    case GEOM_BOX: *h = s; break;
-    case GEOM_CYLINDER: *h = V3{s.x, s.x, s.y}; break;
-    default: {  // mesh: bounds of the hull vertices
-      int id = m.geom_dataid[g];
-      V3 lo{INFINITY, INFINITY, INFINITY}, hi{-INFINITY, -INFINITY, -INFINITY};
-      for (int k = 0; k < m.hull_vnum[id]; k++) {
-        V3 v = ld3(m.hull_vert + 3 * (m.hull_vadr[id] + k));
-        lo = V3{fmin(lo.x, v.x), fmin(lo.y, v.y), fmin(lo.z, v.z)};
-        hi = vmax(hi, v);
-      }
-      *c = (lo + hi) * 0.5;
-      *h = (hi - lo) * 0.5;
-    }
-  }
-}
-
 // Returns the contact count; contacts land in scratch in pair order (and
 // hit order within a pair), as in the reference's sequential pair loop.
 template <int G>
 __device__ int collide(const Tile<G>& T, const DModel& m, const WsLayout& w, const ScrLayout& s, const EnvCtx& e,
                        int* status) {
   int lane = T.lane();
-  double* ws = e.ws;
   const double* prm = e.prm;
-  double* gaabb = ws + w.gaabb;
-  for (int g = lane; g < m.ngeom; g += G) {
-    V3 c, h;
-    local_aabb(m, prm, g, &c, &h);
-    if (!isfinite(h.x)) {
-      st3(gaabb + 6 * g, V3{0, 0, 0});
-      st3(gaabb + 6 * g + 3, h);
-      continue;
-    }
-    M3 r = ld9(ws + w.gxmat + 9 * g);
-    V3 center = ld3(ws + w.gxpos + 3 * g) + mv(r, c);
-    V3 half{fabs(r.m[0]) * h.x + fabs(r.m[1]) * h.y + fabs(r.m[2]) * h.z,
-            fabs(r.m[3]) * h.x + fabs(r.m[4]) * h.y + fabs(r.m[5]) * h.z,
-            fabs(r.m[6]) * h.x + fabs(r.m[7]) * h.y + fabs(r.m[8]) * h.z};
-    st3(gaabb + 6 * g, center);
-    st3(gaabb + 6 * g + 3, half);
-  }
-  T.sync();
+  const double* gr = e.scr + s.geoms;  // poses and boxes from the tree walk
   double* con = e.scr + s.contacts;
   int ncon = 0;
   int st = 0;
@@ -78,13 +36,15 @@ __device__ int collide(const Tile<G>& T, const DModel& m, const WsLayout& w, con
       unsigned t2 = (unsigned)prm[m.p_contype + g2], a2 = (unsigned)prm[m.p_conaff + g2];
       bool masks = (t1 & a2) != 0 || (t2 & a1) != 0;
       if (masks) {
-        V3 c1 = ld3(gaabb + 6 * g1), h1 = ld3(gaabb + 6 * g1 + 3);
-        V3 c2 = ld3(gaabb + 6 * g2), h2 = ld3(gaabb + 6 * g2 + 3);
+        const double* r1 = gr + G_STRIDE * g1;
+        const double* r2 = gr + G_STRIDE * g2;
+        V3 c1 = ld3(r1 + G_AABB), h1 = ld3(r1 + G_AABB + 3);
+        V3 c2 = ld3(r2 + G_AABB), h2 = ld3(r2 + G_AABB + 3);
         bool sep = fabs(c1.x - c2.x) > h1.x + h2.x + m.margin || fabs(c1.y - c2.y) > h1.y + h2.y + m.margin ||
                    fabs(c1.z - c2.z) > h1.z + h2.z + m.margin;
         if (!sep) {
-          GPose a{m.geom_type[g1], ld3(ws + w.gxpos + 3 * g1), ld9(ws + w.gxmat + 9 * g1), ld3(prm + m.p_size + 3 * g1)};
-          GPose b{m.geom_type[g2], ld3(ws + w.gxpos + 3 * g2), ld9(ws + w.gxmat + 9 * g2), ld3(prm + m.p_size + 3 * g2)};
+          GPose a{m.geom_type[g1], ld3(r1 + G_POS), ld9(r1 + G_MAT), ld3(prm + m.p_size + 3 * g1)};
+          GPose b{m.geom_type[g2], ld3(r2 + G_POS), ld9(r2 + G_MAT), ld3(prm + m.p_size + 3 * g2)};
           if (needs_general(a.type, b.type)) st |= ST_UNSUPPORTED_PAIR;
           else collide_primitive(a, b, m.margin, hits);
         }
@@ -302,7 +262,7 @@ __device__ int build_rows(const Tile<G>& T, const DModel& m, const WsLayout& w, 
 
 // ---------------------------------------------------------------- dense Newton
 struct NewtonBufs {
-  double *a0, *grad, *p, *tmp, *tmp2, *mp, *hess;
+  double *a0, *grad, *p, *tmp, *tmp2, *mp, *hess, *rinv;
 };
 
 __device__ inline bool row_active(const double* rr, double v) { return rr[R_FLAGS] != 0.0 || v < 0.0; }
@@ -339,7 +299,8 @@ __device__ double cost(const Tile<G>& T, int k, int nr, const double* J, double*
 // newton.rs:224-358: `a` holds the unconstrained acceleration on entry and
 // the constrained one on exit. Returns the iteration count.
 template <int G>
-__device__ int newton_dense(const Tile<G>& T, int k, int nr, const double* J, double* R, const double* M, double* a,
+__device__ __noinline__ int newton_dense(const Tile<G>& T, int k, int nr, const double* J, double* R, const double* M,
+                                         double* a,
                             const double* warm, int max_iters, double tol, const NewtonBufs& B) {
   int lane = T.lane();
   double *a0 = B.a0, *grad = B.grad, *p = B.p, *tmp = B.tmp, *tmp2 = B.tmp2, *mp = B.mp, *H = B.hess;
@@ -405,10 +366,10 @@ __device__ int newton_dense(const Tile<G>& T, int k, int nr, const double* J, do
       H[i * k + j] = h;
     }
     T.sync();
-    if (!chol_blocks(T, H, k, k, 1, nullptr, nullptr, k)) break;
+    if (!chol_blocks(T, H, k, k, 1, nullptr, nullptr, k, B.rinv)) break;
     for (int i = lane; i < k; i += G) p[i] = -grad[i];
     T.sync();
-    solve_blocks(T, H, k, k, 1, nullptr, p);
+    solve_blocks(T, H, k, k, 1, nullptr, nullptr, k, B.rinv, p);
     // exact line search on the piecewise quadratic along p
     mul_m(T, M, k, p, mp);
     double s1 = 0.0, s2 = 0.0;
@@ -462,7 +423,7 @@ __device__ int newton_dense(const Tile<G>& T, int k, int nr, const double* J, do
 
 // newton.rs:361-371: qfrc[idx[i]] += -J' D (J a - aref) over active rows
 template <int G>
-__device__ void add_constraint_force(const Tile<G>& T, int k, int nr, const double* J, double* R, const double* a,
+__device__ __noinline__ void add_constraint_force(const Tile<G>& T, int k, int nr, const double* J, double* R, const double* a,
                                      const int* idx, double* qfrc) {
   int lane = T.lane();
   for (int r = lane; r < nr; r += G) {
@@ -484,33 +445,20 @@ __device__ void add_constraint_force(const Tile<G>& T, int k, int nr, const doub
   T.sync();
 }
 
-// newton.rs:378-473: islands over dof blocks, each a dense subproblem.
+// newton.rs:391-473 for models with several dof blocks: islands are the
+// blocks joined by rows touching more than one; each is solved as its own
+// dense subproblem (in place when one island spans every block).
 template <int G>
-__device__ int newton_solve(const Tile<G>& T, const DModel& m, const WsLayout& w, const ScrLayout& s,
-                            const EnvCtx& e, int nr, double* a, const double* warm) {
+__device__ __noinline__ int newton_islands(const Tile<G>& T, const DModel& m, const WsLayout& w, const ScrLayout& s,
+                                           const EnvCtx& e, int nr, double* a, const double* warm,
+                                           const NewtonBufs& B) {
   int lane = T.lane(), nv = m.nv;
   double* ws = e.ws;
   double* qfrc = ws + w.qfrc_c;
-  for (int i = lane; i < nv; i += G) qfrc[i] = 0.0;
-  T.sync();
-  if (nr == 0) return 0;
   double* J = e.scr + s.jac;
   double* R = e.scr + s.rows;
-  for (int r = lane; r < nr; r += G) R[R_STRIDE * r + R_ACT] = -1.0;  // no previous active set
-  T.sync();
-  NewtonBufs B{ws + w.a0, ws + w.grad, ws + w.p, ws + w.tmp, ws + w.tmp2, ws + w.mp, ws + w.fac};
   int max_iters = m.iterations;
   double tol = m.tolerance;
-  if (m.nblock == 1) {
-    // one tree: the rows either touch it (one island spanning everything)
-    // or none has a nonzero entry (no island: nothing is solved)
-    bool nz = false;
-    for (int t = lane; t < nr * nv; t += G) nz |= J[t] != 0.0;
-    if (!T.any(nz)) return 0;
-    int it = newton_dense(T, nv, nr, J, R, ws + w.qm, a, warm, max_iters, tol, B);
-    add_constraint_force(T, nv, nr, J, R, a, (const int*)nullptr, qfrc);
-    return it;
-  }
   // rows -> touched blocks (bit mask), then union-find on lane 0
   int* iscr = (int*)(e.scr + s.isl_of_row);       // [maxrows] island of each row (-1 none)
   int* blk_isl = (int*)(e.scr + s.isl_dof);       // [nblock] island id (min block of component)
@@ -612,6 +560,32 @@ __device__ int newton_solve(const Tile<G>& T, const DModel& m, const WsLayout& w
   return iters;
 }
 
+// newton.rs:378-473
+template <int G>
+__device__ int newton_solve(const Tile<G>& T, const DModel& m, const WsLayout& w, const ScrLayout& s,
+                            const EnvCtx& e, int nr, double* a, const double* warm) {
+  int lane = T.lane(), nv = m.nv;
+  double* ws = e.ws;
+  double* qfrc = ws + w.qfrc_c;
+  for (int i = lane; i < nv; i += G) qfrc[i] = 0.0;
+  T.sync();
+  if (nr == 0) return 0;
+  double* J = e.scr + s.jac;
+  double* R = e.scr + s.rows;
+  for (int r = lane; r < nr; r += G) R[R_STRIDE * r + R_ACT] = -1.0;  // no previous active set
+  T.sync();
+  NewtonBufs B{ws + w.a0, ws + w.grad, ws + w.p, ws + w.tmp, ws + w.tmp2, ws + w.mp, ws + w.fac, ws + w.rinv};
+  if (m.nblock > 1) return newton_islands(T, m, w, s, e, nr, a, warm, B);
+  // one tree: the rows either touch it (one island spanning everything)
+  // or none has a nonzero entry (no island: nothing is solved)
+  bool nz = false;
+  for (int t = lane; t < nr * nv; t += G) nz |= J[t] != 0.0;
+  if (!T.any(nz)) return 0;
+  int it = newton_dense(T, nv, nr, J, R, ws + w.qm, a, warm, m.iterations, m.tolerance, B);
+  add_constraint_force(T, nv, nr, J, R, a, (const int*)nullptr, qfrc);
+  return it;
+}
+
 // forward.rs:407-431,392-401: factor M + h D per dof block into ws fac
 template <int G>
 __device__ bool factor_mass(const Tile<G>& T, const DModel& m, const WsLayout& w, const EnvCtx& e, double h) {
@@ -639,12 +613,7 @@ __device__ bool factor_mass(const Tile<G>& T, const DModel& m, const WsLayout& w
     }
   }
   T.sync();
-  int maxbs = 0;
-  for (int b = 0; b < m.nblock; b++) {
-    int sz = m.block_adr[2 * b + 1] - m.block_adr[2 * b];
-    maxbs = sz > maxbs ? sz : maxbs;
-  }
-  return chol_blocks(T, F, nv, nv, m.nblock, m.block_adr, m.dof_block, maxbs);
+  return chol_blocks(T, F, nv, nv, m.nblock, m.block_adr, m.dof_block, m.maxbs, ws + w.rinv);
 }
 
 // forward.rs:454-456
