@@ -134,6 +134,18 @@ int pg_step(pg_handle* h, int64_t start, int64_t end, int64_t nstep);
  * FP64 on the handle's device, read in stream order on pg_stream. */
 int pg_step_device(pg_handle* h, int64_t start, int64_t end, int64_t nstep, const double* ctrl_dev);
 
+/* pg_step without allocating: no counterpart in the reference. For callers
+ * that cannot have a call allocate device memory (another component owns the
+ * GPU's memory, a latency-critical loop must stay out of the allocator, or
+ * memory is already exhausted). Scratch comes from a fixed 16 MiB array in
+ * the library's device image, one per GPU that loads the library, held until
+ * exit; as many envs step at once as fit in it, the rest follow in the same
+ * launch. A model whose per-block scratch exceeds the array is rejected with
+ * PG_ERR_UNSUPPORTED. The first call on a device looks the array up (make it
+ * before any stream capture). All calls share the array and keep its last
+ * contents: calls that overlap on the GPU race. Stream-ordered like pg_step. */
+int pg_step_static(pg_handle* h, int64_t start, int64_t end, int64_t nstep);
+
 /* Batch::rollout (crates/pippin/src/batch.rs:46-59): ctrl is
  * (end-start, nstep, nu), qpos_out (end-start, nstep, nq) or NULL. Host
  * buffers; returns when qpos_out is filled. */

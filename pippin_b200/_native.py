@@ -36,6 +36,7 @@ SIGNATURES = [
     ("pg_dims", _i32, [_vp, C.POINTER(PgModelDims)]),
     ("pg_step", _i32, [_vp, _i64, _i64, _i64]),
     ("pg_step_device", _i32, [_vp, _i64, _i64, _i64, _vp]),
+    ("pg_step_static", _i32, [_vp, _i64, _i64, _i64]),
     ("pg_rollout", _i32, [_vp, _i64, _i64, _i64, _pd, _pd]),
     ("pg_reset", _i32, [_vp, _pi64, _i64]),
     ("pg_get", _i32, [_vp, _i32, _i64, _i64, _pd, _sz]),

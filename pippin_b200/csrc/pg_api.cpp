@@ -1014,6 +1014,28 @@ int read_params(Handle* h, int64_t start, int64_t end, std::vector<double>& out)
 
 }  // namespace
 
+namespace pg {
+// Launch arguments of pg_step for [start, end), for entry points that launch
+// the step kernel with other scratch (pg_noalloc.cu). Validates like pg_step.
+int internal_step_args(pg_handle* h, int64_t start, int64_t end, int64_t nstep, StepArgs* a, LaunchCfg* cfg,
+                       cudaStream_t* stream, int* device) {
+  if (!h) return fail(PG_ERR_INVALID, "NULL handle");
+  int rc = check_range(h, start, end);
+  if (rc) return rc;
+  if (nstep < 0 || nstep > (1 << 30)) return fail(PG_ERR_INVALID, "nstep out of range");
+  CK(cudaSetDevice(h->device));
+  *a = make_args(h);
+  a->start = (int)start;
+  a->count = (int)(end - start);
+  a->nstep = (int)nstep;
+  *cfg = h->cfg;
+  *stream = h->stream;
+  *device = h->device;
+  return PG_OK;
+}
+void internal_set_error(const std::string& msg) { g_err = msg; }
+}  // namespace pg
+
 extern "C" {
 
 const char* pg_last_error(void) { return g_err.c_str(); }

@@ -1,0 +1,101 @@
+// pg_step_static: stepping that allocates nothing.
+//
+// pg_step draws its per-tile scratch (contacts, constraint rows, island
+// buffers) from a buffer the handle cudaMalloc'd. Some callers cannot let a
+// call allocate device memory: code running while another component owns
+// the device memory (a caching allocator that has reserved it all, or a
+// fixed memory budget), latency-critical control loops that must not enter
+// the allocator, and callers that have already run out of memory and still
+// need to advance the simulation. For them this entry point takes its
+// scratch from a fixed array in the library's device image instead.
+//
+// The array is PG_STATIC_SCRATCH_BYTES (16 MiB) per GPU that loads the
+// library, held until the process exits. A call steps as many envs at once
+// as fit in it (16 MiB / per-tile scratch) and loops over the rest, so it is
+// slower than pg_step on large batches; a model whose per-tile scratch alone
+// exceeds the array is rejected. All calls share the array and keep its last
+// contents: calls whose work overlaps on the GPU (two handles or two streams
+// stepping at the same time on one device) race on it.
+#include <cuda_runtime.h>
+
+#include <mutex>
+#include <string>
+
+#include "../../include/pippin_b200.h"
+#include "pg_kernels.h"
+#include "pg_model.h"
+
+namespace pg {
+// fills the launch arguments of pg_step for [start, end) (pg_api.cpp)
+int internal_step_args(pg_handle* h, int64_t start, int64_t end, int64_t nstep, StepArgs* a, LaunchCfg* cfg,
+                       cudaStream_t* stream, int* device);
+void internal_set_error(const std::string& msg);
+}  // namespace pg
+
+namespace {
+
+constexpr size_t PG_STATIC_SCRATCH_BYTES = size_t(16) << 20;
+constexpr size_t PG_STATIC_COUNTER_BYTES = 256;  // work counter, then tile scratch
+
+// Device-side scratch shared by every pg_step_static call on a device. Host
+// code must not use this name as an address: its device address comes from
+// cudaGetSymbolAddress below.
+static __device__ __align__(256) unsigned char g_static_scratch[PG_STATIC_SCRATCH_BYTES];
+
+constexpr int MAX_DEVICES = 64;
+std::mutex g_setup_mu;
+unsigned char* g_scratch_ptr[MAX_DEVICES] = {nullptr};
+
+// Once per device, with that device current: the array's device address.
+int scratch_address(int device, unsigned char** out) {
+  if (device < 0 || device >= MAX_DEVICES) return PG_ERR_INVALID;
+  std::lock_guard<std::mutex> g(g_setup_mu);
+  if (!g_scratch_ptr[device]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+    if (e != cudaSuccess) {
+      pg::internal_set_error(std::string("cudaGetSymbolAddress(static scratch): ") + cudaGetErrorString(e));
+      return PG_ERR_CUDA;
+    }
+    g_scratch_ptr[device] = static_cast<unsigned char*>(p);
+  }
+  *out = g_scratch_ptr[device];
+  return PG_OK;
+}
+
+}  // namespace
+
+extern "C" int pg_step_static(pg_handle* h, int64_t start, int64_t end, int64_t nstep) {
+  pg::StepArgs a;
+  pg::LaunchCfg cfg;
+  cudaStream_t stream;
+  int device = 0;
+  int rc = pg::internal_step_args(h, start, end, nstep, &a, &cfg, &stream, &device);
+  if (rc != PG_OK) return rc;
+  if (end == start || nstep == 0) return PG_OK;
+  unsigned char* base = nullptr;
+  if ((rc = scratch_address(device, &base)) != PG_OK) return rc;
+  size_t tile_bytes = (size_t)a.s.stride * sizeof(double);
+  size_t tiles = (PG_STATIC_SCRATCH_BYTES - PG_STATIC_COUNTER_BYTES) / tile_bytes;
+  if (tiles < (size_t)cfg.tiles_per_block) {
+    pg::internal_set_error("pg_step_static: this model needs " + std::to_string(tile_bytes * cfg.tiles_per_block) +
+                           " bytes of scratch per block, more than the " +
+                           std::to_string(PG_STATIC_SCRATCH_BYTES - PG_STATIC_COUNTER_BYTES) +
+                           "-byte static scratch holds (use pg_step)");
+    return PG_ERR_UNSUPPORTED;
+  }
+  int blocks = (int)std::min<size_t>((size_t)cfg.blocks, tiles / cfg.tiles_per_block);
+  int64_t need = ((end - start) + cfg.tiles_per_block - 1) / cfg.tiles_per_block;
+  if (need < blocks) blocks = (int)need;
+  cfg.blocks = blocks;
+  a.queue = reinterpret_cast<int*>(base);
+  a.scratch = reinterpret_cast<double*>(base + PG_STATIC_COUNTER_BYTES);
+  // the counter keeps the previous call's value: it must start at zero
+  cudaError_t e = cudaMemsetAsync(a.queue, 0, sizeof(int), stream);
+  if (e == cudaSuccess) e = pg::launch_step(a, cfg, stream);
+  if (e != cudaSuccess) {
+    pg::internal_set_error(std::string("pg_step_static: ") + cudaGetErrorString(e));
+    return PG_ERR_CUDA;
+  }
+  return PG_OK;
+}
