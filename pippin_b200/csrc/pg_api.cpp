@@ -357,8 +357,9 @@ struct DevArena {
 struct Handle {
   HostModel hm;
   DModel dm{};
-  WsLayout w{};
+  WsLayout w{}, wn{};
   ScrLayout s{};
+  WorkLayout k{};
   int64_t n = 0;
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -367,10 +368,11 @@ struct Handle {
   int32_t *iters = nullptr, *ncon = nullptr, *nrows = nullptr, *status = nullptr;
   double* scratch = nullptr;
   size_t scratch_tiles = 0;
+  double* work = nullptr;  // [env][k.stride]
   int* queue = nullptr;
   std::vector<double> base_params;
   int warm_mode = WARM_REF_PREV_QACC;
-  LaunchCfg cfg{32, 4, 0};
+  SubstepCfg cfg{{16, 4, 0}, {32, 4, 0}, {16, 4, 0}};
   int sm_count = 0;
   size_t smem_optin = 0;
   // growable device buffers
@@ -417,7 +419,10 @@ StepArgs make_args(Handle* h) {
   StepArgs a{};
   a.m = h->dm;
   a.w = h->w;
+  a.wn = h->wn;
   a.s = h->s;
+  a.k = h->k;
+  a.work = h->work;
   a.st.qpos = h->qpos;
   a.st.qvel = h->qvel;
   a.st.ctrl = h->ctrl;
@@ -440,8 +445,9 @@ StepArgs make_args(Handle* h) {
   return a;
 }
 
-// workspace and scratch layouts from the model dims
-void layouts(const HostModel& m, int maxcon, int maxrows, WsLayout* w, ScrLayout* s) {
+// Workspace layouts of the smooth-dynamics phase (w) and the Newton phase
+// (wn), the Newton phase's tile scratch (s) and the per-env work record (k).
+void layouts(const HostModel& m, int maxcon, int maxrows, WsLayout* w, WsLayout* wn, ScrLayout* s, WorkLayout* k) {
   int off = 0;
   auto take = [&](int n) {
     int o = off;
@@ -449,23 +455,23 @@ void layouts(const HostModel& m, int maxcon, int maxrows, WsLayout* w, ScrLayout
     return o;
   };
   int nb = m.nbody, nv = m.nv, ng = m.ngeom, nu = m.nu;
-  // live for the whole substep
+  *w = WsLayout{};
+  std::fill_n(reinterpret_cast<int*>(w), sizeof(WsLayout) / sizeof(int), -1);
+  // smooth phase: live throughout
   w->qpos = take(m.nq);
   w->qvel = take(nv);
   w->ctrl = take(nu);
-  w->qacc = take(nv);
   w->applied = take(nv);
   w->qm = take(nv * nv);
   w->cdof = take(6 * nv);
   w->smooth = take(nv);
-  w->qfrc_c = take(nv);
   w->acc = take(nv);
   w->rinv = take(nv);
   w->actforce = take(nu);
   w->actclamped = take(nu);
   w->misc = take(8);
   int region = off;
-  // tree walks and passive/actuator forces
+  // tree walks and passive/actuator forces ...
   w->xpos = take(3 * nb);
   w->xquat = take(4 * nb);
   w->xmat = take(9 * nb);
@@ -477,23 +483,54 @@ void layouts(const HostModel& m, int maxcon, int maxrows, WsLayout* w, ScrLayout
   w->passive = take(nv);
   w->actf = take(nv);
   int tree_end = off;
-  // factorisations and Newton reuse the same region
+  // ... then the factorisations in the same region
   off = region;
   w->fac = take(nv * nv);
-  w->a0 = take(nv);
-  w->grad = take(nv);
-  w->p = take(nv);
-  w->tmp = take(nv);
-  w->tmp2 = take(nv);
-  w->mp = take(nv);
-  w->vel = take(nv);
-  w->warm = take(nv);
   w->stride = std::max(off, tree_end);
+
+  // Newton phase
+  off = 0;
+  *wn = WsLayout{};
+  std::fill_n(reinterpret_cast<int*>(wn), sizeof(WsLayout) / sizeof(int), -1);
+  wn->qpos = take(m.nq);
+  wn->qvel = take(nv);
+  wn->qacc = take(nv);
+  wn->qm = take(nv * nv);
+  wn->cdof = take(6 * nv);
+  wn->smooth = take(nv);
+  wn->acc = take(nv);
+  wn->qfrc_c = take(nv);
+  wn->rinv = take(nv);
+  wn->fac = take(nv * nv);
+  wn->a0 = take(nv);
+  wn->grad = take(nv);
+  wn->p = take(nv);
+  wn->tmp = take(nv);
+  wn->tmp2 = take(nv);
+  wn->mp = take(nv);
+  wn->vel = take(nv);
+  wn->warm = take(nv);
+  wn->misc = take(8);
+  wn->stride = off;
+
+  // per-env work record
+  off = 0;
+  k->qm = take(nv * nv);
+  k->cdof = take(6 * nv);
+  k->a0 = take(nv);
+  k->smooth = take(nv);
+  k->bias = take(nv);
+  k->lh = take(nv * nv);
+  k->rinvh = take(nv);
+  k->meta = take(K_META_SIZE);
+  k->geoms = take(ng * G_STRIDE);
+  k->contacts = take(maxcon * C_STRIDE);
+  k->stride = off;
 
   off = 0;
   int rhs = nv + 6 * nb + 32;  // set_const right-hand sides + per-lane row copies
-  s->geoms = take(ng * G_STRIDE);
-  s->contacts = take(maxcon * C_STRIDE);
+  s->geoms = -1;
+  s->contacts = -1;
   s->jac = take(std::max(maxrows * nv, rhs * nv));
   s->rows = take(std::max(maxrows * R_STRIDE, rhs));
   s->chol = take(nv * nv);
@@ -526,82 +563,90 @@ std::vector<int> dmodel_pointer_fields() {
   return o;
 }
 
-size_t block_smem_bytes(const Handle* h, const LaunchCfg& c) {
-  size_t staged = h->dm.arena_bytes <= STAGE_LIMIT ? (size_t)staged_model_bytes(h->dm.arena_bytes) : 0;
-  return staged + (size_t)c.tiles_per_block * h->w.stride * sizeof(double);
-}
-
-int choose_grid(Handle* h, const LaunchCfg& want, LaunchCfg* out) {
+// Resident grid of a launch shape for one phase. `phase` is K_SMOOTH (whose
+// shape set_const and poses share), K_COLLIDE or K_NEWTON.
+int choose_grid(Handle* h, int phase, const LaunchCfg& want, LaunchCfg* out) {
   LaunchCfg c = want;
-  size_t smem = block_smem_bytes(h, c);
-  if (smem > h->smem_optin) return fail(PG_ERR_INVALID, "launch shape needs more shared memory than a block has");
   int threads = c.tiles_per_block * c.G;
   if (threads > 256 || threads < 32) return fail(PG_ERR_INVALID, "launch shape: 32..256 threads per block");
+  StepArgs a = make_args(h);
+  std::vector<int> kinds = {phase};
+  if (phase == K_SMOOTH) kinds = {K_SMOOTH, K_SET_CONST, K_POSES};
   int per_sm = 0;
-  for (int k : {K_STEP, K_FORWARD, K_SET_CONST, K_POSES}) {
+  for (int k : kinds) {
+    size_t smem = kernel_smem(k, a, c.tiles_per_block);
+    if (smem > h->smem_optin) return fail(PG_ERR_INVALID, "launch shape needs more shared memory than a block has");
     const void* fn = tile_kernel(k, c.G);
     if (!fn) return fail(PG_ERR_INVALID, "lanes per env must be 8, 16 or 32");
     CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int nb = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, threads, smem));
-    if (k == K_STEP) per_sm = nb;
-    else if (nb == 0) return fail(PG_ERR_INVALID, "launch shape does not fit on an SM");
+    if (nb == 0) return fail(PG_ERR_INVALID, "launch shape does not fit on an SM");
+    if (k == phase) per_sm = nb;
   }
-  if (per_sm < 1) return fail(PG_ERR_INVALID, "launch shape does not fit on an SM");
   c.blocks = per_sm * h->sm_count;
   *out = c;
   return PG_OK;
 }
 
-int ensure_scratch(Handle* h, const LaunchCfg& c) {
-  size_t tiles = (size_t)c.blocks * c.tiles_per_block;
+// tile scratch for the Newton phase and set_const (which runs on the smooth shape)
+int ensure_scratch(Handle* h, const SubstepCfg& c) {
+  size_t tiles = std::max((size_t)c.newton.blocks * c.newton.tiles_per_block,
+                          (size_t)c.smooth.blocks * c.smooth.tiles_per_block);
   if (tiles <= h->scratch_tiles) return PG_OK;
   if (h->scratch) cudaFree(h->scratch);
   h->scratch = nullptr;
+  h->scratch_tiles = 0;
   CK(cudaMalloc(&h->scratch, tiles * h->s.stride * sizeof(double) + 64));
   h->scratch_tiles = tiles;
   return PG_OK;
 }
 
-int apply_cfg(Handle* h, const LaunchCfg& want) {
-  LaunchCfg c;
-  int rc = choose_grid(h, want, &c);
+int apply_cfg(Handle* h, const SubstepCfg& want) {
+  SubstepCfg c;
+  int rc = choose_grid(h, K_SMOOTH, want.smooth, &c.smooth);
+  if (!rc) rc = choose_grid(h, K_COLLIDE, want.collide, &c.collide);
+  if (!rc) rc = choose_grid(h, K_NEWTON, want.newton, &c.newton);
   if (rc) return rc;
-  rc = ensure_scratch(h, c);
-  if (rc) return rc;
+  if ((rc = ensure_scratch(h, c))) return rc;
   h->cfg = c;
   h->version++;
   return PG_OK;
 }
 
-LaunchCfg grid_for(Handle* h, int64_t count) {
-  LaunchCfg c = h->cfg;
+// no more blocks than the range needs
+LaunchCfg fit(LaunchCfg c, int64_t count) {
   int64_t need = (count + c.tiles_per_block - 1) / c.tiles_per_block;
   if (need < c.blocks) c.blocks = (int)std::max<int64_t>(need, 1);
   return c;
 }
-
-int run_tile_kernel(Handle* h, int which, StepArgs& a, int64_t count, const int* envs = nullptr, float* g = nullptr,
-                    float* cm = nullptr, double* dbg = nullptr, int dbg_stride = 0, int maxcon_out = 0) {
-  LaunchCfg c = grid_for(h, count);
-  CK(cudaMemsetAsync(h->queue, 0, sizeof(int), h->stream));
-  cudaError_t e = cudaSuccess;
-  switch (which) {
-    case K_STEP: e = launch_step(a, c, h->stream); break;
-    case K_FORWARD: e = launch_forward(a, c, dbg, dbg_stride, maxcon_out, h->stream); break;
-    case K_SET_CONST: e = launch_set_const(a, c, envs, (int)count, h->stream); break;
-    case K_POSES: e = launch_poses(a, c, g, cm, h->stream); break;
-  }
-  if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
-  return PG_OK;
+SubstepCfg fit(const SubstepCfg& c, int64_t count) {
+  return SubstepCfg{fit(c.smooth, count), fit(c.collide, count), fit(c.newton, count)};
 }
+
+int launch_status(cudaError_t e) { return e == cudaSuccess ? PG_OK : cuda_fail(e, "kernel launch"); }
 
 int set_const_range(Handle* h, int64_t start, int64_t end) {
   if (end <= start) return PG_OK;
   StepArgs a = make_args(h);
   a.start = (int)start;
   a.count = (int)(end - start);
-  return run_tile_kernel(h, K_SET_CONST, a, end - start);
+  return launch_status(launch_set_const(a, fit(h->cfg.smooth, end - start), nullptr, (int)(end - start), h->stream));
+}
+
+// One substep, or the graph-replayed sequence of `nstep` substeps, of envs
+// [start, end) on the handle's stream.
+int enqueue_substeps(Handle* h, StepArgs a, int64_t start, int64_t end, int64_t nstep) {
+  a.start = (int)start;
+  a.count = (int)(end - start);
+  a.nstep = (int)nstep;
+  SubstepCfg c = fit(h->cfg, end - start);
+  for (int64_t k = 0; k < nstep; k++) {
+    a.sidx = (int)k;
+    cudaError_t e = launch_substep(a, c, h->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "substep launch");
+  }
+  return PG_OK;
 }
 
 int check_range(Handle* h, int64_t start, int64_t end) {
@@ -981,7 +1026,7 @@ int build_device_model(Handle* h) {
     for (int k = 0; k < 3; k++) bp[d.p_bias + 3 * u + k] = m.act_bias[3 * u + k];
   }
   for (int k = 0; k < m.nq; k++) bp[d.p_qpos_reset + k] = m.qpos_reset[k];
-  layouts(m, maxcon, maxrows, &h->w, &h->s);
+  layouts(m, maxcon, maxrows, &h->w, &h->wn, &h->s, &h->k);
   return PG_OK;
 }
 
@@ -990,7 +1035,7 @@ void destroy(pg_handle* h) {
   cudaSetDevice(h->device);
   clear_graphs(h);
   void* ptrs[] = {h->d_model, h->qpos, h->qvel, h->ctrl, h->qacc, h->applied, h->params, h->iters, h->ncon,
-                  h->nrows, h->status, h->scratch, h->queue, h->b_ctrl.p, h->b_qout.p, h->b_poses_g.p,
+                  h->nrows, h->status, h->scratch, h->work, h->queue, h->b_ctrl.p, h->b_qout.p, h->b_poses_g.p,
                   h->b_poses_c.p, h->b_dbg.p, h->b_vals.p, h->b_ids.p};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -1017,7 +1062,7 @@ int read_params(Handle* h, int64_t start, int64_t end, std::vector<double>& out)
 namespace pg {
 // Launch arguments of pg_step for [start, end), for entry points that launch
 // the step kernel with other scratch (pg_noalloc.cu). Validates like pg_step.
-int internal_step_args(pg_handle* h, int64_t start, int64_t end, int64_t nstep, StepArgs* a, LaunchCfg* cfg,
+int internal_step_args(pg_handle* h, int64_t start, int64_t end, int64_t nstep, StepArgs* a, SubstepCfg* cfg,
                        cudaStream_t* stream, int* device) {
   if (!h) return fail(PG_ERR_INVALID, "NULL handle");
   int rc = check_range(h, start, end);
@@ -1028,7 +1073,7 @@ int internal_step_args(pg_handle* h, int64_t start, int64_t end, int64_t nstep, 
   a->start = (int)start;
   a->count = (int)(end - start);
   a->nstep = (int)nstep;
-  *cfg = h->cfg;
+  *cfg = fit(h->cfg, end - start);
   *stream = h->stream;
   *device = h->device;
   return PG_OK;
@@ -1075,6 +1120,8 @@ int pg_create(const void* blob, size_t bytes, int64_t n_envs, int device, pg_han
   CK(cudaMalloc(&h->nrows, sizeof(int32_t) * n));
   CK(cudaMalloc(&h->status, sizeof(int32_t) * n));
   CK(cudaMalloc(&h->queue, sizeof(int) * 4));
+  CK(cudaMalloc(&h->work, sizeof(double) * n * h->k.stride));
+  CK(cudaMemsetAsync(h->work, 0, sizeof(double) * n * h->k.stride, h->stream));
   CK(cudaMemsetAsync(h->qvel, 0, sizeof(double) * n * std::max(m.nv, 1), h->stream));
   CK(cudaMemsetAsync(h->ctrl, 0, sizeof(double) * n * std::max(m.nu, 1), h->stream));
   CK(cudaMemsetAsync(h->qacc, 0, sizeof(double) * n * std::max(m.nv, 1), h->stream));
@@ -1095,7 +1142,10 @@ int pg_create(const void* blob, size_t bytes, int64_t n_envs, int device, pg_han
     }
     CK(cudaStreamSynchronize(h->stream));
   }
-  LaunchCfg want{m.nv > 16 ? 32 : 16, 4, 0};
+  int g = m.nv > 16 ? 32 : 16;
+  int npair = (int)m.pairs.size() / 2;
+  int gc = npair > 16 ? 32 : (npair > 8 ? 16 : 8);
+  SubstepCfg want{{g, 4, 0}, {gc, 4, 0}, {g, 4, 0}};
   rc = apply_cfg(h.get(), want);
   if (rc) return rc;
   rc = set_const_range(h.get(), 0, n_envs);
@@ -1136,27 +1186,40 @@ int pg_step(pg_handle* h, int64_t start, int64_t end, int64_t nstep) {
     clear_graphs(h);
     h->graph_version = h->version;
   }
-  auto key = std::make_tuple(start, end, nstep);
-  auto it = h->graphs.find(key);
-  if (it == h->graphs.end()) {
-    if (h->graphs.size() >= 32) clear_graphs(h);
-    StepArgs a = make_args(h);
-    a.start = (int)start;
-    a.count = (int)(end - start);
-    a.nstep = (int)nstep;
-    cudaGraph_t g;
-    CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-    int rc2 = run_tile_kernel(h, K_STEP, a, end - start);
-    cudaError_t ce = cudaStreamEndCapture(h->stream, &g);
-    if (rc2) return rc2;
-    if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamEndCapture");
-    cudaGraphExec_t ex;
-    ce = cudaGraphInstantiate(&ex, g, 0);
-    cudaGraphDestroy(g);
-    if (ce != cudaSuccess) return cuda_fail(ce, "cudaGraphInstantiate");
-    it = h->graphs.emplace(key, ex).first;
+  // substeps are replayed from cached graphs of up to 16 substeps each; the
+  // first substep of the call (sidx 0) restarts the per-env status word
+  const int64_t CHUNK = 16;
+  for (int64_t done = 0; done < nstep;) {
+    int64_t c = std::min(CHUNK, nstep - done);
+    int64_t first = done == 0 ? 0 : 1;
+    auto key = std::make_tuple(start, end, c * 2 + first);
+    auto it = h->graphs.find(key);
+    if (it == h->graphs.end()) {
+      if (h->graphs.size() >= 32) clear_graphs(h);
+      StepArgs a = make_args(h);
+      a.start = (int)start;
+      a.count = (int)(end - start);
+      a.nstep = (int)c;
+      SubstepCfg cfg = fit(h->cfg, end - start);
+      cudaGraph_t g;
+      CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+      cudaError_t le = cudaSuccess;
+      for (int64_t k = 0; k < c && le == cudaSuccess; k++) {
+        a.sidx = (int)(first + k);
+        le = launch_substep(a, cfg, h->stream);
+      }
+      cudaError_t ce = cudaStreamEndCapture(h->stream, &g);
+      if (le != cudaSuccess) return cuda_fail(le, "substep launch");
+      if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamEndCapture");
+      cudaGraphExec_t ex;
+      ce = cudaGraphInstantiate(&ex, g, 0);
+      cudaGraphDestroy(g);
+      if (ce != cudaSuccess) return cuda_fail(ce, "cudaGraphInstantiate");
+      it = h->graphs.emplace(key, ex).first;
+    }
+    CK(cudaGraphLaunch(it->second, h->stream));
+    done += c;
   }
-  CK(cudaGraphLaunch(it->second, h->stream));
   return PG_OK;
 }
 
@@ -1193,7 +1256,7 @@ int pg_rollout(pg_handle* h, int64_t start, int64_t end, int64_t nstep, const do
   a.nstep = (int)nstep;
   a.ctrl_seq = m.nu ? (const double*)h->b_ctrl.p : nullptr;
   a.qpos_out = qpos_out ? (double*)h->b_qout.p : nullptr;
-  if ((rc = run_tile_kernel(h, K_STEP, a, cnt))) return rc;
+  if ((rc = enqueue_substeps(h, a, start, end, nstep))) return rc;
   if (qpos_out) CK(cudaMemcpyAsync(qpos_out, h->b_qout.p, qb, cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   return PG_OK;
@@ -1264,7 +1327,9 @@ int pg_poses(pg_handle* h, int64_t start, int64_t end, pg_pose* geoms, size_t ng
   StepArgs a = make_args(h);
   a.start = (int)start;
   a.count = (int)cnt;
-  if ((rc = run_tile_kernel(h, K_POSES, a, cnt, nullptr, (float*)h->b_poses_g.p, (float*)h->b_poses_c.p))) return rc;
+  if ((rc = launch_status(
+           launch_poses(a, fit(h->cfg.smooth, cnt), (float*)h->b_poses_g.p, (float*)h->b_poses_c.p, h->stream))))
+    return rc;
   if (m.ngeom) CK(cudaMemcpyAsync(geoms, h->b_poses_g.p, sizeof(pg_pose) * cnt * m.ngeom, cudaMemcpyDeviceToHost, h->stream));
   if (m.ncam) CK(cudaMemcpyAsync(cams, h->b_poses_c.p, sizeof(pg_pose) * cnt * m.ncam, cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
@@ -1451,23 +1516,25 @@ int pg_debug_forward(pg_handle* h, int64_t env, double* qm, double* qfrc_bias, d
   if (maxcon < 0) return fail(PG_ERR_INVALID, "maxcon must be non-negative");
   CK(cudaSetDevice(h->device));
   int nv = h->hm.nv;
-  int stride = nv * nv + nv + 1 + 13 * (int)std::min<int64_t>(maxcon, h->dm.maxcon);
-  int rc = grow(h, h->b_dbg, sizeof(double) * stride);
-  if (rc) return rc;
+  // the smooth-dynamics and collision phases of one env leave M, the bias
+  // force and the contacts in that env's work record
   StepArgs a = make_args(h);
   a.start = (int)env;
   a.count = 1;
-  if ((rc = run_tile_kernel(h, K_FORWARD, a, 1, nullptr, nullptr, nullptr, (double*)h->b_dbg.p, stride,
-                            (int)std::min<int64_t>(maxcon, h->dm.maxcon))))
-    return rc;
-  std::vector<double> out(stride);
-  CK(cudaMemcpyAsync(out.data(), h->b_dbg.p, sizeof(double) * stride, cudaMemcpyDeviceToHost, h->stream));
+  int rc = launch_status(launch_smooth_collide(a, fit(h->cfg, 1), h->stream));
+  if (rc) return rc;
+  const WorkLayout& k = h->k;
+  std::vector<double> out(k.stride);
+  CK(cudaMemcpyAsync(out.data(), h->work + (size_t)env * k.stride, sizeof(double) * k.stride, cudaMemcpyDeviceToHost,
+                     h->stream));
   CK(cudaStreamSynchronize(h->stream));
-  if (qm) std::memcpy(qm, out.data(), sizeof(double) * nv * nv);
-  if (qfrc_bias) std::memcpy(qfrc_bias, out.data() + nv * nv, sizeof(double) * nv);
-  int64_t n = (int64_t)out[nv * nv + nv];
+  if (qm) std::memcpy(qm, out.data() + k.qm, sizeof(double) * nv * nv);
+  if (qfrc_bias) std::memcpy(qfrc_bias, out.data() + k.bias, sizeof(double) * nv);
+  int64_t n = (int64_t)out[k.meta + K_META_NCON];
   if (ncon) *ncon = n;
-  if (contacts) std::memcpy(contacts, out.data() + nv * nv + nv + 1, sizeof(double) * 13 * std::min(n, maxcon));
+  if (contacts)
+    for (int64_t c = 0; c < std::min(n, maxcon); c++)
+      std::memcpy(contacts + 13 * c, out.data() + k.contacts + C_STRIDE * c, sizeof(double) * 13);
   return PG_OK;
 }
 
@@ -1484,18 +1551,22 @@ int pg_invweight(pg_handle* h, int64_t env, double* body, double* dof) {
 
 int pg_set_launch(pg_handle* h, int lanes_per_env, int envs_per_block) {
   if (!h) return fail(PG_ERR_INVALID, "NULL handle");
-  LaunchCfg c = h->cfg;
-  if (lanes_per_env > 0) c.G = lanes_per_env;
-  if (envs_per_block > 0) c.tiles_per_block = envs_per_block;
+  // the shape applies to every phase kernel of the substep
+  SubstepCfg c = h->cfg;
+  for (LaunchCfg* p : {&c.smooth, &c.collide, &c.newton}) {
+    if (lanes_per_env > 0) p->G = lanes_per_env;
+    if (envs_per_block > 0) p->tiles_per_block = envs_per_block;
+  }
   CK(cudaSetDevice(h->device));
   return apply_cfg(h, c);
 }
 
 int pg_get_launch(const pg_handle* h, int* lanes_per_env, int* envs_per_block, int* blocks) {
   if (!h) return fail(PG_ERR_INVALID, "NULL handle");
-  if (lanes_per_env) *lanes_per_env = h->cfg.G;
-  if (envs_per_block) *envs_per_block = h->cfg.tiles_per_block;
-  if (blocks) *blocks = h->cfg.blocks;
+  // the Newton phase's shape (the longest-running kernel of a substep)
+  if (lanes_per_env) *lanes_per_env = h->cfg.newton.G;
+  if (envs_per_block) *envs_per_block = h->cfg.newton.tiles_per_block;
+  if (blocks) *blocks = h->cfg.newton.blocks;
   return PG_OK;
 }
 
@@ -1520,49 +1591,59 @@ int pg_autotune(pg_handle* h, int64_t nstep) {
     for (size_t k = 0; k < fields.size(); k++)
       cudaMemcpyAsync(fields[k], saved[k], sizeof(double) * n * widths[k], cudaMemcpyDeviceToDevice, h->stream);
   };
-  LaunchCfg best = h->cfg;
-  float best_ms = 1e30f;
+  // coordinate search: each phase's shape in turn, the others held at the
+  // best found so far, timed over `nstep` whole substeps
+  SubstepCfg best = h->cfg;
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
   int rc = PG_OK;
-  for (int G : {8, 16, 32}) {
-    for (int tpb : {1, 2, 4, 8, 16}) {
-      LaunchCfg want{G, tpb, 0}, c;
-      if (tpb * G < 32 || tpb * G > 256) continue;
-      if (choose_grid(h, want, &c) != PG_OK) continue;
-      if (ensure_scratch(h, c) != PG_OK) continue;
-      h->cfg = c;
-      StepArgs a = make_args(h);
-      a.start = 0;
-      a.count = (int)n;
-      a.nstep = (int)nstep;
-      restore();
-      run_tile_kernel(h, K_STEP, a, n);  // warm-up
-      restore();
-      cudaEventRecord(e0, h->stream);
-      run_tile_kernel(h, K_STEP, a, n);
-      cudaEventRecord(e1, h->stream);
-      if (cudaEventSynchronize(e1) != cudaSuccess) {
-        rc = cuda_fail(cudaGetLastError(), "autotune trial");
-        break;
-      }
-      float ms = 0;
-      cudaEventElapsedTime(&ms, e0, e1);
-      if (ms < best_ms) {
-        best_ms = ms;
-        best = c;
+  auto trial = [&](const SubstepCfg& c, float* ms) -> int {
+    if (ensure_scratch(h, c) != PG_OK) return 1;
+    h->cfg = c;
+    StepArgs a = make_args(h);
+    restore();
+    enqueue_substeps(h, a, 0, (int64_t)n, nstep);  // warm-up
+    restore();
+    cudaEventRecord(e0, h->stream);
+    enqueue_substeps(h, a, 0, (int64_t)n, nstep);
+    cudaEventRecord(e1, h->stream);
+    if (cudaEventSynchronize(e1) != cudaSuccess) {
+      rc = cuda_fail(cudaGetLastError(), "autotune trial");
+      return 1;
+    }
+    cudaEventElapsedTime(ms, e0, e1);
+    return 0;
+  };
+  float best_ms = 1e30f;
+  if (trial(best, &best_ms)) best_ms = 1e30f;
+  for (int phase : {K_SMOOTH, K_COLLIDE, K_NEWTON}) {
+    if (rc) break;
+    for (int G : {8, 16, 32}) {
+      for (int tpb : {1, 2, 4, 8, 16}) {
+        if (rc) break;
+        if (tpb * G < 32 || tpb * G > 256) continue;
+        SubstepCfg c = best;
+        LaunchCfg& slot = phase == K_SMOOTH ? c.smooth : phase == K_COLLIDE ? c.collide : c.newton;
+        if (choose_grid(h, phase, LaunchCfg{G, tpb, 0}, &slot) != PG_OK) continue;
+        float ms = 0;
+        if (trial(c, &ms)) continue;
+        if (ms < best_ms) {
+          best_ms = ms;
+          best = c;
+        }
       }
     }
-    if (rc) break;
   }
   restore();
   cudaStreamSynchronize(h->stream);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   for (void* p : saved) cudaFree(p);
-  g_err.clear();
-  h->cfg = best;
+  if (!rc) g_err.clear();
+  // re-apply the winner so every kernel's shared-memory attribute matches it
+  if (!rc) rc = apply_cfg(h, best);
+  clear_graphs(h);
   h->version++;
   return rc;
 }

@@ -18,7 +18,9 @@ namespace pg {
 struct EnvCtx {
   double* ws;         // tile workspace (shared memory)
   const double* prm;  // this env's parameter block
-  double* scr;        // tile scratch (global)
+  double* scr;        // tile scratch (global): constraint rows, island buffers
+  double* geo;        // this env's geom records (G_STRIDE each)
+  double* con;        // this env's contacts (C_STRIDE each)
   int env;
 };
 

@@ -1,13 +1,20 @@
 // Kernels of the batched FP64 physics backend.
 //
-// step_kernel is persistent: a grid sized to the GPU's resident capacity,
-// each tile of G lanes pops environment indices from a device work counter
-// (one atomicAdd per env; nothing ever waits on another tile, so no spin
-// can hang) and runs all `nstep` substeps of that env with its state held
-// in shared memory. Envs with many contacts or Newton iterations hold only
-// their own tile, never a whole block or the grid. Each block first copies
-// the model (a few KB) into its shared memory, so the tree walks and the
-// narrow phase read topology and constants at shared-memory latency.
+// A substep (crates/pippin/src/forward.rs:336-389) runs as three phase
+// kernels over the env range, each small enough for the instruction cache:
+//   smooth_kernel   kinematics, CRBA, RNE, passive and actuator forces, the
+//                   factorisation of M and a0 = M^-1 f, and the factor of
+//                   M + hD used at the end (the same control flow in every
+//                   env, so the tiles of a warp stay in lockstep)
+//   collide_kernel  broad and narrow phase
+//   newton_kernel   constraint rows, Newton, implicit-damping solve,
+//                   integration (the phase whose work varies per env)
+// They hand data over in a per-env work record in HBM (it stays in L2 for
+// batches of a few thousand envs). Every kernel is persistent: a grid sized
+// to the GPU's resident capacity whose tiles of G lanes pop env indices from
+// a device counter (one atomicAdd per env; no tile waits on another, so
+// there is no spin to bound). Each block first copies the model (a few KB)
+// into shared memory.
 #include <cuda_runtime.h>
 
 #include "pg_kernels.h"
@@ -38,93 +45,9 @@ __device__ inline const DModel& stage_model(const StepArgs& A, unsigned char* sm
   return *dm;
 }
 
-__device__ inline double* tile_workspace(const StepArgs& A, unsigned char* sm, int tib) {
+__device__ inline double* tile_workspace(const StepArgs& A, unsigned char* sm, int stride, int tib) {
   int off = A.stage_model ? staged_model_bytes(A.m.arena_bytes) : 0;
-  return reinterpret_cast<double*>(sm + off) + (size_t)tib * A.w.stride;
-}
-
-// forward.rs:336-389: one substep of one env, state in the tile workspace
-template <int G>
-__device__ void substep(const Tile<G>& T, const DModel& m, const StepArgs& A, const EnvCtx& e, int* status,
-                        int* iters, int* ncon_out, int* nrows_out) {
-  const WsLayout& w = A.w;
-  const ScrLayout& s = A.s;
-  int lane = T.lane(), nv = m.nv;
-  double* ws = e.ws;
-  double h = m.timestep;
-
-  tree_down(T, m, w, e, true, e.scr + s.geoms);
-  tree_up(T, m, w, e, true);
-  passive_actuation(T, m, w, e);
-  int ncon = collide(T, m, w, s, e, status);
-  *ncon_out = ncon;
-
-  double* smooth = ws + w.smooth;
-  double* acc = ws + w.acc;
-  for (int k = lane; k < nv; k += G) {
-    smooth[k] = ws[w.passive + k] + ws[w.actf + k] + ws[w.applied + k] - ws[w.bias + k];
-    acc[k] = smooth[k];
-  }
-  T.sync();
-  // the tree region is dead from here on: factorisations and Newton use it
-  bool damped = has_implicit_terms(m, e.prm);
-  if (!factor_mass(T, m, w, e, 0.0)) {
-    *status |= ST_NOT_SPD;
-    return;
-  }
-  solve_blocks(T, ws + w.fac, nv, nv, m.nblock, m.block_adr, m.dof_block, m.maxbs, ws + w.rinv, acc);
-  int nr = build_rows(T, m, w, s, e, ncon, status);
-  *nrows_out = nr;
-  const double* warm = A.warm_mode == WARM_COLD ? nullptr : ws + w.qacc;
-  *iters = newton_solve(T, m, w, s, e, nr, acc, warm);
-  if (damped) {
-    if (!factor_mass(T, m, w, e, h)) {
-      *status |= ST_NOT_SPD;
-      return;
-    }
-    for (int k = lane; k < nv; k += G) acc[k] = smooth[k] + ws[w.qfrc_c + k];
-    T.sync();
-    solve_blocks(T, ws + w.fac, nv, nv, m.nblock, m.block_adr, m.dof_block, m.maxbs, ws + w.rinv, acc);
-  }
-  double* v = ws + w.vel;
-  double* qvel = ws + w.qvel;
-  for (int k = lane; k < nv; k += G) {
-    double vk = qvel[k] + h * acc[k];
-    v[k] = vk;
-    ws[w.qacc + k] = (vk - qvel[k]) / h;
-  }
-  T.sync();
-  integrate_pos(T, m, ws + w.qpos, v, h);
-  for (int k = lane; k < nv; k += G) qvel[k] = v[k];
-  T.sync();
-}
-
-template <int G>
-__device__ void load_env(const Tile<G>& T, const DModel& m, const StepArgs& A, const EnvCtx& e) {
-  const WsLayout& w = A.w;
-  int lane = T.lane();
-  size_t env = e.env;
-  for (int k = lane; k < m.nq; k += G) e.ws[w.qpos + k] = A.st.qpos[env * m.nq + k];
-  for (int k = lane; k < m.nv; k += G) {
-    e.ws[w.qvel + k] = A.st.qvel[env * m.nv + k];
-    e.ws[w.qacc + k] = A.st.qacc[env * m.nv + k];
-    e.ws[w.applied + k] = A.st.applied[env * m.nv + k];
-  }
-  for (int k = lane; k < m.nu; k += G) e.ws[w.ctrl + k] = A.st.ctrl[env * m.nu + k];
-  T.sync();
-}
-
-template <int G>
-__device__ void store_env(const Tile<G>& T, const DModel& m, const StepArgs& A, const EnvCtx& e) {
-  const WsLayout& w = A.w;
-  int lane = T.lane();
-  size_t env = e.env;
-  for (int k = lane; k < m.nq; k += G) A.st.qpos[env * m.nq + k] = e.ws[w.qpos + k];
-  for (int k = lane; k < m.nv; k += G) {
-    A.st.qvel[env * m.nv + k] = e.ws[w.qvel + k];
-    A.st.qacc[env * m.nv + k] = e.ws[w.qacc + k];
-  }
-  for (int k = lane; k < m.nu; k += G) A.st.ctrl[env * m.nu + k] = e.ws[w.ctrl + k];
+  return reinterpret_cast<double*>(sm + off) + (size_t)tib * stride;
 }
 
 // pops the next work item for the tile (one atomic per env)
@@ -136,80 +59,188 @@ __device__ inline int next_item(const Tile<G>& T, int* queue) {
 }
 
 template <int G>
-__global__ void __launch_bounds__(256) step_kernel(const __grid_constant__ StepArgs A) {
+__device__ inline void copy_in(const Tile<G>& T, double* dst, const double* src, int n) {
+  for (int k = T.lane(); k < n; k += G) dst[k] = src[k];
+}
+
+// ---------------------------------------------------------------- phase 1
+// forward.rs:263-271 (minus collide) and forward.rs:342-356: smooth forces,
+// a0 = M^-1 f, and the factor of M + hD (forward.rs:359-366) when damped.
+template <int G>
+__global__ void __launch_bounds__(256) smooth_kernel(const __grid_constant__ StepArgs A) {
   extern __shared__ __align__(16) unsigned char smem[];
   const DModel& m = stage_model(A, smem);
   cg::thread_block block = cg::this_thread_block();
   Tile<G> T(cg::tiled_partition<G>(block));
-  int tib = threadIdx.x / G;
-  size_t gtile = (size_t)blockIdx.x * (blockDim.x / G) + tib;
+  const WsLayout& w = A.w;
   EnvCtx e;
-  e.ws = tile_workspace(A, smem, tib);
-  e.scr = A.scratch + gtile * (size_t)A.s.stride;
+  e.ws = tile_workspace(A, smem, w.stride, threadIdx.x / G);
+  e.scr = nullptr;
+  e.con = nullptr;
+  int nq = m.nq, nv = m.nv, nu = m.nu;
+  double h = m.timestep;
   for (;;) {
-    int item = next_item(T, A.queue);
+    int item = next_item(T, A.queue + 0);
     if (item >= A.count) break;
-    e.env = A.start + item;
-    e.prm = A.st.params + (size_t)e.env * m.pstride;
-    load_env(T, m, A, e);
-    int status = 0, iters = 0, ncon = 0, nrows = 0;
-    for (int sidx = 0; sidx < A.nstep; sidx++) {
-      if (A.ctrl_seq) {
-        for (int k = T.lane(); k < m.nu; k += G)
-          e.ws[A.w.ctrl + k] = A.ctrl_seq[((size_t)item * A.nstep + sidx) * m.nu + k];
-        T.sync();
-      }
-      substep(T, m, A, e, &status, &iters, &ncon, &nrows);
-      if (A.qpos_out)
-        for (int k = T.lane(); k < m.nq; k += G)
-          A.qpos_out[((size_t)item * A.nstep + sidx) * m.nq + k] = e.ws[A.w.qpos + k];
-      if (status & ST_NOT_SPD) break;
+    size_t env = (size_t)A.start + item;
+    e.env = (int)env;
+    e.prm = A.st.params + env * m.pstride;
+    double* wk = A.work + env * A.k.stride;
+    e.geo = wk + A.k.geoms;
+    double* ws = e.ws;
+    copy_in(T, ws + w.qpos, A.st.qpos + env * nq, nq);
+    copy_in(T, ws + w.qvel, A.st.qvel + env * nv, nv);
+    copy_in(T, ws + w.applied, A.st.applied + env * nv, nv);
+    if (A.ctrl_seq) {
+      const double* c = A.ctrl_seq + ((size_t)item * A.nstep + A.sidx) * nu;
+      copy_in(T, ws + w.ctrl, c, nu);
+      copy_in(T, A.st.ctrl + env * nu, c, nu);  // rollout leaves the last controls in place
+    } else {
+      copy_in(T, ws + w.ctrl, A.st.ctrl + env * nu, nu);
     }
-    store_env(T, m, A, e);
+    T.sync();
+    tree_down(T, m, w, e, true, e.geo);
+    tree_up(T, m, w, e, true);
+    passive_actuation(T, m, w, e);
+    double* smooth = ws + w.smooth;
+    double* acc = ws + w.acc;
+    for (int k = T.lane(); k < nv; k += G) {
+      double f = ws[w.passive + k] + ws[w.actf + k] + ws[w.applied + k] - ws[w.bias + k];
+      smooth[k] = f;
+      acc[k] = f;
+      wk[A.k.bias + k] = ws[w.bias + k];
+    }
+    copy_in(T, wk + A.k.qm, ws + w.qm, nv * nv);
+    copy_in(T, wk + A.k.cdof, ws + w.cdof, 6 * nv);
+    T.sync();
+    // the tree region is dead from here on: the factorisations use it
+    int status = 0;
+    bool damped = has_implicit_terms(m, e.prm);
+    if (factor_mass(T, m, w, e, 0.0)) {
+      solve_blocks(T, ws + w.fac, nv, nv, m.nblock, m.block_adr, m.dof_block, m.maxbs, ws + w.rinv, acc);
+      copy_in(T, wk + A.k.a0, acc, nv);
+      copy_in(T, wk + A.k.smooth, smooth, nv);
+      if (damped) {
+        T.sync();
+        if (factor_mass(T, m, w, e, h)) {
+          copy_in(T, wk + A.k.lh, ws + w.fac, nv * nv);
+          copy_in(T, wk + A.k.rinvh, ws + w.rinv, nv);
+        } else {
+          status |= ST_NOT_SPD;
+        }
+      }
+    } else {
+      status |= ST_NOT_SPD;
+    }
     if (T.lane() == 0) {
-      A.st.iters[e.env] = iters;
-      A.st.ncon[e.env] = ncon;
-      A.st.nrows[e.env] = nrows;
-      A.st.status[e.env] = status;
+      wk[A.k.meta + K_META_STATUS] = status;
+      wk[A.k.meta + K_META_DAMPED] = damped ? 1.0 : 0.0;
     }
     T.sync();
   }
 }
 
-// Forward pass only (forward.rs:263-271) for diagnostics: writes M, bias
-// and the contact list of each env to `dbg`.
+// ---------------------------------------------------------------- phase 2
+// forward.rs:214-260: broad and narrow phase over the candidate pairs
 template <int G>
-__global__ void __launch_bounds__(256) forward_kernel(const __grid_constant__ StepArgs A, double* dbg, int dbg_stride,
-                                                      int maxcon_out) {
+__global__ void __launch_bounds__(256) collide_kernel(const __grid_constant__ StepArgs A) {
   extern __shared__ __align__(16) unsigned char smem[];
   const DModel& m = stage_model(A, smem);
   cg::thread_block block = cg::this_thread_block();
   Tile<G> T(cg::tiled_partition<G>(block));
+  EnvCtx e;
+  e.ws = nullptr;
+  e.scr = nullptr;
+  for (;;) {
+    int item = next_item(T, A.queue + 1);
+    if (item >= A.count) break;
+    size_t env = (size_t)A.start + item;
+    e.env = (int)env;
+    e.prm = A.st.params + env * m.pstride;
+    double* wk = A.work + env * A.k.stride;
+    e.geo = wk + A.k.geoms;
+    e.con = wk + A.k.contacts;
+    int status = 0;
+    int ncon = collide(T, m, A.w, A.s, e, &status);
+    if (T.lane() == 0) {
+      wk[A.k.meta + K_META_NCON] = ncon;
+      wk[A.k.meta + K_META_STATUS] = (double)((int)wk[A.k.meta + K_META_STATUS] | status);
+    }
+    T.sync();
+  }
+}
+
+// ---------------------------------------------------------------- phase 3
+// newton.rs:113-473 and forward.rs:359-389: rows, Newton, the damped
+// solve qacc = (M + hD)^-1 (f + qfrc_constraint), integration.
+template <int G>
+__global__ void __launch_bounds__(256) newton_kernel(const __grid_constant__ StepArgs A) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const DModel& m = stage_model(A, smem);
+  cg::thread_block block = cg::this_thread_block();
+  Tile<G> T(cg::tiled_partition<G>(block));
+  const WsLayout& w = A.wn;
   int tib = threadIdx.x / G;
   size_t gtile = (size_t)blockIdx.x * (blockDim.x / G) + tib;
   EnvCtx e;
-  e.ws = tile_workspace(A, smem, tib);
+  e.ws = tile_workspace(A, smem, w.stride, tib);
   e.scr = A.scratch + gtile * (size_t)A.s.stride;
+  int nq = m.nq, nv = m.nv;
+  double h = m.timestep;
   for (;;) {
-    int item = next_item(T, A.queue);
+    int item = next_item(T, A.queue + 2);
     if (item >= A.count) break;
-    e.env = A.start + item;
-    e.prm = A.st.params + (size_t)e.env * m.pstride;
-    load_env(T, m, A, e);
-    int status = 0;
-    tree_down(T, m, A.w, e, true, e.scr + A.s.geoms);
-    tree_up(T, m, A.w, e, true);
-    passive_actuation(T, m, A.w, e);
-    int ncon = collide(T, m, A.w, A.s, e, &status);
-    double* out = dbg + (size_t)item * dbg_stride;
-    int nv = m.nv;
-    for (int k = T.lane(); k < nv * nv; k += G) out[k] = e.ws[A.w.qm + k];
-    for (int k = T.lane(); k < nv; k += G) out[nv * nv + k] = e.ws[A.w.bias + k];
-    if (T.lane() == 0) out[nv * nv + nv] = ncon;
-    const double* con = e.scr + A.s.contacts;
-    for (int t = T.lane(); t < ncon * 13 && t < maxcon_out * 13; t += G) {
-      int c = t / 13, f = t % 13;
-      out[nv * nv + nv + 1 + t] = con[C_STRIDE * c + f];
+    size_t env = (size_t)A.start + item;
+    e.env = (int)env;
+    e.prm = A.st.params + env * m.pstride;
+    double* wk = A.work + env * A.k.stride;
+    e.geo = wk + A.k.geoms;
+    e.con = wk + A.k.contacts;
+    double* ws = e.ws;
+    int status = (int)wk[A.k.meta + K_META_STATUS];
+    int ncon = (int)wk[A.k.meta + K_META_NCON];
+    int iters = 0, nr = 0;
+    if (!(status & ST_NOT_SPD)) {
+      copy_in(T, ws + w.qpos, A.st.qpos + env * nq, nq);
+      copy_in(T, ws + w.qvel, A.st.qvel + env * nv, nv);
+      copy_in(T, ws + w.qacc, A.st.qacc + env * nv, nv);
+      copy_in(T, ws + w.qm, wk + A.k.qm, nv * nv);
+      copy_in(T, ws + w.cdof, wk + A.k.cdof, 6 * nv);
+      copy_in(T, ws + w.acc, wk + A.k.a0, nv);
+      copy_in(T, ws + w.smooth, wk + A.k.smooth, nv);
+      T.sync();
+      nr = build_rows(T, m, w, A.s, e, ncon, &status);
+      const double* warm = A.warm_mode == WARM_COLD ? nullptr : ws + w.qacc;
+      double* acc = ws + w.acc;
+      iters = newton_solve(T, m, w, A.s, e, nr, acc, warm);
+      if (wk[A.k.meta + K_META_DAMPED] != 0.0) {
+        copy_in(T, ws + w.fac, wk + A.k.lh, nv * nv);
+        copy_in(T, ws + w.rinv, wk + A.k.rinvh, nv);
+        for (int k = T.lane(); k < nv; k += G) acc[k] = ws[w.smooth + k] + ws[w.qfrc_c + k];
+        T.sync();
+        solve_blocks(T, ws + w.fac, nv, nv, m.nblock, m.block_adr, m.dof_block, m.maxbs, ws + w.rinv, acc);
+      }
+      double* v = ws + w.vel;
+      double* qvel = ws + w.qvel;
+      for (int k = T.lane(); k < nv; k += G) {
+        double vk = qvel[k] + h * acc[k];
+        v[k] = vk;
+        ws[w.qacc + k] = (vk - qvel[k]) / h;
+      }
+      T.sync();
+      integrate_pos(T, m, ws + w.qpos, v, h);
+      copy_in(T, A.st.qpos + env * nq, ws + w.qpos, nq);
+      copy_in(T, A.st.qvel + env * nv, v, nv);
+      copy_in(T, A.st.qacc + env * nv, ws + w.qacc, nv);
+      if (A.qpos_out) copy_in(T, A.qpos_out + ((size_t)item * A.nstep + A.sidx) * nq, ws + w.qpos, nq);
+    } else if (A.qpos_out) {
+      copy_in(T, A.qpos_out + ((size_t)item * A.nstep + A.sidx) * nq, A.st.qpos + env * nq, nq);
+    }
+    if (T.lane() == 0) {
+      A.st.iters[env] = iters;
+      A.st.ncon[env] = ncon;
+      A.st.nrows[env] = nr;
+      A.st.status[env] = (A.sidx == 0 ? 0 : A.st.status[env]) | status;
     }
     T.sync();
   }
@@ -226,16 +257,16 @@ __global__ void __launch_bounds__(256) set_const_kernel(const __grid_constant__ 
   size_t gtile = (size_t)blockIdx.x * (blockDim.x / G) + tib;
   const WsLayout& w = A.w;
   EnvCtx e;
-  e.ws = tile_workspace(A, smem, tib);
+  e.ws = tile_workspace(A, smem, w.stride, tib);
   e.scr = A.scratch + gtile * (size_t)A.s.stride;
   int nv = m.nv;
   for (;;) {
-    int item = next_item(T, A.queue);
+    int item = next_item(T, A.queue + 0);
     if (item >= n) break;
     e.env = envs ? envs[item] : A.start + item;
     double* prm = A.st.params + (size_t)e.env * m.pstride;
     e.prm = prm;
-    for (int k = T.lane(); k < m.nq; k += G) e.ws[w.qpos + k] = prm[m.p_qpos_reset + k];
+    copy_in(T, e.ws + w.qpos, prm + m.p_qpos_reset, m.nq);
     T.sync();
     tree_down(T, m, w, e, false, nullptr);
     tree_up(T, m, w, e, false);
@@ -323,19 +354,18 @@ __global__ void __launch_bounds__(256) poses_kernel(const __grid_constant__ Step
   const DModel& m = stage_model(A, smem);
   cg::thread_block block = cg::this_thread_block();
   Tile<G> T(cg::tiled_partition<G>(block));
-  int tib = threadIdx.x / G;
-  size_t gtile = (size_t)blockIdx.x * (blockDim.x / G) + tib;
   const WsLayout& w = A.w;
   EnvCtx e;
-  e.ws = tile_workspace(A, smem, tib);
-  e.scr = A.scratch + gtile * (size_t)A.s.stride;
-  double* gr = e.scr + A.s.geoms;
+  e.ws = tile_workspace(A, smem, w.stride, threadIdx.x / G);
+  e.scr = nullptr;
   for (;;) {
-    int item = next_item(T, A.queue);
+    int item = next_item(T, A.queue + 0);
     if (item >= A.count) break;
-    e.env = A.start + item;
-    e.prm = A.st.params + (size_t)e.env * m.pstride;
-    for (int k = T.lane(); k < m.nq; k += G) e.ws[w.qpos + k] = A.st.qpos[(size_t)e.env * m.nq + k];
+    size_t env = (size_t)A.start + item;
+    e.env = (int)env;
+    e.prm = A.st.params + env * m.pstride;
+    double* gr = A.work + env * A.k.stride + A.k.geoms;
+    copy_in(T, e.ws + w.qpos, A.st.qpos + env * m.nq, m.nq);
     T.sync();
     tree_down(T, m, w, e, false, gr);
     for (int g = T.lane(); g < m.ngeom; g += G) {
@@ -382,8 +412,9 @@ __global__ void reset_kernel(const __grid_constant__ StepArgs A, const int64_t* 
 template <int G>
 static const void* kernel_ptr(int which) {
   switch (which) {
-    case K_STEP: return (const void*)step_kernel<G>;
-    case K_FORWARD: return (const void*)forward_kernel<G>;
+    case K_SMOOTH: return (const void*)smooth_kernel<G>;
+    case K_COLLIDE: return (const void*)collide_kernel<G>;
+    case K_NEWTON: return (const void*)newton_kernel<G>;
     case K_SET_CONST: return (const void*)set_const_kernel<G>;
     case K_POSES: return (const void*)poses_kernel<G>;
   }
@@ -399,37 +430,56 @@ const void* tile_kernel(int which, int G) {
   return nullptr;
 }
 
-size_t block_smem(const StepArgs& a, const LaunchCfg& c) {
-  return (a.stage_model ? (size_t)staged_model_bytes(a.m.arena_bytes) : 0) +
-         (size_t)c.tiles_per_block * a.w.stride * sizeof(double);
+size_t kernel_smem(int which, const StepArgs& a, int tiles_per_block) {
+  size_t staged = a.stage_model ? (size_t)staged_model_bytes(a.m.arena_bytes) : 0;
+  switch (which) {
+    case K_COLLIDE: return staged;
+    case K_NEWTON: return staged + (size_t)tiles_per_block * a.wn.stride * sizeof(double);
+    default: return staged + (size_t)tiles_per_block * a.w.stride * sizeof(double);
+  }
 }
 
-#define PG_LAUNCH(KERNEL, ...)                                                      \
+#define PG_LAUNCH(WHICH, KERNEL, CFG, ...)                                          \
   do {                                                                              \
-    size_t smem = block_smem(a, c);                                                 \
-    dim3 grid(c.blocks), block(c.tiles_per_block * c.G);                           \
-    switch (c.G) {                                                                  \
+    size_t smem = kernel_smem(WHICH, a, (CFG).tiles_per_block);                     \
+    dim3 grid((CFG).blocks), block((CFG).tiles_per_block * (CFG).G);               \
+    switch ((CFG).G) {                                                              \
       case 8: KERNEL<8><<<grid, block, smem, s>>>(__VA_ARGS__); break;              \
       case 16: KERNEL<16><<<grid, block, smem, s>>>(__VA_ARGS__); break;            \
       case 32: KERNEL<32><<<grid, block, smem, s>>>(__VA_ARGS__); break;            \
       default: return cudaErrorInvalidValue;                                        \
     }                                                                               \
-    return cudaGetLastError();                                                      \
+    cudaError_t _e = cudaGetLastError();                                            \
+    if (_e != cudaSuccess) return _e;                                               \
   } while (0)
 
-cudaError_t launch_step(const StepArgs& a, const LaunchCfg& c, cudaStream_t s) { PG_LAUNCH(step_kernel, a); }
+cudaError_t launch_smooth_collide(const StepArgs& a, const SubstepCfg& c, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(a.queue, 0, 4 * sizeof(int), s);
+  if (e != cudaSuccess) return e;
+  PG_LAUNCH(K_SMOOTH, smooth_kernel, c.smooth, a);
+  PG_LAUNCH(K_COLLIDE, collide_kernel, c.collide, a);
+  return cudaSuccess;
+}
 
-cudaError_t launch_forward(const StepArgs& a, const LaunchCfg& c, double* dbg, int dbg_stride, int maxcon_out,
-                           cudaStream_t s) {
-  PG_LAUNCH(forward_kernel, a, dbg, dbg_stride, maxcon_out);
+cudaError_t launch_substep(const StepArgs& a, const SubstepCfg& c, cudaStream_t s) {
+  cudaError_t e = launch_smooth_collide(a, c, s);
+  if (e != cudaSuccess) return e;
+  PG_LAUNCH(K_NEWTON, newton_kernel, c.newton, a);
+  return cudaSuccess;
 }
 
 cudaError_t launch_set_const(const StepArgs& a, const LaunchCfg& c, const int* envs, int n, cudaStream_t s) {
-  PG_LAUNCH(set_const_kernel, a, envs, n);
+  cudaError_t e = cudaMemsetAsync(a.queue, 0, 4 * sizeof(int), s);
+  if (e != cudaSuccess) return e;
+  PG_LAUNCH(K_SET_CONST, set_const_kernel, c, a, envs, n);
+  return cudaSuccess;
 }
 
 cudaError_t launch_poses(const StepArgs& a, const LaunchCfg& c, float* geoms, float* cams, cudaStream_t s) {
-  PG_LAUNCH(poses_kernel, a, geoms, cams);
+  cudaError_t e = cudaMemsetAsync(a.queue, 0, 4 * sizeof(int), s);
+  if (e != cudaSuccess) return e;
+  PG_LAUNCH(K_POSES, poses_kernel, c, a, geoms, cams);
+  return cudaSuccess;
 }
 
 cudaError_t launch_reset(const StepArgs& a, const int64_t* ids, int n, cudaStream_t s) {

@@ -6,7 +6,8 @@
 
 namespace pg {
 
-enum { K_STEP = 0, K_FORWARD = 1, K_SET_CONST = 2, K_POSES = 3 };
+// tile kernels (one env per tile of G lanes, persistent over a work counter)
+enum { K_SMOOTH = 0, K_COLLIDE = 1, K_NEWTON = 2, K_SET_CONST = 3, K_POSES = 4, K_COUNT = 5 };
 
 struct LaunchCfg {
   int G;                // lanes per environment (8, 16, 32)
@@ -14,10 +15,19 @@ struct LaunchCfg {
   int blocks;           // persistent grid size
 };
 
+// launch shapes of the three phases of a substep
+struct SubstepCfg {
+  LaunchCfg smooth, collide, newton;
+};
+
 const void* tile_kernel(int which, int G);
-cudaError_t launch_step(const StepArgs& a, const LaunchCfg& c, cudaStream_t s);
-cudaError_t launch_forward(const StepArgs& a, const LaunchCfg& c, double* dbg, int dbg_stride, int maxcon_out,
-                           cudaStream_t s);
+// shared bytes per block of kernel `which` for the given tiles per block
+size_t kernel_smem(int which, const StepArgs& a, int tiles_per_block);
+
+// One substep of envs [a.start, a.start + a.count): counter reset, then the
+// smooth-dynamics, collision and Newton phase kernels, in stream order.
+cudaError_t launch_substep(const StepArgs& a, const SubstepCfg& c, cudaStream_t s);
+cudaError_t launch_smooth_collide(const StepArgs& a, const SubstepCfg& c, cudaStream_t s);
 cudaError_t launch_set_const(const StepArgs& a, const LaunchCfg& c, const int* envs, int n, cudaStream_t s);
 cudaError_t launch_poses(const StepArgs& a, const LaunchCfg& c, float* geoms, float* cams, cudaStream_t s);
 cudaError_t launch_reset(const StepArgs& a, const int64_t* ids, int n, cudaStream_t s);

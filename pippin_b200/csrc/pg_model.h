@@ -156,6 +156,16 @@ struct ScrLayout {
   int stride;
 };
 
+// Per-env work record in HBM, handed from one phase kernel to the next
+// (offsets in doubles): what smooth dynamics leaves for the collision and
+// Newton phases, the geoms and contacts of the narrow phase, and a small
+// meta block (contact count, status bits, whether implicit damping applies).
+enum { K_META_NCON = 0, K_META_STATUS = 1, K_META_DAMPED = 2, K_META_SIZE = 4 };
+struct WorkLayout {
+  int qm, cdof, a0, smooth, bias, lh, rinvh, geoms, contacts, meta;
+  int stride;
+};
+
 struct EnvState {
   double* qpos;
   double* qvel;
@@ -177,12 +187,16 @@ constexpr int MAX_PTR_FIELDS = 80;
 
 struct StepArgs {
   DModel m;
-  WsLayout w;
+  WsLayout w;   // smooth-dynamics phase (also set_const, poses)
+  WsLayout wn;  // Newton phase
   ScrLayout s;
+  WorkLayout k;
   EnvState st;
-  double* scratch;   // [tiles][s.stride]
-  int* queue;        // work counter (reset to 0 before each launch)
+  double* scratch;   // [tiles][s.stride] (the Newton phase's rows and islands)
+  double* work;      // [env][k.stride]
+  int* queue;        // work counters, one per phase kernel (reset before each substep)
   int start, count, nstep;
+  int sidx;          // substep index within the call
   int warm_mode;
   const double* ctrl_seq;  // optional (count, nstep, nu): per-substep controls
   double* qpos_out;        // optional (count, nstep, nq): qpos after each substep

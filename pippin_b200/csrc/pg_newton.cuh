@@ -20,8 +20,8 @@ __device__ int collide(const Tile<G>& T, const DModel& m, const WsLayout& w, con
                        int* status) {
   int lane = T.lane();
   const double* prm = e.prm;
-  const double* gr = e.scr + s.geoms;  // poses and boxes from the tree walk
-  double* con = e.scr + s.contacts;
+  const double* gr = e.geo;  // poses and boxes from the tree walk
+  double* con = e.con;
   int ncon = 0;
   int st = 0;
   for (int base = 0; base < m.npair; base += G) {
@@ -111,7 +111,7 @@ __device__ int build_rows(const Tile<G>& T, const DModel& m, const WsLayout& w, 
   int lane = T.lane(), nv = m.nv;
   const double* ws = e.ws;
   const double* prm = e.prm;
-  double* con = e.scr + s.contacts;
+  double* con = e.con;
   double* J = e.scr + s.jac;
   double* R = e.scr + s.rows;
   const double* cdof = ws + w.cdof;

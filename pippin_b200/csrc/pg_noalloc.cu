@@ -18,6 +18,7 @@
 // stepping at the same time on one device) race on it.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <mutex>
 #include <string>
 
@@ -27,7 +28,7 @@
 
 namespace pg {
 // fills the launch arguments of pg_step for [start, end) (pg_api.cpp)
-int internal_step_args(pg_handle* h, int64_t start, int64_t end, int64_t nstep, StepArgs* a, LaunchCfg* cfg,
+int internal_step_args(pg_handle* h, int64_t start, int64_t end, int64_t nstep, StepArgs* a, SubstepCfg* cfg,
                        cudaStream_t* stream, int* device);
 void internal_set_error(const std::string& msg);
 }  // namespace pg
@@ -35,7 +36,7 @@ void internal_set_error(const std::string& msg);
 namespace {
 
 constexpr size_t PG_STATIC_SCRATCH_BYTES = size_t(16) << 20;
-constexpr size_t PG_STATIC_COUNTER_BYTES = 256;  // work counter, then tile scratch
+constexpr size_t PG_STATIC_COUNTER_BYTES = 256;  // phase work counters, then tile scratch
 
 // Device-side scratch shared by every pg_step_static call on a device. Host
 // code must not use this name as an address: its device address comes from
@@ -67,7 +68,7 @@ int scratch_address(int device, unsigned char** out) {
 
 extern "C" int pg_step_static(pg_handle* h, int64_t start, int64_t end, int64_t nstep) {
   pg::StepArgs a;
-  pg::LaunchCfg cfg;
+  pg::SubstepCfg cfg;
   cudaStream_t stream;
   int device = 0;
   int rc = pg::internal_step_args(h, start, end, nstep, &a, &cfg, &stream, &device);
@@ -75,24 +76,26 @@ extern "C" int pg_step_static(pg_handle* h, int64_t start, int64_t end, int64_t 
   if (end == start || nstep == 0) return PG_OK;
   unsigned char* base = nullptr;
   if ((rc = scratch_address(device, &base)) != PG_OK) return rc;
+  // only the Newton phase uses tile scratch: its grid is capped by the array
+  pg::LaunchCfg& nc = cfg.newton;
   size_t tile_bytes = (size_t)a.s.stride * sizeof(double);
   size_t tiles = (PG_STATIC_SCRATCH_BYTES - PG_STATIC_COUNTER_BYTES) / tile_bytes;
-  if (tiles < (size_t)cfg.tiles_per_block) {
-    pg::internal_set_error("pg_step_static: this model needs " + std::to_string(tile_bytes * cfg.tiles_per_block) +
+  if (tiles < (size_t)nc.tiles_per_block) {
+    pg::internal_set_error("pg_step_static: this model needs " + std::to_string(tile_bytes * nc.tiles_per_block) +
                            " bytes of scratch per block, more than the " +
                            std::to_string(PG_STATIC_SCRATCH_BYTES - PG_STATIC_COUNTER_BYTES) +
                            "-byte static scratch holds (use pg_step)");
     return PG_ERR_UNSUPPORTED;
   }
-  int blocks = (int)std::min<size_t>((size_t)cfg.blocks, tiles / cfg.tiles_per_block);
-  int64_t need = ((end - start) + cfg.tiles_per_block - 1) / cfg.tiles_per_block;
-  if (need < blocks) blocks = (int)need;
-  cfg.blocks = blocks;
+  nc.blocks = (int)std::min<size_t>((size_t)nc.blocks, tiles / nc.tiles_per_block);
   a.queue = reinterpret_cast<int*>(base);
   a.scratch = reinterpret_cast<double*>(base + PG_STATIC_COUNTER_BYTES);
-  // the counter keeps the previous call's value: it must start at zero
-  cudaError_t e = cudaMemsetAsync(a.queue, 0, sizeof(int), stream);
-  if (e == cudaSuccess) e = pg::launch_step(a, cfg, stream);
+  // each substep restarts the phase counters before its kernels
+  cudaError_t e = cudaSuccess;
+  for (int64_t k = 0; k < nstep && e == cudaSuccess; k++) {
+    a.sidx = (int)k;
+    e = pg::launch_substep(a, cfg, stream);
+  }
   if (e != cudaSuccess) {
     pg::internal_set_error(std::string("pg_step_static: ") + cudaGetErrorString(e));
     return PG_ERR_CUDA;
