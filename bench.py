@@ -32,6 +32,14 @@ sys.path.insert(0, ROOT)
 TOL = 1e-10
 ITERS = 30
 
+# oracle FLOP-counter stages computed by each phase kernel
+PHASE_STAGES = {"smooth": ("kinematics", "crba", "vel_rne", "passive_act", "factor_solve"),
+                "collide": ("collide",),
+                "newton": ("rows", "newton", "pgs", "integrate")}
+# DRAM bytes (read + write) per env of each phase kernel, from one ncu capture
+# of the Ant workload at 4096 envs (profiles/phase_kernels_ant.md)
+NCU_TRAFFIC_PER_ENV = {"smooth": 2872.0, "collide": 6322.0, "newton": 5374.0}
+
 
 def parse():
     ap = argparse.ArgumentParser()
@@ -294,6 +302,21 @@ def run_ours(args):
         e1.synchronize()
         e2e_ms += e0.elapsed_time(e1)
     barrier()
+
+    # per-phase device time over K further substeps of the same workload
+    # (fresh state, same warm-up), one event pair per phase kernel
+    phys.set(Field.QPOS, range(n), q)
+    phys.set(Field.QVEL, range(n), v)
+    for k in range(W):
+        phys.step_device(range(n), 1, ctrl_all[k].data_ptr())
+    phys.synchronize()
+    phase_ms = {"smooth": 0.0, "collide": 0.0, "newton": 0.0}
+    for k in range(K):
+        flush.fill_(float(k))
+        torch.cuda.synchronize()
+        for name, ms in phys.time_phases(range(n), 1, ctrl_all[W + k].data_ptr()).items():
+            phase_ms[name] += ms
+    barrier()
     clock_info = clocks.stop()
 
     times = torch.tensor([ms_ref, ms_cold, e2e_ms], dtype=torch.float64, device=dev)
@@ -309,8 +332,11 @@ def run_ours(args):
     if rank == 0:
         peak = fp64_peak(local)
         flops_step, per_stage = algorithmic_flops(blob, m)
-        per_launch_ms = ms_ref / K
-        achieved = flops_step * n / (per_launch_ms * 1e-3) / 1e12
+        phase_flops = {ph: sum(per_stage.get(st, 0.0) for st in stages) for ph, stages in PHASE_STAGES.items()}
+        top = max(phase_ms, key=phase_ms.get)
+        per_launch_ms = phase_ms[top] / K
+        achieved = phase_flops[top] * n / (per_launch_ms * 1e-3) / 1e12
+        phase_total = sum(phase_ms.values())
         bytes_step = (m.nq + m.nv + m.nv + m.nu) * 8 + (m.nq + m.nv + m.nv) * 8
         line = {
             "metric": "Ant env-steps/s", "value": value, "unit": "env-steps/s", "n_gpus": ws, "steps": K,
@@ -320,16 +346,21 @@ def run_ours(args):
                            launch={"lanes_per_env": lanes, "envs_per_block": per_block, "blocks": blocks}),
             "e2e": {"value": e2e, "unit": "env-steps/s", "h2d_bytes_per_step": n * m.nu * 8,
                     "d2h_bytes_per_step": n * m.nq * 8},
-            "gpu_launches": K,
+            "gpu_launches": 3 * K,
             "variants": {"newton_ref_prev_qacc": value, "newton_cold": value_cold,
                          "mean_iters_ref": float(st["iters"].mean()), "mean_iters_cold": float(st_cold["iters"].mean()),
                          "p99_iters_ref": float(np.percentile(st["iters"], 99)),
                          "mean_ncon": float(st["ncon"].mean()), "mean_rows": float(st["nrows"].mean())},
-            "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak, "traffic": None,
-                         "note": f"{flops_step:.0f} algorithmic FP64 ops per env-step (oracle counters) x {n} envs "
-                                 "per launch / step-kernel time; peak = live DFMA microbenchmark (pg_fp64_peak)",
-                         "hbm_achieved_gbs": bytes_step * n / (per_launch_ms * 1e-3) / 1e9},
+            "roofline": {"bound": "fp64", "kernel": f"{top}_kernel", "achieved": achieved, "peak": peak,
+                         "unit": "TFLOP/s", "frac": achieved / peak,
+                         "traffic": NCU_TRAFFIC_PER_ENV.get(top, 0.0) * n or None,
+                         "note": f"{phase_flops[top]:.0f} algorithmic FP64 ops per env in the {top} phase (oracle "
+                                 f"counters, {flops_step:.0f} per whole env-step) x {n} envs per launch / that "
+                                 "kernel's mean event-timed duration; peak = live DFMA microbenchmark (pg_fp64_peak); "
+                                 "traffic = ncu DRAM bytes per env of that kernel x envs",
+                         "hbm_achieved_gbs": bytes_step * n / (ms_ref / K * 1e-3) / 1e9},
+            "phases": {ph: {"ms_per_launch": phase_ms[ph] / K, "share": phase_ms[ph] / phase_total,
+                            "fp64_ops_per_env": phase_flops[ph]} for ph in phase_ms},
             "clocks": clock_info,
         }
         if ws == 1 and not args.no_cpu_baseline:

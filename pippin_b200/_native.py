@@ -63,6 +63,7 @@ SIGNATURES = [
     ("pg_stream", _vp, [_vp]),
     ("pg_last_error", C.c_char_p, []),
     ("pg_fp64_peak", _i32, [_i32, _i32, _pd, _pd]),
+    ("pg_time_phases", _i32, [_vp, _i64, _i64, _i64, _vp, _pf]),
 ]
 
 _lib = None

@@ -1648,6 +1648,48 @@ int pg_autotune(pg_handle* h, int64_t nstep) {
   return rc;
 }
 
+int pg_time_phases(pg_handle* h, int64_t start, int64_t end, int64_t nstep, const double* ctrl_dev, float* ms_out) {
+  if (!h || !ms_out) return fail(PG_ERR_INVALID, "NULL argument");
+  int rc = check_range(h, start, end);
+  if (rc) return rc;
+  if (nstep < 0 || nstep > (1 << 30)) return fail(PG_ERR_INVALID, "nstep out of range");
+  for (int k = 0; k < 3; k++) ms_out[k] = 0.0f;
+  int64_t cnt = end - start;
+  if (cnt == 0 || nstep == 0) return PG_OK;
+  CK(cudaSetDevice(h->device));
+  if (h->hm.nu > 0 && ctrl_dev)
+    CK(cudaMemcpyAsync(h->ctrl + start * h->hm.nu, ctrl_dev, sizeof(double) * cnt * h->hm.nu, cudaMemcpyDeviceToDevice,
+                       h->stream));
+  StepArgs a = make_args(h);
+  a.start = (int)start;
+  a.count = (int)cnt;
+  a.nstep = (int)nstep;
+  SubstepCfg c = fit(h->cfg, cnt);
+  const LaunchCfg* shape[3] = {&c.smooth, &c.collide, &c.newton};
+  const int which[3] = {K_SMOOTH, K_COLLIDE, K_NEWTON};
+  cudaEvent_t ev[4];
+  for (auto& e : ev) CK(cudaEventCreate(&e));
+  cudaError_t e = cudaSuccess;
+  for (int64_t k = 0; k < nstep && e == cudaSuccess; k++) {
+    a.sidx = (int)k;
+    e = reset_queue(a, h->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(ev[0], h->stream);
+    for (int p = 0; p < 3 && e == cudaSuccess; p++) {
+      e = launch_phase(which[p], a, *shape[p], h->stream);
+      if (e == cudaSuccess) e = cudaEventRecord(ev[p + 1], h->stream);
+    }
+    if (e == cudaSuccess) e = cudaEventSynchronize(ev[3]);
+    for (int p = 0; p < 3 && e == cudaSuccess; p++) {
+      float ms = 0.0f;
+      e = cudaEventElapsedTime(&ms, ev[p], ev[p + 1]);
+      ms_out[p] += ms;
+    }
+  }
+  for (auto& x : ev) cudaEventDestroy(x);
+  if (e != cudaSuccess) return cuda_fail(e, "pg_time_phases");
+  return PG_OK;
+}
+
 int pg_synchronize(pg_handle* h) {
   if (!h) return fail(PG_ERR_INVALID, "NULL handle");
   CK(cudaSetDevice(h->device));

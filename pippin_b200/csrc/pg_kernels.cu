@@ -468,6 +468,18 @@ cudaError_t launch_substep(const StepArgs& a, const SubstepCfg& c, cudaStream_t 
   return cudaSuccess;
 }
 
+cudaError_t reset_queue(const StepArgs& a, cudaStream_t s) { return cudaMemsetAsync(a.queue, 0, 4 * sizeof(int), s); }
+
+cudaError_t launch_phase(int which, const StepArgs& a, const LaunchCfg& c, cudaStream_t s) {
+  switch (which) {
+    case K_SMOOTH: PG_LAUNCH(K_SMOOTH, smooth_kernel, c, a); break;
+    case K_COLLIDE: PG_LAUNCH(K_COLLIDE, collide_kernel, c, a); break;
+    case K_NEWTON: PG_LAUNCH(K_NEWTON, newton_kernel, c, a); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaSuccess;
+}
+
 cudaError_t launch_set_const(const StepArgs& a, const LaunchCfg& c, const int* envs, int n, cudaStream_t s) {
   cudaError_t e = cudaMemsetAsync(a.queue, 0, 4 * sizeof(int), s);
   if (e != cudaSuccess) return e;

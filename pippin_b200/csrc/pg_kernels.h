@@ -28,6 +28,9 @@ size_t kernel_smem(int which, const StepArgs& a, int tiles_per_block);
 // smooth-dynamics, collision and Newton phase kernels, in stream order.
 cudaError_t launch_substep(const StepArgs& a, const SubstepCfg& c, cudaStream_t s);
 cudaError_t launch_smooth_collide(const StepArgs& a, const SubstepCfg& c, cudaStream_t s);
+// the pieces of launch_substep: the counter reset and one phase kernel
+cudaError_t reset_queue(const StepArgs& a, cudaStream_t s);
+cudaError_t launch_phase(int which, const StepArgs& a, const LaunchCfg& c, cudaStream_t s);
 cudaError_t launch_set_const(const StepArgs& a, const LaunchCfg& c, const int* envs, int n, cudaStream_t s);
 cudaError_t launch_poses(const StepArgs& a, const LaunchCfg& c, float* geoms, float* cams, cudaStream_t s);
 cudaError_t launch_reset(const StepArgs& a, const int64_t* ids, int n, cudaStream_t s);

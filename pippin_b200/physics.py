@@ -244,6 +244,14 @@ class CudaPhysics:
         s, e = _span(envs)
         self._check(self._L.pg_step_device(self._h, s, e, int(nstep), C.c_void_p(ctrl_dev_ptr)))
 
+    def time_phases(self, envs: EnvRange, nstep: int, ctrl_dev_ptr: int = 0) -> dict:
+        """Step like step_device, timing each phase kernel with CUDA events;
+        returns the summed device milliseconds per phase."""
+        s, e = _span(envs)
+        ms = (C.c_float * 3)()
+        self._check(self._L.pg_time_phases(self._h, s, e, int(nstep), C.c_void_p(ctrl_dev_ptr or None), ms))
+        return {"smooth": ms[0], "collide": ms[1], "newton": ms[2]}
+
     def reset(self, envs: Sequence[int]):
         ids = np.ascontiguousarray(np.asarray(list(envs), dtype=np.int64))
         self._check(self._L.pg_reset(self._h, ids.ctypes.data_as(C.POINTER(C.c_int64)), len(ids)))
