@@ -63,6 +63,19 @@ __device__ inline void copy_in(const Tile<G>& T, double* dst, const double* src,
   for (int k = T.lane(); k < n; k += G) dst[k] = src[k];
 }
 
+// Global -> shared copies issued back to back without waiting (cp.async);
+// load_wait() completes this lane's copies, a tile sync then publishes them.
+__device__ inline void cp_async8(double* dst_shared, const double* src_global) {
+  unsigned d = (unsigned)__cvta_generic_to_shared(dst_shared);
+  size_t s = __cvta_generic_to_global(src_global);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(s) : "memory");
+}
+template <int G>
+__device__ inline void load_async(const Tile<G>& T, double* dst_shared, const double* src_global, int n) {
+  for (int k = T.lane(); k < n; k += G) cp_async8(dst_shared + k, src_global + k);
+}
+__device__ inline void load_wait() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 // ---------------------------------------------------------------- phase 1
 // forward.rs:263-271 (minus collide) and forward.rs:342-356: smooth forces,
 // a0 = M^-1 f, and the factor of M + hD (forward.rs:359-366) when damped.
@@ -88,16 +101,17 @@ __global__ void __launch_bounds__(256) smooth_kernel(const __grid_constant__ Ste
     double* wk = A.work + env * A.k.stride;
     e.geo = wk + A.k.geoms;
     double* ws = e.ws;
-    copy_in(T, ws + w.qpos, A.st.qpos + env * nq, nq);
-    copy_in(T, ws + w.qvel, A.st.qvel + env * nv, nv);
-    copy_in(T, ws + w.applied, A.st.applied + env * nv, nv);
+    load_async(T, ws + w.qpos, A.st.qpos + env * nq, nq);
+    load_async(T, ws + w.qvel, A.st.qvel + env * nv, nv);
+    load_async(T, ws + w.applied, A.st.applied + env * nv, nv);
     if (A.ctrl_seq) {
       const double* c = A.ctrl_seq + ((size_t)item * A.nstep + A.sidx) * nu;
-      copy_in(T, ws + w.ctrl, c, nu);
+      load_async(T, ws + w.ctrl, c, nu);
       copy_in(T, A.st.ctrl + env * nu, c, nu);  // rollout leaves the last controls in place
     } else {
-      copy_in(T, ws + w.ctrl, A.st.ctrl + env * nu, nu);
+      load_async(T, ws + w.ctrl, A.st.ctrl + env * nu, nu);
     }
+    load_wait();
     T.sync();
     tree_down(T, m, w, e, true, e.geo);
     tree_up(T, m, w, e, true);
@@ -117,7 +131,7 @@ __global__ void __launch_bounds__(256) smooth_kernel(const __grid_constant__ Ste
     int status = 0;
     bool damped = has_implicit_terms(m, e.prm);
     if (factor_mass(T, m, w, e, 0.0)) {
-      solve_blocks(T, ws + w.fac, nv, nv, m.nblock, m.block_adr, m.dof_block, m.maxbs, ws + w.rinv, acc);
+      solve_auto(T, ws + w.fac, nv, nv, m.nblock, m.block_adr, m.dof_block, m.maxbs, ws + w.rinv, acc);
       copy_in(T, wk + A.k.a0, acc, nv);
       copy_in(T, wk + A.k.smooth, smooth, nv);
       if (damped) {
@@ -201,24 +215,26 @@ __global__ void __launch_bounds__(256) newton_kernel(const __grid_constant__ Ste
     int ncon = (int)wk[A.k.meta + K_META_NCON];
     int iters = 0, nr = 0;
     if (!(status & ST_NOT_SPD)) {
-      copy_in(T, ws + w.qpos, A.st.qpos + env * nq, nq);
-      copy_in(T, ws + w.qvel, A.st.qvel + env * nv, nv);
-      copy_in(T, ws + w.qacc, A.st.qacc + env * nv, nv);
-      copy_in(T, ws + w.qm, wk + A.k.qm, nv * nv);
-      copy_in(T, ws + w.cdof, wk + A.k.cdof, 6 * nv);
-      copy_in(T, ws + w.acc, wk + A.k.a0, nv);
-      copy_in(T, ws + w.smooth, wk + A.k.smooth, nv);
+      load_async(T, ws + w.qpos, A.st.qpos + env * nq, nq);
+      load_async(T, ws + w.qvel, A.st.qvel + env * nv, nv);
+      load_async(T, ws + w.qacc, A.st.qacc + env * nv, nv);
+      load_async(T, ws + w.qm, wk + A.k.qm, nv * nv);
+      load_async(T, ws + w.cdof, wk + A.k.cdof, 6 * nv);
+      load_async(T, ws + w.acc, wk + A.k.a0, nv);
+      load_async(T, ws + w.smooth, wk + A.k.smooth, nv);
+      load_wait();
       T.sync();
       nr = build_rows(T, m, w, A.s, e, ncon, &status);
       const double* warm = A.warm_mode == WARM_COLD ? nullptr : ws + w.qacc;
       double* acc = ws + w.acc;
       iters = newton_solve(T, m, w, A.s, e, nr, acc, warm);
       if (wk[A.k.meta + K_META_DAMPED] != 0.0) {
-        copy_in(T, ws + w.fac, wk + A.k.lh, nv * nv);
-        copy_in(T, ws + w.rinv, wk + A.k.rinvh, nv);
+        load_async(T, ws + w.fac, wk + A.k.lh, nv * nv);
+        load_async(T, ws + w.rinv, wk + A.k.rinvh, nv);
         for (int k = T.lane(); k < nv; k += G) acc[k] = ws[w.smooth + k] + ws[w.qfrc_c + k];
+        load_wait();
         T.sync();
-        solve_blocks(T, ws + w.fac, nv, nv, m.nblock, m.block_adr, m.dof_block, m.maxbs, ws + w.rinv, acc);
+        solve_auto(T, ws + w.fac, nv, nv, m.nblock, m.block_adr, m.dof_block, m.maxbs, ws + w.rinv, acc);
       }
       double* v = ws + w.vel;
       double* qvel = ws + w.qvel;
@@ -277,7 +293,7 @@ __global__ void __launch_bounds__(256) set_const_kernel(const __grid_constant__ 
     double* rinv = e.ws + w.rinv;
     for (int t = T.lane(); t < nv * nv; t += G) L[t] = e.ws[w.qm + t];
     T.sync();
-    bool ok = chol_blocks(T, L, nv, nv, 1, nullptr, nullptr, nv, rinv);
+    bool ok = chol_auto(T, L, nv, nv, 1, nullptr, nullptr, nv, rinv);
     // one right-hand side per lane: unit vectors, then per body 3 axes x
     // (translation, rotation) rows; x = M^-1 row, quad = row . x
     double* xs = e.scr + A.s.jac;  // [rhs][nv]

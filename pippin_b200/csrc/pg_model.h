@@ -137,6 +137,10 @@ struct WsLayout {
   int xpos, xquat, xmat, cinert, cvel, cacc, cfrc, bias, passive, actf;
   // factorisations and Newton (alias the tree region)
   int fac, a0, grad, p, tmp, tmp2, mp, vel, warm;
+  // register Newton (nv <= 16, one dof tree): constraint rows [16][nv],
+  // Hessian factor [nv][nv], published vector [16] and row coefficients [16]
+  // (placed over buffers that path leaves unused; -1 when it does not apply)
+  int sj, sl, sx, sc;
   int stride;
 };
 

@@ -8,7 +8,7 @@
 #pragma once
 #include "pg_collide.cuh"
 #include "pg_dynamics.cuh"
-#include "pg_linalg.cuh"
+#include "pg_small.cuh"
 
 namespace pg {
 
@@ -366,10 +366,10 @@ __device__ __noinline__ int newton_dense(const Tile<G>& T, int k, int nr, const 
       H[i * k + j] = h;
     }
     T.sync();
-    if (!chol_blocks(T, H, k, k, 1, nullptr, nullptr, k, B.rinv)) break;
+    if (!chol_auto(T, H, k, k, 1, nullptr, nullptr, k, B.rinv)) break;
     for (int i = lane; i < k; i += G) p[i] = -grad[i];
     T.sync();
-    solve_blocks(T, H, k, k, 1, nullptr, nullptr, k, B.rinv, p);
+    solve_auto(T, H, k, k, 1, nullptr, nullptr, k, B.rinv, p);
     // exact line search on the piecewise quadratic along p
     mul_m(T, M, k, p, mp);
     double s1 = 0.0, s2 = 0.0;
@@ -443,6 +443,185 @@ __device__ __noinline__ void add_constraint_force(const Tile<G>& T, int k, int n
     qfrc[o] = q;
   }
   T.sync();
+}
+
+// ------------------------------------------------------- register-resident Newton
+// Shared buffers of newton_small (offsets sj, sl, sx, sc of the workspace).
+struct SmallBufs {
+  double* J;  // [16][k] constraint rows, copied in
+  double* L;  // [k][k] Hessian factor
+  double* x;  // [16] the vector being multiplied, one component per lane
+  double* c;  // [16] per-row coefficients
+};
+
+// newton.rs:224-371 for k <= 16 unknowns and nr <= 16 rows, with one unknown
+// and one row per lane: the lane's row of M and of the Hessian stay in
+// registers, the rows of J are copied into shared memory once, and each
+// product M x / J x reads the published x as broadcast loads. A lane holds at
+// most one term of every sum, so the sums are formed exactly as newton_dense
+// forms them; only the factorisation differs (chol_reg). Adds the constraint
+// force to qfrc (newton.rs:361-371) and leaves the solution in a; returns the
+// iteration count. J rows are read from Jsrc (stride k), row constants from R.
+template <int G>
+__device__ __noinline__ int newton_small(const Tile<G>& T, int k, int nr, const double* Jsrc, const double* R,
+                                         const double* M, double* a, const double* warm, int max_iters, double tol,
+                                         const SmallBufs& B, double* qfrc) {
+  static_assert(G >= SMALL_N, "one lane per unknown and per row");
+  const int i = T.lane();
+  const bool dof = i < k, rowl = i < nr;
+  double mrow[SMALL_N];
+#pragma unroll
+  for (int q = 0; q < SMALL_N; q++) mrow[q] = (dof && q < k) ? M[i * k + q] : 0.0;
+  const double a0 = dof ? a[i] : 0.0;
+  const double wi = (warm && dof) ? warm[i] : 0.0;
+  double aref = 0.0, dr = 0.0;
+  bool bil = false;
+  if (rowl) {
+    const double* rr = R + R_STRIDE * i;
+    aref = rr[R_AREF];
+    dr = rr[R_D];
+    bil = rr[R_FLAGS] != 0.0;
+  }
+  for (int t = i; t < nr * k; t += G) B.J[t] = Jsrc[t];
+  const double* Jr = B.J + i * k;  // this lane's row (rowl only)
+  // publish one component per lane for the broadcast reads that follow
+  auto publish = [&](double v) {
+    T.sync();
+    if (dof) B.x[i] = v;
+    T.sync();
+  };
+  auto coeffs = [&](double v) {
+    T.sync();
+    if (rowl) B.c[i] = v;
+    T.sync();
+  };
+  // newton.rs:96-110
+  auto cost = [&](double xi) -> double {
+    double tmp = xi - a0;
+    publish(tmp);
+    double tmp2 = dof ? dot_ref_reg(mrow, B.x, k) : 0.0;
+    double c = 0.5 * T.sum(dof ? tmp * tmp2 : 0.0);
+    publish(xi);
+    double cr = 0.0;
+    if (rowl) {
+      double jar = dot_ref_sm(Jr, B.x, k) - aref;
+      if (bil || jar < 0.0) cr = 0.5 * dr * jar * jar;
+    }
+    return c + T.sum(cr);
+  };
+  double ai = a0;
+  if (warm) {
+    double c0 = cost(a0);
+    double c1 = cost(wi);
+    if (c1 < c0) ai = wi;
+  }
+  publish(a0);
+  double ma0 = dof ? dot_ref_reg(mrow, B.x, k) : 0.0;
+  double scale = 1.0 + sqrt(T.sum(ma0 * ma0));
+  int iters = 0;
+  int maxit = max_iters > 1 ? max_iters : 1;
+  double prev = -1.0;  // the row's activity in the previous iteration (none yet)
+  double jar = 0.0, act = 0.0;
+  while (iters < maxit) {
+    iters++;
+    // gradient M (a - a0) + sum over active rows of D jar J_r (newton.rs:254-270)
+    double tmp = ai - a0;
+    publish(tmp);
+    double grad = dof ? dot_ref_reg(mrow, B.x, k) : 0.0;
+    publish(ai);
+    bool same = true;
+    if (rowl) {
+      jar = dot_ref_sm(Jr, B.x, k) - aref;
+      act = (bil || jar < 0.0) ? 1.0 : 0.0;
+      same = act == prev;
+      prev = act;
+    }
+    coeffs(act != 0.0 ? dr * jar : 0.0);
+    if (dof)
+      for (int r = 0; r < nr; r++) {
+        double cf = B.c[r];
+        if (cf != 0.0) grad += cf * B.J[r * k + i];
+      }
+    double gnorm = sqrt(T.sum(dof ? grad * grad : 0.0));
+    bool unchanged = T.all(same);
+    if (gnorm < tol * scale || (nr <= 128 && unchanged && iters > 1)) break;
+    // H = M + J_A' D J_A, this lane's row (lower part)
+    double h[SMALL_N];
+#pragma unroll
+    for (int q = 0; q < SMALL_N; q++) h[q] = mrow[q];
+    coeffs(act != 0.0 ? dr : 0.0);
+    if (dof)
+      for (int r = 0; r < nr; r++) {
+        double d = B.c[r];
+        if (d == 0.0) continue;
+        const double* jr = B.J + r * k;
+        double ji = jr[i];
+        if (ji == 0.0) continue;
+        double e = d * ji;
+#pragma unroll
+        for (int q = 0; q < SMALL_N; q++)
+          if (q <= i && q < k) h[q] += e * jr[q];
+      }
+    double rv = 0.0;
+    if (!chol_reg(T, h, k, B.L, k, &rv)) break;
+    double p = solve_reg(T, B.L, k, k, rv, dof ? -grad : 0.0);
+    // exact line search on the piecewise quadratic along p (newton.rs:317-354)
+    publish(p);
+    double mp = dof ? dot_ref_reg(mrow, B.x, k) : 0.0;
+    double jp = rowl ? dot_ref_sm(Jr, B.x, k) : 0.0;
+    double mpp = T.sum(dof ? p * mp : 0.0), mpg = T.sum(dof ? tmp * mp : 0.0);
+    auto deriv = [&](double al, double* d1o, double* d2o) {
+      double d1 = 0.0, d2 = 0.0;
+      if (rowl) {
+        double v = jar + al * jp;
+        if (bil || v < 0.0) {
+          double dq = dr * jp;
+          d1 += dq * v;
+          d2 += dq * jp;
+        }
+      }
+      *d1o = (al * mpp + mpg) + T.sum(d1);
+      *d2o = mpp + T.sum(d2);
+    };
+    double lo = 0.0, hi = INFINITY, al = 1.0;
+    double d10, d20;
+    deriv(0.0, &d10, &d20);
+    double ltol = 1e-12 * fmax(fabs(d10), 1e-30);
+    for (int it = 0; it < 50; it++) {
+      double d1, d2;
+      deriv(al, &d1, &d2);
+      if (fabs(d1) <= ltol) break;
+      if (d1 < 0.0) lo = al;
+      else hi = al;
+      double next = al - d1 / fmax(d2, 1e-30);
+      if (next <= lo || next >= hi) next = isfinite(hi) ? 0.5 * (lo + hi) : 2.0 * fmax(al, lo);
+      if (fabs(next - al) <= 1e-14 * fmax(fabs(al), 1.0)) {
+        al = next;
+        break;
+      }
+      al = next;
+    }
+    ai += al * p;
+  }
+  // qfrc_constraint += -D (J a - aref) J' over active rows (newton.rs:361-371)
+  publish(ai);
+  double f = 0.0;
+  if (rowl) {
+    double v = dot_ref_sm(Jr, B.x, k) - aref;
+    f = (bil || v < 0.0) ? -dr * v : 0.0;
+  }
+  coeffs(f);
+  if (dof) {
+    double q = qfrc[i];
+    for (int r = 0; r < nr; r++) {
+      double cf = B.c[r];
+      if (cf != 0.0) q += cf * B.J[r * k + i];
+    }
+    qfrc[i] = q;
+    a[i] = ai;
+  }
+  T.sync();
+  return iters;
 }
 
 // newton.rs:391-473 for models with several dof blocks: islands are the
@@ -581,6 +760,12 @@ __device__ int newton_solve(const Tile<G>& T, const DModel& m, const WsLayout& w
   bool nz = false;
   for (int t = lane; t < nr * nv; t += G) nz |= J[t] != 0.0;
   if (!T.any(nz)) return 0;
+  if constexpr (G >= SMALL_N) {
+    if (nv <= SMALL_N && nr <= SMALL_N && w.sj >= 0) {
+      SmallBufs S{ws + w.sj, ws + w.sl, ws + w.sx, ws + w.sc};
+      return newton_small(T, nv, nr, J, R, ws + w.qm, a, warm, m.iterations, m.tolerance, S, qfrc);
+    }
+  }
   int it = newton_dense(T, nv, nr, J, R, ws + w.qm, a, warm, m.iterations, m.tolerance, B);
   add_constraint_force(T, nv, nr, J, R, a, (const int*)nullptr, qfrc);
   return it;
@@ -613,7 +798,7 @@ __device__ bool factor_mass(const Tile<G>& T, const DModel& m, const WsLayout& w
     }
   }
   T.sync();
-  return chol_blocks(T, F, nv, nv, m.nblock, m.block_adr, m.dof_block, m.maxbs, ws + w.rinv);
+  return chol_auto(T, F, nv, nv, m.nblock, m.block_adr, m.dof_block, m.maxbs, ws + w.rinv);
 }
 
 // forward.rs:454-456
