@@ -517,6 +517,7 @@ void pgs_solve(const Model& m, Data& d, Real* v, std::vector<Real>& v_pos) {
   d.nrows_last = nr;
   v_pos.assign(v, v + nv);
   if (nr == 0) {
+    d.newton_iters = 0;
     std::fill(d.qfrc_constraint.begin(), d.qfrc_constraint.end(), 0.0);
     d.prev_contacts.clear();
     d.prev_lambda.clear();
@@ -601,11 +602,17 @@ void pgs_solve(const Model& m, Data& d, Real* v, std::vector<Real>& v_pos) {
     }
     return max_dv;
   };
-  for (int it = 0; it < opt.iterations; it++)
+  int sweeps = 0;
+  for (int it = 0; it < opt.iterations; it++) {
+    sweeps++;
     if (iterate(true) < PGS_TOLERANCE) break;
+  }
   v_pos.assign(v, v + nv);
-  for (int it = 0; it < std::max(opt.iterations / 3, 2); it++)
+  for (int it = 0; it < std::max(opt.iterations / 3, 2); it++) {
+    sweeps++;
     if (iterate(false) < PGS_TOLERANCE) break;
+  }
+  d.newton_iters = sweeps;  // reported as the solver's iteration count
 
   std::fill(d.qfrc_constraint.begin(), d.qfrc_constraint.end(), 0.0);
   for (int r = 0; r < nr; r++)

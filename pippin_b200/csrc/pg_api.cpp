@@ -369,6 +369,8 @@ struct Handle {
   double* scratch = nullptr;
   size_t scratch_tiles = 0;
   double* work = nullptr;  // [env][k.stride]
+  double* prev_con = nullptr;   // [env][maxcon][P_STRIDE] PGS warm start (allocated with PGS)
+  int32_t* prev_ncon = nullptr;  // [env]
   int* queue = nullptr;
   std::vector<double> base_params;
   int warm_mode = WARM_REF_PREV_QACC;
@@ -433,8 +435,8 @@ StepArgs make_args(Handle* h) {
   a.st.ncon = h->ncon;
   a.st.nrows = h->nrows;
   a.st.status = h->status;
-  a.st.prev_con = nullptr;
-  a.st.prev_ncon = nullptr;
+  a.st.prev_con = h->prev_con;
+  a.st.prev_ncon = h->prev_ncon;
   a.scratch = h->scratch;
   a.queue = h->queue;
   a.warm_mode = h->warm_mode;
@@ -552,6 +554,7 @@ void layouts(const HostModel& m, int maxcon, int maxrows, WsLayout* w, WsLayout*
   s->isl_dof = take(nv + 2);
   s->isl_row = take(maxrows + (nv + maxrows + 1) / 2 + 2);
   s->isl_of_row = take(maxrows / 2 + 2);
+  s->mj = take(maxrows * nv);
   s->stride = off;
 }
 
@@ -1046,7 +1049,7 @@ void destroy(pg_handle* h) {
   cudaSetDevice(h->device);
   clear_graphs(h);
   void* ptrs[] = {h->d_model, h->qpos, h->qvel, h->ctrl, h->qacc, h->applied, h->params, h->iters, h->ncon,
-                  h->nrows, h->status, h->scratch, h->work, h->queue, h->b_ctrl.p, h->b_qout.p, h->b_poses_g.p,
+                  h->nrows, h->status, h->scratch, h->work, h->prev_con, h->prev_ncon, h->queue, h->b_ctrl.p, h->b_qout.p, h->b_poses_g.p,
                   h->b_poses_c.p, h->b_dbg.p, h->b_vals.p, h->b_ids.p};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -1162,6 +1165,8 @@ int pg_create(const void* blob, size_t bytes, int64_t n_envs, int device, pg_han
   rc = set_const_range(h.get(), 0, n_envs);
   if (rc) return rc;
   CK(cudaStreamSynchronize(h->stream));
+  // a model compiled for PGS gets its warm-start buffers now
+  if (h->dm.solver == SOLVER_PGS && (rc = pg_set_solver(h.get(), SOLVER_PGS, -1, -1.0, -1))) return rc;
   *out = h.release();
   return PG_OK;
 }
@@ -1495,7 +1500,15 @@ int pg_name_of(const pg_handle* h, int table, int64_t id, char* buf, size_t len)
 int pg_set_solver(pg_handle* h, int kind, int max_iter, double tolerance, int warm_mode) {
   if (!h) return fail(PG_ERR_INVALID, "NULL handle");
   if (kind > 1 || warm_mode > 2) return fail(PG_ERR_INVALID, "unknown solver or warm-start mode");
-  if (kind == PG_SOLVER_PGS) return fail(PG_ERR_UNSUPPORTED, "PGS is not available in this build");
+  if (kind == PG_SOLVER_PGS && !h->prev_con && h->n > 0) {
+    // the previous step's contacts and impulses of every env (solver.rs:254-289)
+    CK(cudaSetDevice(h->device));
+    size_t per = (size_t)std::max(h->dm.maxcon, 1) * P_STRIDE;
+    CK(cudaMalloc(&h->prev_con, sizeof(double) * per * h->n));
+    CK(cudaMalloc(&h->prev_ncon, sizeof(int32_t) * h->n));
+    CK(cudaMemsetAsync(h->prev_ncon, 0, sizeof(int32_t) * h->n, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+  }
   if (warm_mode == PG_WARM_LEARNED) return fail(PG_ERR_UNSUPPORTED, "no learned warm start is loaded");
   if (kind >= 0) h->dm.solver = kind;
   if (max_iter >= 0) h->dm.iterations = max_iter;

@@ -18,7 +18,7 @@
 #include <cuda_runtime.h>
 
 #include "pg_kernels.h"
-#include "pg_newton.cuh"
+#include "pg_pgs.cuh"
 
 namespace pg {
 
@@ -134,7 +134,9 @@ __global__ void __launch_bounds__(256) smooth_kernel(const __grid_constant__ Ste
       solve_auto(T, ws + w.fac, nv, nv, m.nblock, m.block_adr, m.dof_block, m.maxbs, ws + w.rinv, acc);
       copy_in(T, wk + A.k.a0, acc, nv);
       copy_in(T, wk + A.k.smooth, smooth, nv);
-      if (damped) {
+      // the factor of M + hD: for the damped solve after Newton, and always
+      // for PGS (forward.rs:366-368), which factors M + hD even with D = 0
+      if (damped || m.solver == SOLVER_PGS) {
         T.sync();
         if (factor_mass(T, m, w, e, h)) {
           copy_in(T, wk + A.k.lh, ws + w.fac, nv * nv);
@@ -224,27 +226,45 @@ __global__ void __launch_bounds__(256) newton_kernel(const __grid_constant__ Ste
       load_async(T, ws + w.smooth, wk + A.k.smooth, nv);
       load_wait();
       T.sync();
-      nr = build_rows(T, m, w, A.s, e, ncon, &status);
-      const double* warm = A.warm_mode == WARM_COLD ? nullptr : ws + w.qacc;
       double* acc = ws + w.acc;
-      iters = newton_solve(T, m, w, A.s, e, nr, acc, warm);
-      if (wk[A.k.meta + K_META_DAMPED] != 0.0) {
+      double* v = ws + w.vel;
+      double* vpos = v;
+      double* qvel = ws + w.qvel;
+      if (m.solver == SOLVER_PGS) {
+        // forward.rs:366-375: velocities through M + hD, then PGS on them
         load_async(T, ws + w.fac, wk + A.k.lh, nv * nv);
         load_async(T, ws + w.rinv, wk + A.k.rinvh, nv);
-        for (int k = T.lane(); k < nv; k += G) acc[k] = ws[w.smooth + k] + ws[w.qfrc_c + k];
+        for (int k = T.lane(); k < nv; k += G) acc[k] = ws[w.smooth + k];
         load_wait();
         T.sync();
         solve_auto(T, ws + w.fac, nv, nv, m.nblock, m.block_adr, m.dof_block, m.maxbs, ws + w.rinv, acc);
+        for (int k = T.lane(); k < nv; k += G) v[k] = qvel[k] + h * acc[k];
+        T.sync();
+        vpos = ws + w.tmp;
+        iters = pgs_solve(T, m, w, A.s, e, ncon, v, vpos, ws + w.fac, A.st.prev_con + env * m.maxcon * P_STRIDE,
+                          A.st.prev_ncon + env, &nr, &status);
+        for (int k = T.lane(); k < nv; k += G) ws[w.qacc + k] = (v[k] - qvel[k]) / h;
+        T.sync();
+      } else {
+        nr = build_rows(T, m, w, A.s, e, ncon, &status);
+        const double* warm = A.warm_mode == WARM_COLD ? nullptr : ws + w.qacc;
+        iters = newton_solve(T, m, w, A.s, e, nr, acc, warm);
+        if (wk[A.k.meta + K_META_DAMPED] != 0.0) {
+          load_async(T, ws + w.fac, wk + A.k.lh, nv * nv);
+          load_async(T, ws + w.rinv, wk + A.k.rinvh, nv);
+          for (int k = T.lane(); k < nv; k += G) acc[k] = ws[w.smooth + k] + ws[w.qfrc_c + k];
+          load_wait();
+          T.sync();
+          solve_auto(T, ws + w.fac, nv, nv, m.nblock, m.block_adr, m.dof_block, m.maxbs, ws + w.rinv, acc);
+        }
+        for (int k = T.lane(); k < nv; k += G) {
+          double vk = qvel[k] + h * acc[k];
+          v[k] = vk;
+          ws[w.qacc + k] = (vk - qvel[k]) / h;
+        }
+        T.sync();
       }
-      double* v = ws + w.vel;
-      double* qvel = ws + w.qvel;
-      for (int k = T.lane(); k < nv; k += G) {
-        double vk = qvel[k] + h * acc[k];
-        v[k] = vk;
-        ws[w.qacc + k] = (vk - qvel[k]) / h;
-      }
-      T.sync();
-      integrate_pos(T, m, ws + w.qpos, v, h);
+      integrate_pos(T, m, ws + w.qpos, vpos, h);
       copy_in(T, A.st.qpos + env * nq, ws + w.qpos, nq);
       copy_in(T, A.st.qvel + env * nv, v, nv);
       copy_in(T, A.st.qacc + env * nv, ws + w.qacc, nv);

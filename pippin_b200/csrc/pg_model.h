@@ -157,6 +157,7 @@ struct ScrLayout {
   int isl_dof;   // nv ints stored as doubles
   int isl_row;   // maxrows
   int isl_of_row;
+  int mj;        // maxrows * nv   (PGS: M^-1 J' rows)
   int stride;
 };
 
@@ -185,7 +186,12 @@ struct EnvState {
   double* prev_con;  // [env][maxcon][P_STRIDE]
   int32_t* prev_ncon;
 };
-enum { P_POS = 0, P_NORMAL = 3, P_TANGENT = 6, P_G1 = 9, P_G2 = 10, P_LAMBDA = 11, P_STRIDE = 14 };
+// previous-step contact (PGS warm start): position, friction frame, geoms,
+// impulses (normal, tangent 1, tangent 2)
+enum { P_POS = 0, P_T1 = 3, P_T2 = 6, P_G1 = 9, P_G2 = 10, P_LAMBDA = 11, P_STRIDE = 14 };
+// PGS row record in tile scratch (doubles; solver.rs:18-36)
+enum { PR_KIND = 0, PR_SEP = 1, PR_MU = 2, PR_NORMAL = 3, PR_CONTACT = 4, PR_INVA = 5, PR_LAMBDA = 6, PR_STRIDE = 8 };
+enum { PK_NORMAL = 0, PK_FRICTION = 1, PK_BILATERAL = 2 };
 
 constexpr int MAX_PTR_FIELDS = 80;
 
