@@ -37,7 +37,7 @@ static void segment(const GeomPose& g, Vec3* p0, Vec3* p1) {
 }
 
 // collision.rs:154-162
-static Vec3 closest_on_segment(Vec3 a, Vec3 b, Vec3 p) {
+Vec3 closest_on_segment(Vec3 a, Vec3 b, Vec3 p) {
   Vec3 d = b - a;
   Real l2 = norm2(d);
   if (l2 < 1e-18) return a;
@@ -46,7 +46,7 @@ static Vec3 closest_on_segment(Vec3 a, Vec3 b, Vec3 p) {
 }
 
 // collision.rs:165-201
-static void closest_segments(Vec3 p0, Vec3 p1, Vec3 q0, Vec3 q1, Vec3* x, Vec3* y) {
+void closest_segments(Vec3 p0, Vec3 p1, Vec3 q0, Vec3 q1, Vec3* x, Vec3* y) {
   Vec3 d1 = p1 - p0, d2 = q1 - q0, r = p0 - q0;
   Real a = norm2(d1), e = norm2(d2), f = dot(d2, r);
   Real s, t;
@@ -91,11 +91,7 @@ static void plane_sphere(const GeomPose& plane, Vec3 c, Real r, Real margin, std
   if (depth > -margin) out.push_back(mkhit(c - (n * (dist + r)) * 0.5, n, depth));
 }
 
-struct DistPt {
-  Real d;
-  Vec3 p;
-};
-static void stable_sort_dist(std::vector<DistPt>& v) {
+void stable_sort_dist(std::vector<DistPt>& v) {
   std::stable_sort(v.begin(), v.end(), [](const DistPt& a, const DistPt& b) { return a.d < b.d; });
 }
 
@@ -248,7 +244,7 @@ static void capsule_box(const GeomPose& a, const GeomPose& b, Real margin, std::
 }
 
 // collision.rs:496-511: Sutherland-Hodgman, keep pn.p <= off
-static std::vector<Vec3> clip(const std::vector<Vec3>& poly, Vec3 pn, Real off) {
+std::vector<Vec3> clip(const std::vector<Vec3>& poly, Vec3 pn, Real off) {
   std::vector<Vec3> out;
   size_t n = poly.size();
   for (size_t i = 0; i < n; i++) {
@@ -261,7 +257,7 @@ static std::vector<Vec3> clip(const std::vector<Vec3>& poly, Vec3 pn, Real off) 
 }
 
 // collision.rs:514-531
-static void reduce_to_four(std::vector<DistPt>& pts) {
+void reduce_to_four(std::vector<DistPt>& pts) {
   if (pts.size() <= 4) return;
   std::vector<DistPt> keep;
   DistPt deepest = pts[0];  // min_by: first minimum

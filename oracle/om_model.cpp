@@ -300,6 +300,34 @@ std::shared_ptr<Model> load_blob(const void* p, size_t bytes, std::string* err) 
       m.mesh_hull[i].tri.push_back({(int)htri[a], (int)htri[a + 1], (int)htri[a + 2]});
     }
   }
+  std::vector<int64_t> hfa, hfn, hfva, hfvn, hfv, hea, hen, he;
+  std::vector<Real> hfp;
+  if (!b.i64("hull_face_adr", hfa, nmesh) || !b.i64("hull_face_num", hfn, nmesh) || !b.f64("hull_face_plane", hfp) ||
+      !b.i64("hull_face_vert_adr", hfva) || !b.i64("hull_face_vert_num", hfvn) || !b.i64("hull_face_vert", hfv) ||
+      !b.i64("hull_edge_adr", hea, nmesh) || !b.i64("hull_edge_num", hen, nmesh) || !b.i64("hull_edge", he))
+    return fail();
+  for (long i = 0; i < nmesh; i++) {
+    Hull& h = m.mesh_hull[i];
+    long nv = (long)h.vert.size();
+    for (long f = hfa[i]; f < hfa[i] + hfn[i]; f++) {
+      if (f < 0 || 4 * f + 3 >= (long)hfp.size() || f >= (long)hfva.size() || f >= (long)hfvn.size()) return fail();
+      h.face_n.push_back(v3(hfp[4 * f], hfp[4 * f + 1], hfp[4 * f + 2]));
+      h.face_d.push_back(hfp[4 * f + 3]);
+      std::vector<int> loop;
+      for (long k = 0; k < hfvn[f]; k++) {
+        long at = hfva[f] + k;
+        if (at < 0 || at >= (long)hfv.size() || hfv[at] < 0 || hfv[at] >= nv) return fail();
+        loop.push_back((int)hfv[at]);
+      }
+      h.face_loop.push_back(loop);
+    }
+    for (long e = hea[i]; e < hea[i] + hen[i]; e++) {
+      if (e < 0 || 2 * e + 1 >= (long)he.size() || he[2 * e] < 0 || he[2 * e] >= nv || he[2 * e + 1] < 0 ||
+          he[2 * e + 1] >= nv)
+        return fail();
+      h.edge.push_back({(int)he[2 * e], (int)he[2 * e + 1]});
+    }
+  }
 
   // derived geometry (model.rs:279-316)
   m.geom_rbound.resize(ng);

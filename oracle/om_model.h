@@ -40,6 +40,12 @@ struct SolverOptions {
 struct Hull {  // convex hull of a mesh geom (vertices in the geom frame)
   std::vector<Vec3> vert;
   std::vector<std::array<int, 3>> tri;
+  // polygon faces (outward normal, offset, counter-clockwise vertex loop)
+  // and unique edges, for the general convex narrow phase
+  std::vector<Vec3> face_n;
+  std::vector<Real> face_d;
+  std::vector<std::vector<int>> face_loop;
+  std::vector<std::array<int, 2>> edge;
 };
 
 // model.rs:103-249 (fields the step path reads; names and layouts match)
@@ -198,6 +204,16 @@ struct GeomPose {
   const Hull* hull;
 };
 void collide_pair(const GeomPose& a, const GeomPose& b, Real margin, std::vector<Hit>& out);
+// narrow-phase helpers shared by the primitive and general paths
+struct DistPt {
+  Real d;
+  Vec3 p;
+};
+Vec3 closest_on_segment(Vec3 a, Vec3 b, Vec3 p);
+void closest_segments(Vec3 p0, Vec3 p1, Vec3 q0, Vec3 q1, Vec3* x, Vec3* y);
+std::vector<Vec3> clip(const std::vector<Vec3>& poly, Vec3 pn, Real off);
+void reduce_to_four(std::vector<DistPt>& pts);
+void stable_sort_dist(std::vector<DistPt>& v);
 bool needs_general(int a, int b);
 void collide_general(const GeomPose& a, const GeomPose& b, Real margin, std::vector<Hit>& out);
 

@@ -231,6 +231,53 @@ def convex_hull(points: List[Tuple[float, float, float]]):
     return verts, tris
 
 
+def hull_features(verts, tris):
+    """Polygon faces and edges of a convex hull given as outward triangles.
+
+    Coplanar triangles merge into one face: (outward unit normal, offset d
+    with n . v <= d inside, vertex loop counter-clockwise seen from outside).
+    Edges are the unique vertex pairs that bound two different faces. The
+    general convex narrow phase clips against these polygons and tests their
+    edge directions.
+    """
+    import numpy as np
+
+    v = np.asarray(verts, dtype=np.float64)
+    scale = float(np.abs(v).max()) if len(v) else 1.0
+    tol = 1e-10 * max(scale, 1.0)
+    planes = []
+    for a, b, c in tris:
+        n = np.cross(v[b] - v[a], v[c] - v[a])
+        ln = float(np.linalg.norm(n))
+        n = n / ln if ln > 0 else n
+        planes.append((n, float(n @ v[a])))
+    group = [-1] * len(tris)
+    faces = []
+    for t in range(len(tris)):
+        if group[t] != -1:
+            continue
+        n0, d0 = planes[t]
+        members = [u for u in range(len(tris)) if group[u] == -1 and
+                   float(planes[u][0] @ n0) > 1.0 - 1e-10 and abs(planes[u][1] - d0) <= tol]
+        for u in members:
+            group[u] = len(faces)
+        directed = set()
+        for u in members:
+            a, b, c = tris[u]
+            directed.update(((a, b), (b, c), (c, a)))
+        nxt = {a: b for a, b in directed if (b, a) not in directed}
+        start = min(nxt)
+        loop = [start]
+        while nxt[loop[-1]] != start:
+            loop.append(nxt[loop[-1]])
+            if len(loop) > len(nxt):
+                raise MjcfError("hull face boundary is not a single loop")
+        faces.append((tuple(float(x) for x in n0), d0, loop))
+    edges = sorted({(min(a, b), max(a, b)) for _, _, loop in faces
+                    for a, b in zip(loop, loop[1:] + loop[:1])})
+    return faces, edges
+
+
 def mesh_mass_properties(verts, tris):
     """Volume, com, inertia about com per unit density (mesh.rs:71-105)."""
     vol = 0.0
@@ -1270,6 +1317,29 @@ def to_blob(m: Model) -> bytes:
         i(f"{pre}_tri_adr", ta)
         i(f"{pre}_tri_num", tn)
         i(f"{pre}_tri", flat_t)
+    # polygon faces and edges of each hull (general convex narrow phase)
+    fa, fn, fplane, fva, fvn, fverts, ea, en, flat_e = [], [], [], [], [], [], [], [], []
+    for v, t in zip(m.hull_vert, m.hull_tri):
+        faces, edges = hull_features(v, t)
+        fa.append(len(fplane) // 4)
+        fn.append(len(faces))
+        for nrm, d, loop in faces:
+            fplane.extend([nrm[0], nrm[1], nrm[2], d])
+            fva.append(len(fverts))
+            fvn.append(len(loop))
+            fverts.extend(loop)
+        ea.append(len(flat_e) // 2)
+        en.append(len(edges))
+        flat_e.extend(_flat(edges))
+    i("hull_face_adr", fa)
+    i("hull_face_num", fn)
+    f("hull_face_plane", fplane)
+    i("hull_face_vert_adr", fva)
+    i("hull_face_vert_num", fvn)
+    i("hull_face_vert", fverts)
+    i("hull_edge_adr", ea)
+    i("hull_edge_num", en)
+    i("hull_edge", flat_e)
     names("names_body", m.body_names)
     names("names_jnt", m.jnt_names)
     names("names_geom", m.geom_names)

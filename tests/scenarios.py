@@ -289,6 +289,61 @@ def check_invalid_params_rejected(make, error):
     assert list(out[:, 0]) == [0.1, 0.1]
 
 
+# ---- crates/pippin/tests/mesh.rs (the general convex narrow phase)
+CUBE = ("-0.05 -0.05 -0.05  0.05 -0.05 -0.05  -0.05 0.05 -0.05  0.05 0.05 -0.05 "
+        "-0.05 -0.05 0.05  0.05 -0.05 0.05  -0.05 0.05 0.05  0.05 0.05 0.05")
+MESH_AND_BOX = ('<mujoco><asset><mesh name="cube" vertex="' + CUBE + '"/></asset><worldbody>'
+                '<geom type="plane" size="5 5 .1"/>'
+                '<body name="m" pos="0 0 0.3" euler="4 7 0"><freejoint/><geom type="mesh" mesh="cube"/></body>'
+                '<body name="b" pos="1 0 0.3" euler="4 7 0"><freejoint/><geom type="box" size=".05 .05 .05"/></body>'
+                '</worldbody></mujoco>')
+
+
+def mesh_stack_xml(n=4):
+    xml = ('<mujoco><asset><mesh name="cube" vertex="' + CUBE + '"/></asset><worldbody>'
+           '<geom type="plane" size="5 5 .1"/>')
+    for i in range(n):
+        xml += (f'<body name="c{i}" pos="0 0 {0.05 + 0.101 * i}" euler="0 0 {9 * i}"><freejoint/>'
+                '<geom type="mesh" mesh="cube"/></body>')
+    return xml + '</worldbody></mujoco>'
+
+
+CYLINDERS = ('<mujoco><worldbody><geom type="box" size="1 1 .1" pos="0 0 -.1"/>'
+             '<body name="up" pos="0 0 0.3"><freejoint/><geom type="cylinder" size=".04 .06"/></body>'
+             '<body name="side" pos="0.5 0 0.3" euler="90 0 0"><freejoint/><geom type="cylinder" size=".04 .06"/></body>'
+             '<body name="onup" pos="0 0 0.5"><freejoint/><geom type="cylinder" size=".03 .03"/></body>'
+             '</worldbody></mujoco>')
+
+
+def check_mesh_cube_rests_like_box(make, solver):
+    """mesh.rs:24-45"""
+    s = make(MESH_AND_BOX, 1, solver)
+    s.step(steps(s, 3.0))
+    zm, zb = free_body_pos(s, "m")[2], free_body_pos(s, "b")[2]
+    assert abs(zm - zb) < 1e-3, (zm, zb)
+    assert abs(zm - 0.05) < 2e-3, zm
+    assert np.linalg.norm(s.qvel()[0]) < 1e-3, np.linalg.norm(s.qvel()[0])
+
+
+def check_mesh_cubes_stack(make, solver):
+    """mesh.rs:47-64"""
+    s = make(mesh_stack_xml(), 1, solver)
+    s.step(steps(s, 5.0))
+    top = free_body_pos(s, "c3")
+    assert abs(top[0]) < 5e-3 and abs(top[1]) < 5e-3, top
+    assert abs(top[2] - 0.35) < 1e-2, top
+
+
+def check_cylinders_rest(make, solver):
+    """mesh.rs:66-82"""
+    s = make(CYLINDERS, 1, solver)
+    s.step(steps(s, 3.0))
+    assert abs(free_body_pos(s, "up")[2] - 0.06) < 2e-3, free_body_pos(s, "up")
+    assert abs(free_body_pos(s, "side")[2] - 0.04) < 2e-3, free_body_pos(s, "side")
+    assert abs(free_body_pos(s, "onup")[2] - 0.15) < 3e-3, free_body_pos(s, "onup")
+
+
+GENERAL_CHECKS = [check_mesh_cube_rests_like_box, check_mesh_cubes_stack, check_cylinders_rest]
 CONTACT_CHECKS = [check_box_rests_on_plane, check_sphere_and_capsule_rest, check_box_stack_is_stable,
                   check_friction_holds, check_friction_slides, check_joint_limit, check_shapes_on_box]
 PARAM_CHECKS = [check_friction_per_env, check_size_and_parking, check_mass_per_env]

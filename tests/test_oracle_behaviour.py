@@ -1,6 +1,7 @@
 """The oracle against the reference's behavioural integration tests
-(crates/pippin/tests/contact.rs, crates/pippin-env/tests/params.rs), both
-constraint solvers, plus the rollout/step-loop and reset-reference checks."""
+(crates/pippin/tests/contact.rs, crates/pippin/tests/mesh.rs,
+crates/pippin-env/tests/params.rs), both constraint solvers, plus the
+rollout/step-loop and reset-reference checks."""
 import numpy as np
 import pytest
 
@@ -11,6 +12,12 @@ from tests import scenarios as S
 @pytest.mark.parametrize("solver", [S.NEWTON, S.PGS], ids=["newton", "pgs"])
 @pytest.mark.parametrize("check", S.CONTACT_CHECKS, ids=lambda f: f.__name__)
 def test_contact_behaviour(oracle_lib, check, solver):
+    check(S.OracleSim, solver)
+
+
+@pytest.mark.parametrize("solver", [S.NEWTON, S.PGS], ids=["newton", "pgs"])
+@pytest.mark.parametrize("check", S.GENERAL_CHECKS, ids=lambda f: f.__name__)
+def test_general_convex_behaviour(oracle_lib, check, solver):
     check(S.OracleSim, solver)
 
 
