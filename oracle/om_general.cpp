@@ -166,19 +166,24 @@ static Real closest_point(const Polytope& p, Vec3 x, Vec3* q, int* inside_face) 
   return bd;
 }
 
-// largest separation of b beyond a face of a: (separation, face)
+// Choices between candidates whose values tie up to rounding take the first
+// one within TIE of the best, so that rounding-level differences between
+// two implementations cannot change the contacts.
+static const Real TIE = 1e-10;
+
+// largest separation of b beyond a face of a: (separation, first face
+// within TIE of it)
 static Real face_query(const Polytope& a, const Polytope& b, int* face) {
+  std::vector<Real> sep(a.fn.size());
   Real best = -INFINITY;
-  *face = -1;
   for (size_t f = 0; f < a.fn.size(); f++) {
     Real mn = INFINITY;
     for (const Vec3& x : b.v) mn = rmin(mn, dot(a.fn[f], x));
-    Real s = mn - a.fd[f];
-    if (s > best) {
-      best = s;
-      *face = (int)f;
-    }
+    sep[f] = mn - a.fd[f];
+    best = rmax(best, sep[f]);
   }
+  *face = 0;
+  while (*face + 1 < (int)sep.size() && sep[*face] < best - TIE) (*face)++;
   return best;
 }
 
@@ -228,21 +233,45 @@ static Vec3 centroid(const Polytope& p) {
 
 static Hit hit(Vec3 pos, Vec3 n, Real depth) { return Hit{pos, n, depth, v3zero()}; }
 
+// reduce_to_four's choices (collision.rs:514-531: the deepest point, then
+// the farthest from it, the farthest from their line, the most isolated),
+// each taken within TIE: the first minimum, the last maximum. A clipped
+// regular polygon (a cylinder cap) offers many exact ties.
+static void reduce_to_four_tie(std::vector<DistPt>& pts) {
+  if (pts.size() <= 4) return;
+  auto last_max = [&](auto key) {
+    Real mx = -INFINITY;
+    for (auto& p : pts) mx = rmax(mx, key(p.p));
+    size_t bi = 0;
+    for (size_t i = 0; i < pts.size(); i++)
+      if (key(pts[i].p) >= mx - TIE) bi = i;
+    return pts[bi];
+  };
+  Real mn = INFINITY;
+  for (auto& p : pts) mn = rmin(mn, p.d);
+  size_t di = 0;
+  while (pts[di].d > mn + TIE) di++;
+  std::vector<DistPt> keep{pts[di]};
+  keep.push_back(last_max([&](Vec3 p) { return norm2(p - keep[0].p); }));
+  keep.push_back(last_max([&](Vec3 p) { return norm(cross(keep[1].p - keep[0].p, p - keep[0].p)); }));
+  keep.push_back(last_max([&](Vec3 p) {
+    Real s = INFINITY;
+    for (auto& k : keep) s = rmin(s, norm(k.p - p));
+    return s;
+  }));
+  pts = keep;
+}
+
 // reference face `rf` of polytope r (outward normal nref toward the other
 // shape), incident polytope s: clip s's most anti-parallel face against the
 // side planes of rf and keep the points within the margin (up to four);
 // normals point along `n` (a to b)
 static void clip_faces(const Polytope& r, int rf, const Polytope& s, Vec3 n, Real margin, std::vector<Hit>& out) {
   Vec3 nref = r.fn[rf];
-  int inc = 0;
   Real mn = INFINITY;
-  for (size_t f = 0; f < s.fn.size(); f++) {
-    Real d = dot(s.fn[f], nref);
-    if (d < mn) {
-      mn = d;
-      inc = (int)f;
-    }
-  }
+  for (size_t f = 0; f < s.fn.size(); f++) mn = rmin(mn, dot(s.fn[f], nref));
+  int inc = 0;
+  while (inc + 1 < (int)s.fn.size() && dot(s.fn[inc], nref) > mn + TIE) inc++;
   std::vector<Vec3> poly;
   for (int k : s.loop[inc]) poly.push_back(s.v[k]);
   const auto& l = r.loop[rf];
@@ -257,7 +286,7 @@ static void clip_faces(const Polytope& r, int rf, const Polytope& s, Vec3 n, Rea
     Real sep = dot(p, nref) - r.fd[rf];
     if (sep < margin) pts.push_back({sep, p});
   }
-  reduce_to_four(pts);
+  reduce_to_four_tie(pts);
   for (auto& p : pts) out.push_back(hit(p.p - nref * (p.d * 0.5), n, -p.d));
 }
 
@@ -273,7 +302,7 @@ static void polytope_polytope(const Polytope& a, const Polytope& b, Real margin,
   // overlaps; the shallowest axis wins, a face axis unless an edge axis is
   // clearly shallower (collision.rs:430-436)
   Real oa = -sa, ob = -sb, oe = -se;
-  bool face_a = oa <= ob;
+  bool face_a = !(ob < oa - TIE);
   Real of = face_a ? oa : ob;
   if (ea >= 0 && oe < of && !(of < oe * 1.05 + 1e-4)) {
     Vec3 pa = a.v[a.edge[ea][0]], qa = a.v[a.edge[ea][1]];

@@ -15,7 +15,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libpippin_b200.so")
 SOURCES = ["pg_kernels.cu", "pg_api.cpp", "pg_peak.cu", "pg_noalloc.cu"]
-HEADERS = ["pg_math.cuh", "pg_model.h", "pg_tile.cuh", "pg_dynamics.cuh", "pg_collide.cuh", "pg_linalg.cuh", "pg_small.cuh", "pg_pgs.cuh",
+HEADERS = ["pg_math.cuh", "pg_model.h", "pg_tile.cuh", "pg_dynamics.cuh", "pg_collide.cuh", "pg_linalg.cuh", "pg_small.cuh", "pg_pgs.cuh", "pg_general.cuh",
            "pg_newton.cuh", "pg_kernels.h"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
               "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]

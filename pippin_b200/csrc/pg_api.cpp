@@ -147,6 +147,9 @@ struct HostModel {
   std::vector<double> qpos0, qpos_reset;
   std::vector<int> hull_vadr, hull_vnum, hull_tadr, hull_tnum, hull_tri;
   std::vector<double> hull_vert;
+  // polygon faces (plane, vertex loop) and edges of each hull
+  std::vector<int> hull_fadr, hull_fnum, hull_fvadr, hull_fvnum, hull_fv, hull_eadr, hull_enum, hull_edge;
+  std::vector<double> hull_fplane;
   std::vector<int> mesh_vadr, mesh_vnum, mesh_tadr, mesh_tnum, mesh_tri;
   std::vector<double> mesh_vert;
   std::vector<std::string> names[6];  // body, geom, camera, mesh, joint, actuator
@@ -235,7 +238,12 @@ bool load_model(const void* blob, size_t bytes, HostModel& m, std::string* err) 
             b.get("hull_tri", 2, m.hull_tri, -1, err) && b.get("mesh_vert_adr", 2, m.mesh_vadr, nm, err) &&
             b.get("mesh_vert_num", 2, m.mesh_vnum, nm, err) && b.get("mesh_vert", 1, m.mesh_vert, -1, err) &&
             b.get("mesh_tri_adr", 2, m.mesh_tadr, nm, err) && b.get("mesh_tri_num", 2, m.mesh_tnum, nm, err) &&
-            b.get("mesh_tri", 2, m.mesh_tri, -1, err);
+            b.get("mesh_tri", 2, m.mesh_tri, -1, err) && b.get("hull_face_adr", 2, m.hull_fadr, nm, err) &&
+            b.get("hull_face_num", 2, m.hull_fnum, nm, err) && b.get("hull_face_plane", 1, m.hull_fplane, -1, err) &&
+            b.get("hull_face_vert_adr", 2, m.hull_fvadr, -1, err) &&
+            b.get("hull_face_vert_num", 2, m.hull_fvnum, -1, err) && b.get("hull_face_vert", 2, m.hull_fv, -1, err) &&
+            b.get("hull_edge_adr", 2, m.hull_eadr, nm, err) && b.get("hull_edge_num", 2, m.hull_enum, nm, err) &&
+            b.get("hull_edge", 2, m.hull_edge, -1, err);
   if (!ok) return false;
   const char* tables[6] = {"names_body", "names_geom", "names_cam", "names_mesh", "names_jnt", "names_actuator"};
   for (int t = 0; t < 6; t++) m.names[t] = b.names(tables[t]);
@@ -299,6 +307,24 @@ bool load_model(const void* blob, size_t bytes, HostModel& m, std::string* err) 
       int v = m.hull_tri[3 * m.hull_tadr[i] + t];
       if (v < 0 || v >= m.hull_vnum[i]) return bad("hull triangle vertex");
     }
+    // polygon faces: every loop within the hull's vertices and at most
+    // HULL_FACE_MAX long (the device clips in fixed buffers); edges likewise
+    long nf = (long)m.hull_fvadr.size(), nfv = (long)m.hull_fv.size(), ne = (long)m.hull_edge.size() / 2;
+    if ((long)m.hull_fvnum.size() != nf || (long)m.hull_fplane.size() != 4 * nf) return bad("hull faces");
+    if (m.hull_fadr[i] < 0 || m.hull_fnum[i] < 4 || (long)m.hull_fadr[i] + m.hull_fnum[i] > nf) return bad("hull faces");
+    for (int f = m.hull_fadr[i]; f < m.hull_fadr[i] + m.hull_fnum[i]; f++) {
+      if (m.hull_fvnum[f] < 3 || m.hull_fvnum[f] > HULL_FACE_MAX || m.hull_fvadr[f] < 0 ||
+          (long)m.hull_fvadr[f] + m.hull_fvnum[f] > nfv)
+        return bad("hull face loop (3 to 32 vertices)");
+      for (int k = 0; k < m.hull_fvnum[f]; k++) {
+        int v = m.hull_fv[m.hull_fvadr[f] + k];
+        if (v < 0 || v >= m.hull_vnum[i]) return bad("hull face vertex");
+      }
+    }
+    if (m.hull_eadr[i] < 0 || m.hull_enum[i] < 6 || (long)m.hull_eadr[i] + m.hull_enum[i] > ne) return bad("hull edges");
+    for (int e = m.hull_eadr[i]; e < m.hull_eadr[i] + m.hull_enum[i]; e++)
+      for (int k = 0; k < 2; k++)
+        if (m.hull_edge[2 * e + k] < 0 || m.hull_edge[2 * e + k] >= m.hull_vnum[i]) return bad("hull edge vertex");
     long nmv = (long)m.mesh_vert.size() / 3, nmt = (long)m.mesh_tri.size() / 3;
     if (m.mesh_vadr[i] < 0 || m.mesh_vnum[i] < 0 || m.mesh_vadr[i] + m.mesh_vnum[i] > nmv) return bad("mesh vertices");
     if (m.mesh_tadr[i] < 0 || m.mesh_tnum[i] < 0 || m.mesh_tadr[i] + m.mesh_tnum[i] > nmt) return bad("mesh triangles");
@@ -572,7 +598,8 @@ std::vector<int> dmodel_pointer_fields() {
   PF(act_ctrllimited); PF(act_ctrlrange); PF(act_forcelimited); PF(act_forcerange); PF(act_moment_adr);
   PF(act_moment_num); PF(moment_jnt); PF(moment_coef); PF(eq_j1); PF(eq_j2); PF(eq_poly); PF(eq_solref);
   PF(eq_solimp); PF(qpos0); PF(hull_vadr); PF(hull_vnum); PF(hull_vert); PF(hull_fadr); PF(hull_fnum);
-  PF(hull_face);
+  PF(hull_face); PF(hull_fvadr); PF(hull_fvnum); PF(hull_fv); PF(hull_eadr); PF(hull_enum); PF(hull_edge);
+  PF(hull_eface);
 #undef PF
   return o;
 }
@@ -868,26 +895,25 @@ int build_device_model(Handle* h) {
   for (int j = 0; j < m.njnt; j++)
     if (m.jnt_limited[j] && (m.jnt_type[j] == JNT_HINGE || m.jnt_type[j] == JNT_SLIDE)) nlim++;
   int maxrows = 4 * maxcon + 2 * nlim + m.neq;
-  // hull faces (outward normal, offset) from the triangles, for mesh geoms
-  std::vector<int> hull_fadr(std::max(m.nmesh, 1), 0), hull_fnum(std::max(m.nmesh, 1), 0);
-  std::vector<double> hull_face;
-  for (int i = 0; i < m.nmesh; i++) {
-    hull_fadr[i] = (int)hull_face.size() / 4;
-    for (int t = 0; t < m.hull_tnum[i]; t++) {
-      const int* tri = &m.hull_tri[3 * (m.hull_tadr[i] + t)];
-      const double* va = &m.hull_vert[3 * (m.hull_vadr[i] + tri[0])];
-      const double* vb = &m.hull_vert[3 * (m.hull_vadr[i] + tri[1])];
-      const double* vc = &m.hull_vert[3 * (m.hull_vadr[i] + tri[2])];
-      double e1[3] = {vb[0] - va[0], vb[1] - va[1], vb[2] - va[2]};
-      double e2[3] = {vc[0] - va[0], vc[1] - va[1], vc[2] - va[2]};
-      double n[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
-      double l = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
-      if (l <= 0) continue;
-      for (int k = 0; k < 3; k++) n[k] /= l;
-      hull_face.insert(hull_face.end(), {n[0], n[1], n[2], n[0] * va[0] + n[1] * va[1] + n[2] * va[2]});
-      hull_fnum[i]++;
+  // the two faces of each hull edge (the faces whose loops hold the edge),
+  // for the edge-pair pruning of the general convex narrow phase
+  std::vector<int> hull_eface(2 * m.hull_edge.size() / 2 + 2, -1);
+  for (int i = 0; i < m.nmesh; i++)
+    for (int e = m.hull_eadr[i]; e < m.hull_eadr[i] + m.hull_enum[i]; e++) {
+      int a = m.hull_edge[2 * e], b = m.hull_edge[2 * e + 1];
+      for (int f = 0; f < m.hull_fnum[i]; f++) {
+        int fg = m.hull_fadr[i] + f;
+        int n = m.hull_fvnum[fg];
+        const int* l = &m.hull_fv[m.hull_fvadr[fg]];
+        for (int k = 0; k < n; k++) {
+          int x = l[k], y = l[(k + 1) % n];
+          if ((x == a && y == b) || (x == b && y == a)) {
+            if (hull_eface[2 * e] == -1) hull_eface[2 * e] = f;
+            else if (hull_eface[2 * e + 1] == -1) hull_eface[2 * e + 1] = f;
+          }
+        }
+      }
     }
-  }
 
   d.nq = m.nq;
   d.nv = nv;
@@ -985,9 +1011,16 @@ int build_device_model(Handle* h) {
   ADDI(hull_vadr, m.hull_vadr);
   ADDI(hull_vnum, m.hull_vnum);
   ADDD(hull_vert, m.hull_vert);
-  ADDI(hull_fadr, hull_fadr);
-  ADDI(hull_fnum, hull_fnum);
-  ADDD(hull_face, hull_face);
+  ADDI(hull_fadr, m.hull_fadr);
+  ADDI(hull_fnum, m.hull_fnum);
+  ADDD(hull_face, m.hull_fplane);
+  ADDI(hull_fvadr, m.hull_fvadr);
+  ADDI(hull_fvnum, m.hull_fvnum);
+  ADDI(hull_fv, m.hull_fv);
+  ADDI(hull_eadr, m.hull_eadr);
+  ADDI(hull_enum, m.hull_enum);
+  ADDI(hull_edge, m.hull_edge);
+  ADDI(hull_eface, hull_eface);
 #undef ADDI
 #undef ADDD
   ar.host.resize((ar.host.size() + 15) & ~size_t(15));  // staged in 16-byte chunks

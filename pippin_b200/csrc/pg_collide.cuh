@@ -29,6 +29,7 @@ struct GPose {
   V3 pos;
   M3 mat;
   V3 size;
+  int data;  // mesh id of a mesh geom
 };
 
 __device__ inline void segment(const GPose& g, V3* p0, V3* p1) {

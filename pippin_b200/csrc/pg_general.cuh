@@ -1,0 +1,462 @@
+// General convex narrow phase on the device: the pairs the reference hands
+// to parry3d-f64 (crates/pippin/src/collision.rs:102-147): mesh (convex hull)
+// against anything, and cylinder against non-plane shapes. parry is an
+// un-vendored dependency; this path is this library's own algorithm, the
+// one the oracle restates (one lane per pair, FP64):
+//   box        8 vertices, 6 faces
+//   cylinder   a 16-sided prism (faces at distance r cos(pi/16) from the axis)
+//   mesh       its convex hull: polygon faces (at most HULL_FACE_MAX long) and
+//              edges from the model, with each edge's two faces
+//   sphere     a point of radius r;  capsule  a segment of radius r
+// Polytope pairs: separating axes over both shapes' face normals and the
+// cross products of edge pairs that form a face of the Minkowski difference
+// (the box-box test of collision.rs:383-493, generalised); a face axis wins
+// unless an edge axis is clearly shallower; an edge axis gives one contact at
+// the edges' closest points, a face axis clips the incident face against the
+// reference face's side planes (up to four points kept as reduce_to_four
+// picks them). Spheres and capsules against a polytope use its exact
+// closest point; a plane against a hull takes the four deepest vertices.
+#pragma once
+#include "pg_collide.cuh"
+
+namespace pg {
+
+constexpr int CYL_SIDES = 16;
+constexpr int GEN_CLIP_CAP = 2 * HULL_FACE_MAX;  // incident loop + one vertex per side plane
+
+// box faces (outward normals -z, +x, +y, -y, -x, +z), their loops, edges
+// (vertex i to i | bit) and each edge's two faces; vertex i has coordinate
+// signs (bit0, bit1, bit2) = (x, y, z) positive
+__constant__ int c_box_loop[6][4] = {{0, 2, 3, 1}, {1, 3, 7, 5}, {2, 6, 7, 3}, {0, 1, 5, 4}, {0, 4, 6, 2}, {4, 5, 7, 6}};
+__constant__ int c_box_edge[12][2] = {{0, 1}, {0, 2}, {0, 4}, {1, 3}, {1, 5}, {2, 3},
+                                      {2, 6}, {3, 7}, {4, 5}, {4, 6}, {5, 7}, {6, 7}};
+__constant__ int c_box_eface[12][2] = {{0, 3}, {0, 4}, {3, 4}, {0, 1}, {1, 3}, {0, 2},
+                                       {2, 4}, {1, 2}, {3, 5}, {4, 5}, {1, 5}, {2, 5}};
+__constant__ double c_box_normal[6][3] = {{0, 0, -1}, {1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {-1, 0, 0}, {0, 0, 1}};
+
+// A box, cylinder prism or hull in the world frame, read on demand.
+struct Poly {
+  int kind;
+  V3 pos;
+  M3 mat;
+  V3 size;
+  const DModel* m;
+  int mesh;
+};
+
+__device__ inline int p_nv(const Poly& p) {
+  return p.kind == GEOM_BOX ? 8 : p.kind == GEOM_CYLINDER ? 2 * CYL_SIDES : p.m->hull_vnum[p.mesh];
+}
+__device__ inline V3 p_v(const Poly& p, int i) {
+  if (p.kind == GEOM_BOX) {
+    V3 s{(i & 1) == 0 ? -1.0 : 1.0, (i & 2) == 0 ? -1.0 : 1.0, (i & 4) == 0 ? -1.0 : 1.0};
+    return p.pos + mv(p.mat, V3{p.size.x * s.x, p.size.y * s.y, p.size.z * s.z});
+  }
+  if (p.kind == GEOM_CYLINDER) {
+    int cap = i / CYL_SIDES, k = i % CYL_SIDES;
+    double th = 2.0 * M_PI * k / CYL_SIDES;
+    double r = p.size.x, h = p.size.y;
+    return p.pos + mv(p.mat, V3{r * cos(th), r * sin(th), cap ? h : -h});
+  }
+  return p.pos + mv(p.mat, ld3(p.m->hull_vert + 3 * (p.m->hull_vadr[p.mesh] + i)));
+}
+__device__ inline int p_nf(const Poly& p) {
+  return p.kind == GEOM_BOX ? 6 : p.kind == GEOM_CYLINDER ? CYL_SIDES + 2 : p.m->hull_fnum[p.mesh];
+}
+__device__ inline int p_fvn(const Poly& p, int f) {
+  if (p.kind == GEOM_BOX) return 4;
+  if (p.kind == GEOM_CYLINDER) return f < 2 ? CYL_SIDES : 4;
+  return p.m->hull_fvnum[p.m->hull_fadr[p.mesh] + f];
+}
+__device__ inline int p_fv(const Poly& p, int f, int k) {
+  if (p.kind == GEOM_BOX) return c_box_loop[f][k];
+  if (p.kind == GEOM_CYLINDER) {
+    const int K = CYL_SIDES;
+    if (f == 0) return (K - k) % K;
+    if (f == 1) return K + k;
+    int i = f - 2;
+    return k == 0 ? i : k == 1 ? (i + 1) % K : k == 2 ? K + (i + 1) % K : K + i;
+  }
+  return p.m->hull_fv[p.m->hull_fvadr[p.m->hull_fadr[p.mesh] + f] + k];
+}
+__device__ inline V3 p_fn(const Poly& p, int f) {
+  if (p.kind == GEOM_BOX) return mv(p.mat, V3{c_box_normal[f][0], c_box_normal[f][1], c_box_normal[f][2]});
+  if (p.kind == GEOM_CYLINDER) {
+    if (f < 2) return mv(p.mat, V3{0.0, 0.0, f == 0 ? -1.0 : 1.0});
+    double th = 2.0 * M_PI * ((f - 2) + 0.5) / CYL_SIDES;
+    return mv(p.mat, V3{cos(th), sin(th), 0.0});
+  }
+  return mv(p.mat, ld3(p.m->hull_face + 4 * (p.m->hull_fadr[p.mesh] + f)));
+}
+__device__ inline double p_fd(const Poly& p, int f, V3 n) {
+  if (p.kind == GEOM_MESH) return p.m->hull_face[4 * (p.m->hull_fadr[p.mesh] + f) + 3] + dot(n, p.pos);
+  return dot(n, p_v(p, p_fv(p, f, 0)));
+}
+__device__ inline int p_ne(const Poly& p) {
+  return p.kind == GEOM_BOX ? 12 : p.kind == GEOM_CYLINDER ? 3 * CYL_SIDES : p.m->hull_enum[p.mesh];
+}
+__device__ inline void p_edge(const Poly& p, int e, int* a, int* b) {
+  if (p.kind == GEOM_BOX) {
+    *a = c_box_edge[e][0];
+    *b = c_box_edge[e][1];
+  } else if (p.kind == GEOM_CYLINDER) {
+    const int K = CYL_SIDES;
+    int i = e / 3, t = e % 3;
+    *a = t == 2 ? K + i : i;
+    *b = t == 0 ? K + i : t == 1 ? (i + 1) % K : K + (i + 1) % K;
+  } else {
+    int g = p.m->hull_eadr[p.mesh] + e;
+    *a = p.m->hull_edge[2 * g];
+    *b = p.m->hull_edge[2 * g + 1];
+  }
+}
+__device__ inline void p_eface(const Poly& p, int e, int* f1, int* f2) {
+  if (p.kind == GEOM_BOX) {
+    *f1 = c_box_eface[e][0];
+    *f2 = c_box_eface[e][1];
+  } else if (p.kind == GEOM_CYLINDER) {
+    const int K = CYL_SIDES;
+    int i = e / 3, t = e % 3;
+    if (t == 0) {
+      *f1 = i == 0 ? 2 : 2 + i - 1;
+      *f2 = i == 0 ? 2 + K - 1 : 2 + i;
+    } else {
+      *f1 = t == 1 ? 0 : 1;
+      *f2 = 2 + i;
+    }
+  } else {
+    int g = p.m->hull_eadr[p.mesh] + e;
+    *f1 = p.m->hull_eface[2 * g];
+    *f2 = p.m->hull_eface[2 * g + 1];
+  }
+}
+
+// Point of the polytope closest to x: the signed distance (negative inside,
+// then to the nearest face plane), the point, and the face when inside (-1
+// outside). Outside, the closest point lies on a face (projection inside
+// its loop) or on an edge.
+__device__ __noinline__ double closest_point(const Poly& p, V3 x, V3* q, int* inside_face) {
+  int nf = p_nf(p);
+  double best = -INFINITY;
+  int bf = 0;
+  for (int f = 0; f < nf; f++) {
+    V3 n = p_fn(p, f);
+    double s = dot(n, x) - p_fd(p, f, n);
+    if (s > best) {
+      best = s;
+      bf = f;
+    }
+  }
+  if (best <= 0.0) {
+    *q = x - p_fn(p, bf) * best;
+    *inside_face = bf;
+    return best;
+  }
+  *inside_face = -1;
+  double bd = INFINITY;
+  for (int f = 0; f < nf; f++) {
+    V3 n = p_fn(p, f);
+    double s = dot(n, x) - p_fd(p, f, n);
+    if (s <= 0.0) continue;
+    V3 y = x - n * s;
+    int nl = p_fvn(p, f);
+    bool in = true;
+    for (int k = 0; k < nl && in; k++) {
+      V3 a = p_v(p, p_fv(p, f, k)), b = p_v(p, p_fv(p, f, (k + 1) % nl));
+      V3 sn = cross(b - a, n);
+      if (dot(sn, y - a) > 0.0) in = false;
+    }
+    if (in && s < bd) {
+      bd = s;
+      *q = y;
+    }
+  }
+  int ne = p_ne(p);
+  for (int e = 0; e < ne; e++) {
+    int ia, ib;
+    p_edge(p, e, &ia, &ib);
+    V3 a = p_v(p, ia), b = p_v(p, ib);
+    V3 ab = b - a;
+    double t = clampd(dot(x - a, ab) / fmax(dot(ab, ab), 1e-300), 0.0, 1.0);
+    V3 y = a + ab * t;
+    double d = norm(x - y);
+    if (d < bd) {
+      bd = d;
+      *q = y;
+    }
+  }
+  return bd;
+}
+
+// Choices between candidates whose values tie up to rounding take the first
+// one within GEN_TIE of the best, so that rounding-level differences (from
+// the host's oracle, say) cannot change the contacts.
+constexpr double GEN_TIE = 1e-10;
+
+// largest separation of b beyond a face of a (first face within GEN_TIE)
+__device__ __noinline__ double face_query(const Poly& a, const Poly& b, int* face) {
+  int nf = p_nf(a), nv = p_nv(b);
+  auto sep = [&](int f) {
+    V3 n = p_fn(a, f);
+    double mn = INFINITY;
+    for (int i = 0; i < nv; i++) mn = fmin(mn, dot(n, p_v(b, i)));
+    return mn - p_fd(a, f, n);
+  };
+  double best = -INFINITY;
+  for (int f = 0; f < nf; f++) best = fmax(best, sep(f));
+  int f = 0;
+  while (f + 1 < nf && sep(f) < best - GEN_TIE) f++;
+  *face = f;
+  return best;
+}
+
+// arcs (a, b) and (c, d) of the Gauss map cross: the edges' cross product
+// is a face normal of the Minkowski difference
+__device__ inline bool minkowski_face(V3 a, V3 b, V3 c, V3 d) {
+  V3 bxa = cross(b, a), dxc = cross(d, c);
+  double cba = dot(c, bxa), dba = dot(d, bxa), adc = dot(a, dxc), bdc = dot(b, dxc);
+  return cba * dba < 0.0 && adc * bdc < 0.0 && cba * bdc > 0.0;
+}
+
+// largest separation along the cross product of an edge of a and of b
+__device__ __noinline__ double edge_query(const Poly& a, V3 ca, const Poly& b, int* ea, int* eb, V3* axis) {
+  double best = -INFINITY;
+  *ea = *eb = -1;
+  int nea = p_ne(a), neb = p_ne(b);
+  for (int i = 0; i < nea; i++) {
+    int fa1, fa2, ia, ja;
+    p_eface(a, i, &fa1, &fa2);
+    if (fa2 < 0) continue;
+    p_edge(a, i, &ia, &ja);
+    V3 pa = p_v(a, ia), da = p_v(a, ja) - pa;
+    V3 na1 = p_fn(a, fa1), na2 = p_fn(a, fa2);
+    for (int j = 0; j < neb; j++) {
+      int fb1, fb2, ib, jb;
+      p_eface(b, j, &fb1, &fb2);
+      if (fb2 < 0) continue;
+      V3 nb1 = p_fn(b, fb1), nb2 = p_fn(b, fb2);
+      if (!minkowski_face(na1, na2, -nb1, -nb2)) continue;
+      p_edge(b, j, &ib, &jb);
+      V3 pb = p_v(b, ib), db = p_v(b, jb) - pb;
+      V3 c = cross(da, db);
+      double l = norm(c);
+      if (l < 1e-6 * norm(da) * norm(db)) continue;  // parallel edges: a face axis covers them
+      V3 n = c * (1.0 / l);
+      if (dot(n, pa - ca) < 0.0) n = -n;
+      double s = dot(n, pb - pa);
+      if (s > best) {
+        best = s;
+        *ea = i;
+        *eb = j;
+        *axis = n;
+      }
+    }
+  }
+  return best;
+}
+
+__device__ inline V3 p_centroid(const Poly& p) {
+  V3 c{0.0, 0.0, 0.0};
+  int nv = p_nv(p);
+  for (int i = 0; i < nv; i++) c = c + p_v(p, i);
+  return c * (1.0 / (double)nv);
+}
+
+// reduce_to_four's choices (collision.rs:514-531: the deepest point, then
+// the farthest from it, the farthest from their line, the most isolated),
+// each taken within GEN_TIE: the first minimum, the last maximum. A clipped
+// regular polygon (a cylinder cap) offers many exact ties.
+__device__ __noinline__ int reduce_to_four_tie(DP* pts, int n) {
+  if (n <= 4) return n;
+  DP keep[4];
+  double mn = INFINITY;
+  for (int i = 0; i < n; i++) mn = fmin(mn, pts[i].d);
+  int di = 0;
+  while (pts[di].d > mn + GEN_TIE) di++;
+  keep[0] = pts[di];
+  for (int k = 1; k < 4; k++) {
+    auto key = [&](V3 p) {
+      if (k == 1) return norm2(p - keep[0].p);
+      if (k == 2) return norm(cross(keep[1].p - keep[0].p, p - keep[0].p));
+      double s = INFINITY;
+      for (int j = 0; j < 3; j++) s = fmin(s, norm(keep[j].p - p));
+      return s;
+    };
+    double mx = -INFINITY;
+    for (int i = 0; i < n; i++) mx = fmax(mx, key(pts[i].p));
+    int bi = 0;
+    for (int i = 0; i < n; i++)
+      if (key(pts[i].p) >= mx - GEN_TIE) bi = i;
+    keep[k] = pts[bi];
+  }
+  for (int k = 0; k < 4; k++) pts[k] = keep[k];
+  return 4;
+}
+
+// Sutherland-Hodgman against pn.p <= off into at most `cap` vertices
+__device__ inline int clip_poly_cap(const V3* in, int n, V3 pn, double off, V3* out, int cap) {
+  int k = 0;
+  for (int i = 0; i < n; i++) {
+    V3 a = in[i], b = in[(i + 1) % n];
+    double da = dot(pn, a) - off, db = dot(pn, b) - off;
+    if (da <= 0.0 && k < cap) out[k++] = a;
+    if ((da < 0.0) != (db < 0.0) && fabs(da - db) > 1e-15 && k < cap) out[k++] = a + (b - a) * (da / (da - db));
+  }
+  return k;
+}
+
+// reference face rf of r (outward normal toward s), incident polytope s:
+// clip s's most anti-parallel face against rf's side planes, keep the points
+// within the margin (up to four); normals along n (first geom to second)
+__device__ __noinline__ void clip_faces(const Poly& r, int rf, const Poly& s, V3 n, double margin, Hits& out) {
+  V3 nref = p_fn(r, rf);
+  double dref = p_fd(r, rf, nref);
+  int nfs = p_nf(s), inc = 0;
+  double mn = INFINITY;
+  for (int f = 0; f < nfs; f++) mn = fmin(mn, dot(p_fn(s, f), nref));
+  while (inc + 1 < nfs && dot(p_fn(s, inc), nref) > mn + GEN_TIE) inc++;
+  V3 buf[2][GEN_CLIP_CAP];
+  int np = p_fvn(s, inc), cur = 0;
+  for (int k = 0; k < np; k++) buf[0][k] = p_v(s, p_fv(s, inc, k));
+  int nl = p_fvn(r, rf);
+  for (int k = 0; k < nl; k++) {
+    V3 a = p_v(r, p_fv(r, rf, k)), b = p_v(r, p_fv(r, rf, (k + 1) % nl));
+    V3 sn = normalized(cross(b - a, nref));
+    np = clip_poly_cap(buf[cur], np, sn, dot(sn, a), buf[cur ^ 1], GEN_CLIP_CAP);
+    cur ^= 1;
+    if (np == 0) return;
+  }
+  DP pts[GEN_CLIP_CAP];
+  int n_pts = 0;
+  for (int k = 0; k < np; k++) {
+    double sep = dot(buf[cur][k], nref) - dref;
+    if (sep < margin) pts[n_pts++] = DP{sep, buf[cur][k]};
+  }
+  n_pts = reduce_to_four_tie(pts, n_pts);
+  for (int k = 0; k < n_pts; k++) out.push(pts[k].p - nref * (pts[k].d * 0.5), n, -pts[k].d);
+}
+
+__device__ inline void polytope_polytope(const Poly& a, const Poly& b, double margin, Hits& out) {
+  int fa, fb, ea, eb;
+  V3 axis{0.0, 0.0, 0.0};
+  double sa = face_query(a, b, &fa);
+  if (sa > margin) return;
+  double sb = face_query(b, a, &fb);
+  if (sb > margin) return;
+  double se = edge_query(a, p_centroid(a), b, &ea, &eb, &axis);
+  if (se > margin) return;
+  double oa = -sa, ob = -sb, oe = -se;
+  bool face_a = !(ob < oa - GEN_TIE);
+  double of = face_a ? oa : ob;
+  if (ea >= 0 && oe < of && !(of < oe * 1.05 + 1e-4)) {
+    int i0, i1, j0, j1;
+    p_edge(a, ea, &i0, &i1);
+    p_edge(b, eb, &j0, &j1);
+    V3 x, y;
+    closest_segments(p_v(a, i0), p_v(a, i1), p_v(b, j0), p_v(b, j1), &x, &y);
+    out.push((x + y) * 0.5, axis, oe);
+    return;
+  }
+  if (face_a) clip_faces(a, fa, b, p_fn(a, fa), margin, out);
+  else clip_faces(b, fb, a, -p_fn(b, fb), margin, out);
+}
+
+// sphere (center c, radius r) against a polytope; normal from the sphere
+__device__ inline void sphere_polytope(V3 c, double r, const Poly& p, double margin, Hits& out) {
+  V3 q{0.0, 0.0, 0.0};
+  int face;
+  double dist = closest_point(p, c, &q, &face);
+  if (face < 0) {
+    double depth = r - dist;
+    if (depth <= -margin || dist <= 1e-12) return;
+    V3 n = (q - c) * (1.0 / dist);
+    out.push(q - n * (depth * 0.5), n, depth);
+  } else {
+    V3 n = -p_fn(p, face);
+    double depth = r - dist;
+    out.push(c + n * (r - depth * 0.5), n, depth);
+  }
+}
+
+// capsule against a polytope: the deepest point along the axis (golden
+// section on the signed distance) and the ends, as capsule-box does
+__device__ inline void capsule_polytope(const GPose& a, const Poly& p, double margin, Hits& out) {
+  V3 ax = col(a.mat, 2) * a.size.y;
+  V3 p0 = a.pos - ax, p1 = a.pos + ax;
+  double r = a.size.x;
+  auto f = [&](double t) {
+    V3 q;
+    int face;
+    return closest_point(p, p0 + (p1 - p0) * t, &q, &face);
+  };
+  const double g = 0.61803398875;
+  double lo = 0.0, hi = 1.0;
+  double x1 = hi - g * (hi - lo), x2 = lo + g * (hi - lo);
+  double f1 = f(x1), f2 = f(x2);
+  for (int it = 0; it < 30; it++) {
+    if (f1 < f2) {
+      hi = x2;
+      x2 = x1;
+      f2 = f1;
+      x1 = hi - g * (hi - lo);
+      f1 = f(x1);
+    } else {
+      lo = x1;
+      x1 = x2;
+      f1 = f2;
+      x2 = lo + g * (hi - lo);
+      f2 = f(x2);
+    }
+  }
+  double tmin = 0.5 * (lo + hi);
+  sphere_polytope(p0 + (p1 - p0) * tmin, r, p, margin, out);
+  for (int e = 0; e < 2; e++) {
+    double t = e == 0 ? 0.0 : 1.0;
+    if (fabs(t - tmin) > 0.1 && f(t) < r + margin) sphere_polytope(p0 + (p1 - p0) * t, r, p, margin, out);
+  }
+}
+
+// plane against a hull: the four deepest vertices within the margin, in
+// the order a stable sort by depth gives
+__device__ inline void plane_polytope(const GPose& pl, const Poly& p, double margin, Hits& out) {
+  V3 n = col(pl.mat, 2);
+  DP keep[4];
+  int nk = 0;
+  int nv = p_nv(p);
+  for (int i = 0; i < nv; i++) {
+    V3 x = p_v(p, i);
+    double d = dot(x - pl.pos, n);
+    if (!(d < margin)) continue;
+    if (nk == 4 && !(d < keep[3].d)) continue;
+    int j = nk < 4 ? nk++ : 3;
+    while (j > 0 && keep[j - 1].d > d) {
+      keep[j] = keep[j - 1];
+      j--;
+    }
+    keep[j] = DP{d, x};
+  }
+  for (int k = 0; k < nk; k++) out.push(keep[k].p - n * (keep[k].d * 0.5), n, -keep[k].d);
+}
+
+__device__ __noinline__ void collide_general(const DModel& m, const GPose& a0, const GPose& b0, double margin,
+                                             Hits& out) {
+  bool swap = a0.type > b0.type;  // type order, normals flipped back (collision.rs:59-67)
+  const GPose& a = swap ? b0 : a0;
+  const GPose& b = swap ? a0 : b0;
+  int start = out.n;
+  Poly pb{b.type, b.pos, b.mat, b.size, &m, b.data};
+  if (a.type == GEOM_PLANE) {
+    plane_polytope(a, pb, margin, out);
+  } else if (a.type == GEOM_SPHERE) {
+    sphere_polytope(a.pos, a.size.x, pb, margin, out);
+  } else if (a.type == GEOM_CAPSULE) {
+    capsule_polytope(a, pb, margin, out);
+  } else {
+    Poly pa{a.type, a.pos, a.mat, a.size, &m, a.data};
+    polytope_polytope(pa, pb, margin, out);
+  }
+  if (swap)
+    for (int k = start; k < out.n && k < MAX_HITS; k++) out.h[k].normal = -out.h[k].normal;
+}
+
+}  // namespace pg

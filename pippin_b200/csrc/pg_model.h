@@ -37,6 +37,7 @@ enum { R_AREF = 0, R_D = 1, R_JAR = 2, R_JP = 3, R_POS = 4, R_DIAG = 5, R_FLAGS 
 enum { G_POS = 0, G_MAT = 3, G_AABB = 12, G_STRIDE = 18 };
 
 constexpr int NV_MAX = 64;  // dof-chain masks are 64-bit
+constexpr int HULL_FACE_MAX = 32;  // longest hull face loop the device clips
 
 struct DModel {
   // ---- dims
@@ -113,9 +114,16 @@ struct DModel {
   const int* hull_vadr;
   const int* hull_vnum;
   const double* hull_vert;  // [*][3]
-  const int* hull_fadr;
+  const int* hull_fadr;      // per mesh: first polygon face, count
   const int* hull_fnum;
-  const double* hull_face;  // [*][4]: outward unit normal, offset (n.x <= d)
+  const double* hull_face;   // [*][4]: outward unit normal, offset (n.x <= d)
+  const int* hull_fvadr;     // per face: its vertex loop (counter-clockwise from outside)
+  const int* hull_fvnum;
+  const int* hull_fv;
+  const int* hull_eadr;      // per mesh: first edge, count
+  const int* hull_enum;
+  const int* hull_edge;      // [*][2] vertex pairs
+  const int* hull_eface;     // [*][2] the two faces of each edge (mesh-local face index)
 
   // ---- per-env parameter block offsets (doubles) and stride
   int p_friction, p_size, p_contype, p_conaff, p_mass, p_inertia, p_ipos, p_damping, p_gain, p_bias, p_qpos_reset,

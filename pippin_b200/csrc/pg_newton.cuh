@@ -6,7 +6,7 @@
 // and the cost-gated warm start) and forward.rs:336-480 (substep driver,
 // implicit damping, integration).
 #pragma once
-#include "pg_collide.cuh"
+#include "pg_general.cuh"
 #include "pg_dynamics.cuh"
 #include "pg_small.cuh"
 
@@ -43,9 +43,9 @@ __device__ int collide(const Tile<G>& T, const DModel& m, const WsLayout& w, con
         bool sep = fabs(c1.x - c2.x) > h1.x + h2.x + m.margin || fabs(c1.y - c2.y) > h1.y + h2.y + m.margin ||
                    fabs(c1.z - c2.z) > h1.z + h2.z + m.margin;
         if (!sep) {
-          GPose a{m.geom_type[g1], ld3(r1 + G_POS), ld9(r1 + G_MAT), ld3(prm + m.p_size + 3 * g1)};
-          GPose b{m.geom_type[g2], ld3(r2 + G_POS), ld9(r2 + G_MAT), ld3(prm + m.p_size + 3 * g2)};
-          if (needs_general(a.type, b.type)) st |= ST_UNSUPPORTED_PAIR;
+          GPose a{m.geom_type[g1], ld3(r1 + G_POS), ld9(r1 + G_MAT), ld3(prm + m.p_size + 3 * g1), m.geom_dataid[g1]};
+          GPose b{m.geom_type[g2], ld3(r2 + G_POS), ld9(r2 + G_MAT), ld3(prm + m.p_size + 3 * g2), m.geom_dataid[g2]};
+          if (needs_general(a.type, b.type)) collide_general(m, a, b, m.margin, hits);
           else collide_primitive(a, b, m.margin, hits);
         }
       }

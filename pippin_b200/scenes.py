@@ -155,3 +155,28 @@ REFERENCE_ASSETS = {
     "box_drop.xml": box_drop_xml,
     "tumble.xml": tumble_xml,
 }
+
+
+def hull_tumble_xml(n_hulls: int = 8, seed: int = 0, timestep: float = 0.002) -> str:
+    """Convex hulls tumbling onto a plane (the general convex narrow phase):
+    `n_hulls` free bodies, each a mesh of 8 to 32 points drawn uniformly on
+    an ellipsoid with semi-axes U[0.02, 0.06] (hulled by the model compiler),
+    placed on a grid 0.25 m above the floor with a random orientation."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    assets, bodies = [], []
+    for i in range(n_hulls):
+        npt = int(rng.integers(8, 33))
+        axes = rng.uniform(0.02, 0.06, 3)
+        d = rng.normal(size=(npt, 3))
+        d /= np.linalg.norm(d, axis=1, keepdims=True)
+        pts = d * axes
+        assets.append(f'<mesh name="h{i}" vertex="{" ".join(_fmt(round(x, 6)) for x in pts.ravel())}"/>')
+        x, y = 0.15 * (i % 4) - 0.225, 0.15 * (i // 4) - 0.075
+        e = rng.uniform(-180, 180, 3)
+        bodies.append(f'<body name="b{i}" pos="{_fmt(round(x, 4))} {_fmt(round(y, 4))} 0.25" '
+                      f'euler="{_fmt(round(e[0], 3))} {_fmt(round(e[1], 3))} {_fmt(round(e[2], 3))}">'
+                      f'<freejoint/><geom type="mesh" mesh="h{i}"/></body>')
+    return (f'<mujoco model="hull_tumble"><option timestep="{_fmt(timestep)}"/><asset>{"".join(assets)}</asset>'
+            f'<worldbody><geom name="floor" type="plane" size="5 5 .1"/>{"".join(bodies)}</worldbody></mujoco>')
