@@ -15,9 +15,9 @@
 
 namespace pg {
 
-constexpr double PGS_MAX_BIAS_VELOCITY = 1.0;  // solver.rs:38
-constexpr double PGS_TOLERANCE = 1e-5;         // solver.rs:39
-constexpr double PGS_MATCH_DIST2 = 0.01 * 0.01;  // solver.rs:258
+constexpr double PGS_MAX_BIAS_VELOCITY = 1.0;  // solver.rs:34
+constexpr double PGS_TOLERANCE = 1e-5;         // solver.rs:36
+constexpr double PGS_MATCH_DIST2 = 0.01 * 0.01;  // solver.rs:255
 
 // Rows of the PGS problem (solver.rs:63-163) into J (stride nv) and R
 // (PR_* records). Returns the row count, capped at maxrows.

@@ -230,11 +230,11 @@ def test_pgs_step_parity(name, tol, resting):
     """PGS (solver.rs:63-251) per step on identical input states, with the
     warm start cleared on both backends (reset, then the state set again),
     through falls, contacts and joint limits. A normal row's bias changes
-    branch discontinuously where sep + slop crosses zero (solver.rs:204-219),
+    branch discontinuously where sep + slop crosses zero (solver.rs:176-181),
     which is where resting contacts sit: in the resting stacks a rounding
     difference in the depth can pick the other branch, after which the two
     runs agree only to the sweeps' own stopping tolerance, a 1e-5 velocity
-    change (solver.rs:39). Those scenes are held to 1e-4 on qpos and qvel
+    change (solver.rs:36). Those scenes are held to 1e-4 on qpos and qvel
     instead of 1e-10 on qpos, qvel and qacc."""
     n = 32
     m, g, o = _pgs_pair(name, n)
