@@ -544,12 +544,12 @@ void layouts(const HostModel& m, int maxcon, int maxrows, WsLayout* w, WsLayout*
   // vectors over the factor and Newton vectors it does not use
   if (nv <= 16 && m.dof_blocks.size() / 2 == 1) {
     wn->sl = wn->qm;
-    int need = 16 * nv + 32;
+    int need = ((16 * nv + 1) & ~1) + 16 + 32;
     int base = (wn->mp + ((nv + 1) & ~1)) - wn->fac >= need ? wn->fac : wn->stride;
     wn->sj = base;
     wn->sx = base + ((16 * nv + 1) & ~1);
     wn->sc = wn->sx + 16;
-    wn->stride = std::max(wn->stride, wn->sc + 16);
+    wn->stride = std::max(wn->stride, wn->sc + 32);
   }
 
   // per-env work record

@@ -448,53 +448,71 @@ __device__ __noinline__ void add_constraint_force(const Tile<G>& T, int k, int n
 // ------------------------------------------------------- register-resident Newton
 // Shared buffers of newton_small (offsets sj, sl, sx, sc of the workspace).
 struct SmallBufs {
-  double* J;  // [16][k] constraint rows, copied in
+  double* J;  // [16][k] the first 16 constraint rows, copied in
   double* L;  // [k][k] Hessian factor
   double* x;  // [16] the vector being multiplied, one component per lane
-  double* c;  // [16] per-row coefficients
+  double* c;  // [32] per-row coefficients
 };
 
-// newton.rs:224-371 for k <= 16 unknowns and nr <= 16 rows, with one unknown
-// and one row per lane: the lane's row of M and of the Hessian stay in
-// registers, the rows of J are copied into shared memory once, and each
-// product M x / J x reads the published x as broadcast loads. A lane holds at
-// most one term of every sum, so the sums are formed exactly as newton_dense
-// forms them; only the factorisation differs (chol_reg). Adds the constraint
-// force to qfrc (newton.rs:361-371) and leaves the solution in a; returns the
-// iteration count. J rows are read from Jsrc (stride k), row constants from R.
+constexpr int SMALL_ROWS = 2 * SMALL_N;  // rows the register Newton takes (two per lane)
+
+// newton.rs:224-371 for k <= 16 unknowns and nr <= 32 rows: lane i holds
+// unknown i and rows i and i + 16. The lane's row of M and of the Hessian
+// stay in registers; the first 16 rows of J are copied into shared memory
+// (rows 16..31, rare, are read where build_rows left them); each product
+// M x / J x reads the published x with broadcast loads. On 16-lane tiles
+// every per-lane partial sum holds the same terms in the same order as
+// newton_dense's, so the sums agree with it exactly; only the factorisation
+// differs (chol_reg). Adds the constraint force to qfrc (newton.rs:361-371)
+// and leaves the solution in a; returns the iteration count. J rows are
+// read from Jsrc (stride k), row constants from R.
 template <int G>
 __device__ __noinline__ int newton_small(const Tile<G>& T, int k, int nr, const double* Jsrc, const double* R,
                                          const double* M, double* a, const double* warm, int max_iters, double tol,
                                          const SmallBufs& B, double* qfrc) {
-  static_assert(G >= SMALL_N, "one lane per unknown and per row");
+  static_assert(G >= SMALL_N, "one lane per unknown");
   const int i = T.lane();
-  const bool dof = i < k, rowl = i < nr;
+  const bool dof = i < k;
   double mrow[SMALL_N];
 #pragma unroll
   for (int q = 0; q < SMALL_N; q++) mrow[q] = (dof && q < k) ? M[i * k + q] : 0.0;
   const double a0 = dof ? a[i] : 0.0;
   const double wi = (warm && dof) ? warm[i] : 0.0;
-  double aref = 0.0, dr = 0.0;
-  bool bil = false;
-  if (rowl) {
-    const double* rr = R + R_STRIDE * i;
-    aref = rr[R_AREF];
-    dr = rr[R_D];
-    bil = rr[R_FLAGS] != 0.0;
+  // rows i and i + 16 of this lane
+  bool has[2];
+  double aref[2], dr[2];
+  bool bil[2];
+#pragma unroll
+  for (int s = 0; s < 2; s++) {
+    int r = i + SMALL_N * s;
+    has[s] = i < SMALL_N && r < nr;
+    aref[s] = dr[s] = 0.0;
+    bil[s] = false;
+    if (has[s]) {
+      const double* rr = R + R_STRIDE * r;
+      aref[s] = rr[R_AREF];
+      dr[s] = rr[R_D];
+      bil[s] = rr[R_FLAGS] != 0.0;
+    }
   }
-  for (int t = i; t < nr * k; t += G) B.J[t] = Jsrc[t];
-  const double* Jr = B.J + i * k;  // this lane's row (rowl only)
+  int ncopy = (nr < SMALL_N ? nr : SMALL_N) * k;
+  for (int t = i; t < ncopy; t += G) B.J[t] = Jsrc[t];
+  auto jrow = [&](int r) -> const double* { return r < SMALL_N ? B.J + r * k : Jsrc + r * k; };
   // publish one component per lane for the broadcast reads that follow
   auto publish = [&](double v) {
     T.sync();
     if (dof) B.x[i] = v;
     T.sync();
   };
-  auto coeffs = [&](double v) {
+  // per-row values v[s] of this lane's rows, readable as B.c[r]
+  auto coeffs = [&](const double* v) {
     T.sync();
-    if (rowl) B.c[i] = v;
+#pragma unroll
+    for (int s = 0; s < 2; s++)
+      if (has[s]) B.c[i + SMALL_N * s] = v[s];
     T.sync();
   };
+  auto jdot = [&](int s) { return dot_ref_sm(jrow(i + SMALL_N * s), B.x, k); };
   // newton.rs:96-110
   auto cost = [&](double xi) -> double {
     double tmp = xi - a0;
@@ -503,10 +521,12 @@ __device__ __noinline__ int newton_small(const Tile<G>& T, int k, int nr, const 
     double c = 0.5 * T.sum(dof ? tmp * tmp2 : 0.0);
     publish(xi);
     double cr = 0.0;
-    if (rowl) {
-      double jar = dot_ref_sm(Jr, B.x, k) - aref;
-      if (bil || jar < 0.0) cr = 0.5 * dr * jar * jar;
-    }
+#pragma unroll
+    for (int s = 0; s < 2; s++)
+      if (has[s]) {
+        double jar = jdot(s) - aref[s];
+        if (bil[s] || jar < 0.0) cr += 0.5 * dr[s] * jar * jar;
+      }
     return c + T.sum(cr);
   };
   double ai = a0;
@@ -520,8 +540,8 @@ __device__ __noinline__ int newton_small(const Tile<G>& T, int k, int nr, const 
   double scale = 1.0 + sqrt(T.sum(ma0 * ma0));
   int iters = 0;
   int maxit = max_iters > 1 ? max_iters : 1;
-  double prev = -1.0;  // the row's activity in the previous iteration (none yet)
-  double jar = 0.0, act = 0.0;
+  double prev[2] = {-1.0, -1.0};  // the rows' activity in the previous iteration (none yet)
+  double jar[2] = {0.0, 0.0}, act[2] = {0.0, 0.0}, cv[2];
   while (iters < maxit) {
     iters++;
     // gradient M (a - a0) + sum over active rows of D jar J_r (newton.rs:254-270)
@@ -530,17 +550,21 @@ __device__ __noinline__ int newton_small(const Tile<G>& T, int k, int nr, const 
     double grad = dof ? dot_ref_reg(mrow, B.x, k) : 0.0;
     publish(ai);
     bool same = true;
-    if (rowl) {
-      jar = dot_ref_sm(Jr, B.x, k) - aref;
-      act = (bil || jar < 0.0) ? 1.0 : 0.0;
-      same = act == prev;
-      prev = act;
-    }
-    coeffs(act != 0.0 ? dr * jar : 0.0);
+#pragma unroll
+    for (int s = 0; s < 2; s++)
+      if (has[s]) {
+        jar[s] = jdot(s) - aref[s];
+        act[s] = (bil[s] || jar[s] < 0.0) ? 1.0 : 0.0;
+        if (act[s] != prev[s]) same = false;
+        prev[s] = act[s];
+      }
+#pragma unroll
+    for (int s = 0; s < 2; s++) cv[s] = act[s] != 0.0 ? dr[s] * jar[s] : 0.0;
+    coeffs(cv);
     if (dof)
       for (int r = 0; r < nr; r++) {
         double cf = B.c[r];
-        if (cf != 0.0) grad += cf * B.J[r * k + i];
+        if (cf != 0.0) grad += cf * jrow(r)[i];
       }
     double gnorm = sqrt(T.sum(dof ? grad * grad : 0.0));
     bool unchanged = T.all(same);
@@ -549,12 +573,14 @@ __device__ __noinline__ int newton_small(const Tile<G>& T, int k, int nr, const 
     double h[SMALL_N];
 #pragma unroll
     for (int q = 0; q < SMALL_N; q++) h[q] = mrow[q];
-    coeffs(act != 0.0 ? dr : 0.0);
+#pragma unroll
+    for (int s = 0; s < 2; s++) cv[s] = act[s] != 0.0 ? dr[s] : 0.0;
+    coeffs(cv);
     if (dof)
       for (int r = 0; r < nr; r++) {
         double d = B.c[r];
         if (d == 0.0) continue;
-        const double* jr = B.J + r * k;
+        const double* jr = jrow(r);
         double ji = jr[i];
         if (ji == 0.0) continue;
         double e = d * ji;
@@ -568,18 +594,22 @@ __device__ __noinline__ int newton_small(const Tile<G>& T, int k, int nr, const 
     // exact line search on the piecewise quadratic along p (newton.rs:317-354)
     publish(p);
     double mp = dof ? dot_ref_reg(mrow, B.x, k) : 0.0;
-    double jp = rowl ? dot_ref_sm(Jr, B.x, k) : 0.0;
+    double jp[2];
+#pragma unroll
+    for (int s = 0; s < 2; s++) jp[s] = has[s] ? jdot(s) : 0.0;
     double mpp = T.sum(dof ? p * mp : 0.0), mpg = T.sum(dof ? tmp * mp : 0.0);
     auto deriv = [&](double al, double* d1o, double* d2o) {
       double d1 = 0.0, d2 = 0.0;
-      if (rowl) {
-        double v = jar + al * jp;
-        if (bil || v < 0.0) {
-          double dq = dr * jp;
-          d1 += dq * v;
-          d2 += dq * jp;
+#pragma unroll
+      for (int s = 0; s < 2; s++)
+        if (has[s]) {
+          double v = jar[s] + al * jp[s];
+          if (bil[s] || v < 0.0) {
+            double dq = dr[s] * jp[s];
+            d1 += dq * v;
+            d2 += dq * jp[s];
+          }
         }
-      }
       *d1o = (al * mpp + mpg) + T.sum(d1);
       *d2o = mpp + T.sum(d2);
     };
@@ -605,17 +635,20 @@ __device__ __noinline__ int newton_small(const Tile<G>& T, int k, int nr, const 
   }
   // qfrc_constraint += -D (J a - aref) J' over active rows (newton.rs:361-371)
   publish(ai);
-  double f = 0.0;
-  if (rowl) {
-    double v = dot_ref_sm(Jr, B.x, k) - aref;
-    f = (bil || v < 0.0) ? -dr * v : 0.0;
+#pragma unroll
+  for (int s = 0; s < 2; s++) {
+    cv[s] = 0.0;
+    if (has[s]) {
+      double v = jdot(s) - aref[s];
+      cv[s] = (bil[s] || v < 0.0) ? -dr[s] * v : 0.0;
+    }
   }
-  coeffs(f);
+  coeffs(cv);
   if (dof) {
     double q = qfrc[i];
     for (int r = 0; r < nr; r++) {
       double cf = B.c[r];
-      if (cf != 0.0) q += cf * B.J[r * k + i];
+      if (cf != 0.0) q += cf * jrow(r)[i];
     }
     qfrc[i] = q;
     a[i] = ai;
@@ -761,7 +794,7 @@ __device__ int newton_solve(const Tile<G>& T, const DModel& m, const WsLayout& w
   for (int t = lane; t < nr * nv; t += G) nz |= J[t] != 0.0;
   if (!T.any(nz)) return 0;
   if constexpr (G >= SMALL_N) {
-    if (nv <= SMALL_N && nr <= SMALL_N && w.sj >= 0) {
+    if (nv <= SMALL_N && nr <= SMALL_ROWS && w.sj >= 0) {
       SmallBufs S{ws + w.sj, ws + w.sl, ws + w.sx, ws + w.sc};
       return newton_small(T, nv, nr, J, R, ws + w.qm, a, warm, m.iterations, m.tolerance, S, qfrc);
     }
