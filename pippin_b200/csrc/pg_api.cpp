@@ -489,8 +489,6 @@ void layouts(const HostModel& m, int maxcon, int maxrows, WsLayout* w, WsLayout*
   w->qpos = take(m.nq);
   w->qvel = take(nv);
   w->ctrl = take(nu);
-  w->applied = take(nv);
-  w->qm = take(nv * nv);
   w->cdof = take(6 * nv);
   w->smooth = take(nv);
   w->acc = take(nv);
@@ -502,7 +500,6 @@ void layouts(const HostModel& m, int maxcon, int maxrows, WsLayout* w, WsLayout*
   // tree walks and passive/actuator forces ...
   w->xpos = take(3 * nb);
   w->xquat = take(4 * nb);
-  w->xmat = take(9 * nb);
   w->cinert = take(13 * nb);
   w->cvel = take(6 * nb);
   w->cacc = take(6 * nb);

@@ -29,7 +29,7 @@ __device__ inline void tree_down_body(const DModel& m, const WsLayout& w, const 
   double* ws = e.ws;
   const double* q = ws + w.qpos;
   int p = m.body_parent[b];
-  M3 xmp = ld9(ws + w.xmat + 9 * p);
+  M3 xmp = q_mat(ld4(ws + w.xquat + 4 * p));  // the parent's stored rotation, exactly
   V3 pos = ld3(ws + w.xpos + 3 * p) + mv(xmp, ld3(m.body_pos + 3 * b));
   Q4 quat = q_mul(ld4(ws + w.xquat + 4 * p), ld4(m.body_quat + 4 * b));
   double* cdof = ws + w.cdof;
@@ -75,7 +75,6 @@ __device__ inline void tree_down_body(const DModel& m, const WsLayout& w, const 
   M3 xm = q_mat(quat);
   st3(ws + w.xpos + 3 * b, pos);
   st4(ws + w.xquat + 4 * b, quat);
-  st9(ws + w.xmat + 9 * b, xm);
   const double* prm = e.prm;
   V3 xipos = pos + mv(xm, ld3(prm + m.p_ipos + 3 * b));
   SpI I = spi_from_com(prm[m.p_mass + b], xipos, mrot(ld9(prm + m.p_inertia + 9 * b), xm));
@@ -138,7 +137,7 @@ __device__ void geom_poses(const Tile<G>& T, const DModel& m, const WsLayout& w,
   const double* ws = e.ws;
   for (int g = T.lane(); g < m.ngeom; g += G) {
     int b = m.geom_body[g];
-    M3 xm = ld9(ws + w.xmat + 9 * b);
+    M3 xm = q_mat(ld4(ws + w.xquat + 4 * b));
     V3 gp = ld3(ws + w.xpos + 3 * b) + mv(xm, ld3(m.geom_pos + 3 * g));
     M3 gm = mm(xm, q_mat(ld4(m.geom_quat + 4 * g)));
     double* o = gout + G_STRIDE * g;
@@ -168,7 +167,6 @@ __device__ void tree_down(const Tile<G>& T, const DModel& m, const WsLayout& w, 
   if (lane == 0) {
     st3(ws + w.xpos, V3{0, 0, 0});
     st4(ws + w.xquat, q_identity());
-    st9(ws + w.xmat, m3_identity());
     if (dynamics) {
       st6(ws + w.cvel, sp_zero());
       st6(ws + w.cacc, Sp{V3{0, 0, 0}, -V3{m.gravity[0], m.gravity[1], m.gravity[2]}});
@@ -186,10 +184,11 @@ __device__ void tree_down(const Tile<G>& T, const DModel& m, const WsLayout& w, 
 }
 
 // Up the tree: crb (in place of cinert) and, with `dynamics`, the cfrc sums;
-// then M = cdof' crb cdof along ancestor chains (+ armature) and
-// qfrc_bias = cdof' cfrc.
+// then M = cdof' crb cdof along ancestor chains (+ armature) into qm (nv x nv,
+// shared or global) and qfrc_bias = cdof' cfrc.
 template <int G>
-__device__ void tree_up(const Tile<G>& T, const DModel& m, const WsLayout& w, const EnvCtx& e, bool dynamics) {
+__device__ void tree_up(const Tile<G>& T, const DModel& m, const WsLayout& w, const EnvCtx& e, bool dynamics,
+                        double* qm) {
   double* ws = e.ws;
   int lane = T.lane(), nv = m.nv;
   double* crb = ws + w.cinert;
@@ -215,7 +214,6 @@ __device__ void tree_up(const Tile<G>& T, const DModel& m, const WsLayout& w, co
     }
     T.sync();
   }
-  double* qm = ws + w.qm;
   const double* cdof = ws + w.cdof;
   for (int k = lane; k < nv * nv; k += G) qm[k] = 0.0;
   T.sync();

@@ -63,19 +63,6 @@ __device__ inline void copy_in(const Tile<G>& T, double* dst, const double* src,
   for (int k = T.lane(); k < n; k += G) dst[k] = src[k];
 }
 
-// Global -> shared copies issued back to back without waiting (cp.async);
-// load_wait() completes this lane's copies, a tile sync then publishes them.
-__device__ inline void cp_async8(double* dst_shared, const double* src_global) {
-  unsigned d = (unsigned)__cvta_generic_to_shared(dst_shared);
-  size_t s = __cvta_generic_to_global(src_global);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(s) : "memory");
-}
-template <int G>
-__device__ inline void load_async(const Tile<G>& T, double* dst_shared, const double* src_global, int n) {
-  for (int k = T.lane(); k < n; k += G) cp_async8(dst_shared + k, src_global + k);
-}
-__device__ inline void load_wait() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
-
 // ---------------------------------------------------------------- phase 1
 // forward.rs:263-271 (minus collide) and forward.rs:342-356: smooth forces,
 // a0 = M^-1 f, and the factor of M + hD (forward.rs:359-366) when damped.
@@ -103,7 +90,6 @@ __global__ void __launch_bounds__(256) smooth_kernel(const __grid_constant__ Ste
     double* ws = e.ws;
     load_async(T, ws + w.qpos, A.st.qpos + env * nq, nq);
     load_async(T, ws + w.qvel, A.st.qvel + env * nv, nv);
-    load_async(T, ws + w.applied, A.st.applied + env * nv, nv);
     if (A.ctrl_seq) {
       const double* c = A.ctrl_seq + ((size_t)item * A.nstep + A.sidx) * nu;
       load_async(T, ws + w.ctrl, c, nu);
@@ -114,23 +100,23 @@ __global__ void __launch_bounds__(256) smooth_kernel(const __grid_constant__ Ste
     load_wait();
     T.sync();
     tree_down(T, m, w, e, true, e.geo);
-    tree_up(T, m, w, e, true);
+    tree_up(T, m, w, e, true, wk + A.k.qm);  // M goes straight to the work record
     passive_actuation(T, m, w, e);
     double* smooth = ws + w.smooth;
     double* acc = ws + w.acc;
+    const double* applied = A.st.applied + env * nv;
     for (int k = T.lane(); k < nv; k += G) {
-      double f = ws[w.passive + k] + ws[w.actf + k] + ws[w.applied + k] - ws[w.bias + k];
+      double f = ws[w.passive + k] + ws[w.actf + k] + applied[k] - ws[w.bias + k];
       smooth[k] = f;
       acc[k] = f;
       wk[A.k.bias + k] = ws[w.bias + k];
     }
-    copy_in(T, wk + A.k.qm, ws + w.qm, nv * nv);
     copy_in(T, wk + A.k.cdof, ws + w.cdof, 6 * nv);
     T.sync();
     // the tree region is dead from here on: the factorisations use it
     int status = 0;
     bool damped = has_implicit_terms(m, e.prm);
-    if (factor_mass(T, m, w, e, 0.0)) {
+    if (factor_mass(T, m, w, e, 0.0, wk + A.k.qm)) {
       solve_auto(T, ws + w.fac, nv, nv, m.nblock, m.block_adr, m.dof_block, m.maxbs, ws + w.rinv, acc);
       copy_in(T, wk + A.k.a0, acc, nv);
       copy_in(T, wk + A.k.smooth, smooth, nv);
@@ -138,7 +124,7 @@ __global__ void __launch_bounds__(256) smooth_kernel(const __grid_constant__ Ste
       // for PGS (forward.rs:366-368), which factors M + hD even with D = 0
       if (damped || m.solver == SOLVER_PGS) {
         T.sync();
-        if (factor_mass(T, m, w, e, h)) {
+        if (factor_mass(T, m, w, e, h, wk + A.k.qm)) {
           copy_in(T, wk + A.k.lh, ws + w.fac, nv * nv);
           copy_in(T, wk + A.k.rinvh, ws + w.rinv, nv);
         } else {
@@ -304,15 +290,14 @@ __global__ void __launch_bounds__(256) set_const_kernel(const __grid_constant__ 
     e.prm = prm;
     copy_in(T, e.ws + w.qpos, prm + m.p_qpos_reset, m.nq);
     T.sync();
-    tree_down(T, m, w, e, false, nullptr);
-    tree_up(T, m, w, e, false);
-    if (nv == 0) continue;
-    // M^-1 by Cholesky of the full matrix (forward.rs:286-288); the factor
-    // lives in scratch because the workspace's tree region is still needed
+    // M^-1 by Cholesky of the full matrix (forward.rs:286-288); M and its
+    // factor live in scratch because the workspace's tree region is still
+    // needed
     double* L = e.scr + A.s.chol;
     double* rinv = e.ws + w.rinv;
-    for (int t = T.lane(); t < nv * nv; t += G) L[t] = e.ws[w.qm + t];
-    T.sync();
+    tree_down(T, m, w, e, false, nullptr);
+    tree_up(T, m, w, e, false, L);
+    if (nv == 0) continue;
     bool ok = chol_auto(T, L, nv, nv, 1, nullptr, nullptr, nv, rinv);
     // one right-hand side per lane: unit vectors, then per body 3 axes x
     // (translation, rotation) rows; x = M^-1 row, quad = row . x
@@ -334,7 +319,7 @@ __global__ void __launch_bounds__(256) set_const_kernel(const __grid_constant__ 
             continue;
           }
           V3 dir{axis == 0 ? 1.0 : 0.0, axis == 1 ? 1.0 : 0.0, axis == 2 ? 1.0 : 0.0};
-          V3 xip = ld3(e.ws + w.xpos + 3 * b) + mv(ld9(e.ws + w.xmat + 9 * b), ld3(prm + m.p_ipos + 3 * b));
+          V3 xip = ld3(e.ws + w.xpos + 3 * b) + mv(q_mat(ld4(e.ws + w.xquat + 4 * b)), ld3(prm + m.p_ipos + 3 * b));
           for (int k = m.body_lastdof[b]; k != -1; k = m.dof_parent[k]) {
             Sp c = ld6(e.ws + w.cdof + 6 * k);
             row[k] = kind == 0 ? dot(dir, point_vel(c, xip)) : dot(dir, c.ang);
@@ -410,7 +395,7 @@ __global__ void __launch_bounds__(256) poses_kernel(const __grid_constant__ Step
     }
     for (int c = T.lane(); c < m.ncam; c += G) {
       int b = m.cam_body[c];
-      M3 xm = ld9(e.ws + w.xmat + 9 * b);
+      M3 xm = q_mat(ld4(e.ws + w.xquat + 4 * b));
       V3 pos = ld3(e.ws + w.xpos + 3 * b) + mv(xm, ld3(m.cam_pos + 3 * c));
       M3 mat = mm(xm, q_mat(ld4(m.cam_quat + 4 * c)));
       float* o = cams + ((size_t)item * m.ncam + c) * 12;

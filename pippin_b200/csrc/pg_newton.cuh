@@ -804,14 +804,16 @@ __device__ int newton_solve(const Tile<G>& T, const DModel& m, const WsLayout& w
   return it;
 }
 
-// forward.rs:407-431,392-401: factor M + h D per dof block into ws fac
+// forward.rs:407-431,392-401: factor M + h D per dof block into ws fac;
+// M (nv x nv) is read from global memory
 template <int G>
-__device__ bool factor_mass(const Tile<G>& T, const DModel& m, const WsLayout& w, const EnvCtx& e, double h) {
+__device__ bool factor_mass(const Tile<G>& T, const DModel& m, const WsLayout& w, const EnvCtx& e, double h,
+                            const double* qm) {
   int lane = T.lane(), nv = m.nv;
   double* ws = e.ws;
   double* F = ws + w.fac;
-  const double* qm = ws + w.qm;
-  for (int t = lane; t < nv * nv; t += G) F[t] = qm[t];
+  load_async(T, F, qm, nv * nv);
+  load_wait();
   T.sync();
   for (int k = lane; k < nv; k += G) F[k * nv + k] += h * e.prm[m.p_damping + k];
   T.sync();

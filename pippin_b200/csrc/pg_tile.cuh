@@ -47,4 +47,17 @@ struct Tile {
   }
 };
 
+// Global -> shared copies issued back to back without waiting (cp.async);
+// load_wait() completes this lane's copies, a tile sync then publishes them.
+__device__ inline void cp_async8(double* dst_shared, const double* src_global) {
+  unsigned d = (unsigned)__cvta_generic_to_shared(dst_shared);
+  size_t s = __cvta_generic_to_global(src_global);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(s) : "memory");
+}
+template <int G>
+__device__ inline void load_async(const Tile<G>& T, double* dst_shared, const double* src_global, int n) {
+  for (int k = T.lane(); k < n; k += G) cp_async8(dst_shared + k, src_global + k);
+}
+__device__ inline void load_wait() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 }  // namespace pg
