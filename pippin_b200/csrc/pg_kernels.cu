@@ -88,6 +88,7 @@ __global__ void __launch_bounds__(256) smooth_kernel(const __grid_constant__ Ste
     double* wk = A.work + env * A.k.stride;
     e.geo = wk + A.k.geoms;
     double* ws = e.ws;
+    prefetch_l1(T, e.prm, sizeof(double) * m.pstride);
     load_async(T, ws + w.qpos, A.st.qpos + env * nq, nq);
     load_async(T, ws + w.qvel, A.st.qvel + env * nv, nv);
     if (A.ctrl_seq) {
@@ -115,7 +116,7 @@ __global__ void __launch_bounds__(256) smooth_kernel(const __grid_constant__ Ste
     T.sync();
     // the tree region is dead from here on: the factorisations use it
     int status = 0;
-    bool damped = has_implicit_terms(m, e.prm);
+    bool damped = has_implicit_terms(T, m, e.prm);
     if (factor_mass(T, m, w, e, 0.0, wk + A.k.qm)) {
       solve_auto(T, ws + w.fac, nv, nv, m.nblock, m.block_adr, m.dof_block, m.maxbs, ws + w.rinv, acc);
       copy_in(T, wk + A.k.a0, acc, nv);
@@ -162,6 +163,8 @@ __global__ void __launch_bounds__(256) collide_kernel(const __grid_constant__ St
     double* wk = A.work + env * A.k.stride;
     e.geo = wk + A.k.geoms;
     e.con = wk + A.k.contacts;
+    prefetch_l1(T, e.prm, sizeof(double) * m.pstride);
+    prefetch_l1(T, e.geo, sizeof(double) * G_STRIDE * m.ngeom);
     int status = 0;
     int ncon = collide(T, m, A.w, A.s, e, &status);
     if (T.lane() == 0) {
@@ -199,10 +202,12 @@ __global__ void __launch_bounds__(256) newton_kernel(const __grid_constant__ Ste
     e.geo = wk + A.k.geoms;
     e.con = wk + A.k.contacts;
     double* ws = e.ws;
+    prefetch_l1(T, e.prm, sizeof(double) * m.pstride);
     int status = (int)wk[A.k.meta + K_META_STATUS];
     int ncon = (int)wk[A.k.meta + K_META_NCON];
     int iters = 0, nr = 0;
     if (!(status & ST_NOT_SPD)) {
+      prefetch_l1(T, e.con, sizeof(double) * C_STRIDE * ncon);
       load_async(T, ws + w.qpos, A.st.qpos + env * nq, nq);
       load_async(T, ws + w.qvel, A.st.qvel + env * nv, nv);
       load_async(T, ws + w.qacc, A.st.qacc + env * nv, nv);

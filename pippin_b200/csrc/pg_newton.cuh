@@ -815,8 +815,10 @@ __device__ bool factor_mass(const Tile<G>& T, const DModel& m, const WsLayout& w
   load_async(T, F, qm, nv * nv);
   load_wait();
   T.sync();
-  for (int k = lane; k < nv; k += G) F[k * nv + k] += h * e.prm[m.p_damping + k];
-  T.sync();
+  if (h != 0.0) {
+    for (int k = lane; k < nv; k += G) F[k * nv + k] += h * e.prm[m.p_damping + k];
+    T.sync();
+  }
   if (m.integrator == 1 && lane == 0) {  // implicitfast actuator terms (rare path)
     for (int u = 0; u < m.nu; u++) {
       double kv = -e.prm[m.p_bias + 3 * u + 2] * m.act_gear[u] * m.act_gear[u];
@@ -836,14 +838,14 @@ __device__ bool factor_mass(const Tile<G>& T, const DModel& m, const WsLayout& w
   return chol_auto(T, F, nv, nv, m.nblock, m.block_adr, m.dof_block, m.maxbs, ws + w.rinv);
 }
 
-// forward.rs:454-456
-__device__ inline bool has_implicit_terms(const DModel& m, const double* prm) {
-  for (int k = 0; k < m.nv; k++)
-    if (prm[m.p_damping + k] != 0.0) return true;
+// forward.rs:454-456 (the tile checks its share of dofs and actuators at once)
+template <int G>
+__device__ inline bool has_implicit_terms(const Tile<G>& T, const DModel& m, const double* prm) {
+  bool any = false;
+  for (int k = T.lane(); k < m.nv; k += G) any |= prm[m.p_damping + k] != 0.0;
   if (m.integrator == 1)
-    for (int u = 0; u < m.nu; u++)
-      if (prm[m.p_bias + 3 * u + 2] != 0.0) return true;
-  return false;
+    for (int u = T.lane(); u < m.nu; u += G) any |= prm[m.p_bias + 3 * u + 2] != 0.0;
+  return T.any(any);
 }
 
 // forward.rs:459-480

@@ -60,4 +60,14 @@ __device__ inline void load_async(const Tile<G>& T, double* dst_shared, const do
 }
 __device__ inline void load_wait() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
+// Pull `bytes` of global memory into L1 (one 128-byte line per request,
+// spread over the tile's lanes), so that the dependent loads that follow hit
+// L1 instead of waiting on L2 one after another.
+template <int G>
+__device__ inline void prefetch_l1(const Tile<G>& T, const void* p, size_t bytes) {
+  const char* c = static_cast<const char*>(p);
+  for (size_t off = (size_t)T.lane() * 128; off < bytes; off += (size_t)G * 128)
+    asm volatile("prefetch.global.L1 [%0];\n" ::"l"(c + off));
+}
+
 }  // namespace pg
