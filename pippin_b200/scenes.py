@@ -180,3 +180,124 @@ def hull_tumble_xml(n_hulls: int = 8, seed: int = 0, timestep: float = 0.002) ->
                       f'<freejoint/><geom type="mesh" mesh="h{i}"/></body>')
     return (f'<mujoco model="hull_tumble"><option timestep="{_fmt(timestep)}"/><asset>{"".join(assets)}</asset>'
             f'<worldbody><geom name="floor" type="plane" size="5 5 .1"/>{"".join(bodies)}</worldbody></mujoco>')
+
+
+class TabletopPlan:
+    """A tabletop model shared by every env plus the per-env parameters that
+    make each env different (the slot scheme of python/pippin/scene.py:21-25,
+    325-346): each object slot is a free body holding one geom per candidate
+    shape (box, cylinder, sphere); per env the chosen candidate is enabled
+    (contype/conaffinity 1) and sized, the others are removed from collision,
+    and the body takes the chosen shape's mass and inertia. Unused slots are
+    parked on the floor far from the table with their box enabled."""
+
+    def __init__(self, xml, nq, params, qpos0):
+        self.xml = xml
+        self.nq = nq
+        self.params = params  # [(param id, element, (envs, width) values)], applied in order
+        self.qpos0 = qpos0    # (envs, nq) reset pose
+
+    def apply(self, set_param, reset):
+        """set_param(param_id, element, values) for all envs; then the reset
+        pose (param 11) and reset(), so that qpos starts at it."""
+        for p, elem, vals in self.params:
+            set_param(p, elem, vals)
+        set_param(11, 0, self.qpos0)
+        reset()
+
+
+def tabletop(num_envs: int, seed: int = 0, slots: int = 6, count=(2, 6), timestep: float = 0.002,
+             table=(0.5, 0.4), height: float = 0.4, thickness: float = 0.02) -> TabletopPlan:
+    """Config-3 tabletop: a plane, a table (top and four legs) and `slots`
+    object slots; per env `count` objects (uniform integer range) drawn from
+    {box with half-extents U[0.015, 0.035]^3, cylinder with radius
+    U[0.015, 0.03] and half-height U[0.02, 0.05], sphere with radius
+    U[0.015, 0.035]}, friction U[0.3, 1.0], density U[500, 1500], dropped
+    5-15 cm above the table top at a uniform random orientation."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    tx, ty = table
+    z_top = height
+    legs = (height - 2 * thickness) / 2
+    body = [f'<body name="table" pos="0 0 0"><geom name="table_top" type="box" pos="0 0 {_fmt(height - thickness)}" '
+            f'size="{_fmt(tx)} {_fmt(ty)} {_fmt(thickness)}"/>']
+    for i, (sx, sy) in enumerate([(1, 1), (1, -1), (-1, 1), (-1, -1)]):
+        body.append(f'<geom name="table_leg{i}" type="box" pos="{_fmt(sx * (tx - 0.03))} {_fmt(sy * (ty - 0.03))} '
+                    f'{_fmt(legs)}" size="0.02 0.02 {_fmt(legs)}"/>')
+    body.append('</body>')
+    for s in range(slots):
+        body.append(f'<body name="slot{s}" pos="{_fmt(100 + 2 * s)} 0 0.05"><freejoint name="slot{s}_joint"/>'
+                    f'<geom name="slot{s}_c0" type="box" size="0.035 0.035 0.035"/>'
+                    f'<geom name="slot{s}_c1" type="cylinder" size="0.03 0.05"/>'
+                    f'<geom name="slot{s}_c2" type="sphere" size="0.035"/></body>')
+    xml = (f'<mujoco model="tabletop"><option timestep="{_fmt(timestep)}"/><worldbody>'
+           f'<geom name="floor" type="plane" size="5 5 .1"/>{"".join(body)}</worldbody></mujoco>')
+    # ids follow the compiler's order: world 0, table 1, slots 2..; geoms floor 0,
+    # table 1..5, then 3 per slot; each slot's free joint takes 7 qpos
+    ngeom_static = 6
+    nq = 7 * slots
+    n = num_envs
+    shape = lambda k: (n, k)
+    contype = np.zeros((slots, 3, n, 1))
+    size = np.zeros((slots, 3, n, 3))
+    fric = np.zeros((slots, 3, n, 1))
+    rgba = np.zeros((slots, 3, n, 4))
+    mass = np.zeros((slots, n, 1))
+    inertia = np.zeros((slots, n, 3))
+    qpos0 = np.zeros((n, nq))
+    nominal = [(0.035, 0.035, 0.035), (0.03, 0.05, 0.0), (0.035, 0.0, 0.0)]
+    for e in range(n):
+        k = int(rng.integers(count[0], count[1] + 1))
+        placed = []
+        for s in range(slots):
+            active = s < k
+            c = int(rng.integers(3)) if active else 0
+            dens = rng.uniform(500, 1500)
+            mu = rng.uniform(0.3, 1.0)
+            col = (*rng.uniform(0.2, 0.9, 3), 1.0)
+            if c == 0:
+                a, b, cc = rng.uniform(0.015, 0.035, 3)
+                m = dens * 8 * a * b * cc
+                sz, I = (a, b, cc), (m * (b * b + cc * cc) / 3, m * (a * a + cc * cc) / 3, m * (a * a + b * b) / 3)
+                rad, rest = math.sqrt(a * a + b * b + cc * cc), cc
+            elif c == 1:
+                r, h = rng.uniform(0.015, 0.03), rng.uniform(0.02, 0.05)
+                m = dens * math.pi * r * r * 2 * h
+                ix = m * (3 * r * r + 4 * h * h) / 12
+                sz, I = (r, h, 0.0), (ix, ix, m * r * r / 2)
+                rad, rest = math.sqrt(r * r + h * h), h
+            else:
+                r = rng.uniform(0.015, 0.035)
+                m = dens * 4 / 3 * math.pi * r ** 3
+                sz, I = (r, 0.0, 0.0), (0.4 * m * r * r,) * 3
+                rad, rest = r, r
+            for ci in range(3):
+                on = (ci == c) and active or (not active and ci == 0)
+                contype[s, ci, e, 0] = 1.0 if on else 0.0
+                size[s, ci, e] = sz if ci == c else nominal[ci]
+                fric[s, ci, e, 0] = mu
+                rgba[s, ci, e] = col if (ci == c and active) else (0, 0, 0, 0)
+            mass[s, e, 0] = m
+            inertia[s, e] = I
+            q = qpos0[e, 7 * s:7 * s + 7]
+            if active:
+                for _ in range(100):
+                    x, y = rng.uniform(-tx + 0.1, tx - 0.1), rng.uniform(-ty + 0.1, ty - 0.1)
+                    if all((x - px) ** 2 + (y - py) ** 2 > (rad + pr) ** 2 for px, py, pr in placed):
+                        break
+                placed.append((x, y, rad))
+                w = rng.normal(size=4)
+                w /= np.linalg.norm(w)
+                q[:] = (x, y, z_top + rad + rng.uniform(0.05, 0.15), *w)
+            else:
+                q[:] = (100 + 2 * s + 0.01 * e, 0.0, rest + 1e-3, 1.0, 0.0, 0.0, 0.0)
+    params = []
+    for s in range(slots):
+        for ci in range(3):
+            g = ngeom_static + 3 * s + ci
+            params += [(3, g, contype[s, ci]), (4, g, contype[s, ci]), (1, g, size[s, ci]), (0, g, fric[s, ci]),
+                       (2, g, rgba[s, ci])]
+        b = 2 + s
+        params += [(5, b, mass[s]), (9, b, inertia[s])]  # mass first: it rescales inertia (params.rs:145-156)
+    return TabletopPlan(xml, nq, params, qpos0)
