@@ -14,8 +14,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libpippin_b200.so")
-SOURCES = ["pg_kernels.cu", "pg_api.cpp", "pg_peak.cu", "pg_noalloc.cu"]
-HEADERS = ["pg_math.cuh", "pg_model.h", "pg_tile.cuh", "pg_dynamics.cuh", "pg_collide.cuh", "pg_linalg.cuh", "pg_small.cuh", "pg_pgs.cuh", "pg_general.cuh",
+SOURCES = ["pg_kernels.cu", "pg_api.cpp", "pg_peak.cu", "pg_noalloc.cu", "pg_mlp.cu"]
+HEADERS = ["pg_math.cuh", "pg_model.h", "pg_tile.cuh", "pg_dynamics.cuh", "pg_collide.cuh", "pg_linalg.cuh", "pg_small.cuh", "pg_pgs.cuh", "pg_general.cuh", "pg_mlp.h",
            "pg_newton.cuh", "pg_kernels.h"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
               "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
@@ -33,7 +33,7 @@ def _stale() -> bool:
         return True
     t = os.path.getmtime(LIB)
     deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS]
-    deps += [os.path.join(HERE, "..", "include", h) for h in ("pippin_b200.h", "pippin_b200_tools.h")]
+    deps += [os.path.join(HERE, "..", "include", h) for h in ("pippin_b200.h", "pippin_b200_tools.h", "pippin_b200_mlp.h")]
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 

@@ -1,0 +1,508 @@
+// The learned warm start's network: inference on the tensor cores and
+// training kernels.
+//
+// Inference (mlp_forward_kernel): one warp per 16 samples, mma.sync
+// m16n8k16 with BF16 operands and FP32 accumulation. The BF16 weights (84 KB
+// with row padding) are staged in shared memory once per block; a layer's
+// FP32 accumulator fragments become the next layer's BF16 A fragments in
+// registers (the C layout of one n8 tile pair is the A layout of one k16
+// tile), so activations never leave the warp.
+//
+// Training (mlp_train_*): FP32 throughout (master weights, activations,
+// gradients, Adam moments), simple tiled kernels: the network is small
+// (36,611 parameters) and a batch of a few thousand samples is a few GFLOP.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "pg_mlp.h"
+
+namespace pg {
+
+static uint16_t to_bf16(float x) {
+  __nv_bfloat16 b = __float2bfloat16_rn(x);
+  uint16_t u;
+  std::memcpy(&u, &b, 2);
+  return u;
+}
+
+void mlp_pack(const float* wt, uint16_t* w, float* f) {
+  std::fill(w, w + MLP_BF16_ELEMS, to_bf16(0.0f));
+  std::fill(f, f + MLP_F32_ELEMS, 0.0f);
+  uint16_t* w1 = w;
+  uint16_t* w2 = w1 + MLP_H * MLP_LD1;
+  uint16_t* w3 = w2 + MLP_H * MLP_LDH;
+  uint16_t* w4 = w3 + MLP_H * MLP_LDH;
+  for (int n = 0; n < MLP_H; n++)
+    for (int k = 0; k < MLP_IN; k++) w1[n * MLP_LD1 + k] = to_bf16(wt[MLP_W1 + n * MLP_IN + k]);
+  for (int n = 0; n < MLP_H; n++)
+    for (int k = 0; k < MLP_H; k++) {
+      w2[n * MLP_LDH + k] = to_bf16(wt[MLP_W2 + n * MLP_H + k]);
+      w3[n * MLP_LDH + k] = to_bf16(wt[MLP_W3 + n * MLP_H + k]);
+    }
+  for (int n = 0; n < MLP_OUT; n++)
+    for (int k = 0; k < MLP_H; k++) w4[n * MLP_LDH + k] = to_bf16(wt[MLP_W4 + n * MLP_H + k]);
+  std::memcpy(f, wt + MLP_IN_MEAN, sizeof(float) * (2 * MLP_IN + MLP_OUT));
+  float* b = f + 2 * MLP_IN + MLP_OUT;
+  std::memcpy(b, wt + MLP_B1, sizeof(float) * MLP_H);
+  std::memcpy(b + MLP_H, wt + MLP_B2, sizeof(float) * MLP_H);
+  std::memcpy(b + 2 * MLP_H, wt + MLP_B3, sizeof(float) * MLP_H);
+  std::memcpy(b + 3 * MLP_H, wt + MLP_B4, sizeof(float) * MLP_OUT);
+}
+
+// ---------------------------------------------------------------- inference
+__device__ inline uint32_t pack_bf16(float lo, float hi) {
+  __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<uint32_t*>(&v);
+}
+
+__device__ inline void mma_bf16(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// B fragment of W (row n = output, k = input; row stride ld) for the n8 tile
+// at n0 and the k16 tile at k0
+__device__ inline void bfrag(const uint16_t* W, int ld, int n0, int k0, int g, int tq, uint32_t* b0, uint32_t* b1) {
+  const uint16_t* r = W + (n0 + g) * ld + k0 + 2 * tq;
+  *b0 = *reinterpret_cast<const uint32_t*>(r);
+  *b1 = *reinterpret_cast<const uint32_t*>(r + 8);
+}
+
+// one hidden layer: acc = A W^T over KT k-tiles, bias, ReLU, repacked as the
+// next layer's A fragments (8 k-tiles of 16)
+template <int KT>
+__device__ inline void hidden_layer(const uint32_t (&a)[KT][4], const uint16_t* W, int ld, const float* bias, int g,
+                                    int tq, uint32_t (&out)[8][4]) {
+#pragma unroll
+  for (int t = 0; t < 8; t++) {  // output k-tile t = n-tiles 2t, 2t+1
+    float c0[4] = {0.f, 0.f, 0.f, 0.f}, c1[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int kt = 0; kt < KT; kt++) {
+      uint32_t b0, b1;
+      bfrag(W, ld, 16 * t, 16 * kt, g, tq, &b0, &b1);
+      mma_bf16(c0, a[kt], b0, b1);
+      bfrag(W, ld, 16 * t + 8, 16 * kt, g, tq, &b0, &b1);
+      mma_bf16(c1, a[kt], b0, b1);
+    }
+    int n0 = 16 * t + 2 * tq, n1 = n0 + 8;
+    out[t][0] = pack_bf16(fmaxf(c0[0] + bias[n0], 0.f), fmaxf(c0[1] + bias[n0 + 1], 0.f));
+    out[t][1] = pack_bf16(fmaxf(c0[2] + bias[n0], 0.f), fmaxf(c0[3] + bias[n0 + 1], 0.f));
+    out[t][2] = pack_bf16(fmaxf(c1[0] + bias[n1], 0.f), fmaxf(c1[1] + bias[n1 + 1], 0.f));
+    out[t][3] = pack_bf16(fmaxf(c1[2] + bias[n1], 0.f), fmaxf(c1[3] + bias[n1 + 1], 0.f));
+  }
+}
+
+constexpr int MLP_WARPS = 4;  // 64 samples per block
+
+__global__ void __launch_bounds__(32 * MLP_WARPS) mlp_forward_kernel(MlpDevice d, const float* X, int64_t n, float* Y) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  uint16_t* W = reinterpret_cast<uint16_t*>(smem);
+  float* F = reinterpret_cast<float*>(smem + sizeof(uint16_t) * MLP_BF16_ELEMS);
+  {
+    const int4* src = reinterpret_cast<const int4*>(d.w);
+    int4* dst = reinterpret_cast<int4*>(W);
+    for (int i = threadIdx.x; i < (int)(sizeof(uint16_t) * MLP_BF16_ELEMS / 16); i += blockDim.x) dst[i] = src[i];
+    for (int i = threadIdx.x; i < MLP_F32_ELEMS; i += blockDim.x) F[i] = d.f[i];
+  }
+  __syncthreads();
+  const uint16_t* W1 = W;
+  const uint16_t* W2 = W1 + MLP_H * MLP_LD1;
+  const uint16_t* W3 = W2 + MLP_H * MLP_LDH;
+  const uint16_t* W4 = W3 + MLP_H * MLP_LDH;
+  const float* mean = F;
+  const float* scale = F + MLP_IN;
+  const float* oscale = F + 2 * MLP_IN;
+  const float* b1 = F + 2 * MLP_IN + MLP_OUT;
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int g = lane >> 2, tq = lane & 3;
+  for (int64_t base = ((int64_t)blockIdx.x * MLP_WARPS + warp) * 16; base < n; base += (int64_t)gridDim.x * MLP_WARPS * 16) {
+    int64_t r0 = base + g, r1 = base + g + 8;
+    auto x = [&](int64_t r, int c) -> float {
+      return (r < n && c < MLP_IN) ? (X[r * MLP_IN + c] - mean[c]) * scale[c] : 0.f;
+    };
+    uint32_t a1[2][4];
+#pragma unroll
+    for (int kt = 0; kt < 2; kt++) {
+      int c = 16 * kt + 2 * tq;
+      a1[kt][0] = pack_bf16(x(r0, c), x(r0, c + 1));
+      a1[kt][1] = pack_bf16(x(r1, c), x(r1, c + 1));
+      a1[kt][2] = pack_bf16(x(r0, c + 8), x(r0, c + 9));
+      a1[kt][3] = pack_bf16(x(r1, c + 8), x(r1, c + 9));
+    }
+    uint32_t h1[8][4], h2[8][4];
+    hidden_layer<2>(a1, W1, MLP_LD1, b1, g, tq, h1);
+    hidden_layer<8>(h1, W2, MLP_LDH, b1 + MLP_H, g, tq, h2);
+    hidden_layer<8>(h2, W3, MLP_LDH, b1 + 2 * MLP_H, g, tq, h1);
+    float c[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int kt = 0; kt < 8; kt++) {
+      uint32_t b0, bb;
+      bfrag(W4, MLP_LDH, 0, 16 * kt, g, tq, &b0, &bb);
+      mma_bf16(c, h1[kt], b0, bb);
+    }
+    const float* b4 = b1 + 3 * MLP_H;
+    for (int j = 0; j < 4; j++) {
+      int col = 2 * tq + (j & 1);
+      int64_t r = j < 2 ? r0 : r1;
+      if (col < MLP_OUT && r < n) Y[r * MLP_OUT + col] = (c[j] + b4[col]) * oscale[col];
+    }
+  }
+}
+
+cudaError_t mlp_forward(const MlpDevice& d, const float* X, int64_t n, float* Y, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  size_t smem = sizeof(uint16_t) * MLP_BF16_ELEMS + sizeof(float) * MLP_F32_ELEMS;
+  cudaError_t e = cudaFuncSetAttribute(mlp_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int64_t blocks = (n + 16 * MLP_WARPS - 1) / (16 * MLP_WARPS);
+  if (blocks > 2048) blocks = 2048;
+  mlp_forward_kernel<<<(unsigned)blocks, 32 * MLP_WARPS, smem, s>>>(d, X, n, Y);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- training
+// C[i][j] = act(sum_k A(i, k) B(k, j) + bias[j]), A(i, k) = A[i*sai + k*sak],
+// B(k, j) = B[k*sbk + j*sbj]; act = ReLU when relu != 0; rows of C are
+// multiplied by (mask[i][j] > 0) when a mask is given (the ReLU derivative)
+constexpr int GT = 32;
+__global__ void __launch_bounds__(256) gemm_kernel(int M, int N, int K, const float* A, long sai, long sak,
+                                                   const float* B, long sbk, long sbj, float* C, const float* bias,
+                                                   int relu, const float* mask) {
+  __shared__ float As[GT][GT + 1], Bs[GT][GT + 1];
+  int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  int i0 = blockIdx.y * GT, j0 = blockIdx.x * GT;
+  float acc[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
+  for (int k0 = 0; k0 < K; k0 += GT) {
+    for (int t = threadIdx.x; t < GT * GT; t += 256) {
+      int r = t / GT, c = t % GT;
+      int i = i0 + r, k = k0 + c;
+      As[r][c] = (i < M && k < K) ? A[i * sai + k * sak] : 0.f;
+      int kk = k0 + r, j = j0 + c;
+      Bs[r][c] = (kk < K && j < N) ? B[kk * sbk + j * sbj] : 0.f;
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int k = 0; k < GT; k++) {
+      float a0 = As[2 * ty][k], a1 = As[2 * ty + 1][k];
+      float b0 = Bs[k][2 * tx], b1 = Bs[k][2 * tx + 1];
+      acc[0][0] += a0 * b0;
+      acc[0][1] += a0 * b1;
+      acc[1][0] += a1 * b0;
+      acc[1][1] += a1 * b1;
+    }
+    __syncthreads();
+  }
+  for (int u = 0; u < 2; u++)
+    for (int v = 0; v < 2; v++) {
+      int i = i0 + 2 * ty + u, j = j0 + 2 * tx + v;
+      if (i >= M || j >= N) continue;
+      float x = acc[u][v] + (bias ? bias[j] : 0.f);
+      if (relu) x = fmaxf(x, 0.f);
+      if (mask && !(mask[(long)i * N + j] > 0.f)) x = 0.f;
+      C[(long)i * N + j] = x;
+    }
+}
+
+static cudaError_t gemm(int M, int N, int K, const float* A, long sai, long sak, const float* B, long sbk, long sbj,
+                        float* C, const float* bias, int relu, const float* mask, cudaStream_t s) {
+  dim3 grid((N + GT - 1) / GT, (M + GT - 1) / GT);
+  gemm_kernel<<<grid, 256, 0, s>>>(M, N, K, A, sai, sak, B, sbk, sbj, C, bias, relu, mask);
+  return cudaGetLastError();
+}
+
+// db[j] = sum_i dY[i][j]
+__global__ void colsum_kernel(const float* dY, int M, int N, float* db) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= N) return;
+  float s = 0.f;
+  for (int i = 0; i < M; i++) s += dY[(long)i * N + j];
+  db[j] = s;
+}
+
+// dO = 2 (O - Y) / (M * 3); loss += sum (O - Y)^2 / (M * 3)
+__global__ void mse_kernel(const float* O, const float* Y, int M, float* dO, double* loss) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= M * MLP_OUT) return;
+  float d = O[t] - Y[t];
+  float inv = 1.0f / (float)(M * MLP_OUT);
+  dO[t] = 2.0f * d * inv;
+  atomicAdd(loss, (double)(d * d) * inv);
+}
+
+// Adam (Kingma & Ba 2015) on every parameter
+__global__ void adam_kernel(float* p, const float* g, float* m, float* v, int n, float lr, float b1, float b2,
+                            float eps, float c1, float c2) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  float gt = g[t];
+  float mt = b1 * m[t] + (1.f - b1) * gt, vt = b2 * v[t] + (1.f - b2) * gt * gt;
+  m[t] = mt;
+  v[t] = vt;
+  p[t] -= lr * (mt / c1) / (sqrtf(vt / c2) + eps);
+}
+
+// rows of src picked by idx into dst (width w)
+__global__ void gather_kernel(const float* src, const int* idx, int n, int w, float* dst) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n * w) return;
+  dst[t] = src[(long)idx[t / w] * w + t % w];
+}
+
+// Forward and backward of the normalised network on one batch: activations
+// in H (3 x M x 128) and O (M x 3), gradients of the mean squared error into
+// grad (same layout as the parameters). P and grad start at W1.
+struct TrainBufs {
+  float *H, *O, *dO, *dA, *dB;
+  double* loss;
+};
+static cudaError_t mlp_batch_grad(const float* P, const float* Xn, const float* Yn, int M, float* grad,
+                                  const TrainBufs& t, cudaStream_t s) {
+  auto w = [&](int off) { return P + (off - MLP_W1); };
+  auto gw = [&](int off) { return grad + (off - MLP_W1); };
+  float* H1 = t.H;
+  float* H2 = t.H + (long)M * MLP_H;
+  float* H3 = t.H + 2L * M * MLP_H;
+  cudaError_t e;
+#define G_(call) \
+  if ((e = (call)) != cudaSuccess) return e
+  G_(gemm(M, MLP_H, MLP_IN, Xn, MLP_IN, 1, w(MLP_W1), 1, MLP_IN, H1, w(MLP_B1), 1, nullptr, s));
+  G_(gemm(M, MLP_H, MLP_H, H1, MLP_H, 1, w(MLP_W2), 1, MLP_H, H2, w(MLP_B2), 1, nullptr, s));
+  G_(gemm(M, MLP_H, MLP_H, H2, MLP_H, 1, w(MLP_W3), 1, MLP_H, H3, w(MLP_B3), 1, nullptr, s));
+  G_(gemm(M, MLP_OUT, MLP_H, H3, MLP_H, 1, w(MLP_W4), 1, MLP_H, t.O, w(MLP_B4), 0, nullptr, s));
+  mse_kernel<<<(M * MLP_OUT + 255) / 256, 256, 0, s>>>(t.O, Yn, M, t.dO, t.loss);
+  // layer 4: dW4 = dO' H3, db4, dH3 = dO W4 * (H3 > 0)
+  G_(gemm(MLP_OUT, MLP_H, M, t.dO, 1, MLP_OUT, H3, MLP_H, 1, gw(MLP_W4), nullptr, 0, nullptr, s));
+  colsum_kernel<<<1, 32, 0, s>>>(t.dO, M, MLP_OUT, gw(MLP_B4));
+  G_(gemm(M, MLP_H, MLP_OUT, t.dO, MLP_OUT, 1, w(MLP_W4), MLP_H, 1, t.dA, nullptr, 0, H3, s));
+  // layer 3
+  G_(gemm(MLP_H, MLP_H, M, t.dA, 1, MLP_H, H2, MLP_H, 1, gw(MLP_W3), nullptr, 0, nullptr, s));
+  colsum_kernel<<<1, MLP_H, 0, s>>>(t.dA, M, MLP_H, gw(MLP_B3));
+  G_(gemm(M, MLP_H, MLP_H, t.dA, MLP_H, 1, w(MLP_W3), MLP_H, 1, t.dB, nullptr, 0, H2, s));
+  // layer 2
+  G_(gemm(MLP_H, MLP_H, M, t.dB, 1, MLP_H, H1, MLP_H, 1, gw(MLP_W2), nullptr, 0, nullptr, s));
+  colsum_kernel<<<1, MLP_H, 0, s>>>(t.dB, M, MLP_H, gw(MLP_B2));
+  G_(gemm(M, MLP_H, MLP_H, t.dB, MLP_H, 1, w(MLP_W2), MLP_H, 1, t.dA, nullptr, 0, H1, s));
+  // layer 1
+  G_(gemm(MLP_H, MLP_IN, M, t.dA, 1, MLP_H, Xn, MLP_IN, 1, gw(MLP_W1), nullptr, 0, nullptr, s));
+  colsum_kernel<<<1, MLP_H, 0, s>>>(t.dA, M, MLP_H, gw(MLP_B1));
+#undef G_
+  return cudaGetLastError();
+}
+
+}  // namespace pg
+
+// ---------------------------------------------------------------- C-ABI
+#include "../../include/pippin_b200.h"
+#include "../../include/pippin_b200_mlp.h"
+
+namespace pg {
+void internal_set_error(const std::string& msg);
+}
+
+namespace {
+
+using namespace pg;
+
+int mlp_fail(int code, const std::string& msg) {
+  internal_set_error(msg);
+  return code;
+}
+#define MCK(x)                                                                                  \
+  do {                                                                                          \
+    cudaError_t _e = (x);                                                                       \
+    if (_e != cudaSuccess) return mlp_fail(PG_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(_e)); \
+  } while (0)
+
+// device buffers freed on scope exit
+struct DevBufs {
+  std::vector<void*> ptrs;
+  ~DevBufs() {
+    for (void* p : ptrs) cudaFree(p);
+  }
+  template <class T>
+  cudaError_t alloc(T** p, size_t n) {
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, sizeof(T) * std::max<size_t>(n, 1));
+    if (e == cudaSuccess) ptrs.push_back(q);
+    *p = static_cast<T*>(q);
+    return e;
+  }
+};
+
+// normalised copies of X (with the blob's mean and scale) and Y (/ out scale)
+void normalise(const float* wt, const float* X, const float* Y, int64_t n, std::vector<float>& Xn,
+               std::vector<float>& Yn) {
+  Xn.resize((size_t)n * MLP_IN);
+  Yn.resize((size_t)n * MLP_OUT);
+  for (int64_t i = 0; i < n; i++) {
+    for (int k = 0; k < MLP_IN; k++)
+      Xn[i * MLP_IN + k] = (X[i * MLP_IN + k] - wt[MLP_IN_MEAN + k]) * wt[MLP_IN_SCALE + k];
+    for (int k = 0; k < MLP_OUT; k++) Yn[i * MLP_OUT + k] = Y[i * MLP_OUT + k] / wt[MLP_OUT_SCALE + k];
+  }
+}
+
+uint64_t splitmix(uint64_t& s) {
+  uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+double uniform01(uint64_t& s) { return (double)(splitmix(s) >> 11) * (1.0 / 9007199254740992.0); }
+
+}  // namespace
+
+extern "C" {
+
+int pg_mlp_forward(const float* weights, size_t wlen, const float* X, int64_t n, float* Y) {
+  if (!weights || wlen != (size_t)MLP_SIZE) return mlp_fail(PG_ERR_LENGTH, "mlp weights must hold 36662 floats");
+  if (n < 0 || (n > 0 && (!X || !Y))) return mlp_fail(PG_ERR_INVALID, "NULL argument");
+  if (n == 0) return PG_OK;
+  std::vector<uint16_t> wb(MLP_BF16_ELEMS);
+  std::vector<float> fb(MLP_F32_ELEMS);
+  mlp_pack(weights, wb.data(), fb.data());
+  DevBufs d;
+  uint16_t* dw;
+  float *df, *dx, *dy;
+  MCK(d.alloc(&dw, MLP_BF16_ELEMS));
+  MCK(d.alloc(&df, MLP_F32_ELEMS));
+  MCK(d.alloc(&dx, (size_t)n * MLP_IN));
+  MCK(d.alloc(&dy, (size_t)n * MLP_OUT));
+  MCK(cudaMemcpy(dw, wb.data(), sizeof(uint16_t) * MLP_BF16_ELEMS, cudaMemcpyHostToDevice));
+  MCK(cudaMemcpy(df, fb.data(), sizeof(float) * MLP_F32_ELEMS, cudaMemcpyHostToDevice));
+  MCK(cudaMemcpy(dx, X, sizeof(float) * n * MLP_IN, cudaMemcpyHostToDevice));
+  MCK(mlp_forward(MlpDevice{dw, df}, dx, n, dy, 0));
+  MCK(cudaMemcpy(Y, dy, sizeof(float) * n * MLP_OUT, cudaMemcpyDeviceToHost));
+  return PG_OK;
+}
+
+int pg_mlp_loss_grad(const float* weights, size_t wlen, const float* X, const float* Y, int64_t n, float* grad,
+                     size_t glen, double* loss) {
+  if (!weights || wlen != (size_t)MLP_SIZE) return mlp_fail(PG_ERR_LENGTH, "mlp weights must hold 36662 floats");
+  if (!grad || glen != (size_t)MLP_PARAMS) return mlp_fail(PG_ERR_LENGTH, "gradient must hold 36611 floats");
+  if (n <= 0 || n > (1 << 24) || !X || !Y) return mlp_fail(PG_ERR_INVALID, "need 1 to 2^24 samples");
+  std::vector<float> Xn, Yn;
+  normalise(weights, X, Y, n, Xn, Yn);
+  int M = (int)n;
+  DevBufs d;
+  float *P, *G, *dX, *dY;
+  TrainBufs t;
+  MCK(d.alloc(&P, MLP_PARAMS));
+  MCK(d.alloc(&G, MLP_PARAMS));
+  MCK(d.alloc(&dX, (size_t)M * MLP_IN));
+  MCK(d.alloc(&dY, (size_t)M * MLP_OUT));
+  MCK(d.alloc(&t.H, 3 * (size_t)M * MLP_H));
+  MCK(d.alloc(&t.O, (size_t)M * MLP_OUT));
+  MCK(d.alloc(&t.dO, (size_t)M * MLP_OUT));
+  MCK(d.alloc(&t.dA, (size_t)M * MLP_H));
+  MCK(d.alloc(&t.dB, (size_t)M * MLP_H));
+  MCK(d.alloc(&t.loss, 1));
+  MCK(cudaMemcpy(P, weights + MLP_W1, sizeof(float) * MLP_PARAMS, cudaMemcpyHostToDevice));
+  MCK(cudaMemcpy(dX, Xn.data(), sizeof(float) * Xn.size(), cudaMemcpyHostToDevice));
+  MCK(cudaMemcpy(dY, Yn.data(), sizeof(float) * Yn.size(), cudaMemcpyHostToDevice));
+  MCK(cudaMemset(t.loss, 0, sizeof(double)));
+  MCK(mlp_batch_grad(P, dX, dY, M, G, t, 0));
+  MCK(cudaMemcpy(grad, G, sizeof(float) * MLP_PARAMS, cudaMemcpyDeviceToHost));
+  double l = 0.0;
+  MCK(cudaMemcpy(&l, t.loss, sizeof(double), cudaMemcpyDeviceToHost));
+  if (loss) *loss = l;
+  return PG_OK;
+}
+
+int pg_mlp_train(const float* X, const float* Y, int64_t n, int epochs, int batch, float lr, uint64_t seed,
+                 float* weights, size_t wlen, double* epoch_loss) {
+  if (!weights || wlen != (size_t)MLP_SIZE) return mlp_fail(PG_ERR_LENGTH, "mlp weights must hold 36662 floats");
+  if (n <= 0 || n > (1 << 26) || !X || !Y) return mlp_fail(PG_ERR_INVALID, "need 1 to 2^26 samples");
+  if (epochs < 0 || batch < 1 || batch > 65536 || !(lr > 0.0f)) return mlp_fail(PG_ERR_INVALID, "bad training options");
+  // normalisation: feature mean / std, target std (features of zero spread keep scale 1)
+  std::vector<float> wt(MLP_SIZE, 0.0f);
+  for (int k = 0; k < MLP_IN; k++) {
+    double s = 0.0, s2 = 0.0;
+    for (int64_t i = 0; i < n; i++) {
+      double x = X[i * MLP_IN + k];
+      s += x;
+      s2 += x * x;
+    }
+    double mean = s / n, var = std::max(s2 / n - mean * mean, 0.0);
+    wt[MLP_IN_MEAN + k] = (float)mean;
+    wt[MLP_IN_SCALE + k] = var > 1e-20 ? (float)(1.0 / std::sqrt(var)) : 1.0f;
+  }
+  for (int k = 0; k < MLP_OUT; k++) {
+    double s2 = 0.0;
+    for (int64_t i = 0; i < n; i++) s2 += (double)Y[i * MLP_OUT + k] * Y[i * MLP_OUT + k];
+    double rms = std::sqrt(s2 / n);
+    wt[MLP_OUT_SCALE + k] = rms > 1e-20 ? (float)rms : 1.0f;
+  }
+  // He-uniform initialisation, zero biases
+  uint64_t st = seed;
+  auto init = [&](int off, int rows, int cols) {
+    double a = std::sqrt(6.0 / cols);
+    for (int i = 0; i < rows * cols; i++) wt[off + i] = (float)((2.0 * uniform01(st) - 1.0) * a);
+  };
+  init(MLP_W1, MLP_H, MLP_IN);
+  init(MLP_W2, MLP_H, MLP_H);
+  init(MLP_W3, MLP_H, MLP_H);
+  init(MLP_W4, MLP_OUT, MLP_H);
+  std::vector<float> Xn, Yn;
+  normalise(wt.data(), X, Y, n, Xn, Yn);
+  int M = (int)std::min<int64_t>(batch, n);
+  DevBufs d;
+  float *P, *G, *Mo, *Vo, *dX, *dY, *bX, *bY;
+  int* idx;
+  TrainBufs t;
+  MCK(d.alloc(&P, MLP_PARAMS));
+  MCK(d.alloc(&G, MLP_PARAMS));
+  MCK(d.alloc(&Mo, MLP_PARAMS));
+  MCK(d.alloc(&Vo, MLP_PARAMS));
+  MCK(d.alloc(&dX, (size_t)n * MLP_IN));
+  MCK(d.alloc(&dY, (size_t)n * MLP_OUT));
+  MCK(d.alloc(&bX, (size_t)M * MLP_IN));
+  MCK(d.alloc(&bY, (size_t)M * MLP_OUT));
+  MCK(d.alloc(&idx, (size_t)n));
+  MCK(d.alloc(&t.H, 3 * (size_t)M * MLP_H));
+  MCK(d.alloc(&t.O, (size_t)M * MLP_OUT));
+  MCK(d.alloc(&t.dO, (size_t)M * MLP_OUT));
+  MCK(d.alloc(&t.dA, (size_t)M * MLP_H));
+  MCK(d.alloc(&t.dB, (size_t)M * MLP_H));
+  MCK(d.alloc(&t.loss, 1));
+  MCK(cudaMemcpy(P, wt.data() + MLP_W1, sizeof(float) * MLP_PARAMS, cudaMemcpyHostToDevice));
+  MCK(cudaMemset(Mo, 0, sizeof(float) * MLP_PARAMS));
+  MCK(cudaMemset(Vo, 0, sizeof(float) * MLP_PARAMS));
+  MCK(cudaMemcpy(dX, Xn.data(), sizeof(float) * Xn.size(), cudaMemcpyHostToDevice));
+  MCK(cudaMemcpy(dY, Yn.data(), sizeof(float) * Yn.size(), cudaMemcpyHostToDevice));
+  std::vector<int> perm((size_t)n);
+  const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+  int64_t step = 0;
+  for (int ep = 0; ep < epochs; ep++) {
+    for (int64_t i = 0; i < n; i++) perm[i] = (int)i;
+    for (int64_t i = n - 1; i > 0; i--) std::swap(perm[i], perm[(size_t)(uniform01(st) * (i + 1))]);
+    MCK(cudaMemcpy(idx, perm.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    MCK(cudaMemset(t.loss, 0, sizeof(double)));
+    int nb = 0;
+    for (int64_t s0 = 0; s0 + M <= n; s0 += M, nb++) {
+      gather_kernel<<<(M * MLP_IN + 255) / 256, 256>>>(dX, idx + s0, M, MLP_IN, bX);
+      gather_kernel<<<(M * MLP_OUT + 255) / 256, 256>>>(dY, idx + s0, M, MLP_OUT, bY);
+      MCK(mlp_batch_grad(P, bX, bY, M, G, t, 0));
+      step++;
+      float c1 = 1.f - std::pow(b1, (float)step), c2 = 1.f - std::pow(b2, (float)step);
+      adam_kernel<<<(MLP_PARAMS + 255) / 256, 256>>>(P, G, Mo, Vo, MLP_PARAMS, lr, b1, b2, eps, c1, c2);
+      MCK(cudaGetLastError());
+    }
+    double l = 0.0;
+    MCK(cudaMemcpy(&l, t.loss, sizeof(double), cudaMemcpyDeviceToHost));
+    if (epoch_loss) epoch_loss[ep] = nb ? l / nb : 0.0;
+  }
+  MCK(cudaMemcpy(wt.data() + MLP_W1, P, sizeof(float) * MLP_PARAMS, cudaMemcpyDeviceToHost));
+  std::memcpy(weights, wt.data(), sizeof(float) * MLP_SIZE);
+  return PG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,47 @@
+// Layout of the learned warm start's network (24 -> 128 -> 128 -> 128 -> 3,
+// ReLU between layers) as one FP32 array: input normalisation, output scale,
+// then each layer's weights [out][in] and bias.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+namespace pg {
+
+constexpr int MLP_IN = 24, MLP_H = 128, MLP_OUT = 3;
+constexpr int MLP_IN_MEAN = 0;                              // [24] feature mean
+constexpr int MLP_IN_SCALE = MLP_IN_MEAN + MLP_IN;          // [24] 1 / feature std
+constexpr int MLP_OUT_SCALE = MLP_IN_SCALE + MLP_IN;        // [3] target std
+constexpr int MLP_W1 = MLP_OUT_SCALE + MLP_OUT;             // [128][24]
+constexpr int MLP_B1 = MLP_W1 + MLP_H * MLP_IN;             // [128]
+constexpr int MLP_W2 = MLP_B1 + MLP_H;                      // [128][128]
+constexpr int MLP_B2 = MLP_W2 + MLP_H * MLP_H;
+constexpr int MLP_W3 = MLP_B2 + MLP_H;                      // [128][128]
+constexpr int MLP_B3 = MLP_W3 + MLP_H * MLP_H;
+constexpr int MLP_W4 = MLP_B3 + MLP_H;                      // [3][128]
+constexpr int MLP_B4 = MLP_W4 + MLP_OUT * MLP_H;            // [3]
+constexpr int MLP_SIZE = MLP_B4 + MLP_OUT;                  // 36662 floats
+constexpr int MLP_PARAMS = MLP_SIZE - MLP_W1;               // 36611 trained parameters
+
+// BF16 copy of the weights for the tensor-core forward pass, rows padded so
+// that the fragment loads of a warp hit distinct shared-memory banks
+constexpr int MLP_K1 = 32;                 // layer-1 inputs padded to a k-tile multiple
+constexpr int MLP_LD1 = MLP_K1 + 8;        // row stride of W1 (bf16)
+constexpr int MLP_LDH = MLP_H + 8;         // row stride of W2, W3, W4 (bf16)
+constexpr int MLP_N4 = 8;                  // layer-4 outputs padded to an n-tile
+constexpr int MLP_BF16_ELEMS = MLP_H * MLP_LD1 + 2 * MLP_H * MLP_LDH + MLP_N4 * MLP_LDH;
+// FP32 side data of the forward pass: in mean, in scale, out scale, biases
+constexpr int MLP_F32_ELEMS = 2 * MLP_IN + MLP_OUT + 3 * MLP_H + MLP_N4;
+
+struct MlpDevice {
+  const uint16_t* w;  // MLP_BF16_ELEMS bf16 (W1 | W2 | W3 | W4, padded)
+  const float* f;     // MLP_F32_ELEMS (in_mean | in_scale | out_scale | b1 | b2 | b3 | b4 padded)
+};
+
+// packs the FP32 array into the forward pass's device layout (host side)
+void mlp_pack(const float* weights, uint16_t* w_bf16, float* f32);
+// Y[n][3] = net(X[n][24]) on the tensor cores, on stream s
+cudaError_t mlp_forward(const MlpDevice& d, const float* X, int64_t n, float* Y, cudaStream_t s);
+
+}  // namespace pg
