@@ -191,6 +191,28 @@ int pg_set_solver(pg_handle* h, int kind, int max_iter, double tolerance, int wa
 int pg_stats(pg_handle* h, int64_t start, int64_t end, int32_t* iters, int32_t* ncon, int32_t* nrows,
              int32_t* status);
 
+/* Learned Newton warm start. No counterpart in the reference, which starts
+ * Newton from the previous step's acceleration when that lowers the cost
+ * (newton.rs:238-245). With a network loaded and warm mode PG_WARM_LEARNED,
+ * each substep lists the touching contacts (24 features each), predicts
+ * their frame forces on the tensor cores, and offers a0 + M^-1 J' f as the
+ * starting point behind the same cost gate; the solution and its tolerance
+ * are unchanged. Applies to models with one dof tree and at most 16 dofs
+ * (the register Newton path); other envs start cold.
+ * pg_set_warm_mlp: weights as in include/pippin_b200_mlp.h (36662 floats). */
+int pg_set_warm_mlp(pg_handle* h, const float* weights, size_t len);
+
+/* Training pairs for the warm start: one substep of envs [start, end) (with
+ * the current controls, like pg_step), returning for each touching contact
+ * solved on the register Newton path its 24 features (X) and the converged
+ * forces of its four pyramid rows (rows; the frame forces are
+ * f_n = r0 + r1 + r2 + r3, f_t1 = mu (r0 - r1), f_t2 = mu (r2 - r3), mu =
+ * feature 1). X holds pg_warm_capacity * 24 floats, rows pg_warm_capacity * 4.
+ * *n gets the number of pairs written. */
+int pg_warm_samples(pg_handle* h, int64_t start, int64_t end, float* X, size_t xlen, float* rows, size_t rlen,
+                    int64_t* n);
+int64_t pg_warm_capacity(const pg_handle* h);
+
 /* Forward pass of one env without integration (forward.rs:263-271), for
  * per-stage parity checks: qm (nv*nv), qfrc_bias (nv), contacts as 13
  * doubles each (pos[3] normal[3] tangent[3] depth geom1 geom2 feature). */

@@ -64,6 +64,9 @@ SIGNATURES = [
     ("pg_last_error", C.c_char_p, []),
     ("pg_fp64_peak", _i32, [_i32, _i32, _pd, _pd]),
     ("pg_time_phases", _i32, [_vp, _i64, _i64, _i64, _vp, _pf]),
+    ("pg_set_warm_mlp", _i32, [_vp, _pf, _sz]),
+    ("pg_warm_samples", _i32, [_vp, _i64, _i64, _pf, _sz, _pf, _sz, _pi64]),
+    ("pg_warm_capacity", _i64, [_vp]),
     ("pg_mlp_forward", _i32, [_pf, _sz, _pf, _i64, _pf]),
     ("pg_mlp_loss_grad", _i32, [_pf, _sz, _pf, _pf, _i64, _pf, _sz, _pd]),
     ("pg_mlp_train", _i32, [_pf, _pf, _i64, _i32, _i32, C.c_float, C.c_uint64, _pf, _sz, _pd]),

@@ -15,6 +15,7 @@
 
 #include "../../include/pippin_b200.h"
 #include "pg_kernels.h"
+#include "pg_mlp.h"
 #include "pg_model.h"
 
 using namespace pg;
@@ -398,6 +399,9 @@ struct Handle {
   double* prev_con = nullptr;   // [env][maxcon][P_STRIDE] PGS warm start (allocated with PGS)
   int32_t* prev_ncon = nullptr;  // [env]
   int* queue = nullptr;
+  // learned warm start: contact list, network, and whether one is loaded
+  LearnArgs learn{};
+  bool mlp_loaded = false;
   std::vector<double> base_params;
   int warm_mode = WARM_REF_PREV_QACC;
   SubstepCfg cfg{{16, 4, 0}, {32, 4, 0}, {16, 4, 0}};
@@ -466,6 +470,8 @@ StepArgs make_args(Handle* h) {
   a.scratch = h->scratch;
   a.queue = h->queue;
   a.warm_mode = h->warm_mode;
+  a.learn = h->learn;
+  a.learn.count = h->queue + 3;
   a.stage_model = h->dm.arena_bytes <= STAGE_LIMIT ? 1 : 0;
   std::vector<int> po = dmodel_pointer_fields();
   a.n_ptr = (int)std::min<size_t>(po.size(), MAX_PTR_FIELDS);
@@ -1080,7 +1086,8 @@ void destroy(pg_handle* h) {
   clear_graphs(h);
   void* ptrs[] = {h->d_model, h->qpos, h->qvel, h->ctrl, h->qacc, h->applied, h->params, h->iters, h->ncon,
                   h->nrows, h->status, h->scratch, h->work, h->prev_con, h->prev_ncon, h->queue, h->b_ctrl.p, h->b_qout.p, h->b_poses_g.p,
-                  h->b_poses_c.p, h->b_dbg.p, h->b_vals.p, h->b_ids.p};
+                  h->b_poses_c.p, h->b_dbg.p, h->b_vals.p, h->b_ids.p, h->learn.feat, h->learn.force,
+                  h->learn.rows, (void*)h->learn.mlp_w, (void*)h->learn.mlp_f};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -1539,7 +1546,8 @@ int pg_set_solver(pg_handle* h, int kind, int max_iter, double tolerance, int wa
     CK(cudaMemsetAsync(h->prev_ncon, 0, sizeof(int32_t) * h->n, h->stream));
     CK(cudaStreamSynchronize(h->stream));
   }
-  if (warm_mode == PG_WARM_LEARNED) return fail(PG_ERR_UNSUPPORTED, "no learned warm start is loaded");
+  if (warm_mode == PG_WARM_LEARNED && !h->mlp_loaded)
+    return fail(PG_ERR_UNSUPPORTED, "no learned warm start is loaded (pg_set_warm_mlp)");
   if (kind >= 0) h->dm.solver = kind;
   if (max_iter >= 0) h->dm.iterations = max_iter;
   if (tolerance >= 0) h->dm.tolerance = tolerance;
@@ -1743,6 +1751,97 @@ int pg_time_phases(pg_handle* h, int64_t start, int64_t end, int64_t nstep, cons
   if (e != cudaSuccess) return cuda_fail(e, "pg_time_phases");
   return PG_OK;
 }
+
+// the learned warm start's contact list: every env's touching contacts, up
+// to 32 per env on average
+static int64_t learn_cap(const Handle* h) {
+  int64_t cap = h->n * (int64_t)std::min(std::max(h->dm.maxcon, 1), 32);
+  return std::min<int64_t>(cap, (1ll << 30) / LEARN_NF);
+}
+static int ensure_learn(Handle* h) {
+  if (h->learn.feat) return PG_OK;
+  int64_t cap = learn_cap(h);
+  h->learn.cap = (int)cap;
+  CK(cudaMalloc(&h->learn.feat, sizeof(float) * cap * LEARN_NF));
+  CK(cudaMalloc(&h->learn.force, sizeof(float) * cap * 3));
+  CK(cudaMalloc(&h->learn.rows, sizeof(float) * cap * 4));
+  return PG_OK;
+}
+
+int pg_set_warm_mlp(pg_handle* h, const float* weights, size_t len) {
+  if (!h || !weights) return fail(PG_ERR_INVALID, "NULL argument");
+  if (len != (size_t)MLP_SIZE) return fail(PG_ERR_LENGTH, "warm-start network must hold 36662 floats");
+  for (size_t k = 0; k < len; k++)
+    if (!std::isfinite(weights[k])) return fail(PG_ERR_INVALID, "warm-start network has a non-finite weight");
+  CK(cudaSetDevice(h->device));
+  int rc = ensure_learn(h);
+  if (rc) return rc;
+  if (!h->learn.mlp_w) {
+    uint16_t* w = nullptr;
+    float* f = nullptr;
+    CK(cudaMalloc(&w, sizeof(uint16_t) * MLP_BF16_ELEMS));
+    CK(cudaMalloc(&f, sizeof(float) * MLP_F32_ELEMS));
+    h->learn.mlp_w = w;
+    h->learn.mlp_f = f;
+  }
+  std::vector<uint16_t> wb(MLP_BF16_ELEMS);
+  std::vector<float> fb(MLP_F32_ELEMS);
+  mlp_pack(weights, wb.data(), fb.data());
+  CK(cudaMemcpyAsync((void*)h->learn.mlp_w, wb.data(), sizeof(uint16_t) * wb.size(), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync((void*)h->learn.mlp_f, fb.data(), sizeof(float) * fb.size(), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  CK(mlp_prepare());
+  h->learn.mode = LEARN_PREDICT;
+  h->mlp_loaded = true;
+  h->version++;
+  return PG_OK;
+}
+
+int pg_warm_samples(pg_handle* h, int64_t start, int64_t end, float* X, size_t xlen, float* rows, size_t rlen,
+                    int64_t* n) {
+  if (!h || !n) return fail(PG_ERR_INVALID, "NULL argument");
+  int rc = check_range(h, start, end);
+  if (rc) return rc;
+  *n = 0;
+  if (end == start) return PG_OK;
+  CK(cudaSetDevice(h->device));
+  if ((rc = ensure_learn(h))) return rc;
+  if (xlen < (size_t)h->learn.cap * LEARN_NF || rlen < (size_t)h->learn.cap * 4)
+    return fail(PG_ERR_LENGTH, "sample buffers must hold pg_warm_capacity samples");
+  // one substep with the contact list on and the converged row forces
+  // dumped; rows the dump does not reach stay NaN and are dropped
+  CK(cudaMemsetAsync(h->learn.rows, 0xFF, sizeof(float) * h->learn.cap * 4, h->stream));
+  StepArgs a = make_args(h);
+  a.learn.mode = LEARN_DUMP;
+  a.start = (int)start;
+  a.count = (int)(end - start);
+  a.nstep = 1;
+  a.sidx = 0;
+  if ((rc = launch_status(launch_substep(a, fit(h->cfg, end - start), h->stream)))) return rc;
+  int count = 0;
+  CK(cudaMemcpyAsync(&count, h->queue + 3, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  int64_t m = std::min(count, h->learn.cap);
+  std::vector<float> fx((size_t)m * LEARN_NF), fr((size_t)m * 4);
+  if (m) {
+    CK(cudaMemcpyAsync(fx.data(), h->learn.feat, sizeof(float) * fx.size(), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(fr.data(), h->learn.rows, sizeof(float) * fr.size(), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+  }
+  int64_t k = 0;
+  for (int64_t i = 0; i < m; i++) {
+    if (!(std::isfinite(fr[4 * i]) && std::isfinite(fr[4 * i + 1]) && std::isfinite(fr[4 * i + 2]) &&
+          std::isfinite(fr[4 * i + 3])))
+      continue;
+    std::memcpy(X + k * LEARN_NF, &fx[i * LEARN_NF], sizeof(float) * LEARN_NF);
+    std::memcpy(rows + k * 4, &fr[4 * i], sizeof(float) * 4);
+    k++;
+  }
+  *n = k;
+  return PG_OK;
+}
+
+int64_t pg_warm_capacity(const pg_handle* h) { return h ? learn_cap(h) : -1; }
 
 int pg_synchronize(pg_handle* h) {
   if (!h) return fail(PG_ERR_INVALID, "NULL handle");

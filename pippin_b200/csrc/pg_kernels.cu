@@ -18,6 +18,7 @@
 #include <cuda_runtime.h>
 
 #include "pg_kernels.h"
+#include "pg_mlp.h"
 #include "pg_pgs.cuh"
 
 namespace pg {
@@ -172,6 +173,9 @@ __global__ void __launch_bounds__(256) collide_kernel(const __grid_constant__ St
       wk[A.k.meta + K_META_STATUS] = (double)((int)wk[A.k.meta + K_META_STATUS] | status);
     }
     T.sync();
+    if (A.learn.mode != LEARN_OFF)
+      learn_features(T, m, A.learn, e, ncon, A.st.qvel + env * m.nv, wk + A.k.a0, wk + A.k.cdof, wk + A.k.meta);
+    T.sync();
   }
 }
 
@@ -238,8 +242,21 @@ __global__ void __launch_bounds__(256) newton_kernel(const __grid_constant__ Ste
         T.sync();
       } else {
         nr = build_rows(T, m, w, A.s, e, ncon, &status);
-        const double* warm = A.warm_mode == WARM_COLD ? nullptr : ws + w.qacc;
-        iters = newton_solve(T, m, w, A.s, e, nr, acc, warm);
+        const double* warm = A.warm_mode == WARM_REF_PREV_QACC ? ws + w.qacc : nullptr;
+        // the learned warm start's predictions, or the slots for its targets
+        const float *lfeat = nullptr, *lforce = nullptr;
+        float* ldump = nullptr;
+        int lnum = 0;
+        if (A.learn.mode != LEARN_OFF) {
+          int lbase = (int)wk[A.k.meta + K_META_LBASE];
+          lnum = (int)wk[A.k.meta + K_META_LNUM];
+          if (lnum > 0) {
+            lfeat = A.learn.feat + (size_t)lbase * LEARN_NF;
+            if (A.learn.mode == LEARN_PREDICT && A.warm_mode == WARM_LEARNED) lforce = A.learn.force + (size_t)lbase * 3;
+            if (A.learn.mode == LEARN_DUMP) ldump = A.learn.rows + (size_t)lbase * 4;
+          }
+        }
+        iters = newton_solve(T, m, w, A.s, e, nr, acc, warm, lfeat, lforce, lnum, ldump);
         if (wk[A.k.meta + K_META_DAMPED] != 0.0) {
           load_async(T, ws + w.fac, wk + A.k.lh, nv * nv);
           load_async(T, ws + w.rinv, wk + A.k.rinvh, nv);
@@ -490,6 +507,12 @@ cudaError_t launch_smooth_collide(const StepArgs& a, const SubstepCfg& c, cudaSt
 cudaError_t launch_substep(const StepArgs& a, const SubstepCfg& c, cudaStream_t s) {
   cudaError_t e = launch_smooth_collide(a, c, s);
   if (e != cudaSuccess) return e;
+  if (a.learn.mode == LEARN_PREDICT && a.warm_mode == WARM_LEARNED) {
+    // frame forces of every touching contact the collision phase listed
+    e = mlp_forward(MlpDevice{a.learn.mlp_w, a.learn.mlp_f}, a.learn.feat, a.learn.cap, a.learn.force, s,
+                    a.learn.count, 296);
+    if (e != cudaSuccess) return e;
+  }
   PG_LAUNCH(K_NEWTON, newton_kernel, c.newton, a);
   return cudaSuccess;
 }

@@ -103,7 +103,9 @@ __device__ inline void hidden_layer(const uint32_t (&a)[KT][4], const uint16_t* 
 
 constexpr int MLP_WARPS = 4;  // 64 samples per block
 
-__global__ void __launch_bounds__(32 * MLP_WARPS) mlp_forward_kernel(MlpDevice d, const float* X, int64_t n, float* Y) {
+__global__ void __launch_bounds__(32 * MLP_WARPS) mlp_forward_kernel(MlpDevice d, const float* X, int64_t n, float* Y,
+                                                                     const int* ncount) {
+  if (ncount) n = min(n, (int64_t)*ncount);  // samples counted on the device
   extern __shared__ __align__(16) unsigned char smem[];
   uint16_t* W = reinterpret_cast<uint16_t*>(smem);
   float* F = reinterpret_cast<float*>(smem + sizeof(uint16_t) * MLP_BF16_ELEMS);
@@ -158,14 +160,18 @@ __global__ void __launch_bounds__(32 * MLP_WARPS) mlp_forward_kernel(MlpDevice d
   }
 }
 
-cudaError_t mlp_forward(const MlpDevice& d, const float* X, int64_t n, float* Y, cudaStream_t s) {
+static size_t mlp_smem() { return sizeof(uint16_t) * MLP_BF16_ELEMS + sizeof(float) * MLP_F32_ELEMS; }
+
+cudaError_t mlp_prepare() {
+  return cudaFuncSetAttribute(mlp_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mlp_smem());
+}
+
+cudaError_t mlp_forward(const MlpDevice& d, const float* X, int64_t n, float* Y, cudaStream_t s, const int* ncount,
+                        int max_blocks) {
   if (n <= 0) return cudaSuccess;
-  size_t smem = sizeof(uint16_t) * MLP_BF16_ELEMS + sizeof(float) * MLP_F32_ELEMS;
-  cudaError_t e = cudaFuncSetAttribute(mlp_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
   int64_t blocks = (n + 16 * MLP_WARPS - 1) / (16 * MLP_WARPS);
-  if (blocks > 2048) blocks = 2048;
-  mlp_forward_kernel<<<(unsigned)blocks, 32 * MLP_WARPS, smem, s>>>(d, X, n, Y);
+  if (blocks > max_blocks) blocks = max_blocks;
+  mlp_forward_kernel<<<(unsigned)blocks, 32 * MLP_WARPS, mlp_smem(), s>>>(d, X, n, Y, ncount);
   return cudaGetLastError();
 }
 
@@ -379,6 +385,7 @@ int pg_mlp_forward(const float* weights, size_t wlen, const float* X, int64_t n,
   MCK(cudaMemcpy(dw, wb.data(), sizeof(uint16_t) * MLP_BF16_ELEMS, cudaMemcpyHostToDevice));
   MCK(cudaMemcpy(df, fb.data(), sizeof(float) * MLP_F32_ELEMS, cudaMemcpyHostToDevice));
   MCK(cudaMemcpy(dx, X, sizeof(float) * n * MLP_IN, cudaMemcpyHostToDevice));
+  MCK(mlp_prepare());
   MCK(mlp_forward(MlpDevice{dw, df}, dx, n, dy, 0));
   MCK(cudaMemcpy(Y, dy, sizeof(float) * n * MLP_OUT, cudaMemcpyDeviceToHost));
   return PG_OK;

@@ -173,7 +173,24 @@ struct ScrLayout {
 // (offsets in doubles): what smooth dynamics leaves for the collision and
 // Newton phases, the geoms and contacts of the narrow phase, and a small
 // meta block (contact count, status bits, whether implicit damping applies).
-enum { K_META_NCON = 0, K_META_STATUS = 1, K_META_DAMPED = 2, K_META_SIZE = 4 };
+enum { K_META_NCON = 0, K_META_STATUS = 1, K_META_DAMPED = 2, K_META_LBASE = 3, K_META_LNUM = 4, K_META_SIZE = 6 };
+
+// Learned warm start: features of the touching contacts of all envs in one
+// compact list (slots taken with a device counter), the network's frame
+// forces for them, and, when collecting training data, the converged forces
+// of their four pyramid rows.
+enum { LEARN_OFF = 0, LEARN_PREDICT = 1, LEARN_DUMP = 2 };
+constexpr int LEARN_NF = 24;  // features per contact
+struct LearnArgs {
+  int mode;
+  int cap;          // slots in the list
+  int* count;       // slots taken this substep (reset with the work counters)
+  float* feat;      // [cap][24]
+  float* force;     // [cap][3]  predicted frame forces
+  float* rows;      // [cap][4]  converged pyramid row forces (LEARN_DUMP)
+  const uint16_t* mlp_w;  // the network (pg_mlp.h MlpDevice)
+  const float* mlp_f;
+};
 struct WorkLayout {
   int qm, cdof, a0, smooth, bias, lh, rinvh, geoms, contacts, meta;
   int stride;
@@ -216,6 +233,7 @@ struct StepArgs {
   int start, count, nstep;
   int sidx;          // substep index within the call
   int warm_mode;
+  LearnArgs learn;
   const double* ctrl_seq;  // optional (count, nstep, nu): per-substep controls
   double* qpos_out;        // optional (count, nstep, nq): qpos after each substep
   // model staging: byte offsets of the pointer fields of DModel, and

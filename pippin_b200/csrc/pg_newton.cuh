@@ -102,6 +102,68 @@ __device__ inline double pair_jac(const DModel& m, const double* cdof, int b1, i
   return v;
 }
 
+// Features of the touching contacts (depth > 0, in contact order: the order
+// build_rows gives their pyramid rows) for the learned warm start, into one
+// slot each of the env-shared list; the env's first slot and count go to its
+// work-record meta (count -1 when the list is full). Per contact, in its
+// frame (n, t1, t2): depth, friction, J qvel (3), J a0 (3), the bodies'
+// translational and rotational invweight sums, the normal (3), the env's
+// touching-contact count, the timestep, the point relative to each geom's
+// center (3 + 3), both geom types, and 1.
+template <int G>
+__device__ void learn_features(const Tile<G>& T, const DModel& m, const LearnArgs& L, const EnvCtx& e, int ncon,
+                               const double* qvel, const double* a0, const double* cdof, double* meta) {
+  int lane = T.lane(), nv = m.nv;
+  const double* con = e.con;
+  const double* prm = e.prm;
+  int nt = 0;
+  for (int c = lane; c < ncon; c += G) nt += con[C_STRIDE * c + C_DEPTH] > 0.0 ? 1 : 0;
+  nt = T.isum(nt);
+  int base = 0;
+  if (lane == 0 && nt > 0) base = atomicAdd(L.count, nt);
+  base = T.bcast(base, 0);
+  bool room = base + nt <= L.cap;
+  if (lane == 0) {
+    meta[K_META_LBASE] = base;
+    meta[K_META_LNUM] = room ? nt : -1;
+  }
+  if (!room || nt == 0) return;
+  int done = 0;
+  for (int c0 = 0; c0 < ncon; c0 += G) {
+    int c = c0 + lane;
+    bool touch = c < ncon && con[C_STRIDE * c + C_DEPTH] > 0.0;
+    int tot;
+    int rank = done + T.excl_scan(touch ? 1 : 0, &tot);
+    if (touch) {
+      const double* r = con + C_STRIDE * c;
+      int g1 = (int)r[C_G1], g2 = (int)r[C_G2];
+      int b1 = m.geom_body[g1], b2 = m.geom_body[g2];
+      V3 p = ld3(r + C_POS);
+      V3 dir[3] = {ld3(r + C_NORMAL), ld3(r + C_T1), ld3(r + C_T2)};
+      double jv[3] = {0, 0, 0}, ja[3] = {0, 0, 0};
+      for (int k = 0; k < nv; k++)
+        for (int d = 0; d < 3; d++) {
+          double j = pair_jac(m, cdof, b1, b2, p, dir[d], k);
+          jv[d] += j * qvel[k];
+          ja[d] += j * a0[k];
+        }
+      const double* gp1 = e.geo + G_STRIDE * g1 + G_POS;
+      const double* gp2 = e.geo + G_STRIDE * g2 + G_POS;
+      float* f = L.feat + (size_t)(base + rank) * LEARN_NF;
+      double v[LEARN_NF] = {r[C_DEPTH],
+                            fmax(prm[m.p_friction + g1], prm[m.p_friction + g2]),
+                            jv[0], jv[1], jv[2], ja[0], ja[1], ja[2],
+                            prm[m.p_body_invw + 2 * b1] + prm[m.p_body_invw + 2 * b2],
+                            prm[m.p_body_invw + 2 * b1 + 1] + prm[m.p_body_invw + 2 * b2 + 1],
+                            dir[0].x, dir[0].y, dir[0].z, (double)nt, m.timestep,
+                            p.x - gp2[0], p.y - gp2[1], p.z - gp2[2], p.x - gp1[0], p.y - gp1[1], p.z - gp1[2],
+                            (double)m.geom_type[g1], (double)m.geom_type[g2], 1.0};
+      for (int k = 0; k < LEARN_NF; k++) f[k] = (float)v[k];
+    }
+    done += tot;
+  }
+}
+
 // newton.rs:113-218. Returns the row count. Row order: 4 pyramid rows per
 // touching contact (contact order), violated joint limits (joint order,
 // lower side first), joint equalities.
@@ -466,10 +528,19 @@ constexpr int SMALL_ROWS = 2 * SMALL_N;  // rows the register Newton takes (two 
 // differs (chol_reg). Adds the constraint force to qfrc (newton.rs:361-371)
 // and leaves the solution in a; returns the iteration count. J rows are
 // read from Jsrc (stride k), row constants from R.
+//
+// Learned warm start (lforce != nullptr, lnum touching contacts whose
+// pyramid rows are the first 4 lnum rows): the predicted frame forces
+// (f_n, f_t1, f_t2) become row forces f_n / 4 +- f_tk / (2 mu), so that
+// sum_r f_r J_r = f_n J_n + f_t1 J_t1 + f_t2 J_t2, and the candidate start is
+// a0 + M^-1 sum_r f_r J_r', behind the same cost gate as the previous-step
+// start (newton.rs:238-245). With ldump, the converged forces of those rows
+// are written there (4 per contact) as training targets.
 template <int G>
 __device__ __noinline__ int newton_small(const Tile<G>& T, int k, int nr, const double* Jsrc, const double* R,
                                          const double* M, double* a, const double* warm, int max_iters, double tol,
-                                         const SmallBufs& B, double* qfrc) {
+                                         const SmallBufs& B, double* qfrc, const float* lfeat, const float* lforce,
+                                         int lnum, float* ldump) {
   static_assert(G >= SMALL_N, "one lane per unknown");
   const int i = T.lane();
   const bool dof = i < k;
@@ -530,10 +601,41 @@ __device__ __noinline__ int newton_small(const Tile<G>& T, int k, int nr, const 
     return c + T.sum(cr);
   };
   double ai = a0;
-  if (warm) {
+  double wl = wi;
+  bool use_warm = warm != nullptr;
+  if (lforce && lnum > 0 && 4 * lnum <= nr) {
+    double cv0[2];
+#pragma unroll
+    for (int s = 0; s < 2; s++) {
+      int r = i + SMALL_N * s;
+      cv0[s] = 0.0;
+      if (has[s] && r < 4 * lnum) {
+        int c = r / 4, q = r % 4;
+        double mu = lfeat[c * LEARN_NF + 1];
+        double fn = lforce[3 * c], ft = lforce[3 * c + 1 + q / 2];
+        cv0[s] = 0.25 * fn + (mu > 0.0 ? ((q & 1) ? -ft : ft) / (2.0 * mu) : 0.0);
+      }
+    }
+    coeffs(cv0);
+    double x = 0.0;
+    if (dof)
+      for (int r = 0; r < 4 * lnum; r++) {
+        double cf = B.c[r];
+        if (cf != 0.0) x += cf * jrow(r)[i];
+      }
+    double hl[SMALL_N];
+#pragma unroll
+    for (int q = 0; q < SMALL_N; q++) hl[q] = (q <= i) ? mrow[q] : 0.0;
+    double rv = 0.0;
+    if (chol_reg(T, hl, k, B.L, k, &rv)) {
+      wl = a0 + solve_reg(T, B.L, k, k, rv, dof ? x : 0.0);
+      use_warm = true;
+    }
+  }
+  if (use_warm) {
     double c0 = cost(a0);
-    double c1 = cost(wi);
-    if (c1 < c0) ai = wi;
+    double c1 = cost(wl);
+    if (c1 < c0) ai = wl;
   }
   publish(a0);
   double ma0 = dof ? dot_ref_reg(mrow, B.x, k) : 0.0;
@@ -653,6 +755,8 @@ __device__ __noinline__ int newton_small(const Tile<G>& T, int k, int nr, const 
     qfrc[i] = q;
     a[i] = ai;
   }
+  if (ldump && lnum > 0 && 4 * lnum <= nr)
+    for (int t = i; t < 4 * lnum; t += G) ldump[t] = (float)B.c[t];
   T.sync();
   return iters;
 }
@@ -775,7 +879,8 @@ __device__ __noinline__ int newton_islands(const Tile<G>& T, const DModel& m, co
 // newton.rs:378-473
 template <int G>
 __device__ int newton_solve(const Tile<G>& T, const DModel& m, const WsLayout& w, const ScrLayout& s,
-                            const EnvCtx& e, int nr, double* a, const double* warm) {
+                            const EnvCtx& e, int nr, double* a, const double* warm, const float* lfeat = nullptr,
+                            const float* lforce = nullptr, int lnum = 0, float* ldump = nullptr) {
   int lane = T.lane(), nv = m.nv;
   double* ws = e.ws;
   double* qfrc = ws + w.qfrc_c;
@@ -796,7 +901,8 @@ __device__ int newton_solve(const Tile<G>& T, const DModel& m, const WsLayout& w
   if constexpr (G >= SMALL_N) {
     if (nv <= SMALL_N && nr <= SMALL_ROWS && w.sj >= 0) {
       SmallBufs S{ws + w.sj, ws + w.sl, ws + w.sx, ws + w.sc};
-      return newton_small(T, nv, nr, J, R, ws + w.qm, a, warm, m.iterations, m.tolerance, S, qfrc);
+      return newton_small(T, nv, nr, J, R, ws + w.qm, a, warm, m.iterations, m.tolerance, S, qfrc, lfeat, lforce,
+                          lnum, ldump);
     }
   }
   int it = newton_dense(T, nv, nr, J, R, ws + w.qm, a, warm, m.iterations, m.tolerance, B);

@@ -89,6 +89,7 @@ extern "C" int pg_step_static(pg_handle* h, int64_t start, int64_t end, int64_t 
   }
   nc.blocks = (int)std::min<size_t>((size_t)nc.blocks, tiles / nc.tiles_per_block);
   a.queue = reinterpret_cast<int*>(base);
+  a.learn.count = a.queue + 3;
   a.scratch = reinterpret_cast<double*>(base + PG_STATIC_COUNTER_BYTES);
   // each substep restarts the phase counters before its kernels
   cudaError_t e = cudaSuccess;

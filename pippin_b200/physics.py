@@ -244,6 +244,26 @@ class CudaPhysics:
         s, e = _span(envs)
         self._check(self._L.pg_step_device(self._h, s, e, int(nstep), C.c_void_p(ctrl_dev_ptr)))
 
+    def set_warm_mlp(self, weights):
+        """Load a learned warm-start network (36662 floats, pippin_b200.warm)."""
+        w = np.ascontiguousarray(weights, dtype=np.float32)
+        self._check(self._L.pg_set_warm_mlp(self._h, w.ctypes.data_as(C.POINTER(C.c_float)), w.size))
+
+    def warm_samples(self, envs: EnvRange):
+        """One substep of `envs`; returns the touching contacts' features
+        (n, 24) and converged frame forces (n, 3) (f_n, f_t1, f_t2) as float32."""
+        s, e = _span(envs)
+        cap = int(self._L.pg_warm_capacity(self._h))
+        X = np.zeros((cap, 24), np.float32)
+        R = np.zeros((cap, 4), np.float32)
+        n = C.c_int64()
+        self._check(self._L.pg_warm_samples(self._h, s, e, X.ctypes.data_as(C.POINTER(C.c_float)), X.size,
+                                            R.ctypes.data_as(C.POINTER(C.c_float)), R.size, C.byref(n)))
+        X, R = X[:n.value], R[:n.value]
+        mu = X[:, 1]
+        F = np.stack([R.sum(axis=1), mu * (R[:, 0] - R[:, 1]), mu * (R[:, 2] - R[:, 3])], axis=1)
+        return X, F.astype(np.float32)
+
     def time_phases(self, envs: EnvRange, nstep: int, ctrl_dev_ptr: int = 0) -> dict:
         """Step like step_device, timing each phase kernel with CUDA events;
         returns the summed device milliseconds per phase."""

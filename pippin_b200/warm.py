@@ -72,3 +72,24 @@ def train(X, Y, epochs=20, batch=4096, lr=1e-3, seed=0):
     _check(L.pg_mlp_train(_pf(X), _pf(Y), X.shape[0], int(epochs), int(batch), float(lr), int(seed), _pf(w), w.size,
                           losses.ctypes.data_as(C.POINTER(C.c_double))))
     return w, losses[:epochs]
+
+
+def collect(phys, steps, controls=None, skip=0):
+    """Step `phys` (all envs) `steps` substeps, gathering (features, frame
+    forces) of the touching contacts after the first `skip` substeps.
+    controls(t) returns the (envs, nu) controls of substep t, or None."""
+    from .physics import Field
+    n = phys.num_envs()
+    xs, fs = [], []
+    for t in range(steps):
+        if controls is not None:
+            phys.set(Field.CTRL, range(n), controls(t))
+        if t < skip:
+            phys.step(range(n), 1)
+            continue
+        X, F = phys.warm_samples(range(n))
+        xs.append(X)
+        fs.append(F)
+    if not xs:
+        return np.zeros((0, N_IN), np.float32), np.zeros((0, N_OUT), np.float32)
+    return np.concatenate(xs), np.concatenate(fs)

@@ -81,3 +81,53 @@ def test_training_fits_a_smooth_target():
     assert losses[-1] < 0.1 * losses[0], losses
     pred = warm.forward(w, X[:2000])
     assert np.mean((pred - Y[:2000]) ** 2) < 0.2 * np.mean(Y[:2000] ** 2)
+
+
+def _ant(n, seed):
+    from pippin_b200 import CudaPhysics, Field, mjcf, scenes
+    m = mjcf.load_string(scenes.ant_xml(tolerance=1e-10, iterations=30))
+    p = CudaPhysics(mjcf.to_blob(m), n)
+    rng = np.random.default_rng(seed)
+    p.set(Field.QPOS, range(n), np.tile(np.array(m.qpos0), (n, 1)) + rng.uniform(-0.1, 0.1, (n, m.nq)))
+    p.set(Field.QVEL, range(n), rng.normal(0, 0.1, (n, m.nv)))
+    return m, p, rng
+
+
+def test_learned_warm_start_on_ant():
+    """Train on converged Ant contact forces, then start Newton from the
+    prediction: the solution is the same as from a cold start (both stop at
+    the 1e-10 gradient tolerance) and fewer iterations are needed."""
+    from pippin_b200 import Field, WarmStart
+    m, p, rng = _ant(2048, 0)
+    X, F = warm.collect(p, 120, controls=lambda t: rng.uniform(-1, 1, (2048, m.nu)), skip=20)
+    assert len(X) > 20000, len(X)
+    assert np.all(np.isfinite(F)) and np.mean(F[:, 0] >= -1e-6) > 0.99  # normal forces push
+    w, losses = warm.train(X, F, epochs=15, batch=2048, lr=1e-3, seed=1)
+    assert losses[-1] < 0.5 * losses[0], losses
+    # held-out states: cold vs learned on identical inputs, step by step
+    m, g, rng = _ant(1024, 5)
+    g.set_warm_mlp(w)
+    n = 1024
+    for t in range(40):
+        g.set(Field.CTRL, range(n), rng.uniform(-1, 1, (n, m.nu)))
+        g.step(range(n), 1)
+    iters = {"cold": [], "learned": []}
+    worst = 0.0
+    for t in range(40):
+        g.set(Field.CTRL, range(n), rng.uniform(-1, 1, (n, m.nu)))
+        st = {f: g.get(f, range(n)) for f in (Field.QPOS, Field.QVEL, Field.QACC)}
+        out = {}
+        for mode, wm in (("cold", WarmStart.COLD), ("learned", WarmStart.LEARNED)):
+            for f in st:
+                g.set(f, range(n), st[f])
+            g.set_solver(warm=int(wm))
+            g.step(range(n), 1)
+            s = g.stats()
+            rows = s["nrows"] > 0
+            iters[mode].append(s["iters"][rows])
+            out[mode] = g.get(Field.QACC, range(n))
+        scale = np.maximum(np.abs(out["cold"]).max(axis=1), 1.0)
+        worst = max(worst, float((np.abs(out["learned"] - out["cold"]).max(axis=1) / scale).max()))
+    cold, learned = np.concatenate(iters["cold"]), np.concatenate(iters["learned"])
+    assert worst < 1e-8, worst
+    assert learned.mean() < cold.mean(), (learned.mean(), cold.mean())
