@@ -37,7 +37,7 @@ PHASE_STAGES = {"smooth": ("kinematics", "crba", "vel_rne", "passive_act", "fact
                 "collide": ("collide",),
                 "newton": ("rows", "newton", "pgs", "integrate")}
 # DRAM bytes (read + write) per env of each phase kernel, from one ncu capture
-# of the Ant workload at 4096 envs (profiles/phase_kernels_ant.md)
+# of the phase kernels on the Ant workload at 4096 envs
 NCU_TRAFFIC_PER_ENV = {"smooth": 2872.0, "collide": 6322.0, "newton": 5374.0}
 
 
@@ -50,6 +50,7 @@ def parse():
     ap.add_argument("--envs", type=int, default=4096, help="envs per GPU")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shape")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned warm-start variant")
     ap.add_argument("--lanes", type=int, default=0, help="force lanes per env (8, 16, 32)")
     ap.add_argument("--per-block", type=int, default=0, help="force envs per block")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
@@ -274,6 +275,26 @@ def run_ours(args):
     phys.set(Field.QVEL, range(n), v)
     ms_cold = timed_device_loop(ctrl_all, K, WarmStart.COLD)
     st_cold = phys.stats()
+    # learned warm start: a network trained on converged contact forces of a
+    # separate 1024-env Ant run, then the same workload again
+    learned = None
+    if not args.no_learned:
+        from pippin_b200 import warm
+        tm, trng = CudaPhysics(blob, 1024, device=local), np.random.default_rng(2000 + rank)
+        tq, tv, _ = initial_state(m, 1024, 3000 + rank)
+        tm.set(Field.QPOS, range(1024), tq)
+        tm.set(Field.QVEL, range(1024), tv)
+        X, F = warm.collect(tm, 150, controls=lambda t: trng.uniform(-1, 1, (1024, m.nu)), skip=20)
+        tm.close()
+        w, losses = warm.train(X, F, epochs=15, batch=2048, lr=1e-3, seed=1)
+        phys.set_warm_mlp(w)
+        phys.set(Field.QPOS, range(n), q)
+        phys.set(Field.QVEL, range(n), v)
+        ms_learned = timed_device_loop(ctrl_all, K, WarmStart.LEARNED)
+        st_l = phys.stats()
+        learned = {"value": n * ws * K / (ms_learned * 1e-3), "mean_iters": float(st_l["iters"].mean()),
+                   "p99_iters": float(np.percentile(st_l["iters"], 99)), "train_samples": int(len(X)),
+                   "train_loss": [float(losses[0]), float(losses[-1])]}
     phys.set_solver(warm=int(WarmStart.REF_PREV_QACC))
 
     # end to end through the C-ABI with host buffers
@@ -350,6 +371,8 @@ def run_ours(args):
             "variants": {"newton_ref_prev_qacc": value, "newton_cold": value_cold,
                          "mean_iters_ref": float(st["iters"].mean()), "mean_iters_cold": float(st_cold["iters"].mean()),
                          "p99_iters_ref": float(np.percentile(st["iters"], 99)),
+                         "p99_iters_cold": float(np.percentile(st_cold["iters"], 99)),
+                         "newton_learned": learned,
                          "mean_ncon": float(st["ncon"].mean()), "mean_rows": float(st["nrows"].mean())},
             "roofline": {"bound": "fp64", "kernel": f"{top}_kernel", "achieved": achieved, "peak": peak,
                          "unit": "TFLOP/s", "frac": achieved / peak,

@@ -9,6 +9,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <tuple>
 #include <vector>
@@ -607,6 +608,20 @@ std::vector<int> dmodel_pointer_fields() {
   return o;
 }
 
+// A kernel's dynamic shared-memory limit is one setting per device shared by
+// every handle: it only ever rises, so a handle with a smaller launch shape
+// cannot lower it under another handle's larger one.
+int allow_smem(int device, const void* fn, size_t smem) {
+  static std::mutex mu;
+  static std::map<std::pair<int, const void*>, size_t> raised;
+  std::lock_guard<std::mutex> g(mu);
+  size_t& cur = raised[{device, fn}];
+  if (smem <= cur) return PG_OK;
+  CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  cur = smem;
+  return PG_OK;
+}
+
 // Resident grid of a launch shape for one phase. `phase` is K_SMOOTH (whose
 // shape set_const and poses share), K_COLLIDE or K_NEWTON.
 int choose_grid(Handle* h, int phase, const LaunchCfg& want, LaunchCfg* out) {
@@ -622,7 +637,7 @@ int choose_grid(Handle* h, int phase, const LaunchCfg& want, LaunchCfg* out) {
     if (smem > h->smem_optin) return fail(PG_ERR_INVALID, "launch shape needs more shared memory than a block has");
     const void* fn = tile_kernel(k, c.G);
     if (!fn) return fail(PG_ERR_INVALID, "lanes per env must be 8, 16 or 32");
-    CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (int rc = allow_smem(h->device, fn, smem)) return rc;
     int nb = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, threads, smem));
     if (nb == 0) return fail(PG_ERR_INVALID, "launch shape does not fit on an SM");

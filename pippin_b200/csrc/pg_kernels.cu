@@ -173,7 +173,7 @@ __global__ void __launch_bounds__(256) collide_kernel(const __grid_constant__ St
       wk[A.k.meta + K_META_STATUS] = (double)((int)wk[A.k.meta + K_META_STATUS] | status);
     }
     T.sync();
-    if (A.learn.mode != LEARN_OFF)
+    if (A.learn.mode == LEARN_DUMP || (A.learn.mode == LEARN_PREDICT && A.warm_mode == WARM_LEARNED))
       learn_features(T, m, A.learn, e, ncon, A.st.qvel + env * m.nv, wk + A.k.a0, wk + A.k.cdof, wk + A.k.meta);
     T.sync();
   }
@@ -247,7 +247,7 @@ __global__ void __launch_bounds__(256) newton_kernel(const __grid_constant__ Ste
         const float *lfeat = nullptr, *lforce = nullptr;
         float* ldump = nullptr;
         int lnum = 0;
-        if (A.learn.mode != LEARN_OFF) {
+        if (A.learn.mode == LEARN_DUMP || (A.learn.mode == LEARN_PREDICT && A.warm_mode == WARM_LEARNED)) {
           int lbase = (int)wk[A.k.meta + K_META_LBASE];
           lnum = (int)wk[A.k.meta + K_META_LNUM];
           if (lnum > 0) {

@@ -474,3 +474,16 @@ def test_tabletop_objects_come_to_rest(solver, vmax):
             if x < 50:  # active slot: on the table top (0.4 m) within its size, not sliding
                 assert 0.4 < z < 0.5, (e, s, z)
                 assert np.linalg.norm(v[e, 6 * s:6 * s + 3]) < vmax, (e, s, v[e, 6 * s:6 * s + 3])
+
+
+def test_handles_with_different_launch_shapes():
+    """A handle created after another with a larger launch shape must not
+    shrink the kernels' shared-memory limit under it."""
+    blob = mjcf.compile_string(scenes.ant_xml())
+    big = CudaPhysics(blob, 512)
+    big.set_launch(16, 16)
+    small = CudaPhysics(blob, 64)
+    small.set_launch(16, 2)
+    big.step(range(512), 3)
+    small.step(range(64), 3)
+    assert not big.stats()["status"].any() and not small.stats()["status"].any()
