@@ -544,16 +544,16 @@ void layouts(const HostModel& m, int maxcon, int maxrows, WsLayout* w, WsLayout*
   wn->warm = take(nv);
   wn->misc = take(8);
   wn->stride = off;
-  // register Newton: the factor over M (read into registers first), rows and
-  // vectors over the factor and Newton vectors it does not use
+  // register Newton: rows and vectors over the factor and Newton vectors it
+  // does not use (M stays put; the Hessian factor lives in registers)
   if (nv <= 16 && m.dof_blocks.size() / 2 == 1) {
-    wn->sl = wn->qm;
     int need = ((16 * nv + 1) & ~1) + 16 + 32;
     int base = (wn->mp + ((nv + 1) & ~1)) - wn->fac >= need ? wn->fac : wn->stride;
     wn->sj = base;
     wn->sx = base + ((16 * nv + 1) & ~1);
     wn->sc = wn->sx + 16;
     wn->stride = std::max(wn->stride, wn->sc + 32);
+    wn->sl = wn->sx;  // the Hessian factor stays in registers
   }
 
   // per-env work record

@@ -511,8 +511,8 @@ __device__ __noinline__ void add_constraint_force(const Tile<G>& T, int k, int n
 // Shared buffers of newton_small (offsets sj, sl, sx, sc of the workspace).
 struct SmallBufs {
   double* J;  // [16][k] the first 16 constraint rows, copied in
-  double* L;  // [k][k] Hessian factor
-  double* x;  // [16] the vector being multiplied, one component per lane
+  double* L;  // unused: the Hessian factor stays in registers
+  double* x;  // [16] the vector being multiplied / the factor's exchange buffer
   double* c;  // [32] per-row coefficients
 };
 
@@ -544,9 +544,7 @@ __device__ __noinline__ int newton_small(const Tile<G>& T, int k, int nr, const 
   static_assert(G >= SMALL_N, "one lane per unknown");
   const int i = T.lane();
   const bool dof = i < k;
-  double mrow[SMALL_N];
-#pragma unroll
-  for (int q = 0; q < SMALL_N; q++) mrow[q] = (dof && q < k) ? M[i * k + q] : 0.0;
+  const double* mrow = M + i * k;  // this lane's row of M (shared memory, dof lanes only)
   const double a0 = dof ? a[i] : 0.0;
   const double wi = (warm && dof) ? warm[i] : 0.0;
   // rows i and i + 16 of this lane
@@ -588,7 +586,7 @@ __device__ __noinline__ int newton_small(const Tile<G>& T, int k, int nr, const 
   auto cost = [&](double xi) -> double {
     double tmp = xi - a0;
     publish(tmp);
-    double tmp2 = dof ? dot_ref_reg(mrow, B.x, k) : 0.0;
+    double tmp2 = dof ? dot_ref_sm(mrow, B.x, k) : 0.0;
     double c = 0.5 * T.sum(dof ? tmp * tmp2 : 0.0);
     publish(xi);
     double cr = 0.0;
@@ -625,10 +623,10 @@ __device__ __noinline__ int newton_small(const Tile<G>& T, int k, int nr, const 
       }
     double hl[SMALL_N];
 #pragma unroll
-    for (int q = 0; q < SMALL_N; q++) hl[q] = (q <= i) ? mrow[q] : 0.0;
+    for (int q = 0; q < SMALL_N; q++) hl[q] = (dof && q <= i) ? mrow[q] : 0.0;
     double rv = 0.0;
-    if (chol_reg(T, hl, k, B.L, k, &rv)) {
-      wl = a0 + solve_reg(T, B.L, k, k, rv, dof ? x : 0.0);
+    if (chol_regx(T, hl, k, B.x, &rv)) {
+      wl = a0 + solve_regx(T, hl, k, rv, dof ? x : 0.0, B.x);
       use_warm = true;
     }
   }
@@ -638,7 +636,7 @@ __device__ __noinline__ int newton_small(const Tile<G>& T, int k, int nr, const 
     if (c1 < c0) ai = wl;
   }
   publish(a0);
-  double ma0 = dof ? dot_ref_reg(mrow, B.x, k) : 0.0;
+  double ma0 = dof ? dot_ref_sm(mrow, B.x, k) : 0.0;
   double scale = 1.0 + sqrt(T.sum(ma0 * ma0));
   int iters = 0;
   int maxit = max_iters > 1 ? max_iters : 1;
@@ -649,7 +647,7 @@ __device__ __noinline__ int newton_small(const Tile<G>& T, int k, int nr, const 
     // gradient M (a - a0) + sum over active rows of D jar J_r (newton.rs:254-270)
     double tmp = ai - a0;
     publish(tmp);
-    double grad = dof ? dot_ref_reg(mrow, B.x, k) : 0.0;
+    double grad = dof ? dot_ref_sm(mrow, B.x, k) : 0.0;
     publish(ai);
     bool same = true;
 #pragma unroll
@@ -674,7 +672,7 @@ __device__ __noinline__ int newton_small(const Tile<G>& T, int k, int nr, const 
     // H = M + J_A' D J_A, this lane's row (lower part)
     double h[SMALL_N];
 #pragma unroll
-    for (int q = 0; q < SMALL_N; q++) h[q] = mrow[q];
+    for (int q = 0; q < SMALL_N; q++) h[q] = (dof && q <= i) ? mrow[q] : 0.0;
 #pragma unroll
     for (int s = 0; s < 2; s++) cv[s] = act[s] != 0.0 ? dr[s] : 0.0;
     coeffs(cv);
@@ -691,11 +689,11 @@ __device__ __noinline__ int newton_small(const Tile<G>& T, int k, int nr, const 
           if (q <= i && q < k) h[q] += e * jr[q];
       }
     double rv = 0.0;
-    if (!chol_reg(T, h, k, B.L, k, &rv)) break;
-    double p = solve_reg(T, B.L, k, k, rv, dof ? -grad : 0.0);
+    if (!chol_regx(T, h, k, B.x, &rv)) break;
+    double p = solve_regx(T, h, k, rv, dof ? -grad : 0.0, B.x);
     // exact line search on the piecewise quadratic along p (newton.rs:317-354)
     publish(p);
-    double mp = dof ? dot_ref_reg(mrow, B.x, k) : 0.0;
+    double mp = dof ? dot_ref_sm(mrow, B.x, k) : 0.0;
     double jp[2];
 #pragma unroll
     for (int s = 0; s < 2; s++) jp[s] = has[s] ? jdot(s) : 0.0;

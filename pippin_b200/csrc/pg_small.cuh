@@ -83,6 +83,66 @@ __device__ inline bool chol_reg(const Tile<G>& T, double (&a)[SMALL_N], int n, d
   return true;
 }
 
+// chol_reg without the factor in shared memory: each finished column goes
+// through the 16-double exchange buffer xb; on return lane i's a[] holds row
+// i of L (a[k], k <= i) and *rv = 1 / L_ii. Two tile syncs per column.
+template <int G>
+__device__ inline bool chol_regx(const Tile<G>& T, double (&a)[SMALL_N], int n, double* xb, double* rv) {
+  const int i = T.lane();
+#pragma unroll
+  for (int j = 0; j < SMALL_N; j++) {
+    if (j >= n) break;
+    double d = T.bcast(a[j], j);
+    if (!(d > 0.0)) return false;  // d is the same on every lane
+    double r = sqrt(d);
+    double inv = 1.0 / r;
+    double l = 0.0;
+    if (i == j) {
+      a[j] = r;
+      *rv = inv;
+    } else if (i > j) {
+      l = a[j] * inv;
+      a[j] = l;
+    }
+    T.sync();
+    if (i < SMALL_N) xb[i] = l;
+    T.sync();
+#pragma unroll
+    for (int k = j + 1; k < SMALL_N; k++)
+      if (k < n) a[k] -= l * xb[k];
+  }
+  return true;
+}
+
+// solve_reg for a factor held in registers (lane i: a[k] = L_ik, k <= i):
+// the backward sweep gets L_ji from lane j's row, published through xb
+template <int G>
+__device__ inline double solve_regx(const Tile<G>& T, const double (&a)[SMALL_N], int n, double ri, double xi,
+                                    double* xb) {
+  const int i = T.lane();
+#pragma unroll
+  for (int j = 0; j < SMALL_N; j++) {
+    if (j >= n) break;
+    double y = T.bcast(xi * ri, j);
+    if (i > j) xi -= a[j] * y;
+  }
+  xi *= ri;
+#pragma unroll
+  for (int j = SMALL_N - 1; j >= 0; j--) {
+    if (j >= n) continue;
+    T.sync();
+    if (i == j) {
+#pragma unroll
+      for (int q = 0; q < SMALL_N; q++)
+        if (q < j) xb[q] = a[q];
+    }
+    T.sync();
+    double y = T.bcast(xi * ri, j);
+    if (i < j) xi -= xb[i] * y;
+  }
+  return xi * ri;
+}
+
 // In-place L L^T = A for the n x n matrix at A (row-major, stride lda; the
 // lower triangle is read, the lower triangle and diagonal are overwritten
 // with L, the strict upper triangle is left alone); rinv[i] = 1 / L_ii.
