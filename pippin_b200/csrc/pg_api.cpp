@@ -528,11 +528,15 @@ void layouts(const HostModel& m, int maxcon, int maxrows, WsLayout* w, WsLayout*
   wn->qvel = take(nv);
   wn->qacc = take(nv);
   wn->qm = take(nv * nv);
-  wn->cdof = take(6 * nv);
   wn->smooth = take(nv);
   wn->acc = take(nv);
   wn->qfrc_c = take(nv);
+  // cdof, rinv and warm side by side: the register Newton keeps its packed
+  // factor there (cdof is dead once the rows are built, rinv and
+  // warm are not used on that path)
+  wn->cdof = take(6 * nv);
   wn->rinv = take(nv);
+  wn->warm = take(nv);
   wn->fac = take(nv * nv);
   wn->a0 = take(nv);
   wn->grad = take(nv);
@@ -541,7 +545,6 @@ void layouts(const HostModel& m, int maxcon, int maxrows, WsLayout* w, WsLayout*
   wn->tmp2 = take(nv);
   wn->mp = take(nv);
   wn->vel = take(nv);
-  wn->warm = take(nv);
   wn->misc = take(8);
   wn->stride = off;
   // register Newton: rows and vectors over the factor and Newton vectors it
@@ -553,7 +556,14 @@ void layouts(const HostModel& m, int maxcon, int maxrows, WsLayout* w, WsLayout*
     wn->sx = base + ((16 * nv + 1) & ~1);
     wn->sc = wn->sx + 16;
     wn->stride = std::max(wn->stride, wn->sc + 32);
-    wn->sl = wn->sx;  // the Hessian factor stays in registers
+    // the Hessian factor's entries below the diagonal, packed
+    int ncol = nv * (nv - 1) / 2;
+    if (wn->fac - wn->cdof >= ncol) {
+      wn->sl = wn->cdof;
+    } else {
+      wn->sl = wn->stride;
+      wn->stride += (ncol + 1) & ~1;
+    }
   }
 
   // per-env work record

@@ -511,21 +511,22 @@ __device__ __noinline__ void add_constraint_force(const Tile<G>& T, int k, int n
 // Shared buffers of newton_small (offsets sj, sl, sx, sc of the workspace).
 struct SmallBufs {
   double* J;  // [16][k] the first 16 constraint rows, copied in
-  double* L;  // unused: the Hessian factor stays in registers
-  double* x;  // [16] the vector being multiplied / the factor's exchange buffer
+  double* L;  // [k(k-1)/2] the Hessian factor's entries below the diagonal, packed by rows
+  double* x;  // [16] the vector being multiplied
   double* c;  // [32] per-row coefficients
 };
 
 constexpr int SMALL_ROWS = 2 * SMALL_N;  // rows the register Newton takes (two per lane)
 
 // newton.rs:224-371 for k <= 16 unknowns and nr <= 32 rows: lane i holds
-// unknown i and rows i and i + 16. The lane's row of M and of the Hessian
-// stay in registers; the first 16 rows of J are copied into shared memory
+// unknown i and rows i and i + 16. M stays in shared memory, the lane's row
+// of the Hessian (and of its factor) in registers, the factor also packed
+// in B.L; the first 16 rows of J are copied into shared memory
 // (rows 16..31, rare, are read where build_rows left them); each product
 // M x / J x reads the published x with broadcast loads. On 16-lane tiles
 // every per-lane partial sum holds the same terms in the same order as
 // newton_dense's, so the sums agree with it exactly; only the factorisation
-// differs (chol_reg). Adds the constraint force to qfrc (newton.rs:361-371)
+// differs (chol_regx). Adds the constraint force to qfrc (newton.rs:361-371)
 // and leaves the solution in a; returns the iteration count. J rows are
 // read from Jsrc (stride k), row constants from R.
 //
@@ -625,18 +626,27 @@ __device__ __noinline__ int newton_small(const Tile<G>& T, int k, int nr, const 
 #pragma unroll
     for (int q = 0; q < SMALL_N; q++) hl[q] = (dof && q <= i) ? mrow[q] : 0.0;
     double rv = 0.0;
-    if (chol_regx(T, hl, k, B.x, &rv)) {
-      wl = a0 + solve_regx(T, hl, k, rv, dof ? x : 0.0, B.x);
+    if (chol_regx(T, hl, k, B.L, &rv)) {
+      wl = a0 + solve_regx(T, hl, k, B.L, rv, dof ? x : 0.0);
       use_warm = true;
     }
   }
+  // x = a0 once: M a0 for the scale, and J a0 for the cold cost, whose
+  // quadratic term is exactly zero (a - a0 = 0)
+  publish(a0);
+  double ma0 = dof ? dot_ref_sm(mrow, B.x, k) : 0.0;
   if (use_warm) {
-    double c0 = cost(a0);
+    double cr = 0.0;
+#pragma unroll
+    for (int s = 0; s < 2; s++)
+      if (has[s]) {
+        double jar = jdot(s) - aref[s];
+        if (bil[s] || jar < 0.0) cr += 0.5 * dr[s] * jar * jar;
+      }
+    double c0 = T.sum(cr);
     double c1 = cost(wl);
     if (c1 < c0) ai = wl;
   }
-  publish(a0);
-  double ma0 = dof ? dot_ref_sm(mrow, B.x, k) : 0.0;
   double scale = 1.0 + sqrt(T.sum(ma0 * ma0));
   int iters = 0;
   int maxit = max_iters > 1 ? max_iters : 1;
@@ -689,8 +699,8 @@ __device__ __noinline__ int newton_small(const Tile<G>& T, int k, int nr, const 
           if (q <= i && q < k) h[q] += e * jr[q];
       }
     double rv = 0.0;
-    if (!chol_regx(T, h, k, B.x, &rv)) break;
-    double p = solve_regx(T, h, k, rv, dof ? -grad : 0.0, B.x);
+    if (!chol_regx(T, h, k, B.L, &rv)) break;
+    double p = solve_regx(T, h, k, B.L, rv, dof ? -grad : 0.0);
     // exact line search on the piecewise quadratic along p (newton.rs:317-354)
     publish(p);
     double mp = dof ? dot_ref_sm(mrow, B.x, k) : 0.0;

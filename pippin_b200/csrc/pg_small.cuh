@@ -4,17 +4,17 @@
 // pg_linalg.cuh.
 //
 // Lane i keeps row i of the matrix in registers. The factorisation is
-// right-looking: at column j every lane forms the pivot L_jj = sqrt(d) and
-// 1/L_jj itself from the diagonal shuffled out of lane j (so no lane waits on
-// a shared write for it), scales its own entry below the pivot, publishes it
-// in the matrix, and after one tile sync applies the rank-1 update to its
-// row, reading the finished column as broadcast loads. A block-diagonal
-// matrix (several dof trees) factors to the same block-diagonal L: entries
-// across blocks start at zero and stay exactly zero.
+// right-looking: at column j every lane forms 1/L_jj = rsqrt(d) and
+// L_jj = d / sqrt(d) itself from the diagonal shuffled out of lane j (so no
+// lane waits on a shared write for it), scales its own entry below the pivot,
+// publishes it, and after one tile sync applies the rank-1 update to its row,
+// reading the finished column as broadcast loads. A block-diagonal matrix
+// (several dof trees) factors to the same block-diagonal L: entries across
+// blocks start at zero and stay exactly zero.
 //
 // The solves keep the unknown of row i in lane i's register; each step of
 // the forward and backward sweep is one shuffle of the finished unknown and
-// one FMA per lane, with the L entries the lane needs loaded up front.
+// one FMA per lane, with the L entry the lane needs read from shared memory.
 #pragma once
 #include "pg_linalg.cuh"
 
@@ -54,7 +54,9 @@ __device__ inline double dot_ref_sm(const double* a, const double* x, int n) {
 // Factor the rows held in registers (lane i: a[k] = A_ik, k <= i) into L,
 // written to L (shared, stride lda: lower triangle and diagonal) as each
 // column finishes and left in a[]; *rv = 1 / L_ii on lane i. Returns false
-// (uniformly over the tile) if a pivot is not positive.
+// (uniformly over the tile) if a pivot is not positive. The pivot's
+// reciprocal comes from one reciprocal square root, not a square root and a
+// division.
 template <int G>
 __device__ inline bool chol_reg(const Tile<G>& T, double (&a)[SMALL_N], int n, double* L, int lda, double* rv) {
   const int i = T.lane();
@@ -64,11 +66,10 @@ __device__ inline bool chol_reg(const Tile<G>& T, double (&a)[SMALL_N], int n, d
     if (j >= n) break;
     double d = T.bcast(a[j], j);
     if (!(d > 0.0)) return false;  // d is the same on every lane
-    double r = sqrt(d);
-    double inv = 1.0 / r;
+    double inv = rsqrt(d);  // 1 / L_jj; L_jj = d / sqrt(d) as d * inv
     double l = 0.0;
     if (i == j) {
-      a[j] = r;
+      a[j] = d * inv;
       *rv = inv;
     } else if (i > j) {
       l = a[j] * inv;
@@ -83,42 +84,45 @@ __device__ inline bool chol_reg(const Tile<G>& T, double (&a)[SMALL_N], int n, d
   return true;
 }
 
-// chol_reg without the factor in shared memory: each finished column goes
-// through the 16-double exchange buffer xb; on return lane i's a[] holds row
-// i of L (a[k], k <= i) and *rv = 1 / L_ii. Two tile syncs per column.
+// chol_reg with the rows of L left in registers (lane i: a[k] = L_ik, k <= i)
+// and the entries below the diagonal also written to the packed store Lr
+// (row k's entries L_k0 .. L_k,k-1 at k(k-1)/2, so that every offset the
+// unrolled loops use is a constant), which is how the lanes exchange them:
+// every entry has its own slot, so one tile sync per column suffices.
+// *rv = 1 / L_ii. Same arithmetic as chol_reg.
 template <int G>
-__device__ inline bool chol_regx(const Tile<G>& T, double (&a)[SMALL_N], int n, double* xb, double* rv) {
+__device__ inline bool chol_regx(const Tile<G>& T, double (&a)[SMALL_N], int n, double* Lr, double* rv) {
   const int i = T.lane();
+  double* row = Lr + (i < n ? i * (i - 1) / 2 : 0);  // this lane's row of the store
 #pragma unroll
   for (int j = 0; j < SMALL_N; j++) {
     if (j >= n) break;
     double d = T.bcast(a[j], j);
     if (!(d > 0.0)) return false;  // d is the same on every lane
-    double r = sqrt(d);
-    double inv = 1.0 / r;
+    double inv = rsqrt(d);  // 1 / L_jj; L_jj = d / sqrt(d) as d * inv
     double l = 0.0;
     if (i == j) {
-      a[j] = r;
+      a[j] = d * inv;
       *rv = inv;
     } else if (i > j) {
       l = a[j] * inv;
       a[j] = l;
+      if (i < n) row[j] = l;
     }
-    T.sync();
-    if (i < SMALL_N) xb[i] = l;
     T.sync();
 #pragma unroll
     for (int k = j + 1; k < SMALL_N; k++)
-      if (k < n) a[k] -= l * xb[k];
+      if (k < n) a[k] -= l * Lr[k * (k - 1) / 2 + j];
   }
   return true;
 }
 
-// solve_reg for a factor held in registers (lane i: a[k] = L_ik, k <= i):
-// the backward sweep gets L_ji from lane j's row, published through xb
+// solve_reg for a factor from chol_regx: the forward sweep uses the row in
+// registers, the backward sweep reads L_ji from the packed store; each step
+// is one shuffle of the finished unknown and one FMA per lane, with no syncs.
 template <int G>
-__device__ inline double solve_regx(const Tile<G>& T, const double (&a)[SMALL_N], int n, double ri, double xi,
-                                    double* xb) {
+__device__ inline double solve_regx(const Tile<G>& T, const double (&a)[SMALL_N], int n, const double* Lr, double ri,
+                                    double xi) {
   const int i = T.lane();
 #pragma unroll
   for (int j = 0; j < SMALL_N; j++) {
@@ -127,18 +131,13 @@ __device__ inline double solve_regx(const Tile<G>& T, const double (&a)[SMALL_N]
     if (i > j) xi -= a[j] * y;
   }
   xi *= ri;
+  const double* col = Lr + (i < SMALL_N ? i : 0);  // col[j(j-1)/2] = L_ji
 #pragma unroll
   for (int j = SMALL_N - 1; j >= 0; j--) {
     if (j >= n) continue;
-    T.sync();
-    if (i == j) {
-#pragma unroll
-      for (int q = 0; q < SMALL_N; q++)
-        if (q < j) xb[q] = a[q];
-    }
-    T.sync();
     double y = T.bcast(xi * ri, j);
-    if (i < j) xi -= xb[i] * y;
+    if (i < j) xi -= col[j * (j - 1) / 2] * y;
+    asm volatile("" ::: "memory");  // one load a step, not all of them up front
   }
   return xi * ri;
 }
