@@ -37,17 +37,20 @@ __device__ inline double dot_ref_reg(const double (&a)[SMALL_N], const double* x
   return t;
 }
 
-// The same for a row in shared memory.
+// The same for a row in shared memory, as a loop (small code).
 __device__ inline double dot_ref_sm(const double* a, const double* x, int n) {
-  double s[4] = {0.0, 0.0, 0.0, 0.0};
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
   int n4 = n >= 8 ? (n & ~3) : 0;
-#pragma unroll
-  for (int k = 0; k < SMALL_N; k++)
-    if (k < n4) s[k & 3] += a[k] * x[k];
-  double t = (s[0] + s[1]) + (s[2] + s[3]);
-#pragma unroll
-  for (int k = 0; k < SMALL_N; k++)
-    if (k >= n4 && k < n) t += a[k] * x[k];
+#pragma unroll 1
+  for (int k = 0; k < n4; k += 4) {
+    s0 += a[k] * x[k];
+    s1 += a[k + 1] * x[k + 1];
+    s2 += a[k + 2] * x[k + 2];
+    s3 += a[k + 3] * x[k + 3];
+  }
+  double t = (s0 + s1) + (s2 + s3);
+#pragma unroll 1
+  for (int k = n4; k < n; k++) t += a[k] * x[k];
   return t;
 }
 
