@@ -24,6 +24,11 @@ int pg_fp64_peak(int device, int iters, double* tflops, double* ms_out);
 int pg_time_phases(pg_handle* h, int64_t start, int64_t end, int64_t nstep, const double* ctrl_dev,
                    float* ms_out);
 
+/* The launch shape of one phase kernel (0 smooth dynamics, 1 collision,
+ * 2 Newton): lanes per env, envs per block, blocks. Any pointer may be NULL.
+ * Returns PG_OK or PG_ERR_INVALID. */
+int pg_phase_launch(const pg_handle* h, int phase, int* lanes_per_env, int* envs_per_block, int* blocks);
+
 #ifdef __cplusplus
 }
 #endif

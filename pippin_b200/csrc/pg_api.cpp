@@ -1657,6 +1657,16 @@ int pg_get_launch(const pg_handle* h, int* lanes_per_env, int* envs_per_block, i
   return PG_OK;
 }
 
+int pg_phase_launch(const pg_handle* h, int phase, int* lanes_per_env, int* envs_per_block, int* blocks) {
+  if (!h) return fail(PG_ERR_INVALID, "NULL handle");
+  if (phase < 0 || phase > 2) return fail(PG_ERR_INVALID, "phase must be 0, 1 or 2");
+  const LaunchCfg& c = phase == 0 ? h->cfg.smooth : phase == 1 ? h->cfg.collide : h->cfg.newton;
+  if (lanes_per_env) *lanes_per_env = c.G;
+  if (envs_per_block) *envs_per_block = c.tiles_per_block;
+  if (blocks) *blocks = c.blocks;
+  return PG_OK;
+}
+
 int pg_autotune(pg_handle* h, int64_t nstep) {
   if (!h) return fail(PG_ERR_INVALID, "NULL handle");
   if (h->n == 0) return PG_OK;

@@ -51,12 +51,22 @@ __device__ inline double* tile_workspace(const StepArgs& A, unsigned char* sm, i
   return reinterpret_cast<double*>(sm + off) + (size_t)tib * stride;
 }
 
-// pops the next work item for the tile (one atomic per env)
+// Work items of a persistent grid: a tile's first item is its own index in
+// the grid; later ones come from the phase's counter (one atomic per env),
+// offset by the tile count, and only when the grid has fewer tiles than
+// items. A grid with a tile per item takes no atomics and no round trip to
+// the counter before its first env or after its last.
 template <int G>
-__device__ inline int next_item(const Tile<G>& T, int* queue) {
+__device__ inline int first_item() {
+  return blockIdx.x * (blockDim.x / G) + threadIdx.x / G;
+}
+template <int G>
+__device__ inline int next_item(const Tile<G>& T, int* queue, int count) {
+  int ntiles = gridDim.x * (blockDim.x / G);
+  if (ntiles >= count) return count;
   int item = 0;
   if (T.lane() == 0) item = atomicAdd(queue, 1);
-  return T.bcast(item, 0);
+  return ntiles + T.bcast(item, 0);
 }
 
 template <int G>
@@ -80,9 +90,7 @@ __global__ void __launch_bounds__(256) smooth_kernel(const __grid_constant__ Ste
   e.con = nullptr;
   int nq = m.nq, nv = m.nv, nu = m.nu;
   double h = m.timestep;
-  for (;;) {
-    int item = next_item(T, A.queue + 0);
-    if (item >= A.count) break;
+  for (int item = first_item<G>(); item < A.count; item = next_item(T, A.queue + 0, A.count)) {
     size_t env = (size_t)A.start + item;
     e.env = (int)env;
     e.prm = A.st.params + env * m.pstride;
@@ -155,9 +163,7 @@ __global__ void __launch_bounds__(256) collide_kernel(const __grid_constant__ St
   EnvCtx e;
   e.ws = nullptr;
   e.scr = nullptr;
-  for (;;) {
-    int item = next_item(T, A.queue + 1);
-    if (item >= A.count) break;
+  for (int item = first_item<G>(); item < A.count; item = next_item(T, A.queue + 1, A.count)) {
     size_t env = (size_t)A.start + item;
     e.env = (int)env;
     e.prm = A.st.params + env * m.pstride;
@@ -196,9 +202,7 @@ __global__ void __launch_bounds__(256) newton_kernel(const __grid_constant__ Ste
   e.scr = A.scratch + gtile * (size_t)A.s.stride;
   int nq = m.nq, nv = m.nv;
   double h = m.timestep;
-  for (;;) {
-    int item = next_item(T, A.queue + 2);
-    if (item >= A.count) break;
+  for (int item = first_item<G>(); item < A.count; item = next_item(T, A.queue + 2, A.count)) {
     size_t env = (size_t)A.start + item;
     e.env = (int)env;
     e.prm = A.st.params + env * m.pstride;
@@ -207,20 +211,22 @@ __global__ void __launch_bounds__(256) newton_kernel(const __grid_constant__ Ste
     e.con = wk + A.k.contacts;
     double* ws = e.ws;
     prefetch_l1(T, e.prm, sizeof(double) * m.pstride);
+    // the state and the smooth phase's results are on their way while the
+    // meta block is read (an env that stopped stepping does not use them)
+    load_async(T, ws + w.qpos, A.st.qpos + env * nq, nq);
+    load_async(T, ws + w.qvel, A.st.qvel + env * nv, nv);
+    load_async(T, ws + w.qacc, A.st.qacc + env * nv, nv);
+    load_async(T, ws + w.qm, wk + A.k.qm, nv * nv);
+    load_async(T, ws + w.cdof, wk + A.k.cdof, 6 * nv);
+    load_async(T, ws + w.acc, wk + A.k.a0, nv);
+    load_async(T, ws + w.smooth, wk + A.k.smooth, nv);
     int status = (int)wk[A.k.meta + K_META_STATUS];
     int ncon = (int)wk[A.k.meta + K_META_NCON];
+    prefetch_l1(T, e.con, sizeof(double) * C_STRIDE * ncon);
+    load_wait();
+    T.sync();
     int iters = 0, nr = 0;
     if (!(status & ST_NOT_SPD)) {
-      prefetch_l1(T, e.con, sizeof(double) * C_STRIDE * ncon);
-      load_async(T, ws + w.qpos, A.st.qpos + env * nq, nq);
-      load_async(T, ws + w.qvel, A.st.qvel + env * nv, nv);
-      load_async(T, ws + w.qacc, A.st.qacc + env * nv, nv);
-      load_async(T, ws + w.qm, wk + A.k.qm, nv * nv);
-      load_async(T, ws + w.cdof, wk + A.k.cdof, 6 * nv);
-      load_async(T, ws + w.acc, wk + A.k.a0, nv);
-      load_async(T, ws + w.smooth, wk + A.k.smooth, nv);
-      load_wait();
-      T.sync();
       double* acc = ws + w.acc;
       double* v = ws + w.vel;
       double* vpos = v;
@@ -304,9 +310,7 @@ __global__ void __launch_bounds__(256) set_const_kernel(const __grid_constant__ 
   e.ws = tile_workspace(A, smem, w.stride, tib);
   e.scr = A.scratch + gtile * (size_t)A.s.stride;
   int nv = m.nv;
-  for (;;) {
-    int item = next_item(T, A.queue + 0);
-    if (item >= n) break;
+  for (int item = first_item<G>(); item < n; item = next_item(T, A.queue + 0, n)) {
     e.env = envs ? envs[item] : A.start + item;
     double* prm = A.st.params + (size_t)e.env * m.pstride;
     e.prm = prm;
@@ -401,9 +405,7 @@ __global__ void __launch_bounds__(256) poses_kernel(const __grid_constant__ Step
   EnvCtx e;
   e.ws = tile_workspace(A, smem, w.stride, threadIdx.x / G);
   e.scr = nullptr;
-  for (;;) {
-    int item = next_item(T, A.queue + 0);
-    if (item >= A.count) break;
+  for (int item = first_item<G>(); item < A.count; item = next_item(T, A.queue + 0, A.count)) {
     size_t env = (size_t)A.start + item;
     e.env = (int)env;
     e.prm = A.st.params + env * m.pstride;

@@ -370,6 +370,15 @@ class CudaPhysics:
         self._check(self._L.pg_get_launch(self._h, C.byref(g), C.byref(t), C.byref(b)))
         return g.value, t.value, b.value
 
+    def phase_launch(self) -> dict:
+        """Launch shape (lanes per env, envs per block, blocks) of each phase kernel."""
+        out = {}
+        for k, name in enumerate(("smooth", "collide", "newton")):
+            g, t, b = C.c_int32(), C.c_int32(), C.c_int32()
+            self._check(self._L.pg_phase_launch(self._h, k, C.byref(g), C.byref(t), C.byref(b)))
+            out[name] = (g.value, t.value, b.value)
+        return out
+
     def autotune(self, nstep: int = 1):
         self._check(self._L.pg_autotune(self._h, int(nstep)))
         return self.launch()
