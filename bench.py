@@ -56,6 +56,10 @@ def parse():
     ap.add_argument("--lanes", type=int, default=0, help="force lanes per env (8, 16, 32)")
     ap.add_argument("--per-block", type=int, default=0, help="force envs per block")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--learned-eval", action="store_true",
+                    help="the learned warm-start evaluation (Ant and tabletop) instead of the headline")
+    ap.add_argument("--learned-samples", type=int, default=10_000_000, help="training pairs per scene")
+    ap.add_argument("--learned-envs", type=int, default=16384)
     return ap.parse_args()
 
 
@@ -404,10 +408,103 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_learned_eval(args):
+    """The learned Newton warm start on Ant and the tabletop scene: training
+    pairs (24 contact features -> converged frame forces) from the plain
+    solver's own converged solves, a network fitted to them on the GPU, then
+    cold start vs learned start on the same workload at the same 1e-10
+    tolerance (iteration counts and CUDA-graph step time). One JSON line per
+    scene (rank 0; one GPU)."""
+    import torch
+    from pippin_b200 import CudaPhysics, Field, Param, WarmStart, mjcf, scenes, warm
+    n, K, W = args.learned_envs, args.steps, max(args.warmup, 3)
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+
+    def ant(seed):
+        m = mjcf.load_string(scenes.ant_xml(tolerance=TOL, iterations=ITERS))
+        p = CudaPhysics(mjcf.to_blob(m), n)
+        q, v, rng = initial_state(m, n, seed)
+        p.set(Field.QPOS, range(n), q)
+        p.set(Field.QVEL, range(n), v)
+        return m, p, (lambda t: rng.uniform(-1, 1, (n, m.nu))), 20
+
+    def tabletop(seed):
+        plan = scenes.tabletop(n, seed=seed)
+        m = mjcf.load_string(plan.xml)
+        p = CudaPhysics(mjcf.to_blob(m), n)
+        p.set_solver(tolerance=TOL, iterations=ITERS)
+        plan.apply(lambda pid, elem, vals: p.set_param(Param(pid), elem, range(n), vals), lambda: p.reset(range(n)))
+        return m, p, None, 50
+
+    for name, make in (("ant", ant), ("tabletop", tabletop)):
+        t0 = time.perf_counter()
+        m, p, controls, skip = make(11)
+        xs, fs, steps = [], [], 0
+        for t in range(skip):
+            if controls is not None:
+                p.set(Field.CTRL, range(n), controls(t))
+            p.step(range(n), 1)
+        got = 0
+        while got < args.learned_samples and steps < 20000:
+            if controls is not None:
+                p.set(Field.CTRL, range(n), controls(steps))
+            X, F = p.warm_samples(range(n))
+            xs.append(X)
+            fs.append(F)
+            got += len(X)
+            steps += 1
+            if name == "tabletop" and steps % 200 == 0:  # objects at rest: drop a fresh batch
+                p.close()
+                m, p, controls, _ = make(11 + steps)
+        p.close()
+        X, F = np.concatenate(xs)[:args.learned_samples], np.concatenate(fs)[:args.learned_samples]
+        t_collect = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        w, losses = warm.train(X, F, epochs=8, batch=8192, lr=1e-3, seed=1)
+        t_train = time.perf_counter() - t0
+        out = {}
+        for mode, wm in (("cold", WarmStart.COLD), ("learned", WarmStart.LEARNED)):
+            m, p, controls, skip = make(7)
+            p.set_warm_mlp(w)
+            p.set_solver(warm=int(wm))
+            ctrl = None
+            if controls is not None:
+                ctrl = torch.from_numpy(np.stack([controls(t) for t in range(skip + W + K)])).to(dev)
+            for t in range(skip + W):
+                p.step_device(range(n), 1, ctrl[t].data_ptr() if ctrl is not None else 0)
+            p.synchronize()
+            stream = torch.cuda.ExternalStream(p.stream(), device=dev)
+            iters, ms = [], 0.0
+            for k in range(K):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                p.step_device(range(n), 1, ctrl[skip + W + k].data_ptr() if ctrl is not None else 0)
+                e1.record(stream)
+                e1.synchronize()
+                ms += e0.elapsed_time(e1)
+                st = p.stats()
+                iters.append(st["iters"][st["nrows"] > 0])
+            p.close()
+            it = np.concatenate(iters)
+            out[mode] = {"env_steps_per_s": n * K / (ms * 1e-3), "ms_per_step": ms / K,
+                         "mean_iters": float(it.mean()) if len(it) else 0.0,
+                         "p99_iters": float(np.percentile(it, 99)) if len(it) else 0.0}
+        line = {"metric": f"learned warm start, {name}", "impl": "ours", "envs": n, "steps": K, "warmup": W,
+                "tolerance": TOL, "dtype": "f64 physics, bf16 network (fp32 accumulate)", "data": "synthetic",
+                "train": {"samples": int(len(X)), "collect_steps": steps, "epochs": 8, "loss": [float(losses[0]), float(losses[-1])],
+                          "collect_s": t_collect, "train_s": t_train},
+                "iters_over": "envs with constraint rows",
+                "cold": out["cold"], "learned": out["learned"]}
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.learned_eval:
+        run_learned_eval(args)
     else:
         run_ours(args)
 

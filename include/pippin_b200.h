@@ -197,14 +197,14 @@ int pg_stats(pg_handle* h, int64_t start, int64_t end, int32_t* iters, int32_t* 
  * each substep lists the touching contacts (24 features each), predicts
  * their frame forces on the tensor cores, and offers a0 + M^-1 J' f as the
  * starting point behind the same cost gate; the solution and its tolerance
- * are unchanged. Applies to models with one dof tree and at most 16 dofs
- * (the register Newton path); other envs start cold.
+ * are unchanged. Applies to the Newton solver on every model (the register
+ * path and the tile paths with islands).
  * pg_set_warm_mlp: weights as in include/pippin_b200_mlp.h (36662 floats). */
 int pg_set_warm_mlp(pg_handle* h, const float* weights, size_t len);
 
 /* Training pairs for the warm start: one substep of envs [start, end) (with
  * the current controls, like pg_step), returning for each touching contact
- * solved on the register Newton path its 24 features (X) and the converged
+ * solved by Newton its 24 features (X) and the converged
  * forces of its four pyramid rows (rows; the frame forces are
  * f_n = r0 + r1 + r2 + r3, f_t1 = mu (r0 - r1), f_t2 = mu (r2 - r3), mu =
  * feature 1). X holds pg_warm_capacity * 24 floats, rows pg_warm_capacity * 4.

@@ -884,6 +884,56 @@ __device__ __noinline__ int newton_islands(const Tile<G>& T, const DModel& m, co
   return iters;
 }
 
+// The learned warm start on the tile paths (several dof trees, or more dofs
+// or rows than the register Newton takes), as newton_small does it: the
+// predicted frame forces of the lnum touching contacts (whose pyramid rows
+// are the first 4 lnum rows) become row forces f_n / 4 +- f_tk / (2 mu), and
+// out = a + M^-1 sum_r f_r J_r' is the candidate start for the dense
+// solver's cost gate. M is factored per dof block in the Hessian's slot,
+// which is free until Newton starts. Returns false if M is not positive
+// definite (no candidate).
+template <int G>
+__device__ bool learned_start(const Tile<G>& T, const DModel& m, const WsLayout& w, const EnvCtx& e,
+                              const double* J, const double* a, const float* lfeat, const float* lforce, int lnum,
+                              double* out) {
+  int lane = T.lane(), nv = m.nv;
+  double* ws = e.ws;
+  double* F = ws + w.fac;
+  double* rinv = ws + w.rinv;
+  for (int t = lane; t < nv * nv; t += G) F[t] = ws[w.qm + t];
+  for (int i = lane; i < nv; i += G) {
+    double x = 0.0;
+    for (int r = 0; r < 4 * lnum; r++) {
+      int c = r / 4, q = r % 4;
+      double mu = lfeat[c * LEARN_NF + 1];
+      double fn = lforce[3 * c], ft = lforce[3 * c + 1 + q / 2];
+      double f = 0.25 * fn + (mu > 0.0 ? ((q & 1) ? -ft : ft) / (2.0 * mu) : 0.0);
+      if (f != 0.0) x += f * J[r * nv + i];
+    }
+    out[i] = x;
+  }
+  T.sync();
+  if (!chol_auto(T, F, nv, nv, m.nblock, m.block_adr, m.dof_block, m.maxbs, rinv)) return false;
+  solve_auto(T, F, nv, nv, m.nblock, m.block_adr, m.dof_block, m.maxbs, rinv, out);
+  for (int i = lane; i < nv; i += G) out[i] = a[i] + out[i];
+  T.sync();
+  return true;
+}
+
+// The converged forces -D_r (J_r a - aref_r) of rows [0, nrows) (zero where
+// the row is inactive) as training targets of the learned warm start
+// (newton.rs:361-371).
+template <int G>
+__device__ void dump_row_forces(const Tile<G>& T, int nv, const double* J, const double* R, const double* a,
+                                int nrows, float* ldump) {
+  for (int r = T.lane(); r < nrows; r += G) {
+    const double* rr = R + R_STRIDE * r;
+    double v = dot_ref_sm(J + r * nv, a, nv) - rr[R_AREF];
+    ldump[r] = (rr[R_FLAGS] != 0.0 || v < 0.0) ? (float)(-rr[R_D] * v) : 0.0f;
+  }
+  T.sync();
+}
+
 // newton.rs:378-473
 template <int G>
 __device__ int newton_solve(const Tile<G>& T, const DModel& m, const WsLayout& w, const ScrLayout& s,
@@ -900,7 +950,15 @@ __device__ int newton_solve(const Tile<G>& T, const DModel& m, const WsLayout& w
   for (int r = lane; r < nr; r += G) R[R_STRIDE * r + R_ACT] = -1.0;  // no previous active set
   T.sync();
   NewtonBufs B{ws + w.a0, ws + w.grad, ws + w.p, ws + w.tmp, ws + w.tmp2, ws + w.mp, ws + w.fac, ws + w.rinv};
-  if (m.nblock > 1) return newton_islands(T, m, w, s, e, nr, a, warm, B);
+  bool learned = lnum > 0 && 4 * lnum <= nr;
+  if (m.nblock > 1) {
+    // the learned candidate goes over the previous qacc, which the learned
+    // mode does not read and the kernel rewrites after Newton
+    if (learned && lforce && learned_start(T, m, w, e, J, a, lfeat, lforce, lnum, ws + w.qacc)) warm = ws + w.qacc;
+    int it = newton_islands(T, m, w, s, e, nr, a, warm, B);
+    if (learned && ldump) dump_row_forces(T, nv, J, R, a, 4 * lnum, ldump);
+    return it;
+  }
   // one tree: the rows either touch it (one island spanning everything)
   // or none has a nonzero entry (no island: nothing is solved)
   bool nz = false;
@@ -913,8 +971,10 @@ __device__ int newton_solve(const Tile<G>& T, const DModel& m, const WsLayout& w
                           lnum, ldump);
     }
   }
+  if (learned && lforce && learned_start(T, m, w, e, J, a, lfeat, lforce, lnum, ws + w.qacc)) warm = ws + w.qacc;
   int it = newton_dense(T, nv, nr, J, R, ws + w.qm, a, warm, m.iterations, m.tolerance, B);
   add_constraint_force(T, nv, nr, J, R, a, (const int*)nullptr, qfrc);
+  if (learned && ldump) dump_row_forces(T, nv, J, R, a, 4 * lnum, ldump);
   return it;
 }
 

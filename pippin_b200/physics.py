@@ -254,8 +254,8 @@ class CudaPhysics:
         (n, 24) and converged frame forces (n, 3) (f_n, f_t1, f_t2) as float32."""
         s, e = _span(envs)
         cap = int(self._L.pg_warm_capacity(self._h))
-        X = np.zeros((cap, 24), np.float32)
-        R = np.zeros((cap, 4), np.float32)
+        X = np.empty((cap, 24), np.float32)
+        R = np.empty((cap, 4), np.float32)
         n = C.c_int64()
         self._check(self._L.pg_warm_samples(self._h, s, e, X.ctypes.data_as(C.POINTER(C.c_float)), X.size,
                                             R.ctypes.data_as(C.POINTER(C.c_float)), R.size, C.byref(n)))

@@ -131,3 +131,46 @@ def test_learned_warm_start_on_ant():
     cold, learned = np.concatenate(iters["cold"]), np.concatenate(iters["learned"])
     assert worst < 1e-8, worst
     assert learned.mean() < cold.mean(), (learned.mean(), cold.mean())
+
+
+def test_learned_warm_start_on_tabletop():
+    """The learned start on a model with many dof trees (the tile Newton with
+    islands): training pairs come from converged island solves, and starting
+    from the prediction gives the cold start's solution (both stop at the
+    1e-10 gradient tolerance, behind the same per-island cost gate)."""
+    from pippin_b200 import CudaPhysics, Field, Param, WarmStart, mjcf, scenes
+    n = 512
+    plan = scenes.tabletop(n, seed=3)
+    m = mjcf.load_string(plan.xml)
+    p = CudaPhysics(mjcf.to_blob(m), n)
+    p.set_solver(tolerance=1e-10)
+    plan.apply(lambda pid, elem, vals: p.set_param(Param(pid), elem, range(n), vals), lambda: p.reset(range(n)))
+    X, F = warm.collect(p, 160, skip=60)
+    assert len(X) > 20000, len(X)
+    assert np.all(np.isfinite(F)) and np.mean(F[:, 0] >= -1e-6) > 0.99  # normal forces push
+    w, losses = warm.train(X, F, epochs=10, batch=2048, lr=1e-3, seed=1)
+    assert losses[-1] < 0.5 * losses[0], losses
+    # held-out envs, still landing: cold vs learned on identical inputs
+    plan = scenes.tabletop(n, seed=4)
+    g = CudaPhysics(mjcf.to_blob(mjcf.load_string(plan.xml)), n)
+    g.set_solver(tolerance=1e-10)
+    plan.apply(lambda pid, elem, vals: g.set_param(Param(pid), elem, range(n), vals), lambda: g.reset(range(n)))
+    g.set_warm_mlp(w)
+    g.step(range(n), 60)
+    worst, used = 0.0, 0
+    for t in range(30):
+        st = {f: g.get(f, range(n)) for f in (Field.QPOS, Field.QVEL, Field.QACC)}
+        out = {}
+        for mode, wm in (("cold", WarmStart.COLD), ("learned", WarmStart.LEARNED)):
+            for f in st:
+                g.set(f, range(n), st[f])
+            g.set_solver(warm=int(wm))
+            g.step(range(n), 1)
+            s = g.stats()
+            assert not s["status"].any()
+            used += int((s["nrows"] > 0).sum())
+            out[mode] = g.get(Field.QACC, range(n))
+        scale = np.maximum(np.abs(out["cold"]).max(axis=1), 1.0)
+        worst = max(worst, float((np.abs(out["learned"] - out["cold"]).max(axis=1) / scale).max()))
+    assert used > n * 10
+    assert worst < 1e-8, worst
