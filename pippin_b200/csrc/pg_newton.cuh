@@ -538,7 +538,7 @@ constexpr int SMALL_ROWS = 2 * SMALL_N;  // rows the register Newton takes (two 
 // start (newton.rs:238-245). With ldump, the converged forces of those rows
 // are written there (4 per contact) as training targets.
 template <int G>
-__device__ __noinline__ int newton_small(const Tile<G>& T, int k, int nr, const double* Jsrc, const double* R,
+__device__ inline int newton_small(const Tile<G>& T, int k, int nr, const double* Jsrc, const double* R,
                                          const double* M, double* a, const double* warm, int max_iters, double tol,
                                          const SmallBufs& B, double* qfrc, const float* lfeat, const float* lforce,
                                          int lnum, float* ldump) {
