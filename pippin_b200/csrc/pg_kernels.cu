@@ -163,6 +163,8 @@ __global__ void __launch_bounds__(256) collide_kernel(const __grid_constant__ St
   EnvCtx e;
   e.ws = nullptr;
   e.scr = nullptr;
+  // the tile's queue of broad-phase survivors (2G ints)
+  int* queue = reinterpret_cast<int*>(tile_workspace(A, smem, 0, 0)) + (threadIdx.x / G) * COLLIDE_QUEUE;
   for (int item = first_item<G>(); item < A.count; item = next_item(T, A.queue + 1, A.count)) {
     size_t env = (size_t)A.start + item;
     e.env = (int)env;
@@ -173,7 +175,7 @@ __global__ void __launch_bounds__(256) collide_kernel(const __grid_constant__ St
     prefetch_l1(T, e.prm, sizeof(double) * m.pstride);
     prefetch_l1(T, e.geo, sizeof(double) * G_STRIDE * m.ngeom);
     int status = 0;
-    int ncon = collide(T, m, A.w, A.s, e, &status);
+    int ncon = collide(T, m, A.w, A.s, e, &status, queue);
     if (T.lane() == 0) {
       wk[A.k.meta + K_META_NCON] = ncon;
       wk[A.k.meta + K_META_STATUS] = (double)((int)wk[A.k.meta + K_META_STATUS] | status);
@@ -478,7 +480,7 @@ const void* tile_kernel(int which, int G) {
 size_t kernel_smem(int which, const StepArgs& a, int tiles_per_block) {
   size_t staged = a.stage_model ? (size_t)staged_model_bytes(a.m.arena_bytes) : 0;
   switch (which) {
-    case K_COLLIDE: return staged;
+    case K_COLLIDE: return staged + (size_t)tiles_per_block * COLLIDE_QUEUE * sizeof(int);
     case K_NEWTON: return staged + (size_t)tiles_per_block * a.wn.stride * sizeof(double);
     default: return staged + (size_t)tiles_per_block * a.w.stride * sizeof(double);
   }

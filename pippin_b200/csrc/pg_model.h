@@ -38,6 +38,7 @@ enum { G_POS = 0, G_MAT = 3, G_AABB = 12, G_STRIDE = 18 };
 
 constexpr int NV_MAX = 64;  // dof-chain masks are 64-bit
 constexpr int HULL_FACE_MAX = 32;  // longest hull face loop the device clips
+constexpr int COLLIDE_QUEUE = 64;  // broad-phase survivor slots per collide tile (2 x the widest tile)
 
 struct DModel {
   // ---- dims

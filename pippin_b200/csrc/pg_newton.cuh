@@ -15,40 +15,34 @@ namespace pg {
 // ---------------------------------------------------------------- collide
 // Returns the contact count; contacts land in scratch in pair order (and
 // hit order within a pair), as in the reference's sequential pair loop.
+// The broad phase runs over the pairs G at a time and queues the survivors
+// (in pair order) in `queue` (2G ints of shared memory); the narrow phase
+// takes them G at a time, one pair per lane, so a batch of narrow-phase
+// work waits for G survivors instead of running once per G candidates.
 template <int G>
 __device__ int collide(const Tile<G>& T, const DModel& m, const WsLayout& w, const ScrLayout& s, const EnvCtx& e,
-                       int* status) {
+                       int* status, int* queue) {
   int lane = T.lane();
   const double* prm = e.prm;
   const double* gr = e.geo;  // poses and boxes from the tree walk
   double* con = e.con;
   int ncon = 0;
   int st = 0;
-  for (int base = 0; base < m.npair; base += G) {
-    int p = base + lane;
+  // narrow phase of the queued pairs [0, cnt), contacts appended in order
+  auto narrow = [&](int cnt) {
     Hits hits;
     hits.n = 0;
     int g1 = 0, g2 = 0;
-    if (p < m.npair) {
+    if (lane < cnt) {
+      int p = queue[lane];
       g1 = m.pair_g[2 * p];
       g2 = m.pair_g[2 * p + 1];
-      unsigned t1 = (unsigned)prm[m.p_contype + g1], a1 = (unsigned)prm[m.p_conaff + g1];
-      unsigned t2 = (unsigned)prm[m.p_contype + g2], a2 = (unsigned)prm[m.p_conaff + g2];
-      bool masks = (t1 & a2) != 0 || (t2 & a1) != 0;
-      if (masks) {
-        const double* r1 = gr + G_STRIDE * g1;
-        const double* r2 = gr + G_STRIDE * g2;
-        V3 c1 = ld3(r1 + G_AABB), h1 = ld3(r1 + G_AABB + 3);
-        V3 c2 = ld3(r2 + G_AABB), h2 = ld3(r2 + G_AABB + 3);
-        bool sep = fabs(c1.x - c2.x) > h1.x + h2.x + m.margin || fabs(c1.y - c2.y) > h1.y + h2.y + m.margin ||
-                   fabs(c1.z - c2.z) > h1.z + h2.z + m.margin;
-        if (!sep) {
-          GPose a{m.geom_type[g1], ld3(r1 + G_POS), ld9(r1 + G_MAT), ld3(prm + m.p_size + 3 * g1), m.geom_dataid[g1]};
-          GPose b{m.geom_type[g2], ld3(r2 + G_POS), ld9(r2 + G_MAT), ld3(prm + m.p_size + 3 * g2), m.geom_dataid[g2]};
-          if (needs_general(a.type, b.type)) collide_general(m, a, b, m.margin, hits);
-          else collide_primitive(a, b, m.margin, hits);
-        }
-      }
+      const double* r1 = gr + G_STRIDE * g1;
+      const double* r2 = gr + G_STRIDE * g2;
+      GPose a{m.geom_type[g1], ld3(r1 + G_POS), ld9(r1 + G_MAT), ld3(prm + m.p_size + 3 * g1), m.geom_dataid[g1]};
+      GPose b{m.geom_type[g2], ld3(r2 + G_POS), ld9(r2 + G_MAT), ld3(prm + m.p_size + 3 * g2), m.geom_dataid[g2]};
+      if (needs_general(a.type, b.type)) collide_general(m, a, b, m.margin, hits);
+      else collide_primitive(a, b, m.margin, hits);
     }
     int nh = hits.n < MAX_HITS ? hits.n : MAX_HITS;
     int tot;
@@ -74,7 +68,40 @@ __device__ int collide(const Tile<G>& T, const DModel& m, const WsLayout& w, con
       st3(r + C_T2, t2);
     }
     ncon += tot;
+  };
+  int queued = 0;
+  for (int base = 0; base < m.npair; base += G) {
+    int p = base + lane;
+    bool keep = false;
+    if (p < m.npair) {
+      int g1 = m.pair_g[2 * p], g2 = m.pair_g[2 * p + 1];
+      unsigned t1 = (unsigned)prm[m.p_contype + g1], a1 = (unsigned)prm[m.p_conaff + g1];
+      unsigned t2 = (unsigned)prm[m.p_contype + g2], a2 = (unsigned)prm[m.p_conaff + g2];
+      bool masks = (t1 & a2) != 0 || (t2 & a1) != 0;
+      if (masks) {
+        const double* r1 = gr + G_STRIDE * g1;
+        const double* r2 = gr + G_STRIDE * g2;
+        V3 c1 = ld3(r1 + G_AABB), h1 = ld3(r1 + G_AABB + 3);
+        V3 c2 = ld3(r2 + G_AABB), h2 = ld3(r2 + G_AABB + 3);
+        bool sep = fabs(c1.x - c2.x) > h1.x + h2.x + m.margin || fabs(c1.y - c2.y) > h1.y + h2.y + m.margin ||
+                   fabs(c1.z - c2.z) > h1.z + h2.z + m.margin;
+        keep = !sep;
+      }
+    }
+    int tot;
+    int off = T.excl_scan(keep ? 1 : 0, &tot);
+    if (keep) queue[queued + off] = p;  // queued < G before, tot <= G: within 2G
+    queued += tot;
+    T.sync();
+    if (queued >= G) {
+      narrow(G);
+      T.sync();  // the batch is read; move the rest (fewer than G) to the front
+      if (lane < queued - G) queue[lane] = queue[G + lane];
+      queued -= G;
+      T.sync();
+    }
   }
+  if (queued > 0) narrow(queued);
   if (ncon > m.maxcon) ncon = m.maxcon;
   *status |= T.ior(st);
   T.sync();
