@@ -518,6 +518,8 @@ void layouts(const HostModel& m, int maxcon, int maxrows, WsLayout* w, WsLayout*
   // ... then the factorisations in the same region
   off = region;
   w->fac = take(nv * nv);
+  w->fac2 = take(nv * nv);
+  w->rinv2 = take(nv);
   w->stride = std::max(off, tree_end);
 
   // Newton phase

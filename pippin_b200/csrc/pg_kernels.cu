@@ -126,20 +126,16 @@ __global__ void __launch_bounds__(256) smooth_kernel(const __grid_constant__ Ste
     // the tree region is dead from here on: the factorisations use it
     int status = 0;
     bool damped = has_implicit_terms(T, m, e.prm);
-    if (factor_mass(T, m, w, e, 0.0, wk + A.k.qm)) {
+    // the factor of M + hD too: for the damped solve after Newton, and always
+    // for PGS (forward.rs:366-368), which factors M + hD even with D = 0
+    bool both = damped || m.solver == SOLVER_PGS;
+    if (both ? factor_mass2(T, m, w, e, h, wk + A.k.qm) : factor_mass(T, m, w, e, 0.0, wk + A.k.qm)) {
       solve_auto(T, ws + w.fac, nv, nv, m.nblock, m.block_adr, m.dof_block, m.maxbs, ws + w.rinv, acc);
       copy_in(T, wk + A.k.a0, acc, nv);
       copy_in(T, wk + A.k.smooth, smooth, nv);
-      // the factor of M + hD: for the damped solve after Newton, and always
-      // for PGS (forward.rs:366-368), which factors M + hD even with D = 0
-      if (damped || m.solver == SOLVER_PGS) {
-        T.sync();
-        if (factor_mass(T, m, w, e, h, wk + A.k.qm)) {
-          copy_in(T, wk + A.k.lh, ws + w.fac, nv * nv);
-          copy_in(T, wk + A.k.rinvh, ws + w.rinv, nv);
-        } else {
-          status |= ST_NOT_SPD;
-        }
+      if (both) {
+        copy_in(T, wk + A.k.lh, ws + w.fac2, nv * nv);
+        copy_in(T, wk + A.k.rinvh, ws + w.rinv2, nv);
       }
     } else {
       status |= ST_NOT_SPD;

@@ -144,10 +144,11 @@ struct WsLayout {
   int qpos, qvel, ctrl, qacc, applied, qm, cdof, smooth, qfrc_c, acc, rinv, actforce, actclamped, misc;
   // tree walks, passive/actuator forces
   int xpos, xquat, xmat, cinert, cvel, cacc, cfrc, bias, passive, actf;
-  // factorisations and Newton (alias the tree region)
-  int fac, a0, grad, p, tmp, tmp2, mp, vel, warm;
+  // factorisations and Newton (alias the tree region); fac2 / rinv2: the
+  // smooth phase's second factor (M + hD) beside the first (M)
+  int fac, a0, grad, p, tmp, tmp2, mp, vel, warm, fac2, rinv2;
   // register Newton (nv <= 16, one dof tree): constraint rows [16][nv],
-  // Hessian factor [nv][nv], published vector [16] and row coefficients [16]
+  // Hessian factor (packed), published vector [16] and row coefficients [32]
   // (placed over buffers that path leaves unused; -1 when it does not apply)
   int sj, sl, sx, sc;
   int stride;

@@ -1005,6 +1005,30 @@ __device__ int newton_solve(const Tile<G>& T, const DModel& m, const WsLayout& w
   return it;
 }
 
+// forward.rs:412-429: the implicitfast actuator terms h kv g_x g_y of the
+// dofs on one chain, added to F (rare path, lane 0)
+template <int G>
+__device__ void add_actuator_kv(const Tile<G>& T, const DModel& m, const WsLayout& w, const EnvCtx& e, double h,
+                                double* F) {
+  const double* ws = e.ws;
+  int nv = m.nv;
+  if (m.integrator == 1 && T.lane() == 0) {
+    for (int u = 0; u < m.nu; u++) {
+      double kv = -e.prm[m.p_bias + 3 * u + 2] * m.act_gear[u] * m.act_gear[u];
+      if (kv == 0.0 || ws[w.actclamped + u] != 0.0) continue;
+      int a0 = m.act_moment_adr[u], an = m.act_moment_num[u];
+      for (int x = 0; x < an; x++)
+        for (int y = 0; y < an; y++) {
+          int da = m.jnt_dofadr[m.moment_jnt[a0 + x]], db = m.jnt_dofadr[m.moment_jnt[a0 + y]];
+          bool rel = da == db;
+          for (int q = m.dof_parent[db]; q != -1 && !rel; q = m.dof_parent[q]) rel = q == da;
+          for (int q = m.dof_parent[da]; q != -1 && !rel; q = m.dof_parent[q]) rel = q == db;
+          if (rel) F[da * nv + db] += h * kv * m.moment_coef[a0 + x] * m.moment_coef[a0 + y];
+        }
+    }
+  }
+}
+
 // forward.rs:407-431,392-401: factor M + h D per dof block into ws fac;
 // M (nv x nv) is read from global memory
 template <int G>
@@ -1020,23 +1044,35 @@ __device__ bool factor_mass(const Tile<G>& T, const DModel& m, const WsLayout& w
     for (int k = lane; k < nv; k += G) F[k * nv + k] += h * e.prm[m.p_damping + k];
     T.sync();
   }
-  if (m.integrator == 1 && lane == 0) {  // implicitfast actuator terms (rare path)
-    for (int u = 0; u < m.nu; u++) {
-      double kv = -e.prm[m.p_bias + 3 * u + 2] * m.act_gear[u] * m.act_gear[u];
-      if (kv == 0.0 || ws[w.actclamped + u] != 0.0) continue;
-      int a0 = m.act_moment_adr[u], an = m.act_moment_num[u];
-      for (int x = 0; x < an; x++)
-        for (int y = 0; y < an; y++) {
-          int da = m.jnt_dofadr[m.moment_jnt[a0 + x]], db = m.jnt_dofadr[m.moment_jnt[a0 + y]];
-          bool rel = da == db;
-          for (int q = m.dof_parent[db]; q != -1 && !rel; q = m.dof_parent[q]) rel = q == da;
-          for (int q = m.dof_parent[da]; q != -1 && !rel; q = m.dof_parent[q]) rel = q == db;
-          if (rel) F[da * nv + db] += h * kv * m.moment_coef[a0 + x] * m.moment_coef[a0 + y];
-        }
-    }
-  }
+  add_actuator_kv(T, m, w, e, h, F);
   T.sync();
   return chol_auto(T, F, nv, nv, m.nblock, m.block_adr, m.dof_block, m.maxbs, ws + w.rinv);
+}
+
+// The smooth phase's two factors from one load of M: M itself into ws fac
+// (for a0 = M^-1 f) and M + h D into ws fac2 (forward.rs:356-366, for the
+// damped solve after Newton, or PGS), factored side by side on the
+// small-matrix path so that their column chains overlap. False if either is
+// not positive definite.
+template <int G>
+__device__ bool factor_mass2(const Tile<G>& T, const DModel& m, const WsLayout& w, const EnvCtx& e, double h,
+                             const double* qm) {
+  int lane = T.lane(), nv = m.nv;
+  double* ws = e.ws;
+  double *F = ws + w.fac, *F2 = ws + w.fac2;
+  load_async(T, F, qm, nv * nv);
+  load_async(T, F2, qm, nv * nv);
+  load_wait();
+  T.sync();
+  for (int k = lane; k < nv; k += G) F2[k * nv + k] += h * e.prm[m.p_damping + k];
+  T.sync();
+  add_actuator_kv(T, m, w, e, h, F2);
+  T.sync();
+  if constexpr (G >= SMALL_N) {
+    if (nv <= SMALL_N) return chol_small2(T, F, F2, nv, nv, ws + w.rinv, ws + w.rinv2);
+  }
+  if (!chol_blocks(T, F, nv, nv, m.nblock, m.block_adr, m.dof_block, m.maxbs, ws + w.rinv)) return false;
+  return chol_blocks(T, F2, nv, nv, m.nblock, m.block_adr, m.dof_block, m.maxbs, ws + w.rinv2);
 }
 
 // forward.rs:454-456 (the tile checks its share of dofs and actuators at once)

@@ -91,6 +91,45 @@ __device__ inline bool chol_left(const Tile<G>& T, const S& st, int n, double dg
   return true;
 }
 
+// chol_left on two matrices of the same size at once (the smooth phase's M
+// and M + hD): each pass does both columns' dots and pivots, so the two
+// chains of dependent steps overlap. Same arithmetic as two chol_left calls;
+// false if either has a pivot that is not positive.
+template <int G, class S>
+__device__ inline bool chol_left2(const Tile<G>& T, const S& s1, const S& s2, int n, double dg1, double dg2,
+                                  double* rv1, double* rv2) {
+  const int i = T.lane();
+  const bool row = i < n;
+  double* m1 = s1.row(row ? i : 0);
+  double* m2 = s2.row(row ? i : 0);
+  T.sync();  // every row in place
+#pragma unroll 1
+  for (int j = 0; j < n; j++) {
+    const double* r1 = s1.row(j);
+    const double* r2 = s2.row(j);
+    double a1 = 0.0, a2 = 0.0;
+    if (row && i >= j) {
+      a1 = dot_ref_sm(m1, r1, j);
+      a2 = dot_ref_sm(m2, r2, j);
+    }
+    double d1 = T.bcast(dg1 - a1, j);
+    double d2 = T.bcast(dg2 - a2, j);
+    if (!(d1 > 0.0) || !(d2 > 0.0)) return false;  // the same on every lane
+    double inv1 = rsqrt(d1), inv2 = rsqrt(d2);
+    if (i == j) {
+      *rv1 = inv1;
+      *rv2 = inv2;
+      m1[j] = d1 * inv1;
+      m2[j] = d2 * inv2;
+    } else if (row && i > j) {
+      m1[j] = (m1[j] - a1) * inv1;
+      m2[j] = (m2[j] - a2) * inv2;
+    }
+    T.sync();
+  }
+  return true;
+}
+
 // The solution component of lane i of L L^T x = b, given b_i (xi), 1/L_ii
 // (ri) and the factor's store: forward x_i -= L_ij (x_j / L_jj) for i > j,
 // then x_i /= L_ii; backward x_i -= L_ji (x_j / L_jj) for i < j, then
@@ -129,6 +168,25 @@ __device__ __noinline__ bool chol_small(const Tile<G>& T, double* A, int lda, in
   double rv = 0.0;
   if (!chol_left(T, LStrided{A, lda}, n, row ? A[i * lda + i] : 0.0, true, &rv)) return false;
   if (row) rinv[i] = rv;
+  T.sync();
+  return true;
+}
+
+// chol_small on A and A2 (both n x n, stride lda) side by side.
+template <int G>
+__device__ __noinline__ bool chol_small2(const Tile<G>& T, double* A, double* A2, int lda, int n, double* rinv,
+                                         double* rinv2) {
+  static_assert(G >= SMALL_N, "one lane per row");
+  const int i = T.lane();
+  const bool row = i < n;
+  double rv1 = 0.0, rv2 = 0.0;
+  if (!chol_left2(T, LStrided{A, lda}, LStrided{A2, lda}, n, row ? A[i * lda + i] : 0.0,
+                  row ? A2[i * lda + i] : 0.0, &rv1, &rv2))
+    return false;
+  if (row) {
+    rinv[i] = rv1;
+    rinv2[i] = rv2;
+  }
   T.sync();
   return true;
 }
