@@ -487,3 +487,119 @@ def test_handles_with_different_launch_shapes():
     big.step(range(512), 3)
     small.step(range(64), 3)
     assert not big.stats()["status"].any() and not small.stats()["status"].any()
+
+
+def _sample_step_parity(g, blob, n, sample, params=(), tol=TOL_STEP):
+    """One step of `sample` envs on the oracle from the GPU's current state
+    (and the given per-env parameters) against the GPU's own step."""
+    k = len(sample)
+    og = Oracle(blob, k, threads=4)
+    og.set_solver(tolerance=1e-10)
+    for pid, elem, vals in params:
+        og.set_param(pid, elem, np.asarray(vals)[sample], 0, k)
+    for fg, fo in ((Field.QPOS, QPOS), (Field.QVEL, QVEL), (Field.QACC, QACC), (Field.CTRL, CTRL)):
+        og.set(fo, g.get(fg, range(n))[sample])
+    g.step(range(n), 1)
+    og.step(0, k, 1)
+    assert rel(g.get(Field.QACC, range(n))[sample], og.get(QACC)) < tol
+
+
+@pytest.mark.parametrize("name", ["cartpole", "arm3hinge"])
+def test_full_size_contact_free_properties(name):
+    """Config 2 at full size (16384 envs, random states over the joint
+    ranges, qvel N(0, 1), per-env masses x U[0.5, 2], 1 s): finite state, no
+    status flags, invweight0 of sampled envs as the oracle's, and per-step
+    parity on a sample of envs at the end."""
+    n = 16384
+    m = mjcf.load_string(MODELS[name]())
+    blob = mjcf.to_blob(m)
+    g = CudaPhysics(blob, n)
+    g.set_solver(tolerance=1e-10)
+    rng = np.random.default_rng(8)
+    q = np.tile(np.array(m.qpos0), (n, 1))
+    for j in range(m.njnt):
+        qa = m.jnt_qposadr[j]
+        if m.jnt_type[j] == mjcf.JNT_HINGE:
+            q[:, qa] = rng.uniform(-np.pi, np.pi, n)
+        elif m.jnt_type[j] == mjcf.JNT_SLIDE:
+            q[:, qa] = rng.uniform(-0.5, 0.5, n)
+    params = []
+    for b in range(1, m.nbody):
+        vals = (np.array(m.body_mass[b]) * rng.uniform(0.5, 2.0, n)).reshape(n, 1)
+        g.set_param(Param.BODY_MASS, b, range(n), vals)
+        params.append((5, b, vals))
+    g.set(Field.QPOS, range(n), q)
+    g.set(Field.QVEL, range(n), rng.normal(0, 1, (n, m.nv)))
+    steps = int(round(1.0 / m.timestep))
+    traj = g.rollout(rng.uniform(-1, 1, (n, steps, max(m.nu, 0))))
+    assert np.isfinite(traj).all()
+    assert not g.stats()["status"].any()
+    sample = rng.choice(n, 64, replace=False)
+    _sample_step_parity(g, blob, n, sample, params)
+
+
+def test_full_size_tabletop_properties():
+    """Config 3 at full size (8192 envs, 2-6 objects each, 2 s at dt 0.002):
+    finite state, no status flags, unit quaternions, no object through the
+    floor, nearly every active object at rest on the table or on another
+    object (a sphere set rolling keeps rolling: the contact model has no
+    rolling friction), and per-step parity on a sample of envs."""
+    n = 8192
+    plan = scenes.tabletop(n, seed=9)
+    m = mjcf.load_string(plan.xml)
+    blob = mjcf.to_blob(m)
+    g = CudaPhysics(blob, n)
+    g.set_solver(tolerance=1e-10)
+    params = []
+
+    def setp(pid, elem, vals):
+        g.set_param(Param(pid), elem, range(n), vals)
+        params.append((pid, elem, np.asarray(vals).reshape(n, -1)))
+
+    plan.apply(setp, lambda: g.reset(range(n)))
+    g.step(range(n), int(round(2.0 / m.timestep)))
+    q, v = g.get(Field.QPOS, range(n)), g.get(Field.QVEL, range(n))
+    assert np.isfinite(q).all() and np.isfinite(v).all()
+    assert not g.stats()["status"].any()
+    resting, total = 0, 0
+    for s in range(6):
+        np.testing.assert_allclose(np.linalg.norm(q[:, 7 * s + 3:7 * s + 7], axis=1), 1.0, atol=1e-10)
+        assert (q[:, 7 * s + 2] > 0.0).all()
+        active = q[:, 7 * s] < 50
+        z = q[active, 7 * s + 2]
+        still = np.linalg.norm(v[active, 6 * s:6 * s + 3], axis=1) < 1e-3
+        resting += int(((z > 0.4) & (z < 0.6) & still).sum())
+        total += int(active.sum())
+    assert resting >= 0.98 * total, (resting, total)
+    sample = np.random.default_rng(9).choice(n, 32, replace=False)
+    _sample_step_parity(g, blob, n, sample, [p for p in params if p[0] != 11])
+
+
+def test_full_size_hull_tumble_properties():
+    """Config 4 at full size (4096 envs of 8 hulls with 8-32 vertices, linear
+    N(0, 0.5^2) and angular N(0, 3^2) velocities, 1 s, Newton): finite state,
+    no status flags, unit quaternions, contacts, and per-step parity on a
+    sample of envs."""
+    n = 4096
+    xml = scenes.hull_tumble_xml()
+    m = mjcf.load_string(xml)
+    blob = mjcf.to_blob(m)
+    g = CudaPhysics(blob, n)
+    g.set_solver(tolerance=1e-10)
+    rng = np.random.default_rng(10)
+    q = np.tile(np.array(m.qpos0), (n, 1))
+    v = np.zeros((n, m.nv))
+    for b in range(m.nv // 6):
+        v[:, 6 * b:6 * b + 3] = rng.normal(0, 0.5, (n, 3))
+        v[:, 6 * b + 3:6 * b + 6] = rng.normal(0, 3.0, (n, 3))
+    g.set(Field.QPOS, range(n), q)
+    g.set(Field.QVEL, range(n), v)
+    g.step(range(n), int(round(1.0 / m.timestep)))
+    q = g.get(Field.QPOS, range(n))
+    st = g.stats()
+    assert np.isfinite(q).all() and np.isfinite(g.get(Field.QVEL, range(n))).all()
+    assert not st["status"].any()
+    assert st["ncon"].mean() > 1
+    for b in range(m.nq // 7):
+        np.testing.assert_allclose(np.linalg.norm(q[:, 7 * b + 3:7 * b + 7], axis=1), 1.0, atol=1e-10)
+    _sample_step_parity(g, blob, n, rng.choice(n, 32, replace=False))
