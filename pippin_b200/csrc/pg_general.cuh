@@ -2,7 +2,8 @@
 // to parry3d-f64 (crates/pippin/src/collision.rs:102-147): mesh (convex hull)
 // against anything, and cylinder against non-plane shapes. parry is an
 // un-vendored dependency; this path is this library's own algorithm, the
-// one the oracle restates (one lane per pair, FP64):
+// one the oracle restates (FP64; one pair at a time on a whole tile, whose
+// lanes share out the polytope queries' candidates):
 //   box        8 vertices, 6 faces
 //   cylinder   a 16-sided prism (faces at distance r cos(pi/16) from the axis)
 //   mesh       its convex hull: polygon faces (at most HULL_FACE_MAX long) and
@@ -18,6 +19,7 @@
 // closest point; a plane against a hull takes the four deepest vertices.
 #pragma once
 #include "pg_collide.cuh"
+#include "pg_tile.cuh"
 
 namespace pg {
 
@@ -193,8 +195,11 @@ __device__ __noinline__ double closest_point(const Poly& p, V3 x, V3* q, int* in
 // the host's oracle, say) cannot change the contacts.
 constexpr double GEN_TIE = 1e-10;
 
-// largest separation of b beyond a face of a (first face within GEN_TIE)
-__device__ __noinline__ double face_query(const Poly& a, const Poly& b, int* face) {
+// largest separation of b beyond a face of a (first face within GEN_TIE),
+// the faces shared out over the tile's lanes: the maximum, then the lowest
+// face index within GEN_TIE of it, as a loop over the faces in order finds
+template <int G>
+__device__ double face_query(const Tile<G>& T, const Poly& a, const Poly& b, int* face) {
   int nf = p_nf(a), nv = p_nv(b);
   auto sep = [&](int f) {
     V3 n = p_fn(a, f);
@@ -203,10 +208,16 @@ __device__ __noinline__ double face_query(const Poly& a, const Poly& b, int* fac
     return mn - p_fd(a, f, n);
   };
   double best = -INFINITY;
-  for (int f = 0; f < nf; f++) best = fmax(best, sep(f));
-  int f = 0;
-  while (f + 1 < nf && sep(f) < best - GEN_TIE) f++;
-  *face = f;
+  for (int f = T.lane(); f < nf; f += G) best = fmax(best, sep(f));
+  best = T.fmax(best);
+  int first = nf;
+  for (int f = T.lane(); f < nf; f += G)
+    if (!(sep(f) < best - GEN_TIE)) {
+      first = f;
+      break;
+    }
+  first = T.imin(first);
+  *face = first < nf ? first : nf - 1;
   return best;
 }
 
@@ -218,39 +229,50 @@ __device__ inline bool minkowski_face(V3 a, V3 b, V3 c, V3 d) {
   return cba * dba < 0.0 && adc * bdc < 0.0 && cba * bdc > 0.0;
 }
 
-// largest separation along the cross product of an edge of a and of b
-__device__ __noinline__ double edge_query(const Poly& a, V3 ca, const Poly& b, int* ea, int* eb, V3* axis) {
-  double best = -INFINITY;
-  *ea = *eb = -1;
+// largest separation along the cross product of an edge of a and of b; the
+// edge pairs (i, j), in the order i * (edges of b) + j, are shared out over
+// the tile's lanes, and the first pair with the largest separation wins, as
+// a loop over the pairs in order with a strict comparison finds
+template <int G>
+__device__ double edge_query(const Tile<G>& T, const Poly& a, V3 ca, const Poly& b, int* ea, int* eb, V3* axis) {
   int nea = p_ne(a), neb = p_ne(b);
-  for (int i = 0; i < nea; i++) {
-    int fa1, fa2, ia, ja;
+  // separation along the pair's axis; false when the pair is not a candidate
+  auto pair_sep = [&](int i, int j, double* s, V3* n) -> bool {
+    int fa1, fa2, fb1, fb2, ia, ja, ib, jb;
     p_eface(a, i, &fa1, &fa2);
-    if (fa2 < 0) continue;
+    p_eface(b, j, &fb1, &fb2);
+    if (fa2 < 0 || fb2 < 0) return false;
+    if (!minkowski_face(p_fn(a, fa1), p_fn(a, fa2), -p_fn(b, fb1), -p_fn(b, fb2))) return false;
     p_edge(a, i, &ia, &ja);
+    p_edge(b, j, &ib, &jb);
     V3 pa = p_v(a, ia), da = p_v(a, ja) - pa;
-    V3 na1 = p_fn(a, fa1), na2 = p_fn(a, fa2);
-    for (int j = 0; j < neb; j++) {
-      int fb1, fb2, ib, jb;
-      p_eface(b, j, &fb1, &fb2);
-      if (fb2 < 0) continue;
-      V3 nb1 = p_fn(b, fb1), nb2 = p_fn(b, fb2);
-      if (!minkowski_face(na1, na2, -nb1, -nb2)) continue;
-      p_edge(b, j, &ib, &jb);
-      V3 pb = p_v(b, ib), db = p_v(b, jb) - pb;
-      V3 c = cross(da, db);
-      double l = norm(c);
-      if (l < 1e-6 * norm(da) * norm(db)) continue;  // parallel edges: a face axis covers them
-      V3 n = c * (1.0 / l);
-      if (dot(n, pa - ca) < 0.0) n = -n;
-      double s = dot(n, pb - pa);
-      if (s > best) {
-        best = s;
-        *ea = i;
-        *eb = j;
-        *axis = n;
-      }
+    V3 pb = p_v(b, ib), db = p_v(b, jb) - pb;
+    V3 c = cross(da, db);
+    double l = norm(c);
+    if (l < 1e-6 * norm(da) * norm(db)) return false;  // parallel edges: a face axis covers them
+    V3 u = c * (1.0 / l);
+    if (dot(u, pa - ca) < 0.0) u = -u;
+    *s = dot(u, pb - pa);
+    *n = u;
+    return true;
+  };
+  double best = -INFINITY;
+  int bidx = 0x7fffffff;
+  for (int k = T.lane(); k < nea * neb; k += G) {
+    double sk;
+    V3 nk;
+    if (pair_sep(k / neb, k % neb, &sk, &nk) && sk > best) {
+      best = sk;
+      bidx = k;
     }
+  }
+  T.argmax(&best, &bidx);
+  *ea = *eb = -1;
+  if (bidx != 0x7fffffff) {
+    double sk;
+    pair_sep(bidx / neb, bidx % neb, &sk, axis);
+    *ea = bidx / neb;
+    *eb = bidx % neb;
   }
   return best;
 }
@@ -336,14 +358,15 @@ __device__ __noinline__ void clip_faces(const Poly& r, int rf, const Poly& s, V3
   for (int k = 0; k < n_pts; k++) out.push(pts[k].p - nref * (pts[k].d * 0.5), n, -pts[k].d);
 }
 
-__device__ inline void polytope_polytope(const Poly& a, const Poly& b, double margin, Hits& out) {
+template <int G>
+__device__ void polytope_polytope(const Tile<G>& T, const Poly& a, const Poly& b, double margin, Hits& out) {
   int fa, fb, ea, eb;
   V3 axis{0.0, 0.0, 0.0};
-  double sa = face_query(a, b, &fa);
+  double sa = face_query(T, a, b, &fa);
   if (sa > margin) return;
-  double sb = face_query(b, a, &fb);
+  double sb = face_query(T, b, a, &fb);
   if (sb > margin) return;
-  double se = edge_query(a, p_centroid(a), b, &ea, &eb, &axis);
+  double se = edge_query(T, a, p_centroid(a), b, &ea, &eb, &axis);
   if (se > margin) return;
   double oa = -sa, ob = -sb, oe = -se;
   bool face_a = !(ob < oa - GEN_TIE);
@@ -438,8 +461,12 @@ __device__ inline void plane_polytope(const GPose& pl, const Poly& p, double mar
   for (int k = 0; k < nk; k++) out.push(keep[k].p - n * (keep[k].d * 0.5), n, -keep[k].d);
 }
 
-__device__ __noinline__ void collide_general(const DModel& m, const GPose& a0, const GPose& b0, double margin,
-                                             Hits& out) {
+// One pair on the whole tile: every lane passes the same pair and ends with
+// the same contacts; the polytope queries share their candidates out over
+// the lanes, the rest runs on every lane alike.
+template <int G>
+__device__ __noinline__ void collide_general(const Tile<G>& T, const DModel& m, const GPose& a0, const GPose& b0,
+                                             double margin, Hits& out) {
   bool swap = a0.type > b0.type;  // type order, normals flipped back (collision.rs:59-67)
   const GPose& a = swap ? b0 : a0;
   const GPose& b = swap ? a0 : b0;
@@ -453,7 +480,7 @@ __device__ __noinline__ void collide_general(const DModel& m, const GPose& a0, c
     capsule_polytope(a, pb, margin, out);
   } else {
     Poly pa{a.type, a.pos, a.mat, a.size, &m, a.data};
-    polytope_polytope(pa, pb, margin, out);
+    polytope_polytope(T, pa, pb, margin, out);
   }
   if (swap)
     for (int k = start; k < out.n && k < MAX_HITS; k++) out.h[k].normal = -out.h[k].normal;

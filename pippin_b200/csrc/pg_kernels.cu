@@ -150,8 +150,10 @@ __global__ void __launch_bounds__(256) smooth_kernel(const __grid_constant__ Ste
 
 // ---------------------------------------------------------------- phase 2
 // forward.rs:214-260: broad and narrow phase over the candidate pairs
+// two blocks of 256 threads an SM (128 registers a thread): the general
+// narrow phase alone would take every register and halve the resident tiles
 template <int G>
-__global__ void __launch_bounds__(256) collide_kernel(const __grid_constant__ StepArgs A) {
+__global__ void __launch_bounds__(256, 2) collide_kernel(const __grid_constant__ StepArgs A) {
   extern __shared__ __align__(16) unsigned char smem[];
   const DModel& m = stage_model(A, smem);
   cg::thread_block block = cg::this_thread_block();

@@ -29,20 +29,30 @@ __device__ int collide(const Tile<G>& T, const DModel& m, const WsLayout& w, con
   int ncon = 0;
   int st = 0;
   // narrow phase of the queued pairs [0, cnt), contacts appended in order
+  auto pose = [&](int g) {
+    const double* r = gr + G_STRIDE * g;
+    return GPose{m.geom_type[g], ld3(r + G_POS), ld9(r + G_MAT), ld3(prm + m.p_size + 3 * g), m.geom_dataid[g]};
+  };
   auto narrow = [&](int cnt) {
     Hits hits;
     hits.n = 0;
     int g1 = 0, g2 = 0;
+    bool general = false;
     if (lane < cnt) {
       int p = queue[lane];
       g1 = m.pair_g[2 * p];
       g2 = m.pair_g[2 * p + 1];
-      const double* r1 = gr + G_STRIDE * g1;
-      const double* r2 = gr + G_STRIDE * g2;
-      GPose a{m.geom_type[g1], ld3(r1 + G_POS), ld9(r1 + G_MAT), ld3(prm + m.p_size + 3 * g1), m.geom_dataid[g1]};
-      GPose b{m.geom_type[g2], ld3(r2 + G_POS), ld9(r2 + G_MAT), ld3(prm + m.p_size + 3 * g2), m.geom_dataid[g2]};
-      if (needs_general(a.type, b.type)) collide_general(m, a, b, m.margin, hits);
-      else collide_primitive(a, b, m.margin, hits);
+      general = needs_general(m.geom_type[g1], m.geom_type[g2]);
+      if (!general) collide_primitive(pose(g1), pose(g2), m.margin, hits);
+    }
+    // the general pairs one after another, each on the whole tile
+    for (unsigned gm = T.ballot(general); gm; gm &= gm - 1) {
+      int d = __ffs(gm) - 1;
+      int h1 = T.bcast(g1, d), h2 = T.bcast(g2, d);
+      Hits gh;
+      gh.n = 0;
+      collide_general(T, m, pose(h1), pose(h2), m.margin, gh);
+      if (lane == d) hits = gh;
     }
     int nh = hits.n < MAX_HITS ? hits.n : MAX_HITS;
     int tot;

@@ -32,6 +32,30 @@ struct Tile {
     for (int o = G / 2; o > 0; o >>= 1) v |= t.shfl_xor(v, o);
     return v;
   }
+  __device__ double fmax(double v) const {
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) v = ::fmax(v, t.shfl_xor(v, o));
+    return v;
+  }
+  __device__ int imin(int v) const {
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) v = ::min(v, t.shfl_xor(v, o));
+    return v;
+  }
+  // the largest *v over the tile, ties to the smallest *idx; on every lane
+  __device__ void argmax(double* v, int* idx) const {
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) {
+      double ov = t.shfl_xor(*v, o);
+      int oi = t.shfl_xor(*idx, o);
+      if (ov > *v || (ov == *v && oi < *idx)) {
+        *v = ov;
+        *idx = oi;
+      }
+    }
+  }
+  // bit k set when lane k's b is true
+  __device__ unsigned ballot(bool b) const { return t.ballot(b ? 1 : 0); }
   __device__ bool all(bool b) const { return t.all(b ? 1 : 0) != 0; }
   __device__ bool any(bool b) const { return t.any(b ? 1 : 0) != 0; }
   // exclusive prefix sum over lanes; *total gets the sum over the tile
