@@ -26,7 +26,7 @@
 
 namespace pg {
 
-constexpr int SMALL_N = 16;  // largest matrix the register path factors
+constexpr int SMALL_N = 16;  // largest matrix the one-lane-per-row path factors
 
 // dot_ref's summation order (four interleaved partial sums for n >= 8, then
 // the tail) for a row and a vector in shared memory, as a loop (small code).
@@ -265,7 +265,7 @@ __device__ inline double solve_regx(const Tile<G>& T, const double (&a)[SMALL_N]
   return xi * ri;
 }
 
-// Factor / solve on the register path when the tile and the matrix allow it,
+// Factor / solve one lane per row when the tile and the matrix allow it,
 // else on the shared-memory block path. Block arguments as chol_blocks.
 template <int G>
 __device__ inline bool chol_auto(const Tile<G>& T, double* A, int lda, int n, int nblk, const int* blk,
