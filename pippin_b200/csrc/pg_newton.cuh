@@ -689,6 +689,7 @@ __device__ inline int newton_small(const Tile<G>& T, int k, int nr, const double
   int maxit = max_iters > 1 ? max_iters : 1;
   double prev[2] = {-1.0, -1.0};  // the rows' activity in the previous iteration (none yet)
   double jar[2] = {0.0, 0.0}, act[2] = {0.0, 0.0}, cv[2];
+  bool fresh = false;  // left at the convergence check: B.c holds D_r jar_r of the final a
   while (iters < maxit) {
     iters++;
     // gradient M (a - a0) + sum over active rows of D jar J_r (newton.rs:254-270)
@@ -715,7 +716,10 @@ __device__ inline int newton_small(const Tile<G>& T, int k, int nr, const double
       }
     double gnorm = sqrt(T.sum(dof ? grad * grad : 0.0));
     bool unchanged = T.all(same);
-    if (gnorm < tol * scale || (nr <= 128 && unchanged && iters > 1)) break;
+    if (gnorm < tol * scale || (nr <= 128 && unchanged && iters > 1)) {
+      fresh = true;
+      break;
+    }
     // H = M + J_A' D J_A, this lane's row (lower part)
     double h[SMALL_N];
 #pragma unroll
@@ -780,28 +784,40 @@ __device__ inline int newton_small(const Tile<G>& T, int k, int nr, const double
     }
     ai += al * p;
   }
-  // qfrc_constraint += -D (J a - aref) J' over active rows (newton.rs:361-371)
-  publish(ai);
+  // qfrc_constraint += -D (J a - aref) J' over active rows (newton.rs:361-371).
+  // After the convergence check the last gradient's coefficients D_r jar_r
+  // are those of the final a (same a, same active rows): their negatives,
+  // bit for bit; otherwise (iteration cap, failed factorisation) they are
+  // formed again.
+  double sgn = 1.0;
+  if (fresh) {
+    sgn = -1.0;
+  } else {
+    publish(ai);
 #pragma unroll
-  for (int s = 0; s < 2; s++) {
-    cv[s] = 0.0;
-    if (has[s]) {
-      double v = jdot(s) - aref[s];
-      cv[s] = (bil[s] || v < 0.0) ? -dr[s] * v : 0.0;
+    for (int s = 0; s < 2; s++) {
+      cv[s] = 0.0;
+      if (has[s]) {
+        double v = jdot(s) - aref[s];
+        cv[s] = (bil[s] || v < 0.0) ? -dr[s] * v : 0.0;
+      }
     }
+    coeffs(cv);
   }
-  coeffs(cv);
   if (dof) {
     double q = qfrc[i];
     for (int r = 0; r < nr; r++) {
       double cf = B.c[r];
-      if (cf != 0.0) q += cf * jrow(r)[i];
+      if (cf != 0.0) q += (sgn * cf) * jrow(r)[i];
     }
     qfrc[i] = q;
     a[i] = ai;
   }
   if (ldump && lnum > 0 && 4 * lnum <= nr)
-    for (int t = i; t < 4 * lnum; t += G) ldump[t] = (float)B.c[t];
+    for (int t = i; t < 4 * lnum; t += G) {
+      double cf = B.c[t];
+      ldump[t] = cf != 0.0 ? (float)(sgn * cf) : 0.0f;
+    }
   T.sync();
   return iters;
 }
