@@ -84,6 +84,28 @@ def dist_setup(args):
     return ws, rank, local
 
 
+def shard_seeds(rank):
+    """Seeds of a rank's own envs: every rank steps its own independent set
+    (weak scaling; envs never cross ranks, so the step has no collective)."""
+    return {"state": 1000 + rank, "train_state": 3000 + rank, "train_ctrl": 2000 + rank}
+
+
+def whole_job(ms, envs_per_rank, steps, ws):
+    """Max over ranks of each timed total (ms, a list) and the whole-job
+    rates they give: every rank's envs count, the slowest rank's time
+    decides. Takes part in one all-reduce when ws > 1 (every rank calls it)."""
+    import torch
+    t = torch.tensor(ms, dtype=torch.float64)
+    if ws > 1:
+        import torch.distributed as dist
+        if dist.get_backend() == "nccl":
+            t = t.cuda()
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    mx = [float(x) for x in t.cpu()]
+    total = envs_per_rank * ws * steps
+    return mx, [total / (x * 1e-3) for x in mx]
+
+
 # ------------------------------------------------------------------ CPU legs
 def cpu_rollout_rate(blob, m, envs, seconds, fast=True):
     """Oracle rollout (batch.rs:46-59 shape) on all host threads, repeated
@@ -233,7 +255,7 @@ def run_ours(args):
     blob = mjcf.to_blob(m)
     n = args.envs
     phys = CudaPhysics(blob, n, device=local)
-    q, v, rng = initial_state(m, n, 1000 + rank)
+    q, v, rng = initial_state(m, n, shard_seeds(rank)["state"])
     phys.set(Field.QPOS, range(n), q)
     phys.set(Field.QVEL, range(n), v)
     if args.lanes or args.per_block:
@@ -287,8 +309,9 @@ def run_ours(args):
     learned = None
     if not args.no_learned:
         from pippin_b200 import warm
-        tm, trng = CudaPhysics(blob, 1024, device=local), np.random.default_rng(2000 + rank)
-        tq, tv, _ = initial_state(m, 1024, 3000 + rank)
+        seeds = shard_seeds(rank)
+        tm, trng = CudaPhysics(blob, 1024, device=local), np.random.default_rng(seeds["train_ctrl"])
+        tq, tv, _ = initial_state(m, 1024, seeds["train_state"])
         tm.set(Field.QPOS, range(1024), tq)
         tm.set(Field.QVEL, range(1024), tv)
         X, F = warm.collect(tm, 150, controls=lambda t: trng.uniform(-1, 1, (1024, m.nu)), skip=20)
@@ -349,15 +372,7 @@ def run_ours(args):
     barrier()
     clock_info = clocks.stop()
 
-    times = torch.tensor([ms_ref, ms_cold, e2e_ms], dtype=torch.float64, device=dev)
-    if ws > 1:
-        import torch.distributed as dist
-        dist.all_reduce(times, op=dist.ReduceOp.MAX)
-    ms_ref, ms_cold, e2e_ms = (float(x) for x in times.cpu())
-    total_env_steps = n * ws * K
-    value = total_env_steps / (ms_ref * 1e-3)
-    value_cold = total_env_steps / (ms_cold * 1e-3)
-    e2e = total_env_steps / (e2e_ms * 1e-3)
+    (ms_ref, ms_cold, e2e_ms), (value, value_cold, e2e) = whole_job([ms_ref, ms_cold, e2e_ms], n, K, ws)
 
     if rank == 0:
         peak = fp64_peak(local)
