@@ -529,7 +529,12 @@ void layouts(const HostModel& m, int maxcon, int maxrows, WsLayout* w, WsLayout*
   wn->qpos = take(m.nq);
   wn->qvel = take(nv);
   wn->qacc = take(nv);
-  wn->qm = take(nv * nv);
+  // M and the big factor stay in shared memory for models the one-lane-per-row
+  // path takes; larger ones read M from the work record and factor in the
+  // tile's global scratch (its set_const slot), so that their workspace stays
+  // small enough for several tiles an SM
+  bool small_mats = nv <= 16;
+  wn->qm = small_mats ? take(nv * nv) : -1;
   wn->smooth = take(nv);
   wn->acc = take(nv);
   wn->qfrc_c = take(nv);
@@ -539,7 +544,7 @@ void layouts(const HostModel& m, int maxcon, int maxrows, WsLayout* w, WsLayout*
   wn->cdof = take(6 * nv);
   wn->rinv = take(nv);
   wn->warm = take(nv);
-  wn->fac = take(nv * nv);
+  wn->fac = small_mats ? take(nv * nv) : -1;
   wn->a0 = take(nv);
   wn->grad = take(nv);
   wn->p = take(nv);

@@ -22,6 +22,8 @@ struct EnvCtx {
   double* geo;        // this env's geom records (G_STRIDE each)
   double* con;        // this env's contacts (C_STRIDE each)
   int env;
+  const double* qm;   // Newton phase: M (nv x nv), in the workspace or the work record
+  double* fac;        // Newton phase: an nv x nv matrix to factor in (workspace or scratch)
 };
 
 // forward.rs:14-90 + 115-164 for one body, given its parent's results

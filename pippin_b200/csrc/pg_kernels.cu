@@ -188,8 +188,10 @@ __global__ void __launch_bounds__(256, 2) collide_kernel(const __grid_constant__
 // ---------------------------------------------------------------- phase 3
 // newton.rs:113-473 and forward.rs:359-389: rows, Newton, the damped
 // solve qacc = (M + hD)^-1 (f + qfrc_constraint), integration.
+// two blocks of 256 threads an SM (128 registers a thread): 28 tiles of 16
+// lanes an SM, one wave for 4096 Ant envs
 template <int G>
-__global__ void __launch_bounds__(256) newton_kernel(const __grid_constant__ StepArgs A) {
+__global__ void __launch_bounds__(256, 2) newton_kernel(const __grid_constant__ StepArgs A) {
   extern __shared__ __align__(16) unsigned char smem[];
   const DModel& m = stage_model(A, smem);
   cg::thread_block block = cg::this_thread_block();
@@ -216,7 +218,9 @@ __global__ void __launch_bounds__(256) newton_kernel(const __grid_constant__ Ste
     load_async(T, ws + w.qpos, A.st.qpos + env * nq, nq);
     load_async(T, ws + w.qvel, A.st.qvel + env * nv, nv);
     load_async(T, ws + w.qacc, A.st.qacc + env * nv, nv);
-    load_async(T, ws + w.qm, wk + A.k.qm, nv * nv);
+    e.qm = w.qm >= 0 ? ws + w.qm : wk + A.k.qm;
+    e.fac = w.fac >= 0 ? ws + w.fac : e.scr + A.s.chol;
+    if (w.qm >= 0) load_async(T, ws + w.qm, wk + A.k.qm, nv * nv);
     load_async(T, ws + w.cdof, wk + A.k.cdof, 6 * nv);
     load_async(T, ws + w.acc, wk + A.k.a0, nv);
     load_async(T, ws + w.smooth, wk + A.k.smooth, nv);
@@ -233,16 +237,18 @@ __global__ void __launch_bounds__(256) newton_kernel(const __grid_constant__ Ste
       double* qvel = ws + w.qvel;
       if (m.solver == SOLVER_PGS) {
         // forward.rs:366-375: velocities through M + hD, then PGS on them
-        load_async(T, ws + w.fac, wk + A.k.lh, nv * nv);
+        // (the factor read in place when it does not live in the workspace)
+        const double* lh = w.fac >= 0 ? ws + w.fac : wk + A.k.lh;
+        if (w.fac >= 0) load_async(T, ws + w.fac, wk + A.k.lh, nv * nv);
         load_async(T, ws + w.rinv, wk + A.k.rinvh, nv);
         for (int k = T.lane(); k < nv; k += G) acc[k] = ws[w.smooth + k];
         load_wait();
         T.sync();
-        solve_auto(T, ws + w.fac, nv, nv, m.nblock, m.block_adr, m.dof_block, m.maxbs, ws + w.rinv, acc);
+        solve_auto(T, lh, nv, nv, m.nblock, m.block_adr, m.dof_block, m.maxbs, ws + w.rinv, acc);
         for (int k = T.lane(); k < nv; k += G) v[k] = qvel[k] + h * acc[k];
         T.sync();
         vpos = ws + w.tmp;
-        iters = pgs_solve(T, m, w, A.s, e, ncon, v, vpos, ws + w.fac, A.st.prev_con + env * m.maxcon * P_STRIDE,
+        iters = pgs_solve(T, m, w, A.s, e, ncon, v, vpos, lh, A.st.prev_con + env * m.maxcon * P_STRIDE,
                           A.st.prev_ncon + env, &nr, &status);
         for (int k = T.lane(); k < nv; k += G) ws[w.qacc + k] = (v[k] - qvel[k]) / h;
         T.sync();
@@ -264,12 +270,13 @@ __global__ void __launch_bounds__(256) newton_kernel(const __grid_constant__ Ste
         }
         iters = newton_solve(T, m, w, A.s, e, nr, acc, warm, lfeat, lforce, lnum, ldump);
         if (wk[A.k.meta + K_META_DAMPED] != 0.0) {
-          load_async(T, ws + w.fac, wk + A.k.lh, nv * nv);
+          const double* lh = w.fac >= 0 ? ws + w.fac : wk + A.k.lh;
+          if (w.fac >= 0) load_async(T, ws + w.fac, wk + A.k.lh, nv * nv);
           load_async(T, ws + w.rinv, wk + A.k.rinvh, nv);
           for (int k = T.lane(); k < nv; k += G) acc[k] = ws[w.smooth + k] + ws[w.qfrc_c + k];
           load_wait();
           T.sync();
-          solve_auto(T, ws + w.fac, nv, nv, m.nblock, m.block_adr, m.dof_block, m.maxbs, ws + w.rinv, acc);
+          solve_auto(T, lh, nv, nv, m.nblock, m.block_adr, m.dof_block, m.maxbs, ws + w.rinv, acc);
         }
         for (int k = T.lane(); k < nv; k += G) {
           double vk = qvel[k] + h * acc[k];

@@ -886,7 +886,7 @@ __device__ __noinline__ int newton_islands(const Tile<G>& T, const DModel& m, co
   }
   for (int b = 0; b < m.nblock; b++) all_one &= blk_isl[b] == only;
   if (n_isl == 1 && all_one) {
-    int it = newton_dense(T, nv, nr, J, R, ws + w.qm, a, warm, max_iters, tol, B);
+    int it = newton_dense(T, nv, nr, J, R, e.qm, a, warm, max_iters, tol, B);
     add_constraint_force(T, nv, nr, J, R, a, (const int*)nullptr, qfrc);
     return it;
   }
@@ -920,7 +920,7 @@ __device__ __noinline__ int newton_islands(const Tile<G>& T, const DModel& m, co
       nri += tot;
     }
     T.sync();
-    for (int t = lane; t < kk * kk; t += G) subM[t] = ws[w.qm + idx[t / kk] * nv + idx[t % kk]];
+    for (int t = lane; t < kk * kk; t += G) subM[t] = e.qm[idx[t / kk] * nv + idx[t % kk]];
     for (int t = lane; t < nri * kk; t += G) subJ[t] = J[idx[nv + t / kk] * nv + idx[t % kk]];
     for (int t = lane; t < nri * R_STRIDE; t += G) subR[t] = R[R_STRIDE * idx[nv + t / R_STRIDE] + t % R_STRIDE];
     for (int i = lane; i < kk; i += G) {
@@ -951,9 +951,9 @@ __device__ bool learned_start(const Tile<G>& T, const DModel& m, const WsLayout&
                               double* out) {
   int lane = T.lane(), nv = m.nv;
   double* ws = e.ws;
-  double* F = ws + w.fac;
+  double* F = e.fac;
   double* rinv = ws + w.rinv;
-  for (int t = lane; t < nv * nv; t += G) F[t] = ws[w.qm + t];
+  for (int t = lane; t < nv * nv; t += G) F[t] = e.qm[t];
   for (int i = lane; i < nv; i += G) {
     double x = 0.0;
     for (int r = 0; r < 4 * lnum; r++) {
@@ -1002,7 +1002,7 @@ __device__ int newton_solve(const Tile<G>& T, const DModel& m, const WsLayout& w
   double* R = e.scr + s.rows;
   for (int r = lane; r < nr; r += G) R[R_STRIDE * r + R_ACT] = -1.0;  // no previous active set
   T.sync();
-  NewtonBufs B{ws + w.a0, ws + w.grad, ws + w.p, ws + w.tmp, ws + w.tmp2, ws + w.mp, ws + w.fac, ws + w.rinv};
+  NewtonBufs B{ws + w.a0, ws + w.grad, ws + w.p, ws + w.tmp, ws + w.tmp2, ws + w.mp, e.fac, ws + w.rinv};
   bool learned = lnum > 0 && 4 * lnum <= nr;
   if (m.nblock > 1) {
     // the learned candidate goes over the previous qacc, which the learned
@@ -1020,12 +1020,13 @@ __device__ int newton_solve(const Tile<G>& T, const DModel& m, const WsLayout& w
   if constexpr (G >= SMALL_N) {
     if (nv <= SMALL_N && nr <= SMALL_ROWS && w.sj >= 0) {
       SmallBufs S{ws + w.sj, ws + w.sl, ws + w.sx, ws + w.sc};
+      // (this path keeps M in the workspace: its loads are shared-memory loads)
       return newton_small(T, nv, nr, J, R, ws + w.qm, a, warm, m.iterations, m.tolerance, S, qfrc, lfeat, lforce,
                           lnum, ldump);
     }
   }
   if (learned && lforce && learned_start(T, m, w, e, J, a, lfeat, lforce, lnum, ws + w.qacc)) warm = ws + w.qacc;
-  int it = newton_dense(T, nv, nr, J, R, ws + w.qm, a, warm, m.iterations, m.tolerance, B);
+  int it = newton_dense(T, nv, nr, J, R, e.qm, a, warm, m.iterations, m.tolerance, B);
   add_constraint_force(T, nv, nr, J, R, a, (const int*)nullptr, qfrc);
   if (learned && ldump) dump_row_forces(T, nv, J, R, a, 4 * lnum, ldump);
   return it;
