@@ -40,7 +40,7 @@ PHASE_STAGES = {"smooth": ("kinematics", "crba", "vel_rne", "passive_act", "fact
 # of the phase kernels on the Ant workload at 4096 envs after 100 steps (ncu
 # flushes L2 before the captured launch, so the work record the phases hand
 # each other counts here although it stays in L2 between the phases)
-NCU_TRAFFIC_PER_ENV = {"smooth": 4054.0, "collide": 5338.0, "newton": 8782.0}
+NCU_TRAFFIC_PER_ENV = {"smooth": 4047.0, "collide": 6373.0, "newton": 8510.0}
 
 
 def parse():
