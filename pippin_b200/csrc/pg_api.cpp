@@ -1696,33 +1696,54 @@ int pg_autotune(pg_handle* h, int64_t nstep) {
       cudaMemcpyAsync(fields[k], saved[k], sizeof(double) * n * widths[k], cudaMemcpyDeviceToDevice, h->stream);
   };
   // coordinate search: each phase's shape in turn, the others held at the
-  // best found so far, timed over `nstep` whole substeps
+  // best found so far. A candidate is timed on its own phase kernel only
+  // (events around it in `nstep` substeps launched phase by phase), the
+  // fastest of three runs from the saved state after one warm-up run: the
+  // other phases' noise would otherwise decide between shapes a few percent
+  // apart.
   SubstepCfg best = h->cfg;
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
   int rc = PG_OK;
-  auto trial = [&](const SubstepCfg& c, float* ms) -> int {
+  auto trial = [&](const SubstepCfg& c, int phase, float* ms) -> int {
     if (ensure_scratch(h, c) != PG_OK) return 1;
     h->cfg = c;
     StepArgs a = make_args(h);
-    restore();
-    enqueue_substeps(h, a, 0, (int64_t)n, nstep);  // warm-up
-    restore();
-    cudaEventRecord(e0, h->stream);
-    enqueue_substeps(h, a, 0, (int64_t)n, nstep);
-    cudaEventRecord(e1, h->stream);
-    if (cudaEventSynchronize(e1) != cudaSuccess) {
-      rc = cuda_fail(cudaGetLastError(), "autotune trial");
-      return 1;
+    a.start = 0;
+    a.count = (int)n;
+    a.nstep = (int)nstep;
+    SubstepCfg f = fit(c, (int64_t)n);
+    const LaunchCfg* shape[3] = {&f.smooth, &f.collide, &f.newton};
+    *ms = 1e30f;
+    for (int rep = 0; rep < 4; rep++) {
+      restore();
+      float tot = 0.0f;
+      for (int64_t k = 0; k < nstep; k++) {
+        a.sidx = (int)k;
+        cudaError_t e = reset_queue(a, h->stream);
+        for (int p = 0; p < 3 && e == cudaSuccess; p++) {
+          if (p == phase) e = cudaEventRecord(e0, h->stream);
+          if (e == cudaSuccess) e = launch_phase(p, a, *shape[p], h->stream);
+          if (e == cudaSuccess && p == phase) e = cudaEventRecord(e1, h->stream);
+        }
+        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+        float t = 0.0f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&t, e0, e1);
+        if (e != cudaSuccess) {
+          rc = cuda_fail(e, "autotune trial");
+          return 1;
+        }
+        tot += t;
+      }
+      if (rep > 0) *ms = std::min(*ms, tot);
     }
-    cudaEventElapsedTime(ms, e0, e1);
     return 0;
   };
-  float best_ms = 1e30f;
-  if (trial(best, &best_ms)) best_ms = 1e30f;
   for (int phase : {K_SMOOTH, K_COLLIDE, K_NEWTON}) {
     if (rc) break;
+    float best_ms = 1e30f;
+    if (trial(best, phase, &best_ms)) best_ms = 1e30f;
     for (int G : {8, 16, 32}) {
       for (int tpb : {1, 2, 4, 8, 16}) {
         if (rc) break;
@@ -1731,7 +1752,7 @@ int pg_autotune(pg_handle* h, int64_t nstep) {
         LaunchCfg& slot = phase == K_SMOOTH ? c.smooth : phase == K_COLLIDE ? c.collide : c.newton;
         if (choose_grid(h, phase, LaunchCfg{G, tpb, 0}, &slot) != PG_OK) continue;
         float ms = 0;
-        if (trial(c, &ms)) continue;
+        if (trial(c, phase, &ms)) continue;
         if (ms < best_ms) {
           best_ms = ms;
           best = c;
