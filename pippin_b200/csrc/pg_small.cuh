@@ -46,15 +46,12 @@ __device__ inline double dot_ref_sm(const double* a, const double* x, int n) {
   return t;
 }
 
-// Stores of a factor's entries: row k's entries L_k0 .. at row(k).
-struct LStrided {  // a matrix with row stride ld (lower triangle and diagonal)
+// Store of a factor's entries: row k's entries L_k0 .. at row(k), a matrix
+// with row stride ld (lower triangle and diagonal).
+struct LStrided {
   double* p;
   int ld;
   __device__ double* row(int k) const { return p + k * ld; }
-};
-struct LPacked {  // strictly lower entries, packed by rows (row k at k(k-1)/2)
-  double* p;
-  __device__ double* row(int k) const { return p + k * (k - 1) / 2; }
 };
 
 // L L^T = A in place in the store (math.rs:425-447's column order: pivot
