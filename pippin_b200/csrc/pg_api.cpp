@@ -966,6 +966,24 @@ int build_device_model(Handle* h) {
   d.maxrows = maxrows;
   d.maxbs = 0;
   for (int b = 0; b < nblock; b++) d.maxbs = std::max(d.maxbs, m.dof_blocks[2 * b + 1] - m.dof_blocks[2 * b]);
+  // polytope sizes of the general pairs (mesh against anything, cylinder
+  // against a non-plane): the collide kernel caches their world vertices
+  // and face normals per tile
+  d.gen_vmax = d.gen_fmax = 0;
+  for (size_t p = 0; p + 1 < m.pairs.size(); p += 2) {
+    int ta = m.geom_type[m.pairs[p]], tb = m.geom_type[m.pairs[p + 1]];
+    bool general = ta == GEOM_MESH || tb == GEOM_MESH || (ta == GEOM_CYLINDER && tb != GEOM_PLANE) ||
+                   (tb == GEOM_CYLINDER && ta != GEOM_PLANE);
+    if (!general) continue;
+    for (int g : {m.pairs[p], m.pairs[p + 1]}) {
+      int t = m.geom_type[g], nvx = 0, nfx = 0;
+      if (t == GEOM_BOX) nvx = 8, nfx = 6;
+      if (t == GEOM_CYLINDER) nvx = 2 * CYL_SIDES, nfx = CYL_SIDES + 2;
+      if (t == GEOM_MESH) nvx = m.hull_vnum[m.geom_dataid[g]], nfx = m.hull_fnum[m.geom_dataid[g]];
+      d.gen_vmax = std::max(d.gen_vmax, nvx);
+      d.gen_fmax = std::max(d.gen_fmax, nfx);
+    }
+  }
   d.timestep = m.timestep;
   for (int k = 0; k < 3; k++) d.gravity[k] = m.gravity[k];
   d.integrator = m.integrator;

@@ -23,7 +23,6 @@
 
 namespace pg {
 
-constexpr int CYL_SIDES = 16;
 constexpr int GEN_CLIP_CAP = 2 * HULL_FACE_MAX;  // incident loop + one vertex per side plane
 
 // box faces (outward normals -z, +x, +y, -y, -x, +z), their loops, edges
@@ -36,7 +35,9 @@ __constant__ int c_box_eface[12][2] = {{0, 3}, {0, 4}, {3, 4}, {0, 1}, {1, 3}, {
                                        {2, 4}, {1, 2}, {3, 5}, {4, 5}, {1, 5}, {2, 5}};
 __constant__ double c_box_normal[6][3] = {{0, 0, -1}, {1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {-1, 0, 0}, {0, 0, 1}};
 
-// A box, cylinder prism or hull in the world frame, read on demand.
+// A box, cylinder prism or hull in the world frame, read on demand, or from
+// vc / nc (its world vertices and face normals, 3 doubles each) once a tile
+// has filled them (poly_cache).
 struct Poly {
   int kind;
   V3 pos;
@@ -44,12 +45,15 @@ struct Poly {
   V3 size;
   const DModel* m;
   int mesh;
+  const double* vc = nullptr;
+  const double* nc = nullptr;
 };
 
 __device__ inline int p_nv(const Poly& p) {
   return p.kind == GEOM_BOX ? 8 : p.kind == GEOM_CYLINDER ? 2 * CYL_SIDES : p.m->hull_vnum[p.mesh];
 }
 __device__ inline V3 p_v(const Poly& p, int i) {
+  if (p.vc) return ld3(p.vc + 3 * i);
   if (p.kind == GEOM_BOX) {
     V3 s{(i & 1) == 0 ? -1.0 : 1.0, (i & 2) == 0 ? -1.0 : 1.0, (i & 4) == 0 ? -1.0 : 1.0};
     return p.pos + mv(p.mat, V3{p.size.x * s.x, p.size.y * s.y, p.size.z * s.z});
@@ -82,6 +86,7 @@ __device__ inline int p_fv(const Poly& p, int f, int k) {
   return p.m->hull_fv[p.m->hull_fvadr[p.m->hull_fadr[p.mesh] + f] + k];
 }
 __device__ inline V3 p_fn(const Poly& p, int f) {
+  if (p.nc) return ld3(p.nc + 3 * f);
   if (p.kind == GEOM_BOX) return mv(p.mat, V3{c_box_normal[f][0], c_box_normal[f][1], c_box_normal[f][2]});
   if (p.kind == GEOM_CYLINDER) {
     if (f < 2) return mv(p.mat, V3{0.0, 0.0, f == 0 ? -1.0 : 1.0});
@@ -461,17 +466,34 @@ __device__ inline void plane_polytope(const GPose& pl, const Poly& p, double mar
   for (int k = 0; k < nk; k++) out.push(keep[k].p - n * (keep[k].d * 0.5), n, -keep[k].d);
 }
 
+// Fills buf with p's world vertices, then its world face normals (the values
+// p_v and p_fn give), shared out over the tile's lanes, and points p at them.
+// buf holds 3 (nv + nf) doubles.
+template <int G>
+__device__ void poly_cache(const Tile<G>& T, Poly& p, double* buf) {
+  int nv = p_nv(p), nf = p_nf(p);
+  T.sync();  // every lane is done with the previous pair's cache
+  for (int i = T.lane(); i < nv; i += G) st3(buf + 3 * i, p_v(p, i));
+  for (int f = T.lane(); f < nf; f += G) st3(buf + 3 * (nv + f), p_fn(p, f));
+  T.sync();
+  p.vc = buf;
+  p.nc = buf + 3 * nv;
+}
+
 // One pair on the whole tile: every lane passes the same pair and ends with
 // the same contacts; the polytope queries share their candidates out over
-// the lanes, the rest runs on every lane alike.
+// the lanes, the rest runs on every lane alike. With `cache` (6 (gen_vmax +
+// gen_fmax) doubles of the tile's shared memory) the polytopes' world
+// vertices and normals are formed once instead of at every use.
 template <int G>
 __device__ __noinline__ void collide_general(const Tile<G>& T, const DModel& m, const GPose& a0, const GPose& b0,
-                                             double margin, Hits& out) {
+                                             double margin, Hits& out, double* cache) {
   bool swap = a0.type > b0.type;  // type order, normals flipped back (collision.rs:59-67)
   const GPose& a = swap ? b0 : a0;
   const GPose& b = swap ? a0 : b0;
   int start = out.n;
   Poly pb{b.type, b.pos, b.mat, b.size, &m, b.data};
+  if (cache) poly_cache(T, pb, cache);
   if (a.type == GEOM_PLANE) {
     plane_polytope(a, pb, margin, out);
   } else if (a.type == GEOM_SPHERE) {
@@ -480,6 +502,7 @@ __device__ __noinline__ void collide_general(const Tile<G>& T, const DModel& m, 
     capsule_polytope(a, pb, margin, out);
   } else {
     Poly pa{a.type, a.pos, a.mat, a.size, &m, a.data};
+    if (cache) poly_cache(T, pa, cache + 3 * (m.gen_vmax + m.gen_fmax));
     polytope_polytope(T, pa, pb, margin, out);
   }
   if (swap)

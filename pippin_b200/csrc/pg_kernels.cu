@@ -46,6 +46,10 @@ __device__ inline const DModel& stage_model(const StepArgs& A, unsigned char* sm
   return *dm;
 }
 
+// doubles of polytope cache a collide tile needs: world vertices and face
+// normals of both polytopes of a general pair
+__host__ __device__ inline int collide_cache_doubles(const DModel& m) { return 6 * (m.gen_vmax + m.gen_fmax); }
+
 __device__ inline double* tile_workspace(const StepArgs& A, unsigned char* sm, int stride, int tib) {
   int off = A.stage_model ? staged_model_bytes(A.m.arena_bytes) : 0;
   return reinterpret_cast<double*>(sm + off) + (size_t)tib * stride;
@@ -161,8 +165,13 @@ __global__ void __launch_bounds__(256, 2) collide_kernel(const __grid_constant__
   EnvCtx e;
   e.ws = nullptr;
   e.scr = nullptr;
-  // the tile's queue of broad-phase survivors (2G ints)
+  // the tile's queue of broad-phase survivors (2G ints), then its polytope cache
+  int tpb = blockDim.x / G;
   int* queue = reinterpret_cast<int*>(tile_workspace(A, smem, 0, 0)) + (threadIdx.x / G) * COLLIDE_QUEUE;
+  double* gcache = nullptr;
+  if (m.gen_vmax > 0)
+    gcache = reinterpret_cast<double*>(reinterpret_cast<int*>(tile_workspace(A, smem, 0, 0)) + tpb * COLLIDE_QUEUE) +
+             (threadIdx.x / G) * collide_cache_doubles(m);
   for (int item = first_item<G>(); item < A.count; item = next_item(T, A.queue + 1, A.count)) {
     size_t env = (size_t)A.start + item;
     e.env = (int)env;
@@ -173,7 +182,7 @@ __global__ void __launch_bounds__(256, 2) collide_kernel(const __grid_constant__
     prefetch_l1(T, e.prm, sizeof(double) * m.pstride);
     prefetch_l1(T, e.geo, sizeof(double) * G_STRIDE * m.ngeom);
     int status = 0;
-    int ncon = collide(T, m, A.w, A.s, e, &status, queue);
+    int ncon = collide(T, m, A.w, A.s, e, &status, queue, gcache);
     if (T.lane() == 0) {
       wk[A.k.meta + K_META_NCON] = ncon;
       wk[A.k.meta + K_META_STATUS] = (double)((int)wk[A.k.meta + K_META_STATUS] | status);
@@ -485,7 +494,8 @@ const void* tile_kernel(int which, int G) {
 size_t kernel_smem(int which, const StepArgs& a, int tiles_per_block) {
   size_t staged = a.stage_model ? (size_t)staged_model_bytes(a.m.arena_bytes) : 0;
   switch (which) {
-    case K_COLLIDE: return staged + (size_t)tiles_per_block * COLLIDE_QUEUE * sizeof(int);
+    case K_COLLIDE:
+      return staged + (size_t)tiles_per_block * (COLLIDE_QUEUE * sizeof(int) + collide_cache_doubles(a.m) * sizeof(double));
     case K_NEWTON: return staged + (size_t)tiles_per_block * a.wn.stride * sizeof(double);
     default: return staged + (size_t)tiles_per_block * a.w.stride * sizeof(double);
   }

@@ -38,12 +38,14 @@ enum { G_POS = 0, G_MAT = 3, G_AABB = 12, G_STRIDE = 18 };
 
 constexpr int NV_MAX = 64;  // dof-chain masks are 64-bit
 constexpr int HULL_FACE_MAX = 32;  // longest hull face loop the device clips
+constexpr int CYL_SIDES = 16;  // a cylinder in the general narrow phase: a prism of this many sides
 constexpr int COLLIDE_QUEUE = 64;  // broad-phase survivor slots per collide tile (2 x the widest tile)
 
 struct DModel {
   // ---- dims
   int nq, nv, nu, nbody, njnt, ngeom, ncam, neq, npair, nblock, nlevel, nmesh;
   int maxcon, maxrows, maxbs;
+  int gen_vmax, gen_fmax;  // most vertices / faces of a polytope in a general pair (0: no such pair)
   // ---- options (model.rs:60-100)
   double timestep, gravity[3];
   int integrator, solver, iterations;

@@ -19,9 +19,10 @@ namespace pg {
 // (in pair order) in `queue` (2G ints of shared memory); the narrow phase
 // takes them G at a time, one pair per lane, so a batch of narrow-phase
 // work waits for G survivors instead of running once per G candidates.
+// gcache: the tile's polytope cache for general pairs (or nullptr).
 template <int G>
 __device__ int collide(const Tile<G>& T, const DModel& m, const WsLayout& w, const ScrLayout& s, const EnvCtx& e,
-                       int* status, int* queue) {
+                       int* status, int* queue, double* gcache) {
   int lane = T.lane();
   const double* prm = e.prm;
   const double* gr = e.geo;  // poses and boxes from the tree walk
@@ -51,7 +52,7 @@ __device__ int collide(const Tile<G>& T, const DModel& m, const WsLayout& w, con
       int h1 = T.bcast(g1, d), h2 = T.bcast(g2, d);
       Hits gh;
       gh.n = 0;
-      collide_general(T, m, pose(h1), pose(h2), m.margin, gh);
+      collide_general(T, m, pose(h1), pose(h2), m.margin, gh, gcache);
       if (lane == d) hits = gh;
     }
     int nh = hits.n < MAX_HITS ? hits.n : MAX_HITS;
