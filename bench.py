@@ -60,6 +60,8 @@ def parse():
                     help="the learned warm-start evaluation (Ant and tabletop) instead of the headline")
     ap.add_argument("--learned-samples", type=int, default=10_000_000, help="training pairs per scene")
     ap.add_argument("--learned-envs", type=int, default=16384)
+    ap.add_argument("--scene", default="", choices=["", "tabletop", "hull_tumble"],
+                    help="phase timing of another workload (config 3 or 4) beside the oracle, instead of the headline")
     return ap.parse_args()
 
 
@@ -514,12 +516,95 @@ def run_learned_eval(args):
         print(json.dumps(line), flush=True)
 
 
+def run_scene(args):
+    """Device env-steps/s and per-phase time of the tabletop (config 3) or the
+    hull tumble (config 4) after W settling substeps, with the oracle's rate
+    on a bounded sample of the same workload on the host cores beside it.
+    One JSON line (one GPU)."""
+    import torch
+    from oracle.oracle import QPOS, QVEL, Oracle
+    from pippin_b200 import CudaPhysics, Field, Param, mjcf, scenes
+    n, K, W = args.envs, args.steps, max(args.warmup, 3)
+    torch.cuda.set_device(0)
+    if args.scene == "tabletop":
+        plan = scenes.tabletop(n, seed=5)
+        m = mjcf.load_string(plan.xml)
+        desc = (f"tabletop: {n} envs, 2-6 objects each (boxes, cylinders, spheres), dropped 5-15 cm, dt 0.002, "
+                f"Newton tol 1e-10 cap {ITERS}; timed after {W} substeps")
+    else:
+        m = mjcf.load_string(scenes.hull_tumble_xml())
+        desc = (f"hull tumble: {n} envs of 8 hulls (8-32 vertices), v N(0,0.5^2), w N(0,3^2), dt 0.002, "
+                f"Newton tol 1e-10 cap {ITERS}; timed after {W} substeps")
+    blob = mjcf.to_blob(m)
+
+    def setup(sim, count, set_param, reset, set_q, set_v):
+        if args.scene == "tabletop":
+            pl = scenes.tabletop(count, seed=5)
+            for pid, elem, vals in pl.params:
+                set_param(pid, elem, vals)
+            set_param(11, 0, pl.qpos0)
+            reset()
+        else:
+            rng = np.random.default_rng(5)
+            v = np.zeros((count, m.nv))
+            for b in range(m.nv // 6):
+                v[:, 6 * b:6 * b + 3] = rng.normal(0, 0.5, (count, 3))
+                v[:, 6 * b + 3:6 * b + 6] = rng.normal(0, 3.0, (count, 3))
+            set_q(np.tile(np.array(m.qpos0), (count, 1)))
+            set_v(v)
+
+    p = CudaPhysics(blob, n)
+    p.set_solver(tolerance=TOL, iterations=ITERS)
+    setup(p, n, lambda pid, elem, vals: p.set_param(Param(pid), elem, range(n), vals), lambda: p.reset(range(n)),
+          lambda q: p.set(Field.QPOS, range(n), q), lambda v: p.set(Field.QVEL, range(n), v))
+    p.step(range(n), W)
+    p.autotune(nstep=2)
+    stream = torch.cuda.ExternalStream(p.stream(), device=torch.device("cuda", 0))
+    p.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    p.step_device(range(n), K, 0)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    ph = {"smooth": 0.0, "collide": 0.0, "newton": 0.0}
+    for k in range(K):
+        for name, t in p.time_phases(range(n), 1).items():
+            ph[name] += t
+    st = p.stats()
+    launch = p.phase_launch()
+    p.close()
+    # the oracle on a sample of the same workload (same settling, then timed)
+    cn = 256
+    o = Oracle(blob, cn, threads=0, fast=True)
+    o.set_solver(tolerance=TOL, iterations=ITERS)
+    setup(o, cn, lambda pid, elem, vals: o.set_param(pid, elem, np.asarray(vals), 0, cn),
+          lambda: o.reset(list(range(cn))), lambda q: o.set(QPOS, q), lambda v: o.set(QVEL, v))
+    o.step(0, cn, W)
+    t0 = time.perf_counter()
+    ck = max(1, min(K, 50))
+    o.step(0, cn, ck)
+    cpu_rate = cn * ck / (time.perf_counter() - t0)
+    line = {"metric": f"{args.scene} env-steps/s", "value": n * K / (ms * 1e-3), "unit": "env-steps/s",
+            "n_gpus": 1, "steps": K, "warmup": W, "ms_per_step": ms / K, "higher_is_better": True, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": desc, "envs": n},
+            "phases": {k: {"ms_per_launch": v / K, "launch": dict(zip(("lanes_per_env", "envs_per_block", "blocks"),
+                                                                       launch[k]))} for k, v in ph.items()},
+            "mean_ncon": float(st["ncon"].mean()), "mean_rows": float(st["nrows"].mean()),
+            "mean_iters": float(st["iters"].mean()),
+            "cpu_baseline": {"value": cpu_rate, "unit": "env-steps/s", "cores": o.threads, "kind": "port",
+                             "sample": f"{args.scene} {cn} envs x {ck} substeps after the same settling (oracle)"}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
     elif args.learned_eval:
         run_learned_eval(args)
+    elif args.scene:
+        run_scene(args)
     else:
         run_ours(args)
 
