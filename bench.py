@@ -60,8 +60,8 @@ def parse():
                     help="the learned warm-start evaluation (Ant and tabletop) instead of the headline")
     ap.add_argument("--learned-samples", type=int, default=10_000_000, help="training pairs per scene")
     ap.add_argument("--learned-envs", type=int, default=16384)
-    ap.add_argument("--scene", default="", choices=["", "tabletop", "hull_tumble"],
-                    help="phase timing of another workload (config 3 or 4) beside the oracle, instead of the headline")
+    ap.add_argument("--scene", default="", choices=["", "tabletop", "hull_tumble", "cartpole", "arm3hinge"],
+                    help="phase timing of another workload (configs 2-4) beside the oracle, instead of the headline")
     return ap.parse_args()
 
 
@@ -517,12 +517,14 @@ def run_learned_eval(args):
 
 
 def run_scene(args):
-    """Device env-steps/s and per-phase time of the tabletop (config 3) or the
-    hull tumble (config 4) after W settling substeps, with the oracle's rate
-    on a bounded sample of the same workload on the host cores beside it.
-    One JSON line (one GPU)."""
+    """Device env-steps/s and per-phase time of the tabletop (config 3), the
+    hull tumble (config 4) or a contact-free model (config 2: random states
+    over the joint ranges, qvel N(0, 1), per-env masses x U[0.5, 2], random
+    controls held) after W settling substeps, with the oracle's rate on a
+    bounded sample of the same workload on the host cores beside it. One
+    JSON line (one GPU)."""
     import torch
-    from oracle.oracle import QPOS, QVEL, Oracle
+    from oracle.oracle import CTRL, QPOS, QVEL, Oracle
     from pippin_b200 import CudaPhysics, Field, Param, mjcf, scenes
     n, K, W = args.envs, args.steps, max(args.warmup, 3)
     torch.cuda.set_device(0)
@@ -531,19 +533,37 @@ def run_scene(args):
         m = mjcf.load_string(plan.xml)
         desc = (f"tabletop: {n} envs, 2-6 objects each (boxes, cylinders, spheres), dropped 5-15 cm, dt 0.002, "
                 f"Newton tol 1e-10 cap {ITERS}; timed after {W} substeps")
+    elif args.scene in ("cartpole", "arm3hinge"):
+        m = mjcf.load_string(scenes.cartpole_xml() if args.scene == "cartpole" else scenes.arm3hinge_xml())
+        desc = (f"{args.scene}: {n} envs, qpos uniform over the joint ranges (hinges [-pi, pi], slides +-0.5), "
+                f"qvel N(0,1), per-env masses x U[0.5,2], controls U[-1,1] held; timed after {W} substeps")
     else:
         m = mjcf.load_string(scenes.hull_tumble_xml())
         desc = (f"hull tumble: {n} envs of 8 hulls (8-32 vertices), v N(0,0.5^2), w N(0,3^2), dt 0.002, "
                 f"Newton tol 1e-10 cap {ITERS}; timed after {W} substeps")
     blob = mjcf.to_blob(m)
 
-    def setup(sim, count, set_param, reset, set_q, set_v):
+    def setup(sim, count, set_param, reset, set_q, set_v, set_ctrl=None):
         if args.scene == "tabletop":
             pl = scenes.tabletop(count, seed=5)
             for pid, elem, vals in pl.params:
                 set_param(pid, elem, vals)
             set_param(11, 0, pl.qpos0)
             reset()
+        elif args.scene in ("cartpole", "arm3hinge"):
+            rng = np.random.default_rng(5)
+            q = np.tile(np.array(m.qpos0), (count, 1))
+            for j in range(m.njnt):
+                qa = m.jnt_qposadr[j]
+                if m.jnt_type[j] == mjcf.JNT_HINGE:
+                    q[:, qa] = rng.uniform(-np.pi, np.pi, count)
+                elif m.jnt_type[j] == mjcf.JNT_SLIDE:
+                    q[:, qa] = rng.uniform(-0.5, 0.5, count)
+            for b in range(1, m.nbody):
+                set_param(5, b, (np.array(m.body_mass[b]) * rng.uniform(0.5, 2.0, count)).reshape(count, 1))
+            set_q(q)
+            set_v(rng.normal(0, 1, (count, m.nv)))
+            set_ctrl(rng.uniform(-1, 1, (count, m.nu)))
         else:
             rng = np.random.default_rng(5)
             v = np.zeros((count, m.nv))
@@ -556,14 +576,17 @@ def run_scene(args):
     p = CudaPhysics(blob, n)
     p.set_solver(tolerance=TOL, iterations=ITERS)
     setup(p, n, lambda pid, elem, vals: p.set_param(Param(pid), elem, range(n), vals), lambda: p.reset(range(n)),
-          lambda q: p.set(Field.QPOS, range(n), q), lambda v: p.set(Field.QVEL, range(n), v))
+          lambda q: p.set(Field.QPOS, range(n), q), lambda v: p.set(Field.QVEL, range(n), v),
+          lambda c: p.set(Field.CTRL, range(n), c))
     p.step(range(n), W)
     p.autotune(nstep=2)
     stream = torch.cuda.ExternalStream(p.stream(), device=torch.device("cuda", 0))
+    # the held controls, in device memory for pg_step_device
+    ctrl = torch.from_numpy(p.get(Field.CTRL, range(n))).cuda() if m.nu > 0 else None
     p.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    p.step_device(range(n), K, 0)
+    p.step_device(range(n), K, ctrl.data_ptr() if ctrl is not None else 0)
     e1.record(stream)
     e1.synchronize()
     ms = e0.elapsed_time(e1)
@@ -575,14 +598,15 @@ def run_scene(args):
     launch = p.phase_launch()
     p.close()
     # the oracle on a sample of the same workload (same settling, then timed)
-    cn = 256
+    cn = 4096 if args.scene in ("cartpole", "arm3hinge") else 256
     o = Oracle(blob, cn, threads=0, fast=True)
     o.set_solver(tolerance=TOL, iterations=ITERS)
     setup(o, cn, lambda pid, elem, vals: o.set_param(pid, elem, np.asarray(vals), 0, cn),
-          lambda: o.reset(list(range(cn))), lambda q: o.set(QPOS, q), lambda v: o.set(QVEL, v))
+          lambda: o.reset(list(range(cn))), lambda q: o.set(QPOS, q), lambda v: o.set(QVEL, v),
+          lambda c: o.set(CTRL, c))
     o.step(0, cn, W)
     t0 = time.perf_counter()
-    ck = max(1, min(K, 50))
+    ck = max(1, min(K, 100 if cn > 256 else 50))
     o.step(0, cn, ck)
     cpu_rate = cn * ck / (time.perf_counter() - t0)
     line = {"metric": f"{args.scene} env-steps/s", "value": n * K / (ms * 1e-3), "unit": "env-steps/s",
