@@ -1,8 +1,8 @@
 // Oracle (test infrastructure only): general convex narrow phase for the pairs
 // the reference hands to parry3d-f64 0.31.1 (collision.rs:102-147): mesh
 // (convex hull) against anything, and cylinder against non-plane shapes.
-// parry3d-f64 is an un-vendored dependency, so this path is this build's own
-// algorithm, restated here for the CUDA backend's parity tests; its parity
+// parry3d-f64 is an un-vendored dependency, so this path is this library's
+// own algorithm, restated here for the CUDA backend's parity tests; its parity
 // with the reference is unpinned (the reference's mesh.rs behaviour tests
 // pin it instead).
 //

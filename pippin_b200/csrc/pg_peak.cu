@@ -1,5 +1,6 @@
 // FP64 DFMA throughput microbenchmark: the denominator of the FP64-pipe
-// roofline (the driver's measured peaks cover HBM copy and BF16 GEMM only).
+// roofline (measured peak figures for these GPUs cover HBM copy and BF16
+// GEMM only).
 // Every thread runs 8 independent FMA chains for `iters` rounds; the grid
 // is 16 blocks of 256 threads per SM. FLOPs = 2 per FMA.
 #include <cuda_runtime.h>
