@@ -1718,8 +1718,16 @@ int pg_autotune(pg_handle* h, int64_t nstep) {
   // (events around it in `nstep` substeps launched phase by phase), the
   // fastest of three runs from the saved state after one warm-up run: the
   // other phases' noise would otherwise decide between shapes a few percent
-  // apart.
+  // apart. Each run starts with the L2 cache flushed (a write twice its
+  // size after the state is restored), as a step does when the caller's own
+  // work runs between steps: with the work record already in L2 the smooth
+  // phase's shapes tie, with a cold L2 they differ by 5%.
   SubstepCfg best = h->cfg;
+  int l2_bytes = 0;
+  if (cudaDeviceGetAttribute(&l2_bytes, cudaDevAttrL2CacheSize, h->device) != cudaSuccess) l2_bytes = 0;
+  size_t flush_bytes = 2 * (size_t)std::max(l2_bytes, 0);
+  void* flush = nullptr;
+  if (flush_bytes) CK(cudaMalloc(&flush, flush_bytes));
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
@@ -1736,6 +1744,7 @@ int pg_autotune(pg_handle* h, int64_t nstep) {
     *ms = 1e30f;
     for (int rep = 0; rep < 4; rep++) {
       restore();
+      if (flush) cudaMemsetAsync(flush, rep, flush_bytes, h->stream);
       float tot = 0.0f;
       for (int64_t k = 0; k < nstep; k++) {
         a.sidx = (int)k;
@@ -1783,6 +1792,7 @@ int pg_autotune(pg_handle* h, int64_t nstep) {
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   for (void* p : saved) cudaFree(p);
+  if (flush) cudaFree(flush);
   if (!rc) g_err.clear();
   // re-apply the winner so every kernel's shared-memory attribute matches it
   if (!rc) rc = apply_cfg(h, best);
