@@ -62,6 +62,8 @@ def parse():
     ap.add_argument("--learned-envs", type=int, default=16384)
     ap.add_argument("--scene", default="", choices=["", "tabletop", "hull_tumble", "cartpole", "arm3hinge"],
                     help="phase timing of another workload (configs 2-4) beside the oracle, instead of the headline")
+    ap.add_argument("--render", default="", help="batched rendering of Ant poses at these square resolutions "
+                    "(comma-separated, e.g. 64,128) instead of the headline")
     return ap.parse_args()
 
 
@@ -621,6 +623,100 @@ def run_scene(args):
     print(json.dumps(line), flush=True)
 
 
+def hbm_peak() -> float:
+    """Measured HBM copy bandwidth (GB/s) from MEASURED_PEAKS.json, else the
+    pool's earlier measurement of 6650 GB/s."""
+    try:
+        with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"])
+    except (OSError, KeyError, ValueError):
+        return 6650.0
+
+
+def run_render(args):
+    """Frames/s of the batched rasteriser on Ant poses (the reference's
+    render benchmark, crates/pippin-render/examples/render_bench.rs: Ant
+    after 50 steps, one fixed view, RGB + depth + segmentation), one JSON line
+    per resolution. `value` times the kernel from device-resident poses with
+    CUDA events; `e2e` times the host call (poses up, images down)."""
+    import torch
+
+    from pippin_b200 import CudaPhysics, Field, mjcf, scenes
+    from pippin_b200 import render as R
+
+    dev = torch.device("cuda", 0)
+    n, K, W = args.envs, args.steps, max(args.warmup, 3)
+    m = mjcf.load_string(scenes.ant_xml(tolerance=TOL, iterations=ITERS))
+    phys = CudaPhysics(mjcf.to_blob(m), n)
+    q, v, rng = initial_state(m, n, shard_seeds(0)["state"])
+    phys.set(Field.QPOS, range(n), q)
+    phys.set(Field.QVEL, range(n), v)
+    phys.step(range(n), 50)
+    g, c = phys.poses(range(n))
+    sc = phys.scene()
+    phys.close()
+    published = {64: 310_000.0, 128: 195_000.0}  # README.md:115-116, 4096 Ant envs on an Apple GPU
+    for res in [int(x) for x in args.render.split(",")]:
+        cfg = R.RenderConfig(res, res, [R.ViewSource.look_at([1.5, -1.5, 1.2], [0.0, 0.0, 0.3], 45.0)], 0.01, 20.0)
+        r = R.CudaRenderer(sc, cfg)
+        gd = torch.from_numpy(g.reshape(-1)).to(dev)
+        cd = torch.from_numpy(c.reshape(-1).copy()).to(dev)
+        ad = torch.from_numpy(np.tile(r.base_appearance, (n, 1)).reshape(-1)).to(dev)
+        px = n * res * res
+        rgba = torch.empty(px * 4, dtype=torch.uint8, device=dev)
+        depth = torch.empty(px, dtype=torch.float32, device=dev)
+        seg = torch.empty(px, dtype=torch.int32, device=dev)
+        stream = torch.cuda.ExternalStream(r.stream(), device=dev)
+        flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+        def frame():
+            r.render_device(n, gd.data_ptr(), cd.data_ptr(), ad.data_ptr(), rgba.data_ptr(), depth.data_ptr(),
+                            seg.data_ptr())
+
+        for _ in range(W):
+            frame()
+        r.synchronize()
+        total = 0.0
+        for k in range(K):
+            flush.fill_(float(k))
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            frame()
+            e1.record(stream)
+            e1.synchronize()
+            total += e0.elapsed_time(e1)
+        ms = total / K
+        # end to end through the host API: poses in from host memory, images back to host memory
+        for _ in range(2):
+            r.render(0, n, g, c)
+        t0 = time.perf_counter()
+        for _ in range(max(K // 4, 3)):
+            r.render(0, n, g, c)
+        e2e_ms = (time.perf_counter() - t0) * 1e3 / max(K // 4, 3)
+        out_bytes = px * 12
+        line = {"metric": f"Ant frames/s at {res}x{res} (RGBA8 + depth + segmentation)", "value": n / (ms * 1e-3),
+                "unit": "frames/s", "n_gpus": 1, "steps": K, "warmup": W, "ms_per_step": ms,
+                "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": f"ant: {n} envs after 50 steps from qpos0+U[-0.1,0.1], one fixed view "
+                                       f"look_at((1.5,-1.5,1.2),(0,0,0.3)) fovy 45, near 0.01 far 20, {res}x{res}",
+                           "triangles": int(len(r.triangles)), "vertices": int(len(r.vertices)),
+                           "l2": "flushed between timed frames (256 MB write)"},
+                "reference_published": {"value": published.get(res), "unit": "frames/s",
+                                        "note": "Metal renderer, 4096 Ant envs, Apple GPU (README.md:115-116)"},
+                "e2e": {"value": n / (e2e_ms * 1e-3), "unit": "frames/s", "h2d_bytes_per_step": int(g.nbytes + c.nbytes),
+                        "d2h_bytes_per_step": int(out_bytes)},
+                "gpu_launches": K,
+                "roofline": {"bound": "hbm", "kernel": "render_kernel", "achieved": out_bytes / (ms * 1e-3) / 1e9,
+                             "peak": hbm_peak(), "unit": "GB/s", "frac": out_bytes / (ms * 1e-3) / 1e9 / hbm_peak(),
+                             "traffic": None,
+                             "note": "algorithmic bytes = the images written (12 B a pixel); the poses read are "
+                                     "48 B a geom"}}
+        print(json.dumps(line), flush=True)
+        r.close()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -629,6 +725,8 @@ def main():
         run_learned_eval(args)
     elif args.scene:
         run_scene(args)
+    elif args.render:
+        run_render(args)
     else:
         run_ours(args)
 

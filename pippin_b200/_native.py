@@ -71,6 +71,13 @@ SIGNATURES = [
     ("pg_mlp_forward", _i32, [_pf, _sz, _pf, _i64, _pf]),
     ("pg_mlp_loss_grad", _i32, [_pf, _sz, _pf, _pf, _i64, _pf, _sz, _pd]),
     ("pg_mlp_train", _i32, [_pf, _pf, _i64, _i32, _i32, C.c_float, C.c_uint64, _pf, _sz, _pd]),
+    ("pg_render_create", _i32, [_pf, _i64, C.POINTER(C.c_uint32), _i64, _i64, _i64, _pf, _i64, _pf, _i64, _i64, _pf,
+                                _i32, C.POINTER(_vp)]),
+    ("pg_render_destroy", _i32, [_vp]),
+    ("pg_render_frames", _i32, [_vp, _i64, _pf, _sz, _pf, _sz, _pf, _sz, C.POINTER(C.c_uint8), _pf, _pi32]),
+    ("pg_render_frames_device", _i32, [_vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp]),
+    ("pg_render_stream", _vp, [_vp]),
+    ("pg_render_synchronize", _i32, [_vp]),
 ]
 
 _lib = None

@@ -14,7 +14,11 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libpippin_b200.so")
-SOURCES = ["pg_kernels.cu", "pg_api.cpp", "pg_peak.cu", "pg_noalloc.cu", "pg_mlp.cu"]
+SOURCES = ["pg_kernels.cu", "pg_api.cpp", "pg_peak.cu", "pg_noalloc.cu", "pg_mlp.cu", "pg_render.cu"]
+# the rasteriser rounds every product and sum on its own (no FMA contraction),
+# so that its coverage, depth and shading match an IEEE single-precision
+# evaluation of the same expressions on the CPU bit for bit
+EXTRA_FLAGS = {"pg_render.cu": ["-fmad=false"]}
 HEADERS = ["pg_math.cuh", "pg_model.h", "pg_tile.cuh", "pg_dynamics.cuh", "pg_collide.cuh", "pg_linalg.cuh", "pg_small.cuh", "pg_pgs.cuh", "pg_general.cuh", "pg_mlp.h",
            "pg_newton.cuh", "pg_kernels.h"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
@@ -33,7 +37,8 @@ def _stale() -> bool:
         return True
     t = os.path.getmtime(LIB)
     deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS]
-    deps += [os.path.join(HERE, "..", "include", h) for h in ("pippin_b200.h", "pippin_b200_tools.h", "pippin_b200_mlp.h")]
+    deps += [os.path.join(HERE, "..", "include", h)
+             for h in ("pippin_b200.h", "pippin_b200_tools.h", "pippin_b200_mlp.h", "pippin_b200_render.h")]
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 
@@ -45,7 +50,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     objs = []
     for src in SOURCES:
         obj = os.path.join(LIBDIR, src.rsplit(".", 1)[0] + ".o")
-        cmd = [_nvcc(), *NVCC_FLAGS, "-c", os.path.join(CSRC, src), "-o", obj]
+        cmd = [_nvcc(), *NVCC_FLAGS, *EXTRA_FLAGS.get(src, []), "-c", os.path.join(CSRC, src), "-o", obj]
         if src.endswith(".cpp"):
             cmd = [_nvcc(), *NVCC_FLAGS, "-x", "cu", "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:

@@ -1,0 +1,572 @@
+// Batched rasteriser: every (environment, view) image is cut into tiles of
+// 64 x 64 pixels and one block renders one tile at a time (persistent grid,
+// work items handed out in order). A block keeps a visibility buffer for its
+// tile in shared memory: per pixel the 64-bit minimum of (depth bits << 32 |
+// 2 * triangle + sub-triangle), so the nearest fragment wins and equal depths
+// go to the earlier triangle, as a depth test `Less` over triangles drawn in
+// order does. Triangles are transformed, clipped at the near plane and set
+// up one per thread; small ones are scanned by their thread, large ones are
+// queued and scanned by the whole block. A resolve pass then recomputes the
+// winning triangle at each pixel, interpolates its attributes with
+// perspective correction and shades it (render.metal:67-128), writing
+// RGBA8, linear depth and segmentation in (image, y, x) order (:130-145).
+//
+// The file is compiled without FMA contraction: every product and sum is
+// rounded on its own, in the order written, so that a CPU evaluation of the
+// same expressions in IEEE single precision gives the same bits.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/pippin_b200.h"
+#include "../../include/pippin_b200_render.h"
+
+namespace pg {
+void internal_set_error(const std::string& msg);
+}
+
+namespace {
+
+constexpr int RT = 64;            // tile edge, pixels
+constexpr int RTHREADS = 256;     // threads per block
+constexpr int BIG_PIX = 64;       // bounding boxes above this many pixels are scanned by the whole block
+constexpr int QCAP = 2 * RTHREADS;  // queue entries: at most two sub-triangles per thread per round
+constexpr int QWORDS = 14;        // x[3], y[3], z[3], id, x0, y0, x1, y1
+constexpr unsigned long long EMPTY = ~0ull;
+
+struct RArgs {
+  const float* verts;
+  const uint32_t* tris;
+  int ntri, ngeom, ncam, nview;
+  const float* views;
+  int W, H, tiles_x, tiles_y;
+  float near_, far_, A, An, L0, L1, L2;
+  const float* geoms;
+  const float* cams;
+  const float* app;
+  int nenv;
+  uint8_t* rgba;
+  float* depth;
+  int32_t* seg;
+};
+
+// one polygon vertex: camera-space position, camera-space normal, local xy
+struct PV {
+  float a[8];
+};
+
+__device__ __forceinline__ void cam_xform(const float* v, const float* g, const float* ap, const float* c, float* pc) {
+  float p0 = v[0] * ap[4], p1 = v[1] * ap[5], p2 = v[2] * ap[6];
+  float w[3];
+#pragma unroll
+  for (int i = 0; i < 3; i++) w[i] = ((g[3 + 3 * i] * p0 + g[4 + 3 * i] * p1) + g[5 + 3 * i] * p2) + g[i];
+  float d0 = w[0] - c[0], d1 = w[1] - c[1], d2 = w[2] - c[2];
+#pragma unroll
+  for (int i = 0; i < 3; i++) pc[i] = (c[3 + i] * d0 + c[6 + i] * d1) + c[9 + i] * d2;
+}
+
+__device__ __forceinline__ void cam_normal(const float* v, const float* g, const float* ap, const float* c, float* nc) {
+  float n0 = v[4] / fmaxf(ap[4], 1e-6f), n1 = v[5] / fmaxf(ap[5], 1e-6f), n2 = v[6] / fmaxf(ap[6], 1e-6f);
+  float len = sqrtf((n0 * n0 + n1 * n1) + n2 * n2);
+  n0 = n0 / len;
+  n1 = n1 / len;
+  n2 = n2 / len;
+  float w[3];
+#pragma unroll
+  for (int i = 0; i < 3; i++) w[i] = (g[3 + 3 * i] * n0 + g[4 + 3 * i] * n1) + g[5 + 3 * i] * n2;
+#pragma unroll
+  for (int i = 0; i < 3; i++) nc[i] = (c[3 + i] * w[0] + c[6 + i] * w[1]) + c[9 + i] * w[2];
+}
+
+// Sutherland-Hodgman against the near plane (-z >= near) over the edges
+// v0->v1, v1->v2, v2->v0; `K` attributes per vertex are carried along.
+template <int K>
+__device__ __forceinline__ int clip_near(const PV* in, PV* out, float near_) {
+  int n = 0;
+#pragma unroll
+  for (int e = 0; e < 3; e++) {
+    const PV& a = in[e];
+    const PV& b = in[e == 2 ? 0 : e + 1];
+    float da = (-a.a[2]) - near_, db = (-b.a[2]) - near_;
+    bool ia = da >= 0.0f, ib = db >= 0.0f;
+    if (ia) out[n++] = a;
+    if (ia != ib) {
+      float t = da / (da - db);
+#pragma unroll
+      for (int k = 0; k < K; k++) out[n].a[k] = a.a[k] + t * (b.a[k] - a.a[k]);
+      n++;
+    }
+  }
+  return n;
+}
+
+struct SV {  // screen-space vertex
+  float x, y, z, w;
+};
+
+__device__ __forceinline__ SV project(const PV& p, float fx, float fy, const RArgs& A) {
+  SV s;
+  s.w = -p.a[2];
+  float nx = (fx * p.a[0]) / s.w, ny = (fy * p.a[1]) / s.w;
+  s.z = (A.A * p.a[2] + A.An) / s.w;
+  s.x = (nx + 1.0f) * (0.5f * (float)A.W);
+  s.y = (1.0f - ny) * (0.5f * (float)A.H);
+  return s;
+}
+
+__device__ __forceinline__ float edge(float ax, float ay, float bx, float by, float px, float py) {
+  return (bx - ax) * (py - ay) - (by - ay) * (px - ax);
+}
+
+// a pixel centre exactly on an edge belongs to one of the two triangles sharing it
+__device__ __forceinline__ bool owns(float e, float ax, float ay, float bx, float by) {
+  if (e != 0.0f) return e > 0.0f;
+  float dy = by - ay, dx = bx - ax;
+  return dy < 0.0f || (dy == 0.0f && dx > 0.0f);
+}
+
+// orient counter-clockwise in (x right, y down) so that area > 0; returns area (NaN or <= 0: nothing to draw)
+__device__ __forceinline__ float orient(SV* s, int* ord) {
+  float area = edge(s[0].x, s[0].y, s[1].x, s[1].y, s[2].x, s[2].y);
+  if (area < 0.0f) {
+    SV t = s[1];
+    s[1] = s[2];
+    s[2] = t;
+    int o = ord[1];
+    ord[1] = ord[2];
+    ord[2] = o;
+    area = edge(s[0].x, s[0].y, s[1].x, s[1].y, s[2].x, s[2].y);
+  }
+  return area;
+}
+
+// coverage and NDC depth of pixel (px, py); false when not covered or outside [0, 1]
+__device__ __forceinline__ bool cover(const SV* s, float area, int px, int py, float* l, float* z) {
+  float X = (float)px + 0.5f, Y = (float)py + 0.5f;
+  float e0 = edge(s[1].x, s[1].y, s[2].x, s[2].y, X, Y);
+  float e1 = edge(s[2].x, s[2].y, s[0].x, s[0].y, X, Y);
+  float e2 = edge(s[0].x, s[0].y, s[1].x, s[1].y, X, Y);
+  if (!owns(e0, s[1].x, s[1].y, s[2].x, s[2].y) || !owns(e1, s[2].x, s[2].y, s[0].x, s[0].y) ||
+      !owns(e2, s[0].x, s[0].y, s[1].x, s[1].y))
+    return false;
+  l[0] = e0 / area;
+  l[1] = e1 / area;
+  l[2] = e2 / area;
+  *z = (l[0] * s[0].z + l[1] * s[1].z) + l[2] * s[2].z;
+  return *z >= 0.0f && *z <= 1.0f;
+}
+
+__device__ __forceinline__ void bbox(const SV* s, int tx0, int ty0, int tx1, int ty1, int* b) {
+  float mnx = fminf(fminf(s[0].x, s[1].x), s[2].x), mxx = fmaxf(fmaxf(s[0].x, s[1].x), s[2].x);
+  float mny = fminf(fminf(s[0].y, s[1].y), s[2].y), mxy = fmaxf(fmaxf(s[0].y, s[1].y), s[2].y);
+  // pixel centres x + 0.5 in [mnx, mxx]: x in [floor(mnx - 0.5), floor(mxx - 0.5)], widened by one
+  b[0] = max(tx0, (int)floorf(fmaxf(mnx, -2.0f)) - 1);
+  b[1] = max(ty0, (int)floorf(fmaxf(mny, -2.0f)) - 1);
+  b[2] = min(tx1 - 1, (int)floorf(fminf(mxx, 1.0e6f)));
+  b[3] = min(ty1 - 1, (int)floorf(fminf(mxy, 1.0e6f)));
+}
+
+// triangle t's vertices in camera space (K = 3: position only; K = 8: with
+// normal and local xy); false when its geom is hidden in this environment
+template <int K>
+__device__ __forceinline__ bool tri_verts(const RArgs& A, int t, const float* sg, const float* sa, const float* cp,
+                                          PV* v, int* geom) {
+  const uint32_t* ix = A.tris + 3 * (size_t)t;
+  const float* v0 = A.verts + 8 * (size_t)ix[0];
+  int g = (int)__float_as_uint(v0[3]);
+  *geom = g;
+  const float* gp = sg + 12 * g;
+  const float* ap = sa + 8 * g;
+  if (!(ap[3] > 0.0f)) return false;
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    const float* vv = A.verts + 8 * (size_t)ix[k];
+    cam_xform(vv, gp, ap, cp, v[k].a);
+    if (K == 8) {
+      cam_normal(vv, gp, ap, cp, v[k].a + 3);
+      v[k].a[6] = vv[0];
+      v[k].a[7] = vv[1];
+    }
+  }
+  return true;
+}
+
+__global__ void __launch_bounds__(RTHREADS) render_kernel(RArgs A) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  unsigned long long* keys = (unsigned long long*)smem;
+  float* queue = (float*)(keys + RT * RT);
+  float* sg = queue + QCAP * QWORDS;  // this env's geom poses
+  float* sa = sg + 12 * A.ngeom;      // and appearance
+  float* cp = sa + 8 * A.ngeom;       // the view's camera pose
+  __shared__ int qn;
+  const int tid = threadIdx.x;
+  const int tiles = A.tiles_x * A.tiles_y;
+  const long long items = (long long)A.nenv * A.nview * tiles;
+
+  for (long long item = blockIdx.x; item < items; item += gridDim.x) {
+    const int img = (int)(item / tiles), tile = (int)(item % tiles);
+    const int env = img / A.nview, view = img % A.nview;
+    const int tx0 = (tile % A.tiles_x) * RT, ty0 = (tile / A.tiles_x) * RT;
+    const int tx1 = min(tx0 + RT, A.W), ty1 = min(ty0 + RT, A.H);
+    const float* vw = A.views + 16 * view;
+    const int cam = (int)vw[0];
+    const float fx = vw[1], fy = vw[2];
+    for (int i = tid; i < 12 * A.ngeom; i += RTHREADS) sg[i] = A.geoms[(size_t)env * A.ngeom * 12 + i];
+    for (int i = tid; i < 8 * A.ngeom; i += RTHREADS) sa[i] = A.app[(size_t)env * A.ngeom * 8 + i];
+    if (tid < 12) cp[tid] = cam >= 0 ? A.cams[((size_t)env * A.ncam + cam) * 12 + tid] : vw[4 + tid];
+    for (int i = tid; i < RT * RT; i += RTHREADS) keys[i] = EMPTY;
+    if (tid == 0) qn = 0;
+    __syncthreads();
+
+    // ---- visibility
+    for (int base = 0; base < A.ntri; base += RTHREADS) {
+      const int t = base + tid;
+      PV v[3], poly[4];
+      int geom;
+      if (t < A.ntri && tri_verts<3>(A, t, sg, sa, cp, v, &geom)) {
+        int n = clip_near<3>(v, poly, A.near_);
+        SV ps[4];
+        for (int k = 0; k < n; k++) ps[k] = project(poly[k], fx, fy, A);
+        for (int sub = 0; sub + 3 <= n; sub++) {
+          SV s[3] = {ps[0], ps[1 + sub], ps[2 + sub]};
+          int ord[3] = {0, 1, 2};
+          float area = orient(s, ord);
+          if (!(area > 0.0f)) continue;
+          int b[4];
+          bbox(s, tx0, ty0, tx1, ty1, b);
+          if (b[0] > b[2] || b[1] > b[3]) continue;
+          const unsigned id = 2u * (unsigned)t + (unsigned)sub;
+          const int bw = b[2] - b[0] + 1, npix = bw * (b[3] - b[1] + 1);
+          if (npix > BIG_PIX) {
+            int slot = atomicAdd(&qn, 1);
+            float* q = queue + QWORDS * slot;
+            for (int k = 0; k < 3; k++) {
+              q[k] = s[k].x;
+              q[3 + k] = s[k].y;
+              q[6 + k] = s[k].z;
+            }
+            q[9] = __uint_as_float(id);
+            for (int k = 0; k < 4; k++) q[10 + k] = __int_as_float(b[k]);
+            continue;
+          }
+          for (int p = 0; p < npix; p++) {
+            int px = b[0] + p % bw, py = b[1] + p / bw;
+            float l[3], z;
+            if (cover(s, area, px, py, l, &z))
+              atomicMin(&keys[(py - ty0) * RT + (px - tx0)], ((unsigned long long)__float_as_uint(z) << 32) | id);
+          }
+        }
+      }
+      __syncthreads();
+      const int nq = qn;
+      for (int e = 0; e < nq; e++) {
+        const float* q = queue + QWORDS * e;
+        SV s[3];
+        for (int k = 0; k < 3; k++) s[k] = SV{q[k], q[3 + k], q[6 + k], 0.0f};
+        const float area = edge(s[0].x, s[0].y, s[1].x, s[1].y, s[2].x, s[2].y);
+        const unsigned id = __float_as_uint(q[9]);
+        const int bx0 = __float_as_int(q[10]), by0 = __float_as_int(q[11]);
+        const int bw = __float_as_int(q[12]) - bx0 + 1, npix = bw * (__float_as_int(q[13]) - by0 + 1);
+        for (int p = tid; p < npix; p += RTHREADS) {
+          int px = bx0 + p % bw, py = by0 + p / bw;
+          float l[3], z;
+          if (cover(s, area, px, py, l, &z))
+            atomicMin(&keys[(py - ty0) * RT + (px - tx0)], ((unsigned long long)__float_as_uint(z) << 32) | id);
+        }
+      }
+      __syncthreads();
+      if (tid == 0) qn = 0;
+      __syncthreads();
+    }
+
+    // ---- resolve and shade
+    const int tw = tx1 - tx0, npx = tw * (ty1 - ty0);
+    for (int p = tid; p < npx; p += RTHREADS) {
+      const int px = tx0 + p % tw, py = ty0 + p / tw;
+      const unsigned long long key = keys[(py - ty0) * RT + (px - tx0)];
+      const size_t o = ((size_t)img * A.H + py) * A.W + px;
+      uchar4 c = make_uchar4(184, 199, 219, 255);  // the clear colour (0.72, 0.78, 0.86) in RGBA8
+      float d = A.far_;
+      int sgid = -1;
+      if (key != EMPTY) {
+        const unsigned id = (unsigned)(key & 0xffffffffu);
+        const int t = (int)(id >> 1), sub = (int)(id & 1u);
+        PV v[3], poly[4];
+        int geom;
+        tri_verts<8>(A, t, sg, sa, cp, v, &geom);
+        const int n = clip_near<8>(v, poly, A.near_);
+        (void)n;
+        SV s[3] = {project(poly[0], fx, fy, A), project(poly[1 + sub], fx, fy, A), project(poly[2 + sub], fx, fy, A)};
+        int ord[3] = {0, 1 + sub, 2 + sub};
+        const float area = orient(s, ord);
+        float l[3], z;
+        cover(s, area, px, py, l, &z);
+        float q[3];
+        for (int k = 0; k < 3; k++) q[k] = l[k] / s[k].w;
+        const float Q = (q[0] + q[1]) + q[2];
+        float at[6];  // normal xyz, local xy, linear depth
+        for (int j = 0; j < 5; j++)
+          at[j] = ((q[0] * poly[ord[0]].a[3 + j] + q[1] * poly[ord[1]].a[3 + j]) + q[2] * poly[ord[2]].a[3 + j]) / Q;
+        at[5] = ((q[0] * s[0].w + q[1] * s[1].w) + q[2] * s[2].w) / Q;
+        float len = sqrtf((at[0] * at[0] + at[1] * at[1]) + at[2] * at[2]);
+        const float n0 = at[0] / len, n1 = at[1] / len, n2 = at[2] / len;
+        const float head = fabsf(n2);
+        const float keyl = fmaxf((n0 * A.L0 + n1 * A.L1) + n2 * A.L2, 0.0f);
+        float shade = (0.25f + 0.5f * head) + 0.35f * keyl;
+        const uint32_t flags = __float_as_uint(A.verts[8 * (size_t)A.tris[3 * (size_t)t] + 7]);
+        if (flags & 1u) {
+          const int cx = (int)floorf(at[3] / 0.25f), cy = (int)floorf(at[4] / 0.25f);
+          shade = shade * (((cx + cy) & 1) ? 0.8f : 1.05f);
+        }
+        const float* ap = sa + 8 * geom;
+        unsigned char u[3];
+        for (int k = 0; k < 3; k++) {
+          float x = fminf(fmaxf(ap[k] * shade, 0.0f), 1.0f);
+          u[k] = (unsigned char)(x * 255.0f + 0.5f);
+        }
+        c = make_uchar4(u[0], u[1], u[2], 255);
+        d = at[5];
+        sgid = geom;
+      }
+      ((uchar4*)A.rgba)[o] = c;
+      A.depth[o] = d;
+      A.seg[o] = sgid;
+    }
+    __syncthreads();
+  }
+}
+
+size_t render_smem(int ngeom) {
+  return sizeof(unsigned long long) * RT * RT + sizeof(float) * (QCAP * QWORDS + 20 * (size_t)ngeom + 12);
+}
+
+int rfail(int code, const std::string& msg) {
+  pg::internal_set_error(msg);
+  return code;
+}
+
+#define RCK(x)                                                                                      \
+  do {                                                                                              \
+    cudaError_t _e = (x);                                                                           \
+    if (_e != cudaSuccess) return rfail(PG_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(_e)); \
+  } while (0)
+
+}  // namespace
+
+struct pg_renderer {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int nvert = 0, ntri = 0, ngeom = 0, ncam = 0, nview = 0, W = 0, H = 0, sms = 0, per_sm = 0;
+  float uni[8] = {};
+  float *verts = nullptr, *views = nullptr;
+  uint32_t* tris = nullptr;
+  std::vector<float> base_app;
+  // per-call staging, grown on demand
+  size_t cap_env = 0;
+  float *d_geoms = nullptr, *d_cams = nullptr, *d_app = nullptr;
+  uint8_t* d_rgba = nullptr;
+  float* d_depth = nullptr;
+  int32_t* d_seg = nullptr;
+  size_t default_app_env = 0;  // envs the default appearance in d_app covers
+};
+
+namespace {
+
+void free_staging(pg_renderer* r) {
+  for (void* p : {(void*)r->d_geoms, (void*)r->d_cams, (void*)r->d_app, (void*)r->d_rgba, (void*)r->d_depth,
+                  (void*)r->d_seg})
+    if (p) cudaFree(p);
+  r->d_geoms = r->d_cams = r->d_app = r->d_depth = nullptr;
+  r->d_rgba = nullptr;
+  r->d_seg = nullptr;
+  r->cap_env = 0;
+  r->default_app_env = 0;
+}
+
+int launch(pg_renderer* r, int64_t nenv, const float* geoms, const float* cams, const float* app, uint8_t* rgba,
+           float* depth, int32_t* seg) {
+  if (nenv == 0) return PG_OK;
+  RArgs a;
+  a.verts = r->verts;
+  a.tris = r->tris;
+  a.ntri = r->ntri;
+  a.ngeom = r->ngeom;
+  a.ncam = r->ncam;
+  a.nview = r->nview;
+  a.views = r->views;
+  a.W = r->W;
+  a.H = r->H;
+  a.tiles_x = (r->W + RT - 1) / RT;
+  a.tiles_y = (r->H + RT - 1) / RT;
+  a.near_ = r->uni[0];
+  a.far_ = r->uni[1];
+  a.A = r->uni[2];
+  a.An = r->uni[3];
+  a.L0 = r->uni[4];
+  a.L1 = r->uni[5];
+  a.L2 = r->uni[6];
+  a.geoms = geoms;
+  a.cams = cams;
+  a.app = app;
+  a.nenv = (int)nenv;
+  a.rgba = rgba;
+  a.depth = depth;
+  a.seg = seg;
+  long long items = nenv * r->nview * (long long)a.tiles_x * a.tiles_y;
+  long long blocks = std::min<long long>(items, (long long)r->sms * r->per_sm);
+  render_kernel<<<(unsigned)blocks, RTHREADS, render_smem(r->ngeom), r->stream>>>(a);
+  RCK(cudaGetLastError());
+  return PG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pg_render_create(const float* vertices, int64_t nvert, const uint32_t* triangles, int64_t ntri, int64_t ngeom,
+                     int64_t ncam, const float* views, int64_t nview, const float* base_appearance, int64_t width,
+                     int64_t height, const float* uniforms, int device, pg_renderer** out) {
+  if (!out || !views || !base_appearance || !uniforms) return rfail(PG_ERR_INVALID, "NULL argument");
+  *out = nullptr;
+  if (nvert < 0 || ntri < 0 || ngeom < 0 || ncam < 0 || nview < 1 || width < 1 || height < 1)
+    return rfail(PG_ERR_INVALID, "renderer sizes out of range");
+  if ((nvert > 0 && !vertices) || (ntri > 0 && !triangles)) return rfail(PG_ERR_INVALID, "NULL mesh");
+  if (ntri >= (1ll << 30) || nvert >= (1ll << 31) || width > 16384 || height > 16384 || ngeom >= (1 << 20))
+    return rfail(PG_ERR_UNSUPPORTED, "scene or image too large");
+  for (int64_t i = 0; i < 3 * ntri; i++)
+    if ((int64_t)triangles[i] >= nvert) return rfail(PG_ERR_INVALID, "triangle index out of range");
+  for (int64_t i = 0; i < nvert; i++) {
+    uint32_t g;
+    std::memcpy(&g, vertices + 8 * i + 3, 4);
+    if ((int64_t)g >= ngeom) return rfail(PG_ERR_INVALID, "vertex geom id out of range");
+  }
+  for (int64_t v = 0; v < nview; v++) {
+    float c = views[16 * v];
+    if (!(c == -1.0f || (c >= 0.0f && c < (float)ncam && c == (float)(int)c)))
+      return rfail(PG_ERR_INVALID, "view refers to a camera the scene does not have");
+  }
+  if (!(uniforms[0] > 0.0f) || !(uniforms[1] > uniforms[0])) return rfail(PG_ERR_INVALID, "need 0 < near < far");
+  size_t smem = render_smem((int)ngeom);
+  if (smem > 200 * 1024) return rfail(PG_ERR_UNSUPPORTED, "too many geoms for the renderer's shared memory");
+  pg_renderer* r = new pg_renderer();
+  r->device = device;
+  r->nvert = (int)nvert;
+  r->ntri = (int)ntri;
+  r->ngeom = (int)ngeom;
+  r->ncam = (int)ncam;
+  r->nview = (int)nview;
+  r->W = (int)width;
+  r->H = (int)height;
+  std::memcpy(r->uni, uniforms, sizeof(r->uni));
+  r->base_app.assign(base_appearance, base_appearance + 8 * ngeom);
+  auto bail = [&](int rc) {
+    pg_render_destroy(r);
+    return rc;
+  };
+#define RCKB(x)                                                                                   \
+  do {                                                                                            \
+    cudaError_t _e = (x);                                                                         \
+    if (_e != cudaSuccess) return bail(rfail(PG_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(_e))); \
+  } while (0)
+  RCKB(cudaSetDevice(device));
+  RCKB(cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking));
+  RCKB(cudaMalloc(&r->verts, sizeof(float) * 8 * std::max<int64_t>(nvert, 1)));
+  RCKB(cudaMalloc(&r->tris, sizeof(uint32_t) * 3 * std::max<int64_t>(ntri, 1)));
+  RCKB(cudaMalloc(&r->views, sizeof(float) * 16 * nview));
+  if (nvert) RCKB(cudaMemcpy(r->verts, vertices, sizeof(float) * 8 * nvert, cudaMemcpyHostToDevice));
+  if (ntri) RCKB(cudaMemcpy(r->tris, triangles, sizeof(uint32_t) * 3 * ntri, cudaMemcpyHostToDevice));
+  RCKB(cudaMemcpy(r->views, views, sizeof(float) * 16 * nview, cudaMemcpyHostToDevice));
+  RCKB(cudaFuncSetAttribute(render_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  RCKB(cudaDeviceGetAttribute(&r->sms, cudaDevAttrMultiProcessorCount, device));
+  RCKB(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r->per_sm, render_kernel, RTHREADS, smem));
+  if (r->per_sm < 1) return bail(rfail(PG_ERR_UNSUPPORTED, "renderer block does not fit on an SM"));
+#undef RCKB
+  *out = r;
+  return PG_OK;
+}
+
+int pg_render_destroy(pg_renderer* r) {
+  if (!r) return PG_OK;
+  cudaSetDevice(r->device);
+  if (r->stream) cudaStreamSynchronize(r->stream);
+  free_staging(r);
+  if (r->verts) cudaFree(r->verts);
+  if (r->tris) cudaFree(r->tris);
+  if (r->views) cudaFree(r->views);
+  if (r->stream) cudaStreamDestroy(r->stream);
+  delete r;
+  return PG_OK;
+}
+
+int pg_render_frames(pg_renderer* r, int64_t nenv, const float* geoms, size_t geoms_len, const float* cams,
+                     size_t cams_len, const float* appearance, size_t appearance_len, uint8_t* rgba, float* depth,
+                     int32_t* seg) {
+  if (!r) return rfail(PG_ERR_INVALID, "NULL renderer");
+  if (nenv < 0 || nenv > (1 << 24)) return rfail(PG_ERR_INVALID, "nenv out of range");
+  const size_t ne = (size_t)nenv;
+  if (geoms_len != ne * r->ngeom * 12 || cams_len != ne * r->ncam * 12)
+    return rfail(PG_ERR_LENGTH, "expected " + std::to_string(ne * r->ngeom) + " geom and " +
+                                    std::to_string(ne * r->ncam) + " camera poses");
+  if (appearance && appearance_len != ne * r->ngeom * 8)
+    return rfail(PG_ERR_LENGTH, "expected " + std::to_string(ne * r->ngeom) + " appearance entries");
+  if (nenv == 0) return PG_OK;
+  if ((r->ngeom && !geoms) || (r->ncam && !cams) || !rgba || !depth || !seg) return rfail(PG_ERR_INVALID, "NULL buffer");
+  RCK(cudaSetDevice(r->device));
+  const size_t px = ne * r->nview * (size_t)r->W * r->H;
+  if (ne > r->cap_env) {
+    free_staging(r);
+    RCK(cudaMalloc(&r->d_geoms, sizeof(float) * 12 * std::max<size_t>(ne * r->ngeom, 1)));
+    RCK(cudaMalloc(&r->d_cams, sizeof(float) * 12 * std::max<size_t>(ne * r->ncam, 1)));
+    RCK(cudaMalloc(&r->d_app, sizeof(float) * 8 * std::max<size_t>(ne * r->ngeom, 1)));
+    RCK(cudaMalloc(&r->d_rgba, 4 * px));
+    RCK(cudaMalloc(&r->d_depth, 4 * px));
+    RCK(cudaMalloc(&r->d_seg, 4 * px));
+    r->cap_env = ne;
+  }
+  cudaStream_t s = r->stream;
+  if (r->ngeom) RCK(cudaMemcpyAsync(r->d_geoms, geoms, sizeof(float) * 12 * ne * r->ngeom, cudaMemcpyHostToDevice, s));
+  if (r->ncam) RCK(cudaMemcpyAsync(r->d_cams, cams, sizeof(float) * 12 * ne * r->ncam, cudaMemcpyHostToDevice, s));
+  if (appearance) {
+    RCK(cudaMemcpyAsync(r->d_app, appearance, sizeof(float) * 8 * ne * r->ngeom, cudaMemcpyHostToDevice, s));
+    r->default_app_env = 0;
+  } else if (r->default_app_env < ne && r->ngeom) {
+    std::vector<float> def(8 * ne * r->ngeom);
+    for (size_t e = 0; e < ne; e++) std::copy(r->base_app.begin(), r->base_app.end(), def.begin() + 8 * e * r->ngeom);
+    RCK(cudaMemcpyAsync(r->d_app, def.data(), sizeof(float) * def.size(), cudaMemcpyHostToDevice, s));
+    RCK(cudaStreamSynchronize(s));  // `def` is pageable and about to go
+    r->default_app_env = ne;
+  }
+  int rc = launch(r, nenv, r->d_geoms, r->d_cams, r->d_app, r->d_rgba, r->d_depth, r->d_seg);
+  if (rc) return rc;
+  RCK(cudaMemcpyAsync(rgba, r->d_rgba, 4 * px, cudaMemcpyDeviceToHost, s));
+  RCK(cudaMemcpyAsync(depth, r->d_depth, 4 * px, cudaMemcpyDeviceToHost, s));
+  RCK(cudaMemcpyAsync(seg, r->d_seg, 4 * px, cudaMemcpyDeviceToHost, s));
+  RCK(cudaStreamSynchronize(s));
+  return PG_OK;
+}
+
+int pg_render_frames_device(pg_renderer* r, int64_t nenv, const float* geoms, const float* cams,
+                            const float* appearance, uint8_t* rgba, float* depth, int32_t* seg) {
+  if (!r) return rfail(PG_ERR_INVALID, "NULL renderer");
+  if (nenv < 0 || nenv > (1 << 24)) return rfail(PG_ERR_INVALID, "nenv out of range");
+  if (nenv == 0) return PG_OK;
+  if ((r->ngeom && (!geoms || !appearance)) || (r->ncam && !cams) || !rgba || !depth || !seg)
+    return rfail(PG_ERR_INVALID, "NULL buffer");
+  RCK(cudaSetDevice(r->device));
+  return launch(r, nenv, geoms, cams, appearance, rgba, depth, seg);
+}
+
+void* pg_render_stream(const pg_renderer* r) { return r ? (void*)r->stream : nullptr; }
+
+int pg_render_synchronize(pg_renderer* r) {
+  if (!r) return rfail(PG_ERR_INVALID, "NULL renderer");
+  RCK(cudaSetDevice(r->device));
+  RCK(cudaStreamSynchronize(r->stream));
+  return PG_OK;
+}
+
+}  // extern "C"
