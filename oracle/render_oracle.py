@@ -74,9 +74,10 @@ def _clip_near(P, near):
 
 def _project(p, fx, fy, A, An, W, H):
     w = -p[..., 2]
-    nx = (fx * p[..., 0]) / w
-    ny = (fy * p[..., 1]) / w
-    z = (A * p[..., 2] + An) / w
+    iw = f32(1) / w
+    nx = (fx * p[..., 0]) * iw
+    ny = (fy * p[..., 1]) * iw
+    z = (A * p[..., 2] + An) * iw
     x = (nx + f32(1)) * (f32(0.5) * f32(W))
     y = (f32(1) - ny) * (f32(0.5) * f32(H))
     return x, y, z, w
@@ -148,7 +149,7 @@ def render_image(verts, tris, view, uni, W, H, geoms, app, cams):
             inside = (_owns(e0, x[:, 1], y[:, 1], x[:, 2], y[:, 2]) & _owns(e1, x[:, 2], y[:, 2], x[:, 0], y[:, 0])
                       & _owns(e2, x[:, 0], y[:, 0], x[:, 1], y[:, 1]))
             with np.errstate(all="ignore"):
-                zz = ((e0 / area) * z[:, 0] + (e1 / area) * z[:, 1]) + (e2 / area) * z[:, 2]
+                zz = ((e0 * z[:, 0] + e1 * z[:, 1]) + e2 * z[:, 2]) / area
             inside &= (zz >= 0) & (zz <= 1)
             ids = (2 * tid[r] + sub).astype(np.uint64)[:, None]
             key = (zz.astype(f32).view(np.uint32).astype(np.uint64) << np.uint64(32)) | ids

@@ -1,5 +1,5 @@
 // Batched rasteriser: every (environment, view) image is cut into tiles of
-// 64 x 64 pixels and one block renders one tile at a time (persistent grid,
+// 64 x 64 or 128 x 128 pixels and one block renders one tile at a time (persistent grid,
 // work items handed out in order). A block keeps a visibility buffer for its
 // tile in shared memory: per pixel the 64-bit minimum of (depth bits << 32 |
 // 2 * triangle + sub-triangle), so the nearest fragment wins and equal depths
@@ -31,10 +31,11 @@ void internal_set_error(const std::string& msg);
 
 namespace {
 
-constexpr int RT = 64;            // tile edge, pixels
-constexpr int RTHREADS = 256;     // threads per block
+// Tiles of RT x RT pixels with NT threads: 64 x 64 with 256 threads (three
+// blocks an SM) for images up to 64 pixels, 128 x 128 with 512 threads (one
+// block an SM) above, so that a 128 x 128 image transforms its triangles once
+// rather than once per 64 x 64 tile.
 constexpr int BIG_PIX = 64;       // bounding boxes above this many pixels are scanned by the whole block
-constexpr int QCAP = 2 * RTHREADS;  // queue entries: at most two sub-triangles per thread per round
 constexpr int QWORDS = 14;        // x[3], y[3], z[3], id, x0, y0, x1, y1
 constexpr unsigned long long EMPTY = ~0ull;
 
@@ -111,8 +112,9 @@ struct SV {  // screen-space vertex
 __device__ __forceinline__ SV project(const PV& p, float fx, float fy, const RArgs& A) {
   SV s;
   s.w = -p.a[2];
-  float nx = (fx * p.a[0]) / s.w, ny = (fy * p.a[1]) / s.w;
-  s.z = (A.A * p.a[2] + A.An) / s.w;
+  const float iw = 1.0f / s.w;
+  float nx = (fx * p.a[0]) * iw, ny = (fy * p.a[1]) * iw;
+  s.z = (A.A * p.a[2] + A.An) * iw;
   s.x = (nx + 1.0f) * (0.5f * (float)A.W);
   s.y = (1.0f - ny) * (0.5f * (float)A.H);
   return s;
@@ -144,20 +146,28 @@ __device__ __forceinline__ float orient(SV* s, int* ord) {
   return area;
 }
 
-// coverage and NDC depth of pixel (px, py); false when not covered or outside [0, 1]
-__device__ __forceinline__ bool cover(const SV* s, float area, int px, int py, float* l, float* z) {
+// edge functions of pixel (px, py); false when its centre is not covered
+__device__ __forceinline__ bool cover(const SV* s, int px, int py, float* e) {
   float X = (float)px + 0.5f, Y = (float)py + 0.5f;
-  float e0 = edge(s[1].x, s[1].y, s[2].x, s[2].y, X, Y);
-  float e1 = edge(s[2].x, s[2].y, s[0].x, s[0].y, X, Y);
-  float e2 = edge(s[0].x, s[0].y, s[1].x, s[1].y, X, Y);
-  if (!owns(e0, s[1].x, s[1].y, s[2].x, s[2].y) || !owns(e1, s[2].x, s[2].y, s[0].x, s[0].y) ||
-      !owns(e2, s[0].x, s[0].y, s[1].x, s[1].y))
-    return false;
-  l[0] = e0 / area;
-  l[1] = e1 / area;
-  l[2] = e2 / area;
-  *z = (l[0] * s[0].z + l[1] * s[1].z) + l[2] * s[2].z;
-  return *z >= 0.0f && *z <= 1.0f;
+  e[0] = edge(s[1].x, s[1].y, s[2].x, s[2].y, X, Y);
+  e[1] = edge(s[2].x, s[2].y, s[0].x, s[0].y, X, Y);
+  e[2] = edge(s[0].x, s[0].y, s[1].x, s[1].y, X, Y);
+  return owns(e[0], s[1].x, s[1].y, s[2].x, s[2].y) && owns(e[1], s[2].x, s[2].y, s[0].x, s[0].y) &&
+         owns(e[2], s[0].x, s[0].y, s[1].x, s[1].y);
+}
+
+// NDC depth of a covered pixel, interpolated linearly in screen space
+__device__ __forceinline__ float ndc_depth(const SV* s, float area, const float* e) {
+  return ((e[0] * s[0].z + e[1] * s[1].z) + e[2] * s[2].z) / area;
+}
+
+// visibility key of pixel (px, py), or EMPTY
+__device__ __forceinline__ unsigned long long frag_key(const SV* s, float area, int px, int py, unsigned id) {
+  float e[3];
+  if (!cover(s, px, py, e)) return EMPTY;
+  const float z = ndc_depth(s, area, e);
+  if (!(z >= 0.0f && z <= 1.0f)) return EMPTY;
+  return ((unsigned long long)__float_as_uint(z) << 32) | id;
 }
 
 __device__ __forceinline__ void bbox(const SV* s, int tx0, int ty0, int tx1, int ty1, int* b) {
@@ -195,7 +205,48 @@ __device__ __forceinline__ bool tri_verts(const RArgs& A, int t, const float* sg
   return true;
 }
 
-__global__ void __launch_bounds__(RTHREADS) render_kernel(RArgs A) {
+// true when all three vertices lie on the visible side of the near plane:
+// clipping then returns the triangle itself, in the same order
+__device__ __forceinline__ bool in_front(const PV* v, float near_) {
+  return (-v[0].a[2]) - near_ >= 0.0f && (-v[1].a[2]) - near_ >= 0.0f && (-v[2].a[2]) - near_ >= 0.0f;
+}
+
+// one sub-triangle into the tile's visibility buffer: scanned by its own
+// thread when its bounding box is small, else queued for the whole block
+template <int RT>
+__device__ __forceinline__ void raster_sub(SV s0, SV s1, SV s2, unsigned id, int tx0, int ty0, int tx1, int ty1,
+                                           unsigned long long* keys, float* queue, int* qn) {
+  SV s[3] = {s0, s1, s2};
+  int ord[3] = {0, 1, 2};
+  const float area = orient(s, ord);
+  if (!(area > 0.0f)) return;
+  int b[4];
+  bbox(s, tx0, ty0, tx1, ty1, b);
+  if (b[0] > b[2] || b[1] > b[3]) return;
+  const int bw = b[2] - b[0] + 1, npix = bw * (b[3] - b[1] + 1);
+  if (npix > BIG_PIX) {
+    float* q = queue + QWORDS * atomicAdd(qn, 1);
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      q[k] = s[k].x;
+      q[3 + k] = s[k].y;
+      q[6 + k] = s[k].z;
+    }
+    q[9] = __uint_as_float(id);
+#pragma unroll
+    for (int k = 0; k < 4; k++) q[10 + k] = __int_as_float(b[k]);
+    return;
+  }
+  for (int p = 0; p < npix; p++) {
+    const int px = b[0] + p % bw, py = b[1] + p / bw;
+    const unsigned long long k = frag_key(s, area, px, py, id);
+    if (k != EMPTY) atomicMin(&keys[(py - ty0) * RT + (px - tx0)], k);
+  }
+}
+
+template <int RT, int NT>
+__global__ void __launch_bounds__(NT, RT == 64 ? 3 : 1) render_kernel(RArgs A) {
+  constexpr int QCAP = 2 * NT;  // queue entries: at most two sub-triangles per thread per round
   extern __shared__ __align__(16) unsigned char smem[];
   unsigned long long* keys = (unsigned long long*)smem;
   float* queue = (float*)(keys + RT * RT);
@@ -215,77 +266,59 @@ __global__ void __launch_bounds__(RTHREADS) render_kernel(RArgs A) {
     const float* vw = A.views + 16 * view;
     const int cam = (int)vw[0];
     const float fx = vw[1], fy = vw[2];
-    for (int i = tid; i < 12 * A.ngeom; i += RTHREADS) sg[i] = A.geoms[(size_t)env * A.ngeom * 12 + i];
-    for (int i = tid; i < 8 * A.ngeom; i += RTHREADS) sa[i] = A.app[(size_t)env * A.ngeom * 8 + i];
+    for (int i = tid; i < 12 * A.ngeom; i += NT) sg[i] = A.geoms[(size_t)env * A.ngeom * 12 + i];
+    for (int i = tid; i < 8 * A.ngeom; i += NT) sa[i] = A.app[(size_t)env * A.ngeom * 8 + i];
     if (tid < 12) cp[tid] = cam >= 0 ? A.cams[((size_t)env * A.ncam + cam) * 12 + tid] : vw[4 + tid];
-    for (int i = tid; i < RT * RT; i += RTHREADS) keys[i] = EMPTY;
+    for (int i = tid; i < RT * RT; i += NT) keys[i] = EMPTY;
     if (tid == 0) qn = 0;
     __syncthreads();
 
     // ---- visibility
-    for (int base = 0; base < A.ntri; base += RTHREADS) {
+    for (int base = 0; base < A.ntri; base += NT) {
       const int t = base + tid;
-      PV v[3], poly[4];
+      PV v[3];
       int geom;
       if (t < A.ntri && tri_verts<3>(A, t, sg, sa, cp, v, &geom)) {
-        int n = clip_near<3>(v, poly, A.near_);
-        SV ps[4];
-        for (int k = 0; k < n; k++) ps[k] = project(poly[k], fx, fy, A);
-        for (int sub = 0; sub + 3 <= n; sub++) {
-          SV s[3] = {ps[0], ps[1 + sub], ps[2 + sub]};
-          int ord[3] = {0, 1, 2};
-          float area = orient(s, ord);
-          if (!(area > 0.0f)) continue;
-          int b[4];
-          bbox(s, tx0, ty0, tx1, ty1, b);
-          if (b[0] > b[2] || b[1] > b[3]) continue;
-          const unsigned id = 2u * (unsigned)t + (unsigned)sub;
-          const int bw = b[2] - b[0] + 1, npix = bw * (b[3] - b[1] + 1);
-          if (npix > BIG_PIX) {
-            int slot = atomicAdd(&qn, 1);
-            float* q = queue + QWORDS * slot;
-            for (int k = 0; k < 3; k++) {
-              q[k] = s[k].x;
-              q[3 + k] = s[k].y;
-              q[6 + k] = s[k].z;
-            }
-            q[9] = __uint_as_float(id);
-            for (int k = 0; k < 4; k++) q[10 + k] = __int_as_float(b[k]);
-            continue;
-          }
-          for (int p = 0; p < npix; p++) {
-            int px = b[0] + p % bw, py = b[1] + p / bw;
-            float l[3], z;
-            if (cover(s, area, px, py, l, &z))
-              atomicMin(&keys[(py - ty0) * RT + (px - tx0)], ((unsigned long long)__float_as_uint(z) << 32) | id);
+        if (in_front(v, A.near_)) {
+          raster_sub<RT>(project(v[0], fx, fy, A), project(v[1], fx, fy, A), project(v[2], fx, fy, A), 2u * t, tx0,
+                         ty0, tx1, ty1, keys, queue, &qn);
+        } else {
+          PV poly[4];
+          const int n = clip_near<3>(v, poly, A.near_);
+          if (n >= 3) {
+            const SV p0 = project(poly[0], fx, fy, A), p2 = project(poly[2], fx, fy, A);
+            raster_sub<RT>(p0, project(poly[1], fx, fy, A), p2, 2u * t, tx0, ty0, tx1, ty1, keys, queue, &qn);
+            if (n == 4)
+              raster_sub<RT>(p0, p2, project(poly[3], fx, fy, A), 2u * t + 1u, tx0, ty0, tx1, ty1, keys, queue, &qn);
           }
         }
       }
       __syncthreads();
-      const int nq = qn;
-      for (int e = 0; e < nq; e++) {
-        const float* q = queue + QWORDS * e;
-        SV s[3];
-        for (int k = 0; k < 3; k++) s[k] = SV{q[k], q[3 + k], q[6 + k], 0.0f};
-        const float area = edge(s[0].x, s[0].y, s[1].x, s[1].y, s[2].x, s[2].y);
-        const unsigned id = __float_as_uint(q[9]);
-        const int bx0 = __float_as_int(q[10]), by0 = __float_as_int(q[11]);
-        const int bw = __float_as_int(q[12]) - bx0 + 1, npix = bw * (__float_as_int(q[13]) - by0 + 1);
-        for (int p = tid; p < npix; p += RTHREADS) {
-          int px = bx0 + p % bw, py = by0 + p / bw;
-          float l[3], z;
-          if (cover(s, area, px, py, l, &z))
-            atomicMin(&keys[(py - ty0) * RT + (px - tx0)], ((unsigned long long)__float_as_uint(z) << 32) | id);
+      const int nq = qn;  // the same value in every thread: the branch below is uniform
+      if (nq > 0) {
+        for (int e = 0; e < nq; e++) {
+          const float* q = queue + QWORDS * e;
+          SV s[3];
+          for (int k = 0; k < 3; k++) s[k] = SV{q[k], q[3 + k], q[6 + k], 0.0f};
+          const float area = edge(s[0].x, s[0].y, s[1].x, s[1].y, s[2].x, s[2].y);
+          const unsigned id = __float_as_uint(q[9]);
+          const int bx0 = __float_as_int(q[10]), by0 = __float_as_int(q[11]);
+          const int bw = __float_as_int(q[12]) - bx0 + 1, npix = bw * (__float_as_int(q[13]) - by0 + 1);
+          for (int p = tid; p < npix; p += NT) {
+            const int px = bx0 + p % bw, py = by0 + p / bw;
+            const unsigned long long k = frag_key(s, area, px, py, id);
+            if (k != EMPTY) atomicMin(&keys[(py - ty0) * RT + (px - tx0)], k);
+          }
         }
+        __syncthreads();
+        if (tid == 0) qn = 0;
+        __syncthreads();
       }
-      __syncthreads();
-      if (tid == 0) qn = 0;
-      __syncthreads();
     }
 
     // ---- resolve and shade
     const int tw = tx1 - tx0, npx = tw * (ty1 - ty0);
-    for (int p = tid; p < npx; p += RTHREADS) {
+    for (int p = tid; p < npx; p += NT) {
       const int px = tx0 + p % tw, py = ty0 + p / tw;
       const unsigned long long key = keys[(py - ty0) * RT + (px - tx0)];
       const size_t o = ((size_t)img * A.H + py) * A.W + px;
@@ -295,24 +328,43 @@ __global__ void __launch_bounds__(RTHREADS) render_kernel(RArgs A) {
       if (key != EMPTY) {
         const unsigned id = (unsigned)(key & 0xffffffffu);
         const int t = (int)(id >> 1), sub = (int)(id & 1u);
-        PV v[3], poly[4];
+        PV v[3];
         int geom;
         tri_verts<8>(A, t, sg, sa, cp, v, &geom);
-        const int n = clip_near<8>(v, poly, A.near_);
-        (void)n;
-        SV s[3] = {project(poly[0], fx, fy, A), project(poly[1 + sub], fx, fy, A), project(poly[2 + sub], fx, fy, A)};
-        int ord[3] = {0, 1 + sub, 2 + sub};
-        const float area = orient(s, ord);
-        float l[3], z;
-        cover(s, area, px, py, l, &z);
+        PV a0, a1, a2;
+        if (in_front(v, A.near_)) {
+          a0 = v[0];
+          a1 = v[1];
+          a2 = v[2];
+        } else {
+          PV poly[4];
+          clip_near<8>(v, poly, A.near_);
+          a0 = poly[0];
+          a1 = sub ? poly[2] : poly[1];
+          a2 = sub ? poly[3] : poly[2];
+        }
+        SV s[3] = {project(a0, fx, fy, A), project(a1, fx, fy, A), project(a2, fx, fy, A)};
+        float area = edge(s[0].x, s[0].y, s[1].x, s[1].y, s[2].x, s[2].y);
+        if (area < 0.0f) {  // the orientation the visibility pass used
+          const SV ts = s[1];
+          s[1] = s[2];
+          s[2] = ts;
+          const PV ta = a1;
+          a1 = a2;
+          a2 = ta;
+          area = edge(s[0].x, s[0].y, s[1].x, s[1].y, s[2].x, s[2].y);
+        }
+        float e[3];
+        cover(s, px, py, e);
         float q[3];
-        for (int k = 0; k < 3; k++) q[k] = l[k] / s[k].w;
+#pragma unroll
+        for (int k = 0; k < 3; k++) q[k] = (e[k] / area) / s[k].w;
         const float Q = (q[0] + q[1]) + q[2];
         float at[6];  // normal xyz, local xy, linear depth
-        for (int j = 0; j < 5; j++)
-          at[j] = ((q[0] * poly[ord[0]].a[3 + j] + q[1] * poly[ord[1]].a[3 + j]) + q[2] * poly[ord[2]].a[3 + j]) / Q;
+#pragma unroll
+        for (int j = 0; j < 5; j++) at[j] = ((q[0] * a0.a[3 + j] + q[1] * a1.a[3 + j]) + q[2] * a2.a[3 + j]) / Q;
         at[5] = ((q[0] * s[0].w + q[1] * s[1].w) + q[2] * s[2].w) / Q;
-        float len = sqrtf((at[0] * at[0] + at[1] * at[1]) + at[2] * at[2]);
+        const float len = sqrtf((at[0] * at[0] + at[1] * at[1]) + at[2] * at[2]);
         const float n0 = at[0] / len, n1 = at[1] / len, n2 = at[2] / len;
         const float head = fabsf(n2);
         const float keyl = fmaxf((n0 * A.L0 + n1 * A.L1) + n2 * A.L2, 0.0f);
@@ -324,8 +376,9 @@ __global__ void __launch_bounds__(RTHREADS) render_kernel(RArgs A) {
         }
         const float* ap = sa + 8 * geom;
         unsigned char u[3];
+#pragma unroll
         for (int k = 0; k < 3; k++) {
-          float x = fminf(fmaxf(ap[k] * shade, 0.0f), 1.0f);
+          const float x = fminf(fmaxf(ap[k] * shade, 0.0f), 1.0f);
           u[k] = (unsigned char)(x * 255.0f + 0.5f);
         }
         c = make_uchar4(u[0], u[1], u[2], 255);
@@ -340,8 +393,8 @@ __global__ void __launch_bounds__(RTHREADS) render_kernel(RArgs A) {
   }
 }
 
-size_t render_smem(int ngeom) {
-  return sizeof(unsigned long long) * RT * RT + sizeof(float) * (QCAP * QWORDS + 20 * (size_t)ngeom + 12);
+size_t render_smem(int rt, int nt, int ngeom) {
+  return sizeof(unsigned long long) * rt * rt + sizeof(float) * (2 * (size_t)nt * QWORDS + 20 * (size_t)ngeom + 12);
 }
 
 int rfail(int code, const std::string& msg) {
@@ -361,6 +414,7 @@ struct pg_renderer {
   int device = 0;
   cudaStream_t stream = nullptr;
   int nvert = 0, ntri = 0, ngeom = 0, ncam = 0, nview = 0, W = 0, H = 0, sms = 0, per_sm = 0;
+  int rt = 64, nt = 256;  // tile edge and threads per block
   float uni[8] = {};
   float *verts = nullptr, *views = nullptr;
   uint32_t* tris = nullptr;
@@ -400,8 +454,8 @@ int launch(pg_renderer* r, int64_t nenv, const float* geoms, const float* cams, 
   a.views = r->views;
   a.W = r->W;
   a.H = r->H;
-  a.tiles_x = (r->W + RT - 1) / RT;
-  a.tiles_y = (r->H + RT - 1) / RT;
+  a.tiles_x = (r->W + r->rt - 1) / r->rt;
+  a.tiles_y = (r->H + r->rt - 1) / r->rt;
   a.near_ = r->uni[0];
   a.far_ = r->uni[1];
   a.A = r->uni[2];
@@ -418,7 +472,11 @@ int launch(pg_renderer* r, int64_t nenv, const float* geoms, const float* cams, 
   a.seg = seg;
   long long items = nenv * r->nview * (long long)a.tiles_x * a.tiles_y;
   long long blocks = std::min<long long>(items, (long long)r->sms * r->per_sm);
-  render_kernel<<<(unsigned)blocks, RTHREADS, render_smem(r->ngeom), r->stream>>>(a);
+  const size_t smem = render_smem(r->rt, r->nt, r->ngeom);
+  if (r->rt == 128)
+    render_kernel<128, 512><<<(unsigned)blocks, 512, smem, r->stream>>>(a);
+  else
+    render_kernel<64, 256><<<(unsigned)blocks, 256, smem, r->stream>>>(a);
   RCK(cudaGetLastError());
   return PG_OK;
 }
@@ -450,8 +508,10 @@ int pg_render_create(const float* vertices, int64_t nvert, const uint32_t* trian
       return rfail(PG_ERR_INVALID, "view refers to a camera the scene does not have");
   }
   if (!(uniforms[0] > 0.0f) || !(uniforms[1] > uniforms[0])) return rfail(PG_ERR_INVALID, "need 0 < near < far");
-  size_t smem = render_smem((int)ngeom);
-  if (smem > 200 * 1024) return rfail(PG_ERR_UNSUPPORTED, "too many geoms for the renderer's shared memory");
+  const size_t smem_limit = 227 * 1024;
+  const bool large = (width > 64 || height > 64) && render_smem(128, 512, (int)ngeom) <= smem_limit;
+  const size_t smem = large ? render_smem(128, 512, (int)ngeom) : render_smem(64, 256, (int)ngeom);
+  if (smem > smem_limit) return rfail(PG_ERR_UNSUPPORTED, "too many geoms for the renderer's shared memory");
   pg_renderer* r = new pg_renderer();
   r->device = device;
   r->nvert = (int)nvert;
@@ -461,6 +521,8 @@ int pg_render_create(const float* vertices, int64_t nvert, const uint32_t* trian
   r->nview = (int)nview;
   r->W = (int)width;
   r->H = (int)height;
+  r->rt = large ? 128 : 64;
+  r->nt = large ? 512 : 256;
   std::memcpy(r->uni, uniforms, sizeof(r->uni));
   r->base_app.assign(base_appearance, base_appearance + 8 * ngeom);
   auto bail = [&](int rc) {
@@ -480,9 +542,14 @@ int pg_render_create(const float* vertices, int64_t nvert, const uint32_t* trian
   if (nvert) RCKB(cudaMemcpy(r->verts, vertices, sizeof(float) * 8 * nvert, cudaMemcpyHostToDevice));
   if (ntri) RCKB(cudaMemcpy(r->tris, triangles, sizeof(uint32_t) * 3 * ntri, cudaMemcpyHostToDevice));
   RCKB(cudaMemcpy(r->views, views, sizeof(float) * 16 * nview, cudaMemcpyHostToDevice));
-  RCKB(cudaFuncSetAttribute(render_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   RCKB(cudaDeviceGetAttribute(&r->sms, cudaDevAttrMultiProcessorCount, device));
-  RCKB(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r->per_sm, render_kernel, RTHREADS, smem));
+  if (large) {
+    RCKB(cudaFuncSetAttribute(render_kernel<128, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    RCKB(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r->per_sm, render_kernel<128, 512>, 512, smem));
+  } else {
+    RCKB(cudaFuncSetAttribute(render_kernel<64, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    RCKB(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r->per_sm, render_kernel<64, 256>, 256, smem));
+  }
   if (r->per_sm < 1) return bail(rfail(PG_ERR_UNSUPPORTED, "renderer block does not fit on an SM"));
 #undef RCKB
   *out = r;
