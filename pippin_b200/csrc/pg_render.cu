@@ -173,11 +173,12 @@ __device__ __forceinline__ unsigned long long frag_key(const SV* s, float area, 
 __device__ __forceinline__ void bbox(const SV* s, int tx0, int ty0, int tx1, int ty1, int* b) {
   float mnx = fminf(fminf(s[0].x, s[1].x), s[2].x), mxx = fmaxf(fmaxf(s[0].x, s[1].x), s[2].x);
   float mny = fminf(fminf(s[0].y, s[1].y), s[2].y), mxy = fmaxf(fmaxf(s[0].y, s[1].y), s[2].y);
-  // pixel centres x + 0.5 in [mnx, mxx]: x in [floor(mnx - 0.5), floor(mxx - 0.5)], widened by one
-  b[0] = max(tx0, (int)floorf(fmaxf(mnx, -2.0f)) - 1);
-  b[1] = max(ty0, (int)floorf(fmaxf(mny, -2.0f)) - 1);
-  b[2] = min(tx1 - 1, (int)floorf(fminf(mxx, 1.0e6f)));
-  b[3] = min(ty1 - 1, (int)floorf(fminf(mxy, 1.0e6f)));
+  // pixel centres x + 0.5 in [mnx, mxx]: x in [ceil(mnx - 0.5), floor(mxx - 0.5)], widened by a quarter
+  // pixel on each side, far more than the rounding of the edge functions can move an edge
+  b[0] = max(tx0, (int)ceilf(fmaxf(mnx, -2.0f) - 0.75f));
+  b[1] = max(ty0, (int)ceilf(fmaxf(mny, -2.0f) - 0.75f));
+  b[2] = min(tx1 - 1, (int)floorf(fminf(mxx, 1.0e6f) - 0.25f));
+  b[3] = min(ty1 - 1, (int)floorf(fminf(mxy, 1.0e6f) - 0.25f));
 }
 
 // triangle t's vertices in camera space (K = 3: position only; K = 8: with
