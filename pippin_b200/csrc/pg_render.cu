@@ -18,6 +18,8 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -32,15 +34,16 @@ void internal_set_error(const std::string& msg);
 namespace {
 
 // Tiles of RT x RT pixels with NT threads: 64 x 64 with 256 threads (three
-// blocks an SM) for images up to 64 pixels, 128 x 128 with 512 threads (one
-// block an SM) above, so that a 128 x 128 image transforms its triangles once
-// rather than once per 64 x 64 tile.
+// blocks an SM), or 128 x 128 with 512 threads (one block an SM) for images
+// that fit in one such tile, so that they set up their triangles once. Each
+// tile first culls the geoms whose bounding spheres cannot reach it.
 constexpr int BIG_PIX = 64;       // bounding boxes above this many pixels are scanned by the whole block
 constexpr int QWORDS = 14;        // x[3], y[3], z[3], id, x0, y0, x1, y1
 constexpr unsigned long long EMPTY = ~0ull;
 
 struct RArgs {
   const float* verts;
+  const float* radius;  // per geom: the largest vertex distance from its origin, at unit scale
   const uint32_t* tris;
   int ntri, ngeom, ncam, nview;
   const float* views;
@@ -185,7 +188,7 @@ __device__ __forceinline__ void bbox(const SV* s, int tx0, int ty0, int tx1, int
 // normal and local xy); false when its geom is hidden in this environment
 template <int K>
 __device__ __forceinline__ bool tri_verts(const RArgs& A, int t, const float* sg, const float* sa, const float* cp,
-                                          PV* v, int* geom) {
+                                          PV* v, int* geom, const float* seen = nullptr) {
   const uint32_t* ix = A.tris + 3 * (size_t)t;
   const float* v0 = A.verts + 8 * (size_t)ix[0];
   int g = (int)__float_as_uint(v0[3]);
@@ -193,6 +196,7 @@ __device__ __forceinline__ bool tri_verts(const RArgs& A, int t, const float* sg
   const float* gp = sg + 12 * g;
   const float* ap = sa + 8 * g;
   if (!(ap[3] > 0.0f)) return false;
+  if (seen && seen[g] == 0.0f) return false;
 #pragma unroll
   for (int k = 0; k < 3; k++) {
     const float* vv = A.verts + 8 * (size_t)ix[k];
@@ -204,6 +208,32 @@ __device__ __forceinline__ bool tri_verts(const RArgs& A, int t, const float* sg
     }
   }
   return true;
+}
+
+// 1 when geom g's bounding sphere may reach pixels of the tile [tx0, tx1) x
+// [ty0, ty1), else 0: a camera-space box around the sphere is projected
+// through its corners (x / w is monotonic in x and in w on each side) and
+// widened by two pixels; a sphere reaching the near plane is always kept.
+// Only skips work: a kept geom is drawn exactly as without the test.
+__device__ __forceinline__ float geom_seen(const RArgs& A, int g, const float* sg, const float* sa, const float* cp,
+                                           float fx, float fy, int tx0, int ty0, int tx1, int ty1) {
+  const float* gp = sg + 12 * g;
+  const float* ap = sa + 8 * g;
+  const float sc = fmaxf(fmaxf(fabsf(ap[4]), fabsf(ap[5])), fabsf(ap[6]));
+  const float r = A.radius[g] * sc * 1.001f + 1e-5f;
+  const float d0 = gp[0] - cp[0], d1 = gp[1] - cp[1], d2 = gp[2] - cp[2];
+  const float x = (cp[3] * d0 + cp[6] * d1) + cp[9] * d2;
+  const float y = (cp[4] * d0 + cp[7] * d1) + cp[10] * d2;
+  const float w = -((cp[5] * d0 + cp[8] * d1) + cp[11] * d2);
+  if (!(w - r > 2.0f * A.near_)) return 1.0f;
+  const float w0 = w - r, w1 = w + r;
+  const float nx0 = fminf(fx * (x - r) / w0, fx * (x - r) / w1), nx1 = fmaxf(fx * (x + r) / w0, fx * (x + r) / w1);
+  const float ny0 = fminf(fy * (y - r) / w0, fy * (y - r) / w1), ny1 = fmaxf(fy * (y + r) / w0, fy * (y + r) / w1);
+  const float sx0 = (nx0 + 1.0f) * (0.5f * (float)A.W) - 2.0f, sx1 = (nx1 + 1.0f) * (0.5f * (float)A.W) + 2.0f;
+  const float sy0 = (1.0f - ny1) * (0.5f * (float)A.H) - 2.0f, sy1 = (1.0f - ny0) * (0.5f * (float)A.H) + 2.0f;
+  if (!(sx0 == sx0 && sx1 == sx1 && sy0 == sy0 && sy1 == sy1)) return 1.0f;  // NaN: keep
+  const bool out = sx1 < (float)tx0 || sx0 > (float)tx1 || sy1 < (float)ty0 || sy0 > (float)ty1;
+  return out ? 0.0f : 1.0f;
 }
 
 // true when all three vertices lie on the visible side of the near plane:
@@ -254,6 +284,7 @@ __global__ void __launch_bounds__(NT, RT == 64 ? 3 : 1) render_kernel(RArgs A) {
   float* sg = queue + QCAP * QWORDS;  // this env's geom poses
   float* sa = sg + 12 * A.ngeom;      // and appearance
   float* cp = sa + 8 * A.ngeom;       // the view's camera pose
+  float* seen = cp + 12;              // per geom: may reach this tile
   __shared__ int qn;
   const int tid = threadIdx.x;
   const int tiles = A.tiles_x * A.tiles_y;
@@ -273,13 +304,15 @@ __global__ void __launch_bounds__(NT, RT == 64 ? 3 : 1) render_kernel(RArgs A) {
     for (int i = tid; i < RT * RT; i += NT) keys[i] = EMPTY;
     if (tid == 0) qn = 0;
     __syncthreads();
+    for (int g = tid; g < A.ngeom; g += NT) seen[g] = geom_seen(A, g, sg, sa, cp, fx, fy, tx0, ty0, tx1, ty1);
+    __syncthreads();
 
     // ---- visibility
     for (int base = 0; base < A.ntri; base += NT) {
       const int t = base + tid;
       PV v[3];
       int geom;
-      if (t < A.ntri && tri_verts<3>(A, t, sg, sa, cp, v, &geom)) {
+      if (t < A.ntri && tri_verts<3>(A, t, sg, sa, cp, v, &geom, seen)) {
         if (in_front(v, A.near_)) {
           raster_sub<RT>(project(v[0], fx, fy, A), project(v[1], fx, fy, A), project(v[2], fx, fy, A), 2u * t, tx0,
                          ty0, tx1, ty1, keys, queue, &qn);
@@ -395,7 +428,7 @@ __global__ void __launch_bounds__(NT, RT == 64 ? 3 : 1) render_kernel(RArgs A) {
 }
 
 size_t render_smem(int rt, int nt, int ngeom) {
-  return sizeof(unsigned long long) * rt * rt + sizeof(float) * (2 * (size_t)nt * QWORDS + 20 * (size_t)ngeom + 12);
+  return sizeof(unsigned long long) * rt * rt + sizeof(float) * (2 * (size_t)nt * QWORDS + 21 * (size_t)ngeom + 12);
 }
 
 int rfail(int code, const std::string& msg) {
@@ -417,7 +450,7 @@ struct pg_renderer {
   int nvert = 0, ntri = 0, ngeom = 0, ncam = 0, nview = 0, W = 0, H = 0, sms = 0, per_sm = 0;
   int rt = 64, nt = 256;  // tile edge and threads per block
   float uni[8] = {};
-  float *verts = nullptr, *views = nullptr;
+  float *verts = nullptr, *views = nullptr, *radius = nullptr;
   uint32_t* tris = nullptr;
   std::vector<float> base_app;
   // per-call staging, grown on demand
@@ -447,6 +480,7 @@ int launch(pg_renderer* r, int64_t nenv, const float* geoms, const float* cams, 
   if (nenv == 0) return PG_OK;
   RArgs a;
   a.verts = r->verts;
+  a.radius = r->radius;
   a.tris = r->tris;
   a.ntri = r->ntri;
   a.ngeom = r->ngeom;
@@ -510,7 +544,15 @@ int pg_render_create(const float* vertices, int64_t nvert, const uint32_t* trian
   }
   if (!(uniforms[0] > 0.0f) || !(uniforms[1] > uniforms[0])) return rfail(PG_ERR_INVALID, "need 0 < near < far");
   const size_t smem_limit = 227 * 1024;
-  const bool large = (width > 64 || height > 64) && render_smem(128, 512, (int)ngeom) <= smem_limit;
+  // One 128 x 128 tile for images above 64 pixels that fit in it (the image's
+  // triangles are set up once instead of once per 64 x 64 tile); 64 x 64 tiles
+  // otherwise, where the per-tile geom culling skips most triangles (Ant at
+  // 256 x 256: 88k frames/s against 69k with 128 x 128 tiles).
+  // PIPPIN_RENDER_TILE=64 or 128 overrides the choice.
+  const char* tile_env = std::getenv("PIPPIN_RENDER_TILE");
+  const bool fits128 = width <= 128 && height <= 128 && (width > 64 || height > 64);
+  const int want = tile_env ? std::atoi(tile_env) : (fits128 ? 128 : 64);
+  const bool large = want == 128 && render_smem(128, 512, (int)ngeom) <= smem_limit;
   const size_t smem = large ? render_smem(128, 512, (int)ngeom) : render_smem(64, 256, (int)ngeom);
   if (smem > smem_limit) return rfail(PG_ERR_UNSUPPORTED, "too many geoms for the renderer's shared memory");
   pg_renderer* r = new pg_renderer();
@@ -543,6 +585,17 @@ int pg_render_create(const float* vertices, int64_t nvert, const uint32_t* trian
   if (nvert) RCKB(cudaMemcpy(r->verts, vertices, sizeof(float) * 8 * nvert, cudaMemcpyHostToDevice));
   if (ntri) RCKB(cudaMemcpy(r->tris, triangles, sizeof(uint32_t) * 3 * ntri, cudaMemcpyHostToDevice));
   RCKB(cudaMemcpy(r->views, views, sizeof(float) * 16 * nview, cudaMemcpyHostToDevice));
+  {
+    std::vector<float> rad(std::max<int64_t>(ngeom, 1), 0.0f);
+    for (int64_t i = 0; i < nvert; i++) {
+      uint32_t g;
+      std::memcpy(&g, vertices + 8 * i + 3, 4);
+      const float* p = vertices + 8 * i;
+      rad[g] = std::max(rad[g], std::sqrt(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]));
+    }
+    RCKB(cudaMalloc(&r->radius, sizeof(float) * rad.size()));
+    RCKB(cudaMemcpy(r->radius, rad.data(), sizeof(float) * rad.size(), cudaMemcpyHostToDevice));
+  }
   RCKB(cudaDeviceGetAttribute(&r->sms, cudaDevAttrMultiProcessorCount, device));
   if (large) {
     RCKB(cudaFuncSetAttribute(render_kernel<128, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -565,6 +618,7 @@ int pg_render_destroy(pg_renderer* r) {
   if (r->verts) cudaFree(r->verts);
   if (r->tris) cudaFree(r->tris);
   if (r->views) cudaFree(r->views);
+  if (r->radius) cudaFree(r->radius);
   if (r->stream) cudaStreamDestroy(r->stream);
   delete r;
   return PG_OK;

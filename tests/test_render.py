@@ -218,7 +218,7 @@ def test_cuda_renderer_passes_the_reference_analytic_tests(check):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("w,h,seed", [(48, 40, 0), (96, 80, 1), (130, 70, 2)])
+@pytest.mark.parametrize("w,h,seed", [(48, 40, 0), (96, 80, 1), (130, 70, 2), (200, 150, 3)])
 def test_cuda_renderer_matches_the_oracle_bit_for_bit(w, h, seed):
     rng = np.random.default_rng(seed)
     sc = random_scene(rng)
