@@ -676,6 +676,8 @@ def run_render(args):
         for _ in range(W):
             frame()
         r.synchronize()
+        clocks = ClockSampler(0)
+        clocks.start()
         total = 0.0
         for k in range(K):
             flush.fill_(float(k))
@@ -687,6 +689,7 @@ def run_render(args):
             e1.synchronize()
             total += e0.elapsed_time(e1)
         ms = total / K
+        clock_info = clocks.stop()
         # end to end through the host API: poses in from host memory, images back to host memory
         for _ in range(2):
             r.render(0, n, g, c)
@@ -707,7 +710,7 @@ def run_render(args):
                                         "note": "Metal renderer, 4096 Ant envs, Apple GPU (README.md:115-116)"},
                 "e2e": {"value": n / (e2e_ms * 1e-3), "unit": "frames/s", "h2d_bytes_per_step": int(g.nbytes + c.nbytes),
                         "d2h_bytes_per_step": int(out_bytes)},
-                "gpu_launches": K,
+                "gpu_launches": K, "clocks": clock_info,
                 "roofline": {"bound": "hbm", "kernel": "render_kernel", "achieved": out_bytes / (ms * 1e-3) / 1e9,
                              "peak": hbm_peak(), "unit": "GB/s", "frac": out_bytes / (ms * 1e-3) / 1e9 / hbm_peak(),
                              "traffic": None,

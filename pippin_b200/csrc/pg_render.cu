@@ -444,9 +444,12 @@ int rfail(int code, const std::string& msg) {
 
 }  // namespace
 
+constexpr int RCHUNKS = 4;  // host-buffer frames: chunks whose copies back overlap the next chunk's rendering
+
 struct pg_renderer {
   int device = 0;
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr, copy_stream = nullptr;
+  cudaEvent_t done[RCHUNKS] = {};
   int nvert = 0, ntri = 0, ngeom = 0, ncam = 0, nview = 0, W = 0, H = 0, sms = 0, per_sm = 0;
   int rt = 64, nt = 256;  // tile edge and threads per block
   float uni[8] = {};
@@ -579,6 +582,8 @@ int pg_render_create(const float* vertices, int64_t nvert, const uint32_t* trian
   } while (0)
   RCKB(cudaSetDevice(device));
   RCKB(cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking));
+  RCKB(cudaStreamCreateWithFlags(&r->copy_stream, cudaStreamNonBlocking));
+  for (cudaEvent_t& e : r->done) RCKB(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   RCKB(cudaMalloc(&r->verts, sizeof(float) * 8 * std::max<int64_t>(nvert, 1)));
   RCKB(cudaMalloc(&r->tris, sizeof(uint32_t) * 3 * std::max<int64_t>(ntri, 1)));
   RCKB(cudaMalloc(&r->views, sizeof(float) * 16 * nview));
@@ -619,6 +624,10 @@ int pg_render_destroy(pg_renderer* r) {
   if (r->tris) cudaFree(r->tris);
   if (r->views) cudaFree(r->views);
   if (r->radius) cudaFree(r->radius);
+  if (r->copy_stream) cudaStreamSynchronize(r->copy_stream);
+  for (cudaEvent_t& e : r->done)
+    if (e) cudaEventDestroy(e);
+  if (r->copy_stream) cudaStreamDestroy(r->copy_stream);
   if (r->stream) cudaStreamDestroy(r->stream);
   delete r;
   return PG_OK;
@@ -662,11 +671,31 @@ int pg_render_frames(pg_renderer* r, int64_t nenv, const float* geoms, size_t ge
     RCK(cudaStreamSynchronize(s));  // `def` is pageable and about to go
     r->default_app_env = ne;
   }
-  int rc = launch(r, nenv, r->d_geoms, r->d_cams, r->d_app, r->d_rgba, r->d_depth, r->d_seg);
-  if (rc) return rc;
-  RCK(cudaMemcpyAsync(rgba, r->d_rgba, 4 * px, cudaMemcpyDeviceToHost, s));
-  RCK(cudaMemcpyAsync(depth, r->d_depth, 4 * px, cudaMemcpyDeviceToHost, s));
-  RCK(cudaMemcpyAsync(seg, r->d_seg, 4 * px, cudaMemcpyDeviceToHost, s));
+  // every chunk's kernel is queued first, then each chunk's images go back on
+  // the copy stream once its kernel is done, overlapping the later chunks
+  const size_t per_env = (size_t)r->nview * r->W * r->H;
+  size_t bounds[RCHUNKS + 1];
+  for (int k = 0; k <= RCHUNKS; k++) bounds[k] = ne * k / RCHUNKS;
+  for (int k = 0; k < RCHUNKS; k++) {
+    const size_t e0 = bounds[k], e1 = bounds[k + 1];
+    if (e1 == e0) continue;
+    int rc = launch(r, (int64_t)(e1 - e0), r->d_geoms + 12 * e0 * r->ngeom, r->d_cams + 12 * e0 * r->ncam,
+                    r->d_app + 8 * e0 * r->ngeom, r->d_rgba + 4 * e0 * per_env, r->d_depth + e0 * per_env,
+                    r->d_seg + e0 * per_env);
+    if (rc) return rc;
+    RCK(cudaEventRecord(r->done[k], s));
+  }
+  cudaStream_t cs = r->copy_stream;
+  for (int k = 0; k < RCHUNKS; k++) {
+    const size_t e0 = bounds[k], e1 = bounds[k + 1];
+    if (e1 == e0) continue;
+    const size_t o = e0 * per_env, cnt = (e1 - e0) * per_env;
+    RCK(cudaStreamWaitEvent(cs, r->done[k], 0));
+    RCK(cudaMemcpyAsync(rgba + 4 * o, r->d_rgba + 4 * o, 4 * cnt, cudaMemcpyDeviceToHost, cs));
+    RCK(cudaMemcpyAsync(depth + o, r->d_depth + o, 4 * cnt, cudaMemcpyDeviceToHost, cs));
+    RCK(cudaMemcpyAsync(seg + o, r->d_seg + o, 4 * cnt, cudaMemcpyDeviceToHost, cs));
+  }
+  RCK(cudaStreamSynchronize(cs));
   RCK(cudaStreamSynchronize(s));
   return PG_OK;
 }

@@ -282,6 +282,17 @@ def base_appearance(scene: Scene) -> np.ndarray:
     return out
 
 
+def _host(shape, dtype) -> np.ndarray:
+    """A slot's output array, in page-locked memory when torch can provide
+    it, so that the copies back from the device run at full speed."""
+    try:
+        import torch
+        tdt = {np.uint8: torch.uint8, np.float32: torch.float32, np.int32: torch.int32}[np.dtype(dtype).type]
+        return torch.empty(shape, dtype=tdt, pin_memory=True).numpy()
+    except Exception:
+        return np.empty(shape, dtype)
+
+
 def _fp(a: np.ndarray):
     return a.ctypes.data_as(C.POINTER(C.c_float))
 
@@ -347,8 +358,8 @@ class CudaRenderer:
         W, H, nv = self.config.width, self.config.height, len(self.config.views)
         fr = self._slots.get(slot)
         if fr is None or fr.depth.shape[0] != nenv:
-            fr = Frames(np.empty((nenv, nv, H, W, 4), np.uint8), np.empty((nenv, nv, H, W), f32),
-                        np.empty((nenv, nv, H, W), np.int32))
+            fr = Frames(_host((nenv, nv, H, W, 4), np.uint8), _host((nenv, nv, H, W), f32),
+                        _host((nenv, nv, H, W), np.int32))
             self._slots[slot] = fr
         self._check(self._L.pg_render_frames(
             self._h, nenv, _fp(g), g.size, _fp(c), c.size, None if a is None else _fp(a), 0 if a is None else a.size,
