@@ -273,3 +273,34 @@ def test_cuda_renderer_length_errors_and_slots():
     b = r.render(1, 1, pose((1, 0, 0, 0, 1, 0, 0, 0, 1), (5, 0, 0))[None])
     assert (a.segmentation == 0).sum() > 0 and (b.segmentation == 0).sum() == 0  # slot 0 kept
     r.close()
+
+
+def test_c_abi_rejects_bad_scenes_before_touching_the_gpu():
+    """pg_render_create checks its arguments before any CUDA call, so the
+    errors come back (with pg_last_error set) on a machine without a GPU."""
+    import ctypes as C
+
+    from pippin_b200 import _native
+    L = _native.load()
+    sc = Scene([], [geom(Shape.BOX, (0.1, 0.1, 0.1))], [], [CameraDesc("c", 45.0)])
+    cfg = R.RenderConfig(8, 8, [R.ViewSource.scene(0)], 0.01, 10.0)
+    v, t = R.build_mesh(sc)
+    views, uni, app = R.view_table(cfg, sc), R.uniforms(cfg), R.base_appearance(sc)
+
+    def create(verts=v, tris=t, ngeom=1, ncam=1, views=views, uni=uni):
+        h = C.c_void_p()
+        pf = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))  # noqa: E731
+        rc = L.pg_render_create(pf(verts), len(verts), tris.ctypes.data_as(C.POINTER(C.c_uint32)), len(tris), ngeom,
+                                ncam, pf(views), len(views), pf(app), 8, 8, pf(uni), 0, C.byref(h))
+        return rc, _native.last_error()
+
+    bad = t.copy()
+    bad[0, 0] = len(v)
+    assert create(tris=bad) == (_native.PG_ERR_INVALID, "triangle index out of range")
+    assert create(ncam=0) == (_native.PG_ERR_INVALID, "view refers to a camera the scene does not have")
+    far_first = uni.copy()
+    far_first[1] = far_first[0]
+    assert create(uni=far_first) == (_native.PG_ERR_INVALID, "need 0 < near < far")
+    vb = v.copy()
+    vb.view(np.uint32)[0, 3] = 5
+    assert create(verts=vb) == (_native.PG_ERR_INVALID, "vertex geom id out of range")
