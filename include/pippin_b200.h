@@ -141,8 +141,10 @@ int pg_step_device(pg_handle* h, int64_t start, int64_t end, int64_t nstep, cons
  * the library's device image, one per GPU that loads the library, held until
  * exit; as many envs step at once as fit in it, the rest follow in the same
  * launch. A model whose per-block scratch exceeds the array is rejected with
- * PG_ERR_UNSUPPORTED. The first call on a device looks the array up (make it
- * before any stream capture). All calls share the array and keep its last
+ * PG_ERR_UNSUPPORTED. Every call looks the array's device address up again
+ * (so a context the host program resets and makes again is followed); the
+ * first call on a device also loads the library's device image there, so make
+ * it before any stream capture. All calls share the array and keep its last
  * contents: calls that overlap on the GPU race. Stream-ordered like pg_step. */
 int pg_step_static(pg_handle* h, int64_t start, int64_t end, int64_t nstep);
 
@@ -163,6 +165,14 @@ int pg_set(pg_handle* h, int field, int64_t start, int64_t end, const double* sr
  * (end-start) x ngeom poses, cams (end-start) x ncam. */
 int pg_poses(pg_handle* h, int64_t start, int64_t end, pg_pose* geoms, size_t ngeoms_len, pg_pose* cams,
              size_t ncams_len);
+
+/* Physics::poses into device memory, for a renderer on the same GPU (the
+ * zero-copy frame path of crates/pippin-env/src/pipeline.rs:28-40; the values
+ * are pg_poses's, crates/pippin-env/src/pippin_cpu.rs:189-205). geoms_dev
+ * holds (end-start) x ngeom poses, cams_dev (end-start) x ncam (either may be
+ * NULL when its count is 0), both on the handle's device. Enqueued on
+ * pg_stream after the steps before it; returns without waiting. */
+int pg_poses_device(pg_handle* h, int64_t start, int64_t end, pg_pose* geoms_dev, pg_pose* cams_dev);
 
 /* Physics::set_param / get_param (lib.rs:129-141; pippin_cpu.rs:122-143;
  * params.rs:111-177). values are (end-start, width). All-or-nothing:

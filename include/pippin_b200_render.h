@@ -47,7 +47,9 @@ typedef struct pg_renderer pg_renderer;
 #define PG_RENDER_APPEARANCE_WORDS 8
 
 /* Uploads the triangulated scene and the view table to `device`.
- * base_appearance (ngeom x 8) is used when a frame supplies none. */
+ * base_appearance (ngeom x 8) is used when a frame supplies none. At most
+ * 4096 views; a frame renders fewer than 2^31 images (nenv x nview), else
+ * PG_ERR_UNSUPPORTED here or PG_ERR_INVALID from the frame calls. */
 int pg_render_create(const float* vertices, int64_t nvert, const uint32_t* triangles, int64_t ntri, int64_t ngeom,
                      int64_t ncam, const float* views, int64_t nview, const float* base_appearance, int64_t width,
                      int64_t height, const float* uniforms, int device, pg_renderer** out);

@@ -29,6 +29,13 @@ int pg_time_phases(pg_handle* h, int64_t start, int64_t end, int64_t nstep, cons
  * Returns PG_OK or PG_ERR_INVALID. */
 int pg_phase_launch(const pg_handle* h, int phase, int* lanes_per_env, int* envs_per_block, int* blocks);
 
+/* How many Newton-phase tiles pg_step_static runs at once out of its fixed
+ * scratch array, for tiles of `tile_bytes` and blocks of `tiles_per_block`
+ * tiles (a whole number of blocks; the envs beyond them follow in turn).
+ * PG_ERR_UNSUPPORTED, with *tiles = 0 and the message pg_step_static gives,
+ * when one block does not fit. Pure arithmetic: needs no GPU. */
+int pg_static_tiles(size_t tile_bytes, int tiles_per_block, int64_t* tiles);
+
 #ifdef __cplusplus
 }
 #endif

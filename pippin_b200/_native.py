@@ -42,6 +42,7 @@ SIGNATURES = [
     ("pg_get", _i32, [_vp, _i32, _i64, _i64, _pd, _sz]),
     ("pg_set", _i32, [_vp, _i32, _i64, _i64, _pd, _sz]),
     ("pg_poses", _i32, [_vp, _i64, _i64, _pf, _sz, _pf, _sz]),
+    ("pg_poses_device", _i32, [_vp, _i64, _i64, _vp, _vp]),
     ("pg_param_width", _i32, [_vp, _i32]),
     ("pg_set_param", _i32, [_vp, _i32, _i64, _i64, _i64, _pd, _sz]),
     ("pg_get_param", _i32, [_vp, _i32, _i64, _i64, _i64, _pd, _sz]),
@@ -65,6 +66,7 @@ SIGNATURES = [
     ("pg_fp64_peak", _i32, [_i32, _i32, _pd, _pd]),
     ("pg_time_phases", _i32, [_vp, _i64, _i64, _i64, _vp, _pf]),
     ("pg_phase_launch", _i32, [_vp, _i32, _pi32, _pi32, _pi32]),
+    ("pg_static_tiles", _i32, [_sz, _i32, _pi64]),
     ("pg_set_warm_mlp", _i32, [_vp, _pf, _sz]),
     ("pg_warm_samples", _i32, [_vp, _i64, _i64, _pf, _sz, _pf, _sz, _pi64]),
     ("pg_warm_capacity", _i64, [_vp]),

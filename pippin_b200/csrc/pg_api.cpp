@@ -1439,6 +1439,21 @@ int pg_poses(pg_handle* h, int64_t start, int64_t end, pg_pose* geoms, size_t ng
   return PG_OK;
 }
 
+int pg_poses_device(pg_handle* h, int64_t start, int64_t end, pg_pose* geoms_dev, pg_pose* cams_dev) {
+  if (!h) return fail(PG_ERR_INVALID, "NULL handle");
+  int rc = check_range(h, start, end);
+  if (rc) return rc;
+  int64_t cnt = end - start;
+  const HostModel& m = h->hm;
+  if (cnt == 0) return PG_OK;
+  if ((m.ngeom && !geoms_dev) || (m.ncam && !cams_dev)) return fail(PG_ERR_INVALID, "poses_device: NULL buffer");
+  CK(cudaSetDevice(h->device));
+  StepArgs a = make_args(h);
+  a.start = (int)start;
+  a.count = (int)cnt;
+  return launch_status(launch_poses(a, fit(h->cfg.smooth, cnt), (float*)geoms_dev, (float*)cams_dev, h->stream));
+}
+
 int pg_param_width(const pg_handle* h, int param) {
   if (!h || param < 0 || param > PG_PARAM_QPOS0) return -1;
   return param_width(h->hm, param);

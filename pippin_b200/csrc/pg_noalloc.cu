@@ -19,10 +19,10 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
-#include <mutex>
 #include <string>
 
 #include "../../include/pippin_b200.h"
+#include "../../include/pippin_b200_tools.h"
 #include "pg_kernels.h"
 #include "pg_model.h"
 
@@ -37,34 +37,49 @@ namespace {
 
 constexpr size_t PG_STATIC_SCRATCH_BYTES = size_t(16) << 20;
 constexpr size_t PG_STATIC_COUNTER_BYTES = 256;  // phase work counters, then tile scratch
+// pg_step's scratch buffer ends 64 bytes past its last tile; the static
+// tiles leave the same tail free at the array's end
+constexpr size_t PG_STATIC_TAIL_BYTES = 64;
 
 // Device-side scratch shared by every pg_step_static call on a device. Host
 // code must not use this name as an address: its device address comes from
 // cudaGetSymbolAddress below.
 static __device__ __align__(256) unsigned char g_static_scratch[PG_STATIC_SCRATCH_BYTES];
 
-constexpr int MAX_DEVICES = 64;
-std::mutex g_setup_mu;
-unsigned char* g_scratch_ptr[MAX_DEVICES] = {nullptr};
-
-// Once per device, with that device current: the array's device address.
-int scratch_address(int device, unsigned char** out) {
-  if (device < 0 || device >= MAX_DEVICES) return PG_ERR_INVALID;
-  std::lock_guard<std::mutex> g(g_setup_mu);
-  if (!g_scratch_ptr[device]) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
-    if (e != cudaSuccess) {
-      pg::internal_set_error(std::string("cudaGetSymbolAddress(static scratch): ") + cudaGetErrorString(e));
-      return PG_ERR_CUDA;
-    }
-    g_scratch_ptr[device] = static_cast<unsigned char*>(p);
+// The array's device address on the current device. Looked up on every call
+// (the lookup allocates nothing and is cheap), so that a context torn down
+// and made again by the host program (cudaDeviceReset) is followed; the
+// first lookup on a device loads the library's device image there.
+int scratch_address(unsigned char** out) {
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+  if (e != cudaSuccess) {
+    pg::internal_set_error(std::string("cudaGetSymbolAddress(static scratch): ") + cudaGetErrorString(e));
+    return PG_ERR_CUDA;
   }
-  *out = g_scratch_ptr[device];
+  *out = static_cast<unsigned char*>(p);
   return PG_OK;
 }
 
 }  // namespace
+
+extern "C" int pg_static_tiles(size_t tile_bytes, int tiles_per_block, int64_t* tiles) {
+  if (!tiles || tile_bytes == 0 || tiles_per_block <= 0) {
+    pg::internal_set_error("pg_static_tiles: invalid argument");
+    return PG_ERR_INVALID;
+  }
+  const size_t usable = PG_STATIC_SCRATCH_BYTES - PG_STATIC_COUNTER_BYTES - PG_STATIC_TAIL_BYTES;
+  size_t n = usable / tile_bytes;
+  *tiles = 0;
+  if (n < (size_t)tiles_per_block) {
+    pg::internal_set_error("pg_step_static: this model needs " + std::to_string(tile_bytes * tiles_per_block) +
+                           " bytes of scratch per block, more than the " + std::to_string(usable) +
+                           "-byte static scratch holds (use pg_step)");
+    return PG_ERR_UNSUPPORTED;
+  }
+  *tiles = (int64_t)(n / tiles_per_block * tiles_per_block);
+  return PG_OK;
+}
 
 extern "C" int pg_step_static(pg_handle* h, int64_t start, int64_t end, int64_t nstep) {
   pg::StepArgs a;
@@ -74,20 +89,13 @@ extern "C" int pg_step_static(pg_handle* h, int64_t start, int64_t end, int64_t 
   int rc = pg::internal_step_args(h, start, end, nstep, &a, &cfg, &stream, &device);
   if (rc != PG_OK) return rc;
   if (end == start || nstep == 0) return PG_OK;
-  unsigned char* base = nullptr;
-  if ((rc = scratch_address(device, &base)) != PG_OK) return rc;
+  unsigned char* base = nullptr;  // internal_step_args made the handle's device current
+  if ((rc = scratch_address(&base)) != PG_OK) return rc;
   // only the Newton phase uses tile scratch: its grid is capped by the array
   pg::LaunchCfg& nc = cfg.newton;
-  size_t tile_bytes = (size_t)a.s.stride * sizeof(double);
-  size_t tiles = (PG_STATIC_SCRATCH_BYTES - PG_STATIC_COUNTER_BYTES) / tile_bytes;
-  if (tiles < (size_t)nc.tiles_per_block) {
-    pg::internal_set_error("pg_step_static: this model needs " + std::to_string(tile_bytes * nc.tiles_per_block) +
-                           " bytes of scratch per block, more than the " +
-                           std::to_string(PG_STATIC_SCRATCH_BYTES - PG_STATIC_COUNTER_BYTES) +
-                           "-byte static scratch holds (use pg_step)");
-    return PG_ERR_UNSUPPORTED;
-  }
-  nc.blocks = (int)std::min<size_t>((size_t)nc.blocks, tiles / nc.tiles_per_block);
+  int64_t tiles = 0;
+  if ((rc = pg_static_tiles((size_t)a.s.stride * sizeof(double), nc.tiles_per_block, &tiles)) != PG_OK) return rc;
+  nc.blocks = (int)std::min<int64_t>((int64_t)nc.blocks, tiles / nc.tiles_per_block);
   a.queue = reinterpret_cast<int*>(base);
   a.learn.count = a.queue + 3;
   a.scratch = reinterpret_cast<double*>(base + PG_STATIC_COUNTER_BYTES);

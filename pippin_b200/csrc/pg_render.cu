@@ -444,6 +444,7 @@ int rfail(int code, const std::string& msg) {
 
 }  // namespace
 
+constexpr int MAX_VIEWS = 4096;  // views per env (the kernel indexes images as 32-bit ints)
 constexpr int RCHUNKS = 8;  // host-buffer frames: at most this many chunks, whose copies back overlap the next chunk's rendering
 
 struct pg_renderer {
@@ -531,7 +532,8 @@ int pg_render_create(const float* vertices, int64_t nvert, const uint32_t* trian
   if (nvert < 0 || ntri < 0 || ngeom < 0 || ncam < 0 || nview < 1 || width < 1 || height < 1)
     return rfail(PG_ERR_INVALID, "renderer sizes out of range");
   if ((nvert > 0 && !vertices) || (ntri > 0 && !triangles)) return rfail(PG_ERR_INVALID, "NULL mesh");
-  if (ntri >= (1ll << 30) || nvert >= (1ll << 31) || width > 16384 || height > 16384 || ngeom >= (1 << 20))
+  if (ntri >= (1ll << 30) || nvert >= (1ll << 31) || width > 16384 || height > 16384 || ngeom >= (1 << 20) ||
+      nview > MAX_VIEWS)
     return rfail(PG_ERR_UNSUPPORTED, "scene or image too large");
   for (int64_t i = 0; i < 3 * ntri; i++)
     if ((int64_t)triangles[i] >= nvert) return rfail(PG_ERR_INVALID, "triangle index out of range");
@@ -638,6 +640,7 @@ int pg_render_frames(pg_renderer* r, int64_t nenv, const float* geoms, size_t ge
                      int32_t* seg) {
   if (!r) return rfail(PG_ERR_INVALID, "NULL renderer");
   if (nenv < 0 || nenv > (1 << 24)) return rfail(PG_ERR_INVALID, "nenv out of range");
+  if (nenv * r->nview >= (1ll << 31)) return rfail(PG_ERR_INVALID, "nenv x views must stay below 2^31 images");
   const size_t ne = (size_t)nenv;
   if (geoms_len != ne * r->ngeom * 12 || cams_len != ne * r->ncam * 12)
     return rfail(PG_ERR_LENGTH, "expected " + std::to_string(ne * r->ngeom) + " geom and " +
@@ -709,6 +712,7 @@ int pg_render_frames_device(pg_renderer* r, int64_t nenv, const float* geoms, co
                             const float* appearance, uint8_t* rgba, float* depth, int32_t* seg) {
   if (!r) return rfail(PG_ERR_INVALID, "NULL renderer");
   if (nenv < 0 || nenv > (1 << 24)) return rfail(PG_ERR_INVALID, "nenv out of range");
+  if (nenv * r->nview >= (1ll << 31)) return rfail(PG_ERR_INVALID, "nenv x views must stay below 2^31 images");
   if (nenv == 0) return PG_OK;
   if ((r->ngeom && (!geoms || !appearance)) || (r->ncam && !cams) || !rgba || !depth || !seg)
     return rfail(PG_ERR_INVALID, "NULL buffer");

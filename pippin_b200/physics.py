@@ -304,6 +304,14 @@ class CudaPhysics:
                                      cams.ctypes.data_as(pf), cams.size // 12))
         return geoms, cams
 
+    def poses_device(self, envs: EnvRange, geoms_ptr: int, cams_ptr: int = 0):
+        """Poses of `envs` written into device memory on this handle's GPU:
+        geoms_ptr holds (envs, ngeom, 12) float32, cams_ptr (envs, ncam, 12)
+        (0 when the model has no cameras). Enqueued on stream(); no wait."""
+        s, e = _span(envs)
+        self._check(self._L.pg_poses_device(self._h, s, e, C.c_void_p(geoms_ptr or None),
+                                            C.c_void_p(cams_ptr or None)))
+
     def param_width(self, p: Param) -> int:
         return self._L.pg_param_width(self._h, int(p))
 

@@ -13,7 +13,9 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
-REFERENCE = "/root/reference"
+# checkout of the reference repository, for the tests that read its files;
+# unset: those tests use the committed fixtures under tests/golden/ instead
+REFERENCE = os.environ.get("PIPPIN_REFERENCE", "")
 
 
 def pytest_configure(config):
@@ -28,4 +30,4 @@ def oracle_lib():
 
 
 def have_reference():
-    return os.path.isdir(os.path.join(REFERENCE, "assets"))
+    return bool(REFERENCE) and os.path.isdir(os.path.join(REFERENCE, "assets"))

@@ -17,7 +17,9 @@ import os
 import re
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PIPPIN_REFERENCE", "")
+if not REF:
+    sys.exit("usage: make_kats.py <reference checkout>  (or set PIPPIN_REFERENCE)")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_kats.json")
 
 

@@ -347,3 +347,57 @@ GENERAL_CHECKS = [check_mesh_cube_rests_like_box, check_mesh_cubes_stack, check_
 CONTACT_CHECKS = [check_box_rests_on_plane, check_sphere_and_capsule_rest, check_box_stack_is_stable,
                   check_friction_holds, check_friction_slides, check_joint_limit, check_shapes_on_box]
 PARAM_CHECKS = [check_friction_per_env, check_size_and_parking, check_mass_per_env]
+
+
+# ---- hot-path branches the workload models do not reach: joint equality rows
+# (newton.rs:171-195), fixed-tendon transmissions (mjcf.rs:852-947) and the
+# implicitfast actuator terms (forward.rs:407-431). Each scene also touches
+# the floor, so that equality / limit rows meet contact rows in one solve.
+EQUALITY_CHAIN = (
+    '<mujoco><option timestep="0.005"/><worldbody><geom type="plane" size="5 5 .1"/>'
+    '<body name="l1" pos="0 0 0.55"><joint name="j1" axis="0 1 0" range="-100 100"/>'
+    '<geom type="capsule" fromto="0 0 0 0.22 0 0" size="0.03"/>'
+    '<body name="l2" pos="0.22 0 0"><joint name="j2" axis="0 1 0"/>'
+    '<geom type="capsule" fromto="0 0 0 0.22 0 0" size="0.03"/>'
+    '<body name="l3" pos="0.22 0 0"><joint name="j3" axis="0 1 0"/><joint name="j3b" axis="1 0 0"/>'
+    '<geom type="capsule" fromto="0 0 0 0.2 0 0" size="0.03"/>'
+    '<body name="tip" pos="0.2 0 0"><joint name="j4" type="slide" axis="1 0 0" range="-0.05 0.05"/>'
+    '<geom type="sphere" size="0.05"/></body></body></body></body>'
+    '<body name="ball" pos="0.3 0.02 0.2"><freejoint/><geom type="sphere" size="0.06"/></body>'
+    '</worldbody>'
+    '<equality><joint joint1="j2" joint2="j1" polycoef="0.1 0.5 0.3 -0.05 0.01"/>'
+    '<joint joint1="j3b"/><joint joint1="j4" joint2="j3" polycoef="0 0.02 0 0 0" solref="0.05 1"/></equality>'
+    '<actuator><motor joint="j1" gear="8"/><motor joint="j3" gear="3"/></actuator></mujoco>')
+
+TENDON_ARM = (
+    '<mujoco><option timestep="0.004"/><worldbody><geom type="plane" size="5 5 .1"/>'
+    '<body name="base" pos="0 0 0.45"><joint name="yaw" axis="0 0 1" damping="0.2"/>'
+    '<geom type="cylinder" size="0.05 0.04"/>'
+    '<body name="up" pos="0 0 0.05"><joint name="sh" axis="0 1 0" range="-120 120"/>'
+    '<geom type="capsule" fromto="0 0 0 0.25 0 0" size="0.035"/>'
+    '<body name="fore" pos="0.25 0 0"><joint name="el" axis="0 1 0" range="-150 150"/>'
+    '<geom type="capsule" fromto="0 0 0 0.22 0 0" size="0.03"/>'
+    '<body name="hand" pos="0.22 0 0"><joint name="wr" axis="1 0 0"/>'
+    '<geom type="box" size="0.04 0.03 0.02"/></body></body></body></body></worldbody>'
+    '<tendon><fixed name="flex"><joint joint="sh" coef="1"/><joint joint="el" coef="-0.5"/></fixed>'
+    '<fixed name="twist"><joint joint="yaw" coef="0.3"/><joint joint="wr" coef="1"/></fixed></tendon>'
+    '<actuator><motor tendon="flex" gear="12" ctrlrange="-1 1"/><motor tendon="twist" gear="2"/>'
+    '<motor joint="el" gear="4"/></actuator></mujoco>')
+
+IMPLICITFAST_ARM = (
+    '<mujoco><option timestep="0.005" integrator="implicitfast"/>'
+    '<default><joint damping="0.05" armature="0.01"/></default>'
+    '<worldbody><geom type="plane" size="5 5 .1"/>'
+    '<body name="base" pos="0 0 0.4"><joint name="a0" axis="0 0 1"/>'
+    '<geom type="cylinder" size="0.05 0.04"/>'
+    '<body name="l1" pos="0 0 0.05"><joint name="a1" axis="0 1 0" range="-110 110"/>'
+    '<geom type="capsule" fromto="0 0 0 0.24 0 0" size="0.035"/>'
+    '<body name="l2" pos="0.24 0 0"><joint name="a2" axis="0 1 0"/>'
+    '<geom type="capsule" fromto="0 0 0 0.22 0 0" size="0.03"/>'
+    '<body name="l3" pos="0.22 0 0"><joint name="a3" type="slide" axis="1 0 0" range="-0.04 0.04"/>'
+    '<geom type="box" size="0.035 0.035 0.035"/></body></body></body></body>'
+    '<body name="block" pos="0.35 0 0.05"><freejoint/><geom type="box" size="0.05 0.05 0.05"/></body>'
+    '</worldbody>'
+    '<actuator><position joint="a1" kp="40" kv="4"/><velocity joint="a2" kv="3"/>'
+    '<position joint="a0" kp="10" kv="1" ctrlrange="-1 1"/><velocity joint="a3" kv="5" forcerange="-2 2"/>'
+    '<motor joint="a2" gear="2"/></actuator></mujoco>')

@@ -48,3 +48,23 @@ def test_missing_library_fails_loudly(tmp_path):
             _native.load(str(tmp_path / "nope.so"))
         finally:
             _native._lib = None
+
+
+def test_static_scratch_capacity_and_rejection():
+    """pg_step_static's capacity check is pure arithmetic (no GPU): whole
+    blocks of tiles out of the fixed array, and a clear rejection when one
+    block does not fit."""
+    from pippin_b200 import build
+    build.build()
+    L = _native.load()
+    tiles = ctypes.c_int64(-1)
+    usable = (16 << 20) - 256 - 64
+    assert L.pg_static_tiles(1 << 17, 16, ctypes.byref(tiles)) == _native.PG_OK
+    assert tiles.value == usable // (1 << 17) // 16 * 16
+    # an exact fit leaves the 64-byte tail free
+    assert L.pg_static_tiles(usable // 8, 8, ctypes.byref(tiles)) == _native.PG_OK and tiles.value == 8
+    assert L.pg_static_tiles(usable // 8 + 1, 8, ctypes.byref(tiles)) == _native.PG_ERR_UNSUPPORTED
+    assert tiles.value == 0
+    msg = _native.last_error()
+    assert "bytes of scratch per block" in msg and "use pg_step" in msg
+    assert L.pg_static_tiles(0, 8, ctypes.byref(tiles)) == _native.PG_ERR_INVALID

@@ -56,6 +56,12 @@ MODELS = {
     "mesh_stack": lambda: S.mesh_stack_xml(),
     "cylinders": lambda: S.CYLINDERS,
     "hull_tumble": scenes.hull_tumble_xml,
+    # joint equality rows, fixed tendons, implicitfast actuators
+    "equality_chain": lambda: S.EQUALITY_CHAIN,
+    "equality_chain_solo": lambda: S.EQUALITY_CHAIN.replace(
+        '<body name="ball" pos="0.3 0.02 0.2"><freejoint/><geom type="sphere" size="0.06"/></body>', ""),
+    "tendon_arm": lambda: S.TENDON_ARM,
+    "implicitfast_arm": lambda: S.IMPLICITFAST_ARM,
 }
 
 
@@ -217,6 +223,53 @@ def test_general_convex_step_parity(name):
     assert contacts_seen > 0
 
 
+@pytest.mark.parametrize("solver", ["newton", "pgs"])
+@pytest.mark.parametrize("name", ["equality_chain", "equality_chain_solo", "tendon_arm", "implicitfast_arm"])
+def test_branch_step_parity(name, solver):
+    """Per-step output on identical input states for the branches the
+    workload models do not reach: joint equality rows with a polynomial
+    coupling, a fixed joint and a per-equality solref (newton.rs:171-195;
+    the solo chain takes the register Newton, the chain with a free ball the
+    island path), fixed-tendon actuators (mjcf.rs:852-947) and implicitfast
+    position/velocity actuators with joint damping (forward.rs:407-431),
+    each with floor contacts and joint limits. PGS runs with its warm start
+    cleared each step, as in test_pgs_step_parity."""
+    n = 32
+    m, g, o = pair(MODELS[name](), n, tolerance=1e-10)
+    if solver == "pgs":
+        g.set_solver(kind=1)
+        o.set_solver(kind=1)
+    rng = np.random.default_rng(7)
+    q, v = random_state(m, n, rng)
+    g.set(Field.QPOS, range(n), q)
+    g.set(Field.QVEL, range(n), v)
+    rows_seen = contacts_seen = 0
+    for t in range(150):
+        g.set(Field.CTRL, range(n), rng.uniform(-1, 1, (n, m.nu)))
+        if solver == "pgs":
+            st = {f: g.get(f, range(n)) for f in (Field.QPOS, Field.QVEL, Field.QACC, Field.CTRL)}
+            g.reset(range(n))
+            o.reset(list(range(n)))
+            for f, fo in ((Field.QPOS, QPOS), (Field.QVEL, QVEL), (Field.QACC, QACC), (Field.CTRL, CTRL)):
+                g.set(f, range(n), st[f])
+                o.set(fo, st[f])
+        else:
+            _copy_state(g, o, n)
+        g.step(range(n), 1)
+        o.step(0, n, 1)
+        sg, so = g.stats(), o.stats()
+        assert not sg["status"].any(), (t, sg["status"])
+        np.testing.assert_array_equal(sg["ncon"], so["ncon"])
+        np.testing.assert_array_equal(sg["nrows"], so["nrows"])
+        rows_seen += int(so["nrows"].sum())
+        contacts_seen += int(so["ncon"].sum())
+        for fg, fo in ((Field.QACC, QACC), (Field.QVEL, QVEL), (Field.QPOS, QPOS)):
+            a, b = g.get(fg, range(n)), o.get(fo)
+            for e in range(n):
+                assert rel(a[e], b[e]) < TOL_STEP, (t, e, fg, rel(a[e], b[e]))
+    assert rows_seen > 0 and contacts_seen > 0
+
+
 def _pgs_pair(name, n):
     m, g, o = pair(MODELS[name](), n)
     g.set_solver(kind=1)
@@ -319,6 +372,36 @@ def test_poses_and_appearance_match_oracle():
     g.set_param(Param.GEOM_SIZE, 1, range(0, 2), [[0.3, 0, 0], [0.2, 0, 0]])
     o.set_param(1, 1, [[0.3, 0, 0], [0.2, 0, 0]], 0, 2)
     np.testing.assert_array_equal(g.appearance(range(n)), o.appearance())
+
+
+def test_device_poses_equal_host_poses():
+    """pg_poses_device writes the poses pg_poses returns, bit for bit, into
+    device buffers, for a sub-range and in stream order after a step."""
+    import torch
+    n = 40
+    xml = scenes.ant_xml().replace("</worldbody>", '<camera name="side" pos="0 -3 1" euler="70 0 0"/></worldbody>')
+    m = mjcf.load_string(xml)
+    ncam = len(m.cam_body)
+    assert ncam >= 1
+    g = CudaPhysics(mjcf.to_blob(m), n)
+    rng = np.random.default_rng(4)
+    q, v = random_state(m, n, rng)
+    g.set(Field.QPOS, range(n), q)
+    g.set(Field.QVEL, range(n), v)
+    dev = torch.device("cuda", 0)
+    for s, e in ((0, n), (7, 31)):
+        g.step(range(n), 3)
+        hg, hc = g.poses(range(s, e))
+        dg = torch.full(((e - s) * m.ngeom * 12,), float("nan"), dtype=torch.float32, device=dev)
+        dc = torch.full(((e - s) * ncam * 12,), float("nan"), dtype=torch.float32, device=dev)
+        torch.cuda.synchronize()
+        g.poses_device(range(s, e), dg.data_ptr(), dc.data_ptr())
+        g.synchronize()
+        np.testing.assert_array_equal(dg.cpu().numpy().view(np.uint32), hg.reshape(-1).view(np.uint32))
+        np.testing.assert_array_equal(dc.cpu().numpy().view(np.uint32), hc.reshape(-1).view(np.uint32))
+    with pytest.raises(PhysicsError):
+        g.poses_device(range(0, 2), 0, 0)
+    g.close()
 
 
 def test_reset_keeps_qacc_and_restores_state():

@@ -1,6 +1,8 @@
 """Model compiler: the generated workload models equal the reference's
 assets, the blob round-trips through the oracle's reader, and the compile
 step reproduces the reference's structural facts for Ant."""
+import hashlib
+import json
 import os
 from collections import Counter
 
@@ -15,6 +17,17 @@ from tests.conftest import REFERENCE, have_reference
 def test_generated_models_match_reference_assets(asset):
     ref = mjcf.compile_file(os.path.join(REFERENCE, "assets", asset))
     assert mjcf.compile_string(scenes.REFERENCE_ASSETS[asset]()) == ref
+
+
+@pytest.mark.parametrize("asset", sorted(scenes.REFERENCE_ASSETS))
+def test_generated_models_match_recorded_asset_blobs(asset):
+    """The same check without a reference checkout: the blob's SHA-256 equals
+    the one recorded from the reference's asset (tests/golden/make_blob_hashes.py)."""
+    with open(os.path.join(os.path.dirname(__file__), "golden", "reference_blobs.json")) as fh:
+        want = json.load(fh)[asset]
+    blob = mjcf.compile_string(scenes.REFERENCE_ASSETS[asset]())
+    assert len(blob) == want["bytes"]
+    assert hashlib.sha256(blob).hexdigest() == want["sha256"]
 
 
 def test_ant_structure():

@@ -275,6 +275,50 @@ def test_cuda_renderer_length_errors_and_slots():
     r.close()
 
 
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nenv", [5003, 7919])
+def test_host_buffer_frames_in_chunks_match_device_frames(nenv):
+    """Host-buffer frames of thousands of small images render in several
+    chunks (each chunk's copies back overlap the next chunk's kernel). The
+    chunk count comes from the work, and the env counts here do not divide
+    evenly by it. The images must equal the device-buffer path's bit for bit,
+    and a sample of envs the oracle's."""
+    import torch
+    rng = np.random.default_rng(nenv)
+    sc = random_scene(rng)
+    ng = len(sc.geoms)
+    geoms = random_poses(rng, nenv, ng)
+    cams = np.tile(pose(R.ViewSource.look_at([0.8, -0.9, 0.6], [0, 0, 0.1], 50.0).mat, (0.8, -0.9, 0.6)),
+                   (nenv, 1, 1)).astype(f32)
+    app = np.broadcast_to(R.base_appearance(sc), (nenv, ng, 8)).copy()
+    app[::7, 3, 3] = 0.0  # some geoms hidden
+    cfg = R.RenderConfig(16, 16, [R.ViewSource.look_at([1.2, 1.0, 0.9], [0, 0, 0.1], 55.0)], 0.01, 20.0)
+    r = R.CudaRenderer(sc, cfg)
+    try:
+        host = r.render(0, nenv, geoms, cams, app)
+        dev = torch.device("cuda", 0)
+        gd, cd, ad = (torch.from_numpy(np.ascontiguousarray(x).reshape(-1)).to(dev) for x in (geoms, cams, app))
+        px = nenv * 16 * 16
+        rgba = torch.empty(px * 4, dtype=torch.uint8, device=dev)
+        depth = torch.empty(px, dtype=torch.float32, device=dev)
+        seg = torch.empty(px, dtype=torch.int32, device=dev)
+        torch.cuda.synchronize()
+        r.render_device(nenv, gd.data_ptr(), cd.data_ptr(), ad.data_ptr(), rgba.data_ptr(), depth.data_ptr(),
+                        seg.data_ptr())
+        r.synchronize()
+        got_dev = (rgba.cpu().numpy(), depth.cpu().numpy(), seg.cpu().numpy())
+        for a, b, name in zip((host.rgba, host.depth, host.segmentation), got_dev, ("rgba", "depth", "seg")):
+            assert np.array_equal(a.reshape(-1).view(np.uint8), b.reshape(-1).view(np.uint8)), name
+        assert (host.segmentation >= 0).mean() > 0.2
+        # chunk edges and a few envs in between against the oracle
+        sample = sorted({0, 1, nenv // 3, nenv // 2, nenv - 2, nenv - 1})
+        want = oracle_frames(sc, cfg, geoms[sample], cams[sample], app[sample])
+        for a, b in zip((host.rgba[sample], host.depth[sample], host.segmentation[sample]), want):
+            assert np.array_equal(a.view(np.uint8), b.view(np.uint8))
+    finally:
+        r.close()
+
 def test_c_abi_rejects_bad_scenes_before_touching_the_gpu():
     """pg_render_create checks its arguments before any CUDA call, so the
     errors come back (with pg_last_error set) on a machine without a GPU."""
