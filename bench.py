@@ -59,6 +59,11 @@ def parse():
     ap.add_argument("--learned-eval", action="store_true",
                     help="the learned warm-start evaluation (Ant and tabletop) instead of the headline")
     ap.add_argument("--learned-samples", type=int, default=10_000_000, help="training pairs per scene")
+    ap.add_argument("--preroll", type=int, default=100,
+                    help="substeps run before the warm-up (the Ant lands first), outside every timed region")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip configs 2-5 (tabletop, hull tumble, contact-free, learned evaluation) in the line")
+    ap.add_argument("--extras-steps", type=int, default=50, help="timed substeps of each extra config")
     ap.add_argument("--learned-envs", type=int, default=16384)
     ap.add_argument("--scene", default="", choices=["", "tabletop", "hull_tumble", "cartpole", "arm3hinge"],
                     help="phase timing of another workload (configs 2-4) beside the oracle, instead of the headline")
@@ -67,9 +72,10 @@ def parse():
     return ap.parse_args()
 
 
-def workload(envs):
+def workload(envs, preroll=100):
     return {"workload": f"ant: {envs} envs/GPU, dt 0.01, Newton tol 1e-10 cap {ITERS}, "
-                        "qpos0+U[-0.1,0.1], qvel N(0,0.1^2), ctrl U[-1,1] per step",
+                        f"qpos0+U[-0.1,0.1], qvel N(0,0.1^2), ctrl U[-1,1] per step, timed after {preroll} "
+                        "pre-roll substeps (landed)",
             "model": "ant (nq 15, nv 14, nu 8)", "envs_per_gpu": envs, "substeps_per_step": 1,
             "l2": "flushed between timed steps (256 MB write)"}
 
@@ -164,20 +170,21 @@ def run_reference(args):
     q, v, rng = initial_state(m, n, 1)
     o.set(QPOS, q)
     o.set(QVEL, v)
-    ctrls = [rng.uniform(-1, 1, (n, m.nu)) for _ in range(args.warmup + args.steps)]
-    for k in range(args.warmup):
+    P = args.preroll
+    ctrls = [rng.uniform(-1, 1, (n, m.nu)) for _ in range(P + args.warmup + args.steps)]
+    for k in range(P + args.warmup):  # pre-roll (the Ant lands) and warm-up, untimed
         o.set(CTRL, ctrls[k])
         o.step(0, n, 1)
     t0 = time.perf_counter()
     for k in range(args.steps):
-        o.set(CTRL, ctrls[args.warmup + k])
+        o.set(CTRL, ctrls[P + args.warmup + k])
         o.step(0, n, 1)
     el = time.perf_counter() - t0
     value = n * args.steps / el
     line = {"metric": "Ant env-steps/s", "value": value, "unit": "env-steps/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": dict(workload(args.envs), parallelism=f"{o.threads} host threads"), "impl": "reference",
+            "config": dict(workload(args.envs, P), parallelism=f"{o.threads} host threads"), "impl": "reference",
             "cpu_baseline": {"value": value, "unit": "env-steps/s", "cores": o.threads, "kind": "port",
                              "sample": f"Ant {n} envs x {args.steps} steps (Physics::step shape, per-step ctrl)"},
             "e2e": {"value": value, "unit": "env-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -258,10 +265,24 @@ def run_ours(args):
     m = mjcf.load_string(xml)
     blob = mjcf.to_blob(m)
     n = args.envs
-    phys = CudaPhysics(blob, n, device=local)
+    phys = CudaPhysics(blob, n)
     q, v, rng = initial_state(m, n, shard_seeds(rank)["state"])
     phys.set(Field.QPOS, range(n), q)
     phys.set(Field.QVEL, range(n), v)
+    K, W, P = args.steps, args.warmup, args.preroll
+    ctrl_all = torch.from_numpy(rng.uniform(-1, 1, (P + W + K, n, m.nu))).to(dev)
+    # pre-roll (outside every timed region): the Ant falls from qpos0 and
+    # lands, so that the timed steps see ground contact; every variant then
+    # starts from this state
+    phys.set_solver(warm=int(WarmStart.REF_PREV_QACC))
+    for k in range(P):
+        phys.step_device(range(n), 1, ctrl_all[k].data_ptr())
+    snap = {f: phys.get(f, range(n)) for f in (Field.QPOS, Field.QVEL, Field.QACC)}
+
+    def restore():
+        for f, x in snap.items():
+            phys.set(f, range(n), x)
+
     if args.lanes or args.per_block:
         phys.set_launch(args.lanes, args.per_block)
     elif not args.no_autotune:
@@ -271,8 +292,6 @@ def run_ours(args):
     clocks = ClockSampler(local)
     clocks.start()
 
-    K, W = args.steps, args.warmup
-    ctrl_all = torch.from_numpy(rng.uniform(-1, 1, (W + K, n, m.nu))).to(dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     stream = torch.cuda.ExternalStream(phys.stream(), device=dev)
 
@@ -282,70 +301,60 @@ def run_ours(args):
             dist.barrier()
         torch.cuda.synchronize()
 
-    def timed_device_loop(ctrl, steps, warm):
+    def timed_device_loop(warm):
+        restore()
         phys.set_solver(warm=int(warm))
         for k in range(W):
-            phys.step_device(range(n), 1, ctrl[k].data_ptr())
+            phys.step_device(range(n), 1, ctrl_all[P + k].data_ptr())
         phys.synchronize()
         barrier()
         total_ms = 0.0
-        for k in range(steps):
+        iters = []
+        for k in range(K):
             flush.fill_(float(k))
             torch.cuda.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            phys.step_device(range(n), 1, ctrl[W + k].data_ptr())
+            phys.step_device(range(n), 1, ctrl_all[P + W + k].data_ptr())
             e1.record(stream)
             e1.synchronize()
             total_ms += e0.elapsed_time(e1)
+            st = phys.stats()
+            iters.append(st["iters"][st["nrows"] > 0])
         barrier()
-        return total_ms
+        return total_ms, st, np.concatenate(iters)
 
-    ms_ref = timed_device_loop(ctrl_all, K, WarmStart.REF_PREV_QACC)
-    st = phys.stats()
-    # cold-start Newton on the same trajectory distribution (fresh state)
-    phys.set(Field.QPOS, range(n), q)
-    phys.set(Field.QVEL, range(n), v)
-    ms_cold = timed_device_loop(ctrl_all, K, WarmStart.COLD)
-    st_cold = phys.stats()
-    # learned warm start: a network trained on converged contact forces of a
-    # separate 1024-env Ant run, then the same workload again
-    learned = None
-    if not args.no_learned:
-        from pippin_b200 import warm
-        seeds = shard_seeds(rank)
-        tm, trng = CudaPhysics(blob, 1024, device=local), np.random.default_rng(seeds["train_ctrl"])
-        tq, tv, _ = initial_state(m, 1024, seeds["train_state"])
-        tm.set(Field.QPOS, range(1024), tq)
-        tm.set(Field.QVEL, range(1024), tv)
-        X, F = warm.collect(tm, 150, controls=lambda t: trng.uniform(-1, 1, (1024, m.nu)), skip=20)
-        tm.close()
-        w, losses = warm.train(X, F, epochs=15, batch=2048, lr=1e-3, seed=1)
-        phys.set_warm_mlp(w)
-        phys.set(Field.QPOS, range(n), q)
-        phys.set(Field.QVEL, range(n), v)
-        ms_learned = timed_device_loop(ctrl_all, K, WarmStart.LEARNED)
-        st_l = phys.stats()
-        learned = {"value": n * ws * K / (ms_learned * 1e-3), "mean_iters": float(st_l["iters"].mean()),
-                   "p99_iters": float(np.percentile(st_l["iters"], 99)), "train_samples": int(len(X)),
-                   "train_loss": [float(losses[0]), float(losses[-1])]}
+    ms_ref, st, it_ref = timed_device_loop(WarmStart.REF_PREV_QACC)
+    ms_cold, st_cold, it_cold = timed_device_loop(WarmStart.COLD)
+    # learned warm start (one GPU): a network trained on the plain solver's
+    # converged contact forces (config 5's training set: 10M pairs from a
+    # 16384-env Ant run), then the same workload again
+    learned, extras = None, {}
+    if not args.no_learned and ws == 1:
+        ant_line, wts = learned_eval("ant", args.learned_envs, args.learned_samples, args.extras_steps, 5)
+        extras["learned_ant"] = ant_line
+        phys.set_warm_mlp(wts)
+        ms_learned, st_l, it_l = timed_device_loop(WarmStart.LEARNED)
+        learned = {"value": n * ws * K / (ms_learned * 1e-3), "ms_per_step": ms_learned / K,
+                   "mean_iters": float(it_l.mean()) if len(it_l) else 0.0,
+                   "p99_iters": float(np.percentile(it_l, 99)) if len(it_l) else 0.0,
+                   "train_samples": ant_line["train"]["samples"], "train_loss": ant_line["train"]["loss"]}
     phys.set_solver(warm=int(WarmStart.REF_PREV_QACC))
 
     # end to end through the C-ABI with host buffers
     pin_ctrl = torch.empty((n, m.nu), dtype=torch.float64, pin_memory=True).numpy()
     pin_q = torch.empty((n, m.nq), dtype=torch.float64, pin_memory=True).numpy()
     ctrl_host = ctrl_all.cpu().numpy()
-    phys.set(Field.QPOS, range(n), q)
-    phys.set(Field.QVEL, range(n), v)
+    restore()
     for k in range(W):
-        pin_ctrl[:] = ctrl_host[k]
+        pin_ctrl[:] = ctrl_host[P + k]
         phys.set(Field.CTRL, range(n), pin_ctrl)
         phys.step(range(n), 1)
         phys.get(Field.QPOS, range(n), out=pin_q)
     barrier()
     e2e_ms = 0.0
     for k in range(K):
-        pin_ctrl[:] = ctrl_host[W + k]
+        pin_ctrl[:] = ctrl_host[P + W + k]
         flush.fill_(float(k))
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -359,19 +368,18 @@ def run_ours(args):
     barrier()
 
     # per-phase device time over K further substeps of the same workload
-    # (fresh state, same warm-up), one event pair per phase kernel
-    phys.set(Field.QPOS, range(n), q)
-    phys.set(Field.QVEL, range(n), v)
+    # (same start state, same warm-up), one event pair per phase kernel
+    restore()
     for k in range(W):
-        phys.step_device(range(n), 1, ctrl_all[k].data_ptr())
+        phys.step_device(range(n), 1, ctrl_all[P + k].data_ptr())
     phys.synchronize()
     phase_ms = {"smooth": 0.0, "collide": 0.0, "newton": 0.0}
     torch.cuda.nvtx.range_push("phase_timing")  # profilers can limit themselves to these launches
     for k in range(K):
         flush.fill_(float(k))
         torch.cuda.synchronize()
-        for name, ms in phys.time_phases(range(n), 1, ctrl_all[W + k].data_ptr()).items():
-            phase_ms[name] += ms
+        for name, ms in phys.time_phases(range(n), 1, ctrl_all[P + W + k].data_ptr()).items():
+            phase_ms[name] = phase_ms.get(name, 0.0) + ms
     torch.cuda.nvtx.range_pop()
     barrier()
     clock_info = clocks.stop()
@@ -391,15 +399,17 @@ def run_ours(args):
             "metric": "Ant env-steps/s", "value": value, "unit": "env-steps/s", "n_gpus": ws, "steps": K,
             "warmup": W, "ms_per_step": ms_ref / K, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": dict(workload(n), parallelism=f"env-sharded x{ws} (no collective)",
+            "config": dict(workload(n, P), parallelism=f"env-sharded x{ws} (no collective)",
                            launch={"lanes_per_env": lanes, "envs_per_block": per_block, "blocks": blocks}),
             "e2e": {"value": e2e, "unit": "env-steps/s", "h2d_bytes_per_step": n * m.nu * 8,
                     "d2h_bytes_per_step": n * m.nq * 8},
             "gpu_launches": 3 * K,
             "variants": {"newton_ref_prev_qacc": value, "newton_cold": value_cold,
-                         "mean_iters_ref": float(st["iters"].mean()), "mean_iters_cold": float(st_cold["iters"].mean()),
-                         "p99_iters_ref": float(np.percentile(st["iters"], 99)),
-                         "p99_iters_cold": float(np.percentile(st_cold["iters"], 99)),
+                         "mean_iters_ref": float(it_ref.mean()) if len(it_ref) else 0.0,
+                         "mean_iters_cold": float(it_cold.mean()) if len(it_cold) else 0.0,
+                         "p99_iters_ref": float(np.percentile(it_ref, 99)) if len(it_ref) else 0.0,
+                         "p99_iters_cold": float(np.percentile(it_cold, 99)) if len(it_cold) else 0.0,
+                         "iters_over": "envs with constraint rows",
                          "newton_learned": learned,
                          "mean_ncon": float(st["ncon"].mean()), "mean_rows": float(st["nrows"].mean())},
             "roofline": {"bound": "fp64", "kernel": f"{top}_kernel", "achieved": achieved, "peak": peak,
@@ -420,23 +430,35 @@ def run_ours(args):
             rate, cores, sample = cpu_rollout_rate(blob, m, 1024, args.cpu_seconds)
             line["cpu_baseline"] = {"value": rate, "unit": "env-steps/s", "cores": cores, "kind": "port",
                                     "sample": sample}
-        print(json.dumps(line), flush=True)
     phys.close()
+    if rank == 0 and ws == 1 and not args.no_extras:
+        # configs 2-5 beside the headline, each with its oracle sample on the
+        # host cores (bounded: a few seconds of GPU time each)
+        E = args.extras_steps
+        extras["tabletop"] = scene_measure("tabletop", 8192, E, 300)
+        extras["hull_tumble"] = scene_measure("hull_tumble", 4096, E, 250)
+        extras["cartpole"] = scene_measure("cartpole", 16384, 4 * E, 50)
+        extras["arm3hinge"] = scene_measure("arm3hinge", 16384, 4 * E, 50)
+        if not args.no_learned:
+            extras["learned_tabletop"], _ = learned_eval("tabletop", args.learned_envs, args.learned_samples, E, 5)
+    if rank == 0:
+        if extras:
+            line["configs"] = extras
+        print(json.dumps(line), flush=True)
     if ws > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
 
 
-def run_learned_eval(args):
-    """The learned Newton warm start on Ant and the tabletop scene: training
-    pairs (24 contact features -> converged frame forces) from the plain
-    solver's own converged solves, a network fitted to them on the GPU, then
-    cold start vs learned start on the same workload at the same 1e-10
-    tolerance (iteration counts and CUDA-graph step time). One JSON line per
-    scene (rank 0; one GPU)."""
+def learned_eval(name, n, samples, K, W, weights=None, epochs=8):
+    """The learned Newton warm start on Ant or the tabletop scene (config 5):
+    training pairs (24 contact features -> converged frame forces) from the
+    plain solver's own converged solves, a network fitted to them on the GPU
+    (or `weights`, when given), then cold start vs learned start on the same
+    workload at the same 1e-10 tolerance (iteration counts and CUDA-graph
+    step time). Returns (the JSON line as a dict, the weights)."""
     import torch
     from pippin_b200 import CudaPhysics, Field, Param, WarmStart, mjcf, scenes, warm
-    n, K, W = args.learned_envs, args.steps, max(args.warmup, 3)
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
 
@@ -446,7 +468,7 @@ def run_learned_eval(args):
         q, v, rng = initial_state(m, n, seed)
         p.set(Field.QPOS, range(n), q)
         p.set(Field.QVEL, range(n), v)
-        return m, p, (lambda t: rng.uniform(-1, 1, (n, m.nu))), 20
+        return m, p, (lambda t: rng.uniform(-1, 1, (n, m.nu))), 100
 
     def tabletop(seed):
         plan = scenes.tabletop(n, seed=seed)
@@ -454,9 +476,11 @@ def run_learned_eval(args):
         p = CudaPhysics(mjcf.to_blob(m), n)
         p.set_solver(tolerance=TOL, iterations=ITERS)
         plan.apply(lambda pid, elem, vals: p.set_param(Param(pid), elem, range(n), vals), lambda: p.reset(range(n)))
-        return m, p, None, 50
+        return m, p, None, 100
 
-    for name, make in (("ant", ant), ("tabletop", tabletop)):
+    make = ant if name == "ant" else tabletop
+    train = None
+    if weights is None:
         t0 = time.perf_counter()
         m, p, controls, skip = make(11)
         xs, fs, steps = [], [], 0
@@ -465,7 +489,7 @@ def run_learned_eval(args):
                 p.set(Field.CTRL, range(n), controls(t))
             p.step(range(n), 1)
         got = 0
-        while got < args.learned_samples and steps < 20000:
+        while got < samples and steps < 20000:
             if controls is not None:
                 p.set(Field.CTRL, range(n), controls(steps))
             X, F = p.warm_samples(range(n))
@@ -477,67 +501,74 @@ def run_learned_eval(args):
                 p.close()
                 m, p, controls, _ = make(11 + steps)
         p.close()
-        X, F = np.concatenate(xs)[:args.learned_samples], np.concatenate(fs)[:args.learned_samples]
+        X, F = np.concatenate(xs)[:samples], np.concatenate(fs)[:samples]
         t_collect = time.perf_counter() - t0
         t0 = time.perf_counter()
-        w, losses = warm.train(X, F, epochs=8, batch=8192, lr=1e-3, seed=1)
-        t_train = time.perf_counter() - t0
-        out = {}
-        for mode, wm in (("cold", WarmStart.COLD), ("learned", WarmStart.LEARNED)):
-            m, p, controls, skip = make(7)
-            p.set_warm_mlp(w)
-            p.set_solver(warm=int(wm))
-            ctrl = None
-            if controls is not None:
-                ctrl = torch.from_numpy(np.stack([controls(t) for t in range(skip + W + K)])).to(dev)
-            for t in range(skip + W):
-                p.step_device(range(n), 1, ctrl[t].data_ptr() if ctrl is not None else 0)
-            p.synchronize()
-            stream = torch.cuda.ExternalStream(p.stream(), device=dev)
-            iters, ms = [], 0.0
-            for k in range(K):
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record(stream)
-                p.step_device(range(n), 1, ctrl[skip + W + k].data_ptr() if ctrl is not None else 0)
-                e1.record(stream)
-                e1.synchronize()
-                ms += e0.elapsed_time(e1)
-                st = p.stats()
-                iters.append(st["iters"][st["nrows"] > 0])
-            p.close()
-            it = np.concatenate(iters)
-            out[mode] = {"env_steps_per_s": n * K / (ms * 1e-3), "ms_per_step": ms / K,
-                         "mean_iters": float(it.mean()) if len(it) else 0.0,
-                         "p99_iters": float(np.percentile(it, 99)) if len(it) else 0.0}
-        line = {"metric": f"learned warm start, {name}", "impl": "ours", "envs": n, "steps": K, "warmup": W,
-                "tolerance": TOL, "dtype": "f64 physics, bf16 network (fp32 accumulate)", "data": "synthetic",
-                "train": {"samples": int(len(X)), "collect_steps": steps, "epochs": 8, "loss": [float(losses[0]), float(losses[-1])],
-                          "collect_s": t_collect, "train_s": t_train},
-                "iters_over": "envs with constraint rows",
-                "cold": out["cold"], "learned": out["learned"]}
+        weights, losses = warm.train(X, F, epochs=epochs, batch=8192, lr=1e-3, seed=1)
+        train = {"samples": int(len(X)), "collect_steps": steps, "epochs": epochs,
+                 "loss": [float(losses[0]), float(losses[-1])], "collect_s": t_collect,
+                 "train_s": time.perf_counter() - t0}
+    out = {}
+    for mode, wm in (("cold", WarmStart.COLD), ("ref_prev_qacc", WarmStart.REF_PREV_QACC),
+                     ("learned", WarmStart.LEARNED)):
+        m, p, controls, skip = make(7)
+        p.set_warm_mlp(weights)
+        p.set_solver(warm=int(wm))
+        ctrl = None
+        if controls is not None:
+            ctrl = torch.from_numpy(np.stack([controls(t) for t in range(skip + W + K)])).to(dev)
+        for t in range(skip + W):
+            p.step_device(range(n), 1, ctrl[t].data_ptr() if ctrl is not None else 0)
+        p.synchronize()
+        stream = torch.cuda.ExternalStream(p.stream(), device=dev)
+        iters, ms = [], 0.0
+        for k in range(K):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            p.step_device(range(n), 1, ctrl[skip + W + k].data_ptr() if ctrl is not None else 0)
+            e1.record(stream)
+            e1.synchronize()
+            ms += e0.elapsed_time(e1)
+            st = p.stats()
+            iters.append(st["iters"][st["nrows"] > 0])
+        p.close()
+        it = np.concatenate(iters)
+        out[mode] = {"env_steps_per_s": n * K / (ms * 1e-3), "ms_per_step": ms / K,
+                     "mean_iters": float(it.mean()) if len(it) else 0.0,
+                     "p99_iters": float(np.percentile(it, 99)) if len(it) else 0.0}
+    line = {"metric": f"learned warm start, {name}", "impl": "ours", "envs": n, "steps": K, "warmup": W,
+            "tolerance": TOL, "dtype": "f64 physics, bf16 network (fp32 accumulate)", "data": "synthetic",
+            "train": train, "iters_over": "envs with constraint rows", "timed_after_substeps": skip + W}
+    line.update(out)
+    return line, weights
+
+
+def run_learned_eval(args):
+    """--learned-eval: one JSON line per scene (Ant, tabletop), rank 0, one GPU."""
+    for name in ("ant", "tabletop"):
+        line, _ = learned_eval(name, args.learned_envs, args.learned_samples, args.steps, max(args.warmup, 3))
         print(json.dumps(line), flush=True)
 
 
-def run_scene(args):
+def scene_measure(scene, n, K, W, cpu=True):
     """Device env-steps/s and per-phase time of the tabletop (config 3), the
     hull tumble (config 4) or a contact-free model (config 2: random states
     over the joint ranges, qvel N(0, 1), per-env masses x U[0.5, 2], random
     controls held) after W settling substeps, with the oracle's rate on a
-    bounded sample of the same workload on the host cores beside it. One
-    JSON line (one GPU)."""
+    bounded sample of the same workload on the host cores beside it. Returns
+    the JSON line as a dict (one GPU)."""
     import torch
     from oracle.oracle import CTRL, QPOS, QVEL, Oracle
     from pippin_b200 import CudaPhysics, Field, Param, mjcf, scenes
-    n, K, W = args.envs, args.steps, max(args.warmup, 3)
     torch.cuda.set_device(0)
-    if args.scene == "tabletop":
+    if scene == "tabletop":
         plan = scenes.tabletop(n, seed=5)
         m = mjcf.load_string(plan.xml)
         desc = (f"tabletop: {n} envs, 2-6 objects each (boxes, cylinders, spheres), dropped 5-15 cm, dt 0.002, "
                 f"Newton tol 1e-10 cap {ITERS}; timed after {W} substeps")
-    elif args.scene in ("cartpole", "arm3hinge"):
-        m = mjcf.load_string(scenes.cartpole_xml() if args.scene == "cartpole" else scenes.arm3hinge_xml())
-        desc = (f"{args.scene}: {n} envs, qpos uniform over the joint ranges (hinges [-pi, pi], slides +-0.5), "
+    elif scene in ("cartpole", "arm3hinge"):
+        m = mjcf.load_string(scenes.cartpole_xml() if scene == "cartpole" else scenes.arm3hinge_xml())
+        desc = (f"{scene}: {n} envs, qpos uniform over the joint ranges (hinges [-pi, pi], slides +-0.5), "
                 f"qvel N(0,1), per-env masses x U[0.5,2], controls U[-1,1] held; timed after {W} substeps")
     else:
         m = mjcf.load_string(scenes.hull_tumble_xml())
@@ -546,13 +577,13 @@ def run_scene(args):
     blob = mjcf.to_blob(m)
 
     def setup(sim, count, set_param, reset, set_q, set_v, set_ctrl=None):
-        if args.scene == "tabletop":
+        if scene == "tabletop":
             pl = scenes.tabletop(count, seed=5)
             for pid, elem, vals in pl.params:
                 set_param(pid, elem, vals)
             set_param(11, 0, pl.qpos0)
             reset()
-        elif args.scene in ("cartpole", "arm3hinge"):
+        elif scene in ("cartpole", "arm3hinge"):
             rng = np.random.default_rng(5)
             q = np.tile(np.array(m.qpos0), (count, 1))
             for j in range(m.njnt):
@@ -595,12 +626,21 @@ def run_scene(args):
     ph = {"smooth": 0.0, "collide": 0.0, "newton": 0.0}
     for k in range(K):
         for name, t in p.time_phases(range(n), 1).items():
-            ph[name] += t
+            ph[name] = ph.get(name, 0.0) + t
     st = p.stats()
     launch = p.phase_launch()
     p.close()
     # the oracle on a sample of the same workload (same settling, then timed)
-    cn = 4096 if args.scene in ("cartpole", "arm3hinge") else 256
+    cn = 4096 if scene in ("cartpole", "arm3hinge") else 256
+    line = {"metric": f"{scene} env-steps/s", "value": n * K / (ms * 1e-3), "unit": "env-steps/s",
+            "n_gpus": 1, "steps": K, "warmup": W, "ms_per_step": ms / K, "higher_is_better": True, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": desc, "envs": n},
+            "phases": {k: {"ms_per_launch": v / K, "launch": dict(zip(("lanes_per_env", "envs_per_block", "blocks"),
+                                                                       launch[k]))} for k, v in ph.items()},
+            "mean_ncon": float(st["ncon"].mean()), "mean_rows": float(st["nrows"].mean()),
+            "mean_iters": float(st["iters"].mean())}
+    if not cpu:
+        return line
     o = Oracle(blob, cn, threads=0, fast=True)
     o.set_solver(tolerance=TOL, iterations=ITERS)
     setup(o, cn, lambda pid, elem, vals: o.set_param(pid, elem, np.asarray(vals), 0, cn),
@@ -611,15 +651,14 @@ def run_scene(args):
     ck = max(1, min(K, 100 if cn > 256 else 50))
     o.step(0, cn, ck)
     cpu_rate = cn * ck / (time.perf_counter() - t0)
-    line = {"metric": f"{args.scene} env-steps/s", "value": n * K / (ms * 1e-3), "unit": "env-steps/s",
-            "n_gpus": 1, "steps": K, "warmup": W, "ms_per_step": ms / K, "higher_is_better": True, "dtype": "f64",
-            "data": "synthetic", "config": {"workload": desc, "envs": n},
-            "phases": {k: {"ms_per_launch": v / K, "launch": dict(zip(("lanes_per_env", "envs_per_block", "blocks"),
-                                                                       launch[k]))} for k, v in ph.items()},
-            "mean_ncon": float(st["ncon"].mean()), "mean_rows": float(st["nrows"].mean()),
-            "mean_iters": float(st["iters"].mean()),
-            "cpu_baseline": {"value": cpu_rate, "unit": "env-steps/s", "cores": o.threads, "kind": "port",
-                             "sample": f"{args.scene} {cn} envs x {ck} substeps after the same settling (oracle)"}}
+    line["cpu_baseline"] = {"value": cpu_rate, "unit": "env-steps/s", "cores": o.threads, "kind": "port",
+                            "sample": f"{scene} {cn} envs x {ck} substeps after the same settling (oracle)"}
+    o.close()
+    return line
+
+
+def run_scene(args):
+    line = scene_measure(args.scene, args.envs, args.steps, max(args.warmup, 3))
     print(json.dumps(line), flush=True)
 
 
@@ -652,15 +691,19 @@ def run_render(args):
     phys.set(Field.QPOS, range(n), q)
     phys.set(Field.QVEL, range(n), v)
     phys.step(range(n), 50)
-    g, c = phys.poses(range(n))
+    g, c = phys.poses(range(n))  # host copies, for the e2e leg
     sc = phys.scene()
-    phys.close()
+    ctrl = torch.from_numpy(rng.uniform(-1, 1, (n, m.nu))).to(dev)
+    pstream = torch.cuda.ExternalStream(phys.stream(), device=dev)
     published = {64: 310_000.0, 128: 195_000.0}  # README.md:115-116, 4096 Ant envs on an Apple GPU
     for res in [int(x) for x in args.render.split(",")]:
         cfg = R.RenderConfig(res, res, [R.ViewSource.look_at([1.5, -1.5, 1.2], [0.0, 0.0, 0.3], 45.0)], 0.01, 20.0)
         r = R.CudaRenderer(sc, cfg)
-        gd = torch.from_numpy(g.reshape(-1)).to(dev)
-        cd = torch.from_numpy(c.reshape(-1).copy()).to(dev)
+        # poses straight from the physics into the renderer's input buffers
+        gd = torch.empty(n * len(sc.geoms) * 12, dtype=torch.float32, device=dev)
+        cd = torch.empty(max(n * len(sc.cameras) * 12, 1), dtype=torch.float32, device=dev)
+        phys.poses_device(range(n), gd.data_ptr(), cd.data_ptr() if sc.cameras else 0)
+        phys.synchronize()
         ad = torch.from_numpy(np.tile(r.base_appearance, (n, 1)).reshape(-1)).to(dev)
         px = n * res * res
         rgba = torch.empty(px * 4, dtype=torch.uint8, device=dev)
@@ -697,6 +740,30 @@ def run_render(args):
         for _ in range(max(K // 4, 3)):
             r.render(0, n, g, c)
         e2e_ms = (time.perf_counter() - t0) * 1e3 / max(K // 4, 3)
+        # a physics step, its poses into the renderer's buffers and a frame,
+        # all on the device (the renderer's stream waits on the physics one)
+        def chain():
+            phys.step_device(range(n), 1, ctrl.data_ptr())
+            phys.poses_device(range(n), gd.data_ptr(), cd.data_ptr() if sc.cameras else 0)
+            ev = torch.cuda.Event()
+            ev.record(pstream)
+            stream.wait_event(ev)
+            frame()
+
+        for _ in range(W):
+            chain()
+        torch.cuda.synchronize()
+        chain_ms = 0.0
+        for k in range(K):
+            flush.fill_(float(k))
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(pstream)
+            chain()
+            e1.record(stream)
+            e1.synchronize()
+            chain_ms += e0.elapsed_time(e1)
+        chain_ms /= K
         out_bytes = px * 12
         line = {"metric": f"Ant frames/s at {res}x{res} (RGBA8 + depth + segmentation)", "value": n / (ms * 1e-3),
                 "unit": "frames/s", "n_gpus": 1, "steps": K, "warmup": W, "ms_per_step": ms,
@@ -710,6 +777,9 @@ def run_render(args):
                                         "note": "Metal renderer, 4096 Ant envs, Apple GPU (README.md:115-116)"},
                 "e2e": {"value": n / (e2e_ms * 1e-3), "unit": "frames/s", "h2d_bytes_per_step": int(g.nbytes + c.nbytes),
                         "d2h_bytes_per_step": int(out_bytes)},
+                "physics_step_then_frame": {"value": n / (chain_ms * 1e-3), "unit": "env-steps/s with a frame each",
+                                            "ms": chain_ms, "note": "pg_step_device, pg_poses_device into the "
+                                            "renderer's buffers, pg_render_frames_device; no host round trip"},
                 "gpu_launches": K, "clocks": clock_info,
                 "roofline": {"bound": "hbm", "kernel": "render_kernel", "achieved": out_bytes / (ms * 1e-3) / 1e9,
                              "peak": hbm_peak(), "unit": "GB/s", "frac": out_bytes / (ms * 1e-3) / 1e9 / hbm_peak(),
@@ -718,6 +788,7 @@ def run_render(args):
                                      "48 B a geom"}}
         print(json.dumps(line), flush=True)
         r.close()
+    phys.close()
 
 
 def main():

@@ -16,11 +16,12 @@ int pg_fp64_peak(int device, int iters, double* tflops, double* ms_out);
 
 /* Runs `nstep` substeps of envs [start, end) phase kernel by phase kernel,
  * with a CUDA event on the handle's stream between the phases, and adds up
- * the device time of each phase in ms_out[0..2] (smooth dynamics, collision,
- * Newton). ctrl_dev, when not NULL, holds (end - start) x nu controls in
- * device memory, copied in before the first substep as pg_step_device does.
- * Steps the simulation like pg_step; synchronises once per substep.
- * Returns PG_OK or a PG_ERR_* code. */
+ * the device time of each phase in ms_out[0..3] (smooth dynamics, collision,
+ * Newton, and the learned start's inference, which runs between collision
+ * and Newton in PG_WARM_LEARNED mode and is 0 otherwise). ctrl_dev, when not
+ * NULL, holds (end - start) x nu controls in device memory, copied in before
+ * the first substep as pg_step_device does. Steps the simulation like
+ * pg_step; synchronises once per substep. Returns PG_OK or a PG_ERR_* code. */
 int pg_time_phases(pg_handle* h, int64_t start, int64_t end, int64_t nstep, const double* ctrl_dev,
                    float* ms_out);
 

@@ -1136,7 +1136,7 @@ void destroy(pg_handle* h) {
   clear_graphs(h);
   void* ptrs[] = {h->d_model, h->qpos, h->qvel, h->ctrl, h->qacc, h->applied, h->params, h->iters, h->ncon,
                   h->nrows, h->status, h->scratch, h->work, h->prev_con, h->prev_ncon, h->queue, h->b_ctrl.p, h->b_qout.p, h->b_poses_g.p,
-                  h->b_poses_c.p, h->b_dbg.p, h->b_vals.p, h->b_ids.p, h->learn.feat, h->learn.force,
+                  h->b_poses_c.p, h->b_dbg.p, h->b_vals.p, h->b_ids.p, h->learn.items, h->learn.feat, h->learn.force,
                   h->learn.rows, (void*)h->learn.mlp_w, (void*)h->learn.mlp_f};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -1821,7 +1821,7 @@ int pg_time_phases(pg_handle* h, int64_t start, int64_t end, int64_t nstep, cons
   int rc = check_range(h, start, end);
   if (rc) return rc;
   if (nstep < 0 || nstep > (1 << 30)) return fail(PG_ERR_INVALID, "nstep out of range");
-  for (int k = 0; k < 3; k++) ms_out[k] = 0.0f;
+  for (int k = 0; k < 4; k++) ms_out[k] = 0.0f;
   int64_t cnt = end - start;
   if (cnt == 0 || nstep == 0) return PG_OK;
   CK(cudaSetDevice(h->device));
@@ -1833,24 +1833,30 @@ int pg_time_phases(pg_handle* h, int64_t start, int64_t end, int64_t nstep, cons
   a.count = (int)cnt;
   a.nstep = (int)nstep;
   SubstepCfg c = fit(h->cfg, cnt);
-  const LaunchCfg* shape[3] = {&c.smooth, &c.collide, &c.newton};
-  const int which[3] = {K_SMOOTH, K_COLLIDE, K_NEWTON};
-  cudaEvent_t ev[4];
+  // the learned start's inference runs between the collision and Newton
+  // phases, as launch_substep orders it; it is timed on its own
+  const bool learned = a.learn.mode == LEARN_PREDICT && a.warm_mode == WARM_LEARNED;
+  cudaEvent_t ev[5];
   for (auto& e : ev) CK(cudaEventCreate(&e));
   cudaError_t e = cudaSuccess;
   for (int64_t k = 0; k < nstep && e == cudaSuccess; k++) {
     a.sidx = (int)k;
     e = reset_queue(a, h->stream);
     if (e == cudaSuccess) e = cudaEventRecord(ev[0], h->stream);
-    for (int p = 0; p < 3 && e == cudaSuccess; p++) {
-      e = launch_phase(which[p], a, *shape[p], h->stream);
-      if (e == cudaSuccess) e = cudaEventRecord(ev[p + 1], h->stream);
-    }
-    if (e == cudaSuccess) e = cudaEventSynchronize(ev[3]);
-    for (int p = 0; p < 3 && e == cudaSuccess; p++) {
+    if (e == cudaSuccess) e = launch_phase(K_SMOOTH, a, c.smooth, h->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(ev[1], h->stream);
+    if (e == cudaSuccess) e = launch_phase(K_COLLIDE, a, c.collide, h->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(ev[2], h->stream);
+    if (e == cudaSuccess && learned) e = launch_learn(a, true, h->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(ev[3], h->stream);
+    if (e == cudaSuccess) e = launch_phase(K_NEWTON, a, c.newton, h->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(ev[4], h->stream);
+    if (e == cudaSuccess) e = cudaEventSynchronize(ev[4]);
+    const int slot[4] = {0, 1, 3, 2};  // smooth, collide, mlp, newton -> ms_out order
+    for (int p = 0; p < 4 && e == cudaSuccess; p++) {
       float ms = 0.0f;
       e = cudaEventElapsedTime(&ms, ev[p], ev[p + 1]);
-      ms_out[p] += ms;
+      ms_out[slot[p]] += ms;
     }
   }
   for (auto& x : ev) cudaEventDestroy(x);
@@ -1868,6 +1874,7 @@ static int ensure_learn(Handle* h) {
   if (h->learn.feat) return PG_OK;
   int64_t cap = learn_cap(h);
   h->learn.cap = (int)cap;
+  CK(cudaMalloc(&h->learn.items, sizeof(int) * cap * 2));
   CK(cudaMalloc(&h->learn.feat, sizeof(float) * cap * LEARN_NF));
   CK(cudaMalloc(&h->learn.force, sizeof(float) * cap * 3));
   CK(cudaMalloc(&h->learn.rows, sizeof(float) * cap * 4));
@@ -1897,6 +1904,7 @@ int pg_set_warm_mlp(pg_handle* h, const float* weights, size_t len) {
   CK(cudaMemcpyAsync((void*)h->learn.mlp_f, fb.data(), sizeof(float) * fb.size(), cudaMemcpyHostToDevice, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   CK(mlp_prepare());
+  CK(learn_prepare());
   h->learn.mode = LEARN_PREDICT;
   h->mlp_loaded = true;
   h->version++;

@@ -17,8 +17,10 @@
 // into shared memory.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "pg_kernels.h"
-#include "pg_mlp.h"
+#include "pg_mlp.cuh"
 #include "pg_pgs.cuh"
 
 namespace pg {
@@ -189,7 +191,7 @@ __global__ void __launch_bounds__(256, 2) collide_kernel(const __grid_constant__
     }
     T.sync();
     if (A.learn.mode == LEARN_DUMP || (A.learn.mode == LEARN_PREDICT && A.warm_mode == WARM_LEARNED))
-      learn_features(T, m, A.learn, e, ncon, A.st.qvel + env * m.nv, wk + A.k.a0, wk + A.k.cdof, wk + A.k.meta);
+      learn_list(T, A.learn, e, ncon, wk + A.k.meta);
     T.sync();
   }
 }
@@ -309,6 +311,105 @@ __global__ void __launch_bounds__(256, 2) newton_kernel(const __grid_constant__ 
       A.st.status[env] = (A.sidx == 0 ? 0 : A.st.status[env]) | status;
     }
     T.sync();
+  }
+}
+
+// ---------------------------------------------------------------- learned start
+// Features of the learned warm start's slots and, with INFER, the network's
+// predicted frame forces, between the collision and Newton phases. A block
+// takes 16 slots at a time: 8 threads share a slot's 3 x nv contact-frame
+// Jacobian entries (thread t takes dofs t, t + 8, ...) and reduce J qvel and
+// J a0 by shuffles, then write its 24 features (in the contact frame n, t1,
+// t2: depth, friction, J qvel (3), J a0 (3), the two bodies' translational
+// and rotational invweight sums, the normal (3), the env's touching-contact
+// count, the timestep, the point relative to each geom's centre (3 + 3),
+// both geom types, and 1) to the list and to shared memory, where the
+// tensor-core forward pass (mlp_group) reads them.
+__device__ inline double learn_feature(int f, const DModel& m, const double* r, const double* prm, const double* geo,
+                                       const double (&jv)[3], const double (&ja)[3], double nt) {
+  int g1 = (int)r[C_G1], g2 = (int)r[C_G2];
+  int b1 = m.geom_body[g1], b2 = m.geom_body[g2];
+  switch (f) {
+    case 0: return r[C_DEPTH];
+    case 1: return fmax(prm[m.p_friction + g1], prm[m.p_friction + g2]);
+    case 2: case 3: case 4: return jv[f - 2];
+    case 5: case 6: case 7: return ja[f - 5];
+    case 8: return prm[m.p_body_invw + 2 * b1] + prm[m.p_body_invw + 2 * b2];
+    case 9: return prm[m.p_body_invw + 2 * b1 + 1] + prm[m.p_body_invw + 2 * b2 + 1];
+    case 10: case 11: case 12: return r[C_NORMAL + f - 10];
+    case 13: return nt;
+    case 14: return m.timestep;
+    case 15: case 16: case 17: return r[C_POS + f - 15] - geo[G_STRIDE * g2 + G_POS + f - 15];
+    case 18: case 19: case 20: return r[C_POS + f - 18] - geo[G_STRIDE * g1 + G_POS + f - 18];
+    case 21: return (double)m.geom_type[g1];
+    case 22: return (double)m.geom_type[g2];
+    default: return 1.0;
+  }
+}
+
+template <bool INFER>
+__global__ void __launch_bounds__(32 * MLP_WARPS) learn_kernel(const __grid_constant__ StepArgs A) {
+  const LearnArgs& L = A.learn;
+  const int64_t n = min(*L.count, L.cap);
+  if ((int64_t)blockIdx.x * 16 >= n) return;
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ float xs[16 * LEARN_NF];
+  MlpSmem S = mlp_smem_layout(smem);
+  S.X = xs;
+  // the weights arrive while the first group's features are formed
+  if (INFER) stage_weights_begin(MlpDevice{L.mlp_w, L.mlp_f}, S.W, S.F);
+  bool staged = !INFER;
+  const DModel& m = A.m;
+  const int nv = m.nv;
+  const int j = threadIdx.x >> 3, t = threadIdx.x & 7;  // slot of the group, thread of the slot
+  for (int64_t base = (int64_t)blockIdx.x * 16; base < n; base += (int64_t)gridDim.x * 16) {
+    const int64_t slot = base + j;
+    int env = -1, c = 0;
+    if (slot < n) {
+      env = L.items[2 * slot];
+      c = L.items[2 * slot + 1];
+    }
+    const bool live = env >= 0;
+    const double* wk = A.work + (size_t)(live ? env : 0) * A.k.stride;
+    const double* r = wk + A.k.contacts + C_STRIDE * c;
+    double jv[3] = {0.0, 0.0, 0.0}, ja[3] = {0.0, 0.0, 0.0};
+    if (live) {
+      int g1 = (int)r[C_G1], g2 = (int)r[C_G2];
+      int b1 = m.geom_body[g1], b2 = m.geom_body[g2];
+      V3 p = ld3(r + C_POS);
+      V3 dir[3] = {ld3(r + C_NORMAL), ld3(r + C_T1), ld3(r + C_T2)};
+      const double* cdof = wk + A.k.cdof;
+      const double* a0 = wk + A.k.a0;
+      const double* qvel = A.st.qvel + (size_t)env * nv;
+      for (int k = t; k < nv; k += 8)
+        for (int d = 0; d < 3; d++) {
+          double jk = pair_jac(m, cdof, b1, b2, p, dir[d], k);
+          jv[d] += jk * qvel[k];
+          ja[d] += jk * a0[k];
+        }
+    }
+#pragma unroll
+    for (int o = 1; o < 8; o <<= 1)
+      for (int d = 0; d < 3; d++) {
+        jv[d] += __shfl_xor_sync(0xffffffffu, jv[d], o);
+        ja[d] += __shfl_xor_sync(0xffffffffu, ja[d], o);
+      }
+    for (int f = t; f < LEARN_NF; f += 8) {
+      float v = 0.0f;
+      if (live)
+        v = (float)learn_feature(f, m, r, A.st.params + (size_t)env * m.pstride, wk + A.k.geoms, jv, ja,
+                                 wk[A.k.meta + K_META_LNUM]);
+      xs[j * LEARN_NF + f] = v;
+      if (slot < n) L.feat[slot * LEARN_NF + f] = v;
+    }
+    if (!staged) {
+      stage_weights_end();  // (its block barrier also publishes the features)
+      staged = true;
+    } else {
+      __syncthreads();
+    }
+    if (INFER) mlp_group(S, base, n, L.force);
+    else __syncthreads();
   }
 }
 
@@ -526,10 +627,8 @@ cudaError_t launch_smooth_collide(const StepArgs& a, const SubstepCfg& c, cudaSt
 cudaError_t launch_substep(const StepArgs& a, const SubstepCfg& c, cudaStream_t s) {
   cudaError_t e = launch_smooth_collide(a, c, s);
   if (e != cudaSuccess) return e;
-  if (a.learn.mode == LEARN_PREDICT && a.warm_mode == WARM_LEARNED) {
-    // frame forces of every touching contact the collision phase listed
-    e = mlp_forward(MlpDevice{a.learn.mlp_w, a.learn.mlp_f}, a.learn.feat, a.learn.cap, a.learn.force, s,
-                    a.learn.count, 296);
+  if (a.learn.mode == LEARN_DUMP || (a.learn.mode == LEARN_PREDICT && a.warm_mode == WARM_LEARNED)) {
+    e = launch_learn(a, a.learn.mode == LEARN_PREDICT, s);
     if (e != cudaSuccess) return e;
   }
   PG_LAUNCH(K_NEWTON, newton_kernel, c.newton, a);
@@ -537,6 +636,21 @@ cudaError_t launch_substep(const StepArgs& a, const SubstepCfg& c, cudaStream_t 
 }
 
 cudaError_t reset_queue(const StepArgs& a, cudaStream_t s) { return cudaMemsetAsync(a.queue, 0, 4 * sizeof(int), s); }
+
+cudaError_t learn_prepare() {
+  return cudaFuncSetAttribute(learn_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MLP_SMEM);
+}
+
+cudaError_t launch_learn(const StepArgs& a, bool infer, cudaStream_t s) {
+  // the list's slots are counted on the device: the grid covers the
+  // capacity, and blocks past this substep's slots return at once; two
+  // blocks an SM stay resident with the network staged
+  int64_t blocks = std::min<int64_t>((a.learn.cap + 15) / 16, 296);
+  if (blocks < 1) return cudaSuccess;
+  if (infer) learn_kernel<true><<<(unsigned)blocks, 32 * MLP_WARPS, MLP_SMEM, s>>>(a);
+  else learn_kernel<false><<<(unsigned)blocks, 32 * MLP_WARPS, 0, s>>>(a);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_phase(int which, const StepArgs& a, const LaunchCfg& c, cudaStream_t s) {
   switch (which) {

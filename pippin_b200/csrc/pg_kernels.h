@@ -30,6 +30,11 @@ cudaError_t launch_substep(const StepArgs& a, const SubstepCfg& c, cudaStream_t 
 cudaError_t launch_smooth_collide(const StepArgs& a, const SubstepCfg& c, cudaStream_t s);
 // the pieces of launch_substep: the counter reset and one phase kernel
 cudaError_t reset_queue(const StepArgs& a, cudaStream_t s);
+// the learned start's features (and, with infer, its predictions) over the
+// collision phase's contact list; learn_prepare allows the kernel its
+// shared memory (once, before launches or captures)
+cudaError_t launch_learn(const StepArgs& a, bool infer, cudaStream_t s);
+cudaError_t learn_prepare();
 cudaError_t launch_phase(int which, const StepArgs& a, const LaunchCfg& c, cudaStream_t s);
 cudaError_t launch_set_const(const StepArgs& a, const LaunchCfg& c, const int* envs, int n, cudaStream_t s);
 cudaError_t launch_poses(const StepArgs& a, const LaunchCfg& c, float* geoms, float* cams, cudaStream_t s);

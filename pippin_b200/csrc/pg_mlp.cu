@@ -20,7 +20,7 @@
 #include <string>
 #include <vector>
 
-#include "pg_mlp.h"
+#include "pg_mlp.cuh"
 
 namespace pg {
 
@@ -56,122 +56,32 @@ void mlp_pack(const float* wt, uint16_t* w, float* f) {
 }
 
 // ---------------------------------------------------------------- inference
-__device__ inline uint32_t pack_bf16(float lo, float hi) {
-  __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
-  return *reinterpret_cast<uint32_t*>(&v);
-}
-
-__device__ inline void mma_bf16(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-      "{%0,%1,%2,%3};\n"
-      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
-}
-
-// B fragment of W (row n = output, k = input; row stride ld) for the n8 tile
-// at n0 and the k16 tile at k0
-__device__ inline void bfrag(const uint16_t* W, int ld, int n0, int k0, int g, int tq, uint32_t* b0, uint32_t* b1) {
-  const uint16_t* r = W + (n0 + g) * ld + k0 + 2 * tq;
-  *b0 = *reinterpret_cast<const uint32_t*>(r);
-  *b1 = *reinterpret_cast<const uint32_t*>(r + 8);
-}
-
-// one hidden layer: acc = A W^T over KT k-tiles, bias, ReLU, repacked as the
-// next layer's A fragments (8 k-tiles of 16)
-template <int KT>
-__device__ inline void hidden_layer(const uint32_t (&a)[KT][4], const uint16_t* W, int ld, const float* bias, int g,
-                                    int tq, uint32_t (&out)[8][4]) {
-#pragma unroll
-  for (int t = 0; t < 8; t++) {  // output k-tile t = n-tiles 2t, 2t+1
-    float c0[4] = {0.f, 0.f, 0.f, 0.f}, c1[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-    for (int kt = 0; kt < KT; kt++) {
-      uint32_t b0, b1;
-      bfrag(W, ld, 16 * t, 16 * kt, g, tq, &b0, &b1);
-      mma_bf16(c0, a[kt], b0, b1);
-      bfrag(W, ld, 16 * t + 8, 16 * kt, g, tq, &b0, &b1);
-      mma_bf16(c1, a[kt], b0, b1);
-    }
-    int n0 = 16 * t + 2 * tq, n1 = n0 + 8;
-    out[t][0] = pack_bf16(fmaxf(c0[0] + bias[n0], 0.f), fmaxf(c0[1] + bias[n0 + 1], 0.f));
-    out[t][1] = pack_bf16(fmaxf(c0[2] + bias[n0], 0.f), fmaxf(c0[3] + bias[n0 + 1], 0.f));
-    out[t][2] = pack_bf16(fmaxf(c1[0] + bias[n1], 0.f), fmaxf(c1[1] + bias[n1 + 1], 0.f));
-    out[t][3] = pack_bf16(fmaxf(c1[2] + bias[n1], 0.f), fmaxf(c1[3] + bias[n1 + 1], 0.f));
-  }
-}
-
-constexpr int MLP_WARPS = 4;  // 64 samples per block
-
-__global__ void __launch_bounds__(32 * MLP_WARPS) mlp_forward_kernel(MlpDevice d, const float* X, int64_t n, float* Y,
-                                                                     const int* ncount) {
-  if (ncount) n = min(n, (int64_t)*ncount);  // samples counted on the device
+// the standalone forward pass (pg_mlp_forward): features from global memory
+__global__ void __launch_bounds__(32 * MLP_WARPS) mlp_forward_kernel(MlpDevice d, const float* X, int64_t n,
+                                                                     float* Y) {
+  if ((int64_t)blockIdx.x * 16 >= n) return;
   extern __shared__ __align__(16) unsigned char smem[];
-  uint16_t* W = reinterpret_cast<uint16_t*>(smem);
-  float* F = reinterpret_cast<float*>(smem + sizeof(uint16_t) * MLP_BF16_ELEMS);
-  {
-    const int4* src = reinterpret_cast<const int4*>(d.w);
-    int4* dst = reinterpret_cast<int4*>(W);
-    for (int i = threadIdx.x; i < (int)(sizeof(uint16_t) * MLP_BF16_ELEMS / 16); i += blockDim.x) dst[i] = src[i];
-    for (int i = threadIdx.x; i < MLP_F32_ELEMS; i += blockDim.x) F[i] = d.f[i];
-  }
-  __syncthreads();
-  const uint16_t* W1 = W;
-  const uint16_t* W2 = W1 + MLP_H * MLP_LD1;
-  const uint16_t* W3 = W2 + MLP_H * MLP_LDH;
-  const uint16_t* W4 = W3 + MLP_H * MLP_LDH;
-  const float* mean = F;
-  const float* scale = F + MLP_IN;
-  const float* oscale = F + 2 * MLP_IN;
-  const float* b1 = F + 2 * MLP_IN + MLP_OUT;
-  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  int g = lane >> 2, tq = lane & 3;
-  for (int64_t base = ((int64_t)blockIdx.x * MLP_WARPS + warp) * 16; base < n; base += (int64_t)gridDim.x * MLP_WARPS * 16) {
-    int64_t r0 = base + g, r1 = base + g + 8;
-    auto x = [&](int64_t r, int c) -> float {
-      return (r < n && c < MLP_IN) ? (X[r * MLP_IN + c] - mean[c]) * scale[c] : 0.f;
-    };
-    uint32_t a1[2][4];
-#pragma unroll
-    for (int kt = 0; kt < 2; kt++) {
-      int c = 16 * kt + 2 * tq;
-      a1[kt][0] = pack_bf16(x(r0, c), x(r0, c + 1));
-      a1[kt][1] = pack_bf16(x(r1, c), x(r1, c + 1));
-      a1[kt][2] = pack_bf16(x(r0, c + 8), x(r0, c + 9));
-      a1[kt][3] = pack_bf16(x(r1, c + 8), x(r1, c + 9));
+  MlpSmem S = mlp_smem_layout(smem);
+  stage_weights(d, S.W, S.F);
+  for (int64_t base = (int64_t)blockIdx.x * 16; base < n; base += (int64_t)gridDim.x * 16) {
+    for (int t = threadIdx.x; t < 16 * MLP_IN; t += blockDim.x) {
+      int64_t r = base + t / MLP_IN;
+      S.X[t] = r < n ? X[r * MLP_IN + t % MLP_IN] : 0.f;
     }
-    uint32_t h1[8][4], h2[8][4];
-    hidden_layer<2>(a1, W1, MLP_LD1, b1, g, tq, h1);
-    hidden_layer<8>(h1, W2, MLP_LDH, b1 + MLP_H, g, tq, h2);
-    hidden_layer<8>(h2, W3, MLP_LDH, b1 + 2 * MLP_H, g, tq, h1);
-    float c[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-    for (int kt = 0; kt < 8; kt++) {
-      uint32_t b0, bb;
-      bfrag(W4, MLP_LDH, 0, 16 * kt, g, tq, &b0, &bb);
-      mma_bf16(c, h1[kt], b0, bb);
-    }
-    const float* b4 = b1 + 3 * MLP_H;
-    for (int j = 0; j < 4; j++) {
-      int col = 2 * tq + (j & 1);
-      int64_t r = j < 2 ? r0 : r1;
-      if (col < MLP_OUT && r < n) Y[r * MLP_OUT + col] = (c[j] + b4[col]) * oscale[col];
-    }
+    __syncthreads();
+    mlp_group(S, base, n, Y);
   }
 }
-
-static size_t mlp_smem() { return sizeof(uint16_t) * MLP_BF16_ELEMS + sizeof(float) * MLP_F32_ELEMS; }
 
 cudaError_t mlp_prepare() {
-  return cudaFuncSetAttribute(mlp_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mlp_smem());
+  return cudaFuncSetAttribute(mlp_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MLP_SMEM);
 }
 
-cudaError_t mlp_forward(const MlpDevice& d, const float* X, int64_t n, float* Y, cudaStream_t s, const int* ncount,
-                        int max_blocks) {
+cudaError_t mlp_forward(const MlpDevice& d, const float* X, int64_t n, float* Y, cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
-  int64_t blocks = (n + 16 * MLP_WARPS - 1) / (16 * MLP_WARPS);
-  if (blocks > max_blocks) blocks = max_blocks;
-  mlp_forward_kernel<<<(unsigned)blocks, 32 * MLP_WARPS, mlp_smem(), s>>>(d, X, n, Y, ncount);
+  int64_t blocks = (n + 15) / 16;
+  if (blocks > 2048) blocks = 2048;
+  mlp_forward_kernel<<<(unsigned)blocks, 32 * MLP_WARPS, MLP_SMEM, s>>>(d, X, n, Y);
   return cudaGetLastError();
 }
 
@@ -225,23 +135,106 @@ static cudaError_t gemm(int M, int N, int K, const float* A, long sai, long sak,
   return cudaGetLastError();
 }
 
-// db[j] = sum_i dY[i][j]
-__global__ void colsum_kernel(const float* dY, int M, int N, float* db) {
-  int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= N) return;
-  float s = 0.f;
-  for (int i = 0; i < M; i++) s += dY[(long)i * N + j];
-  db[j] = s;
+// Weight gradients C = A' B over a batch (A: K x M, B: K x N, both row-major
+// with row strides lda, ldb; K the batch) split along K: block (x, y, z)
+// sums rows [z kc, (z + 1) kc) of its 32 x 32 tile of C into part[z], and
+// sum_splits adds the splits in order (deterministic). Both operands are
+// read along their rows, so the loads coalesce.
+constexpr int SPLITS = 32;
+__global__ void __launch_bounds__(256) gemm_atb_kernel(int M, int N, int K, int kc, const float* A, int lda,
+                                                       const float* B, int ldb, float* part) {
+  __shared__ float As[GT][GT + 1], Bs[GT][GT + 1];
+  int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  int i0 = blockIdx.y * GT, j0 = blockIdx.x * GT;
+  int k_begin = blockIdx.z * kc, k_end = min(K, k_begin + kc);
+  float acc[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
+  for (int k0 = k_begin; k0 < k_end; k0 += GT) {
+    for (int t = threadIdx.x; t < GT * GT; t += 256) {
+      int kk = t / GT, c = t % GT;
+      int k = k0 + kk;
+      As[kk][c] = (k < k_end && i0 + c < M) ? A[(long)k * lda + i0 + c] : 0.f;
+      Bs[kk][c] = (k < k_end && j0 + c < N) ? B[(long)k * ldb + j0 + c] : 0.f;
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int k = 0; k < GT; k++) {
+      float a0 = As[k][2 * ty], a1 = As[k][2 * ty + 1];
+      float b0 = Bs[k][2 * tx], b1 = Bs[k][2 * tx + 1];
+      acc[0][0] += a0 * b0;
+      acc[0][1] += a0 * b1;
+      acc[1][0] += a1 * b0;
+      acc[1][1] += a1 * b1;
+    }
+    __syncthreads();
+  }
+  float* P = part + (size_t)blockIdx.z * M * N;
+  for (int u = 0; u < 2; u++)
+    for (int v = 0; v < 2; v++) {
+      int i = i0 + 2 * ty + u, j = j0 + 2 * tx + v;
+      if (i < M && j < N) P[(long)i * N + j] = acc[u][v];
+    }
 }
 
-// dO = 2 (O - Y) / (M * 3); loss += sum (O - Y)^2 / (M * 3)
-__global__ void mse_kernel(const float* O, const float* Y, int M, float* dO, double* loss) {
+// out[t] = sum over z of part[z][t], z in order
+__global__ void sum_splits_kernel(const float* part, int splits, int n, float* out) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= M * MLP_OUT) return;
-  float d = O[t] - Y[t];
+  if (t >= n) return;
+  float s = 0.f;
+  for (int z = 0; z < splits; z++) s += part[(size_t)z * n + t];
+  out[t] = s;
+}
+
+// column sums of dY (M x N) split along M: part[z][j] = sum of rows [z rc, (z + 1) rc)
+__global__ void colsum_split_kernel(const float* dY, int M, int N, int rc, float* part) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= N) return;
+  int r0 = blockIdx.y * rc, r1 = min(M, r0 + rc);
+  float s = 0.f;
+  for (int i = r0; i < r1; i++) s += dY[(long)i * N + j];
+  part[(size_t)blockIdx.y * N + j] = s;
+}
+
+static cudaError_t gemm_atb(int M, int N, int K, const float* A, int lda, const float* B, int ldb, float* C,
+                            float* part, cudaStream_t s) {
+  int kc = (K + SPLITS - 1) / SPLITS;
+  dim3 grid((N + GT - 1) / GT, (M + GT - 1) / GT, SPLITS);
+  gemm_atb_kernel<<<grid, 256, 0, s>>>(M, N, K, kc, A, lda, B, ldb, part);
+  sum_splits_kernel<<<(M * N + 255) / 256, 256, 0, s>>>(part, SPLITS, M * N, C);
+  return cudaGetLastError();
+}
+
+static cudaError_t colsum(const float* dY, int M, int N, float* db, float* part, cudaStream_t s) {
+  int rc = (M + SPLITS - 1) / SPLITS;
+  colsum_split_kernel<<<dim3((N + 127) / 128, SPLITS), 128, 0, s>>>(dY, M, N, rc, part);
+  sum_splits_kernel<<<(N + 255) / 256, 256, 0, s>>>(part, SPLITS, N, db);
+  return cudaGetLastError();
+}
+
+// dO = 2 (O - Y) / (M * 3); each block's share of sum (O - Y)^2 / (M * 3) into lpart[block]
+__global__ void __launch_bounds__(256) mse_kernel(const float* O, const float* Y, int M, float* dO, double* lpart) {
+  __shared__ double red[256];
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
   float inv = 1.0f / (float)(M * MLP_OUT);
-  dO[t] = 2.0f * d * inv;
-  atomicAdd(loss, (double)(d * d) * inv);
+  double v = 0.0;
+  if (t < M * MLP_OUT) {
+    float d = O[t] - Y[t];
+    dO[t] = 2.0f * d * inv;
+    v = (double)(d * d) * inv;
+  }
+  red[threadIdx.x] = v;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) lpart[blockIdx.x] = red[0];
+}
+
+// loss += the blocks' shares, in block order (one thread)
+__global__ void loss_add_kernel(const double* lpart, int nblocks, double* loss) {
+  double s = 0.0;
+  for (int b = 0; b < nblocks; b++) s += lpart[b];
+  *loss += s;
 }
 
 // Adam (Kingma & Ba 2015) on every parameter
@@ -268,8 +261,13 @@ __global__ void gather_kernel(const float* src, const int* idx, int n, int w, fl
 // grad (same layout as the parameters). P and grad start at W1.
 struct TrainBufs {
   float *H, *O, *dO, *dA, *dB;
+  float* part;     // SPLITS x 128 x 128 split-K partial sums
+  double* lpart;   // per-block loss shares
   double* loss;
 };
+// the partial-sum buffers' sizes for batches of M samples
+inline size_t train_part_floats() { return (size_t)SPLITS * MLP_H * MLP_H; }
+inline size_t train_lpart_doubles(int M) { return (size_t)(M * MLP_OUT + 255) / 256; }
 static cudaError_t mlp_batch_grad(const float* P, const float* Xn, const float* Yn, int M, float* grad,
                                   const TrainBufs& t, cudaStream_t s) {
   auto w = [&](int off) { return P + (off - MLP_W1); };
@@ -284,22 +282,26 @@ static cudaError_t mlp_batch_grad(const float* P, const float* Xn, const float* 
   G_(gemm(M, MLP_H, MLP_H, H1, MLP_H, 1, w(MLP_W2), 1, MLP_H, H2, w(MLP_B2), 1, nullptr, s));
   G_(gemm(M, MLP_H, MLP_H, H2, MLP_H, 1, w(MLP_W3), 1, MLP_H, H3, w(MLP_B3), 1, nullptr, s));
   G_(gemm(M, MLP_OUT, MLP_H, H3, MLP_H, 1, w(MLP_W4), 1, MLP_H, t.O, w(MLP_B4), 0, nullptr, s));
-  mse_kernel<<<(M * MLP_OUT + 255) / 256, 256, 0, s>>>(t.O, Yn, M, t.dO, t.loss);
+  {
+    int nb = (M * MLP_OUT + 255) / 256;
+    mse_kernel<<<nb, 256, 0, s>>>(t.O, Yn, M, t.dO, t.lpart);
+    loss_add_kernel<<<1, 1, 0, s>>>(t.lpart, nb, t.loss);
+  }
   // layer 4: dW4 = dO' H3, db4, dH3 = dO W4 * (H3 > 0)
-  G_(gemm(MLP_OUT, MLP_H, M, t.dO, 1, MLP_OUT, H3, MLP_H, 1, gw(MLP_W4), nullptr, 0, nullptr, s));
-  colsum_kernel<<<1, 32, 0, s>>>(t.dO, M, MLP_OUT, gw(MLP_B4));
+  G_(gemm_atb(MLP_OUT, MLP_H, M, t.dO, MLP_OUT, H3, MLP_H, gw(MLP_W4), t.part, s));
+  G_(colsum(t.dO, M, MLP_OUT, gw(MLP_B4), t.part, s));
   G_(gemm(M, MLP_H, MLP_OUT, t.dO, MLP_OUT, 1, w(MLP_W4), MLP_H, 1, t.dA, nullptr, 0, H3, s));
   // layer 3
-  G_(gemm(MLP_H, MLP_H, M, t.dA, 1, MLP_H, H2, MLP_H, 1, gw(MLP_W3), nullptr, 0, nullptr, s));
-  colsum_kernel<<<1, MLP_H, 0, s>>>(t.dA, M, MLP_H, gw(MLP_B3));
+  G_(gemm_atb(MLP_H, MLP_H, M, t.dA, MLP_H, H2, MLP_H, gw(MLP_W3), t.part, s));
+  G_(colsum(t.dA, M, MLP_H, gw(MLP_B3), t.part, s));
   G_(gemm(M, MLP_H, MLP_H, t.dA, MLP_H, 1, w(MLP_W3), MLP_H, 1, t.dB, nullptr, 0, H2, s));
   // layer 2
-  G_(gemm(MLP_H, MLP_H, M, t.dB, 1, MLP_H, H1, MLP_H, 1, gw(MLP_W2), nullptr, 0, nullptr, s));
-  colsum_kernel<<<1, MLP_H, 0, s>>>(t.dB, M, MLP_H, gw(MLP_B2));
+  G_(gemm_atb(MLP_H, MLP_H, M, t.dB, MLP_H, H1, MLP_H, gw(MLP_W2), t.part, s));
+  G_(colsum(t.dB, M, MLP_H, gw(MLP_B2), t.part, s));
   G_(gemm(M, MLP_H, MLP_H, t.dB, MLP_H, 1, w(MLP_W2), MLP_H, 1, t.dA, nullptr, 0, H1, s));
   // layer 1
-  G_(gemm(MLP_H, MLP_IN, M, t.dA, 1, MLP_H, Xn, MLP_IN, 1, gw(MLP_W1), nullptr, 0, nullptr, s));
-  colsum_kernel<<<1, MLP_H, 0, s>>>(t.dA, M, MLP_H, gw(MLP_B1));
+  G_(gemm_atb(MLP_H, MLP_IN, M, t.dA, MLP_H, Xn, MLP_IN, gw(MLP_W1), t.part, s));
+  G_(colsum(t.dA, M, MLP_H, gw(MLP_B1), t.part, s));
 #undef G_
   return cudaGetLastError();
 }
@@ -411,6 +413,8 @@ int pg_mlp_loss_grad(const float* weights, size_t wlen, const float* X, const fl
   MCK(d.alloc(&t.dO, (size_t)M * MLP_OUT));
   MCK(d.alloc(&t.dA, (size_t)M * MLP_H));
   MCK(d.alloc(&t.dB, (size_t)M * MLP_H));
+  MCK(d.alloc(&t.part, train_part_floats()));
+  MCK(d.alloc(&t.lpart, train_lpart_doubles(M)));
   MCK(d.alloc(&t.loss, 1));
   MCK(cudaMemcpy(P, weights + MLP_W1, sizeof(float) * MLP_PARAMS, cudaMemcpyHostToDevice));
   MCK(cudaMemcpy(dX, Xn.data(), sizeof(float) * Xn.size(), cudaMemcpyHostToDevice));
@@ -479,6 +483,8 @@ int pg_mlp_train(const float* X, const float* Y, int64_t n, int epochs, int batc
   MCK(d.alloc(&t.dO, (size_t)M * MLP_OUT));
   MCK(d.alloc(&t.dA, (size_t)M * MLP_H));
   MCK(d.alloc(&t.dB, (size_t)M * MLP_H));
+  MCK(d.alloc(&t.part, train_part_floats()));
+  MCK(d.alloc(&t.lpart, train_lpart_doubles(M)));
   MCK(d.alloc(&t.loss, 1));
   MCK(cudaMemcpy(P, wt.data() + MLP_W1, sizeof(float) * MLP_PARAMS, cudaMemcpyHostToDevice));
   MCK(cudaMemset(Mo, 0, sizeof(float) * MLP_PARAMS));

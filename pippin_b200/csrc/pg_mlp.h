@@ -43,9 +43,7 @@ struct MlpDevice {
 void mlp_pack(const float* weights, uint16_t* w_bf16, float* f32);
 // allows the forward kernel its shared memory (once, before launches or captures)
 cudaError_t mlp_prepare();
-// Y[n][3] = net(X[n][24]) on the tensor cores, on stream s; with ncount, the
-// sample count is min(n, *ncount) read on the device
-cudaError_t mlp_forward(const MlpDevice& d, const float* X, int64_t n, float* Y, cudaStream_t s,
-                        const int* ncount = nullptr, int max_blocks = 2048);
+// Y[n][3] = net(X[n][24]) on the tensor cores, on stream s
+cudaError_t mlp_forward(const MlpDevice& d, const float* X, int64_t n, float* Y, cudaStream_t s);
 
 }  // namespace pg

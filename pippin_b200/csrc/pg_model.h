@@ -189,6 +189,7 @@ struct LearnArgs {
   int mode;
   int cap;          // slots in the list
   int* count;       // slots taken this substep (reset with the work counters)
+  int* items;       // [cap][2] (env, contact) of each slot, from the collision phase
   float* feat;      // [cap][24]
   float* force;     // [cap][3]  predicted frame forces
   float* rows;      // [cap][4]  converged pyramid row forces (LEARN_DUMP)

@@ -140,20 +140,16 @@ __device__ inline double pair_jac(const DModel& m, const double* cdof, int b1, i
   return v;
 }
 
-// Features of the touching contacts (depth > 0, in contact order: the order
-// build_rows gives their pyramid rows) for the learned warm start, into one
-// slot each of the env-shared list; the env's first slot and count go to its
-// work-record meta (count -1 when the list is full). Per contact, in its
-// frame (n, t1, t2): depth, friction, J qvel (3), J a0 (3), the bodies'
-// translational and rotational invweight sums, the normal (3), the env's
-// touching-contact count, the timestep, the point relative to each geom's
-// center (3 + 3), both geom types, and 1.
+// The learned warm start's contact list: each touching contact (depth > 0,
+// in contact order, the order build_rows gives their pyramid rows) takes
+// one slot of the env-shared list, recording (env, contact); the env's
+// first slot and count go to its work-record meta (count -1 when the list
+// is full, and that env's slots below the capacity are marked unused). The
+// features and the prediction are formed per slot by learn_kernel.
 template <int G>
-__device__ void learn_features(const Tile<G>& T, const DModel& m, const LearnArgs& L, const EnvCtx& e, int ncon,
-                               const double* qvel, const double* a0, const double* cdof, double* meta) {
-  int lane = T.lane(), nv = m.nv;
+__device__ void learn_list(const Tile<G>& T, const LearnArgs& L, const EnvCtx& e, int ncon, double* meta) {
+  int lane = T.lane();
   const double* con = e.con;
-  const double* prm = e.prm;
   int nt = 0;
   for (int c = lane; c < ncon; c += G) nt += con[C_STRIDE * c + C_DEPTH] > 0.0 ? 1 : 0;
   nt = T.isum(nt);
@@ -165,7 +161,11 @@ __device__ void learn_features(const Tile<G>& T, const DModel& m, const LearnArg
     meta[K_META_LBASE] = base;
     meta[K_META_LNUM] = room ? nt : -1;
   }
-  if (!room || nt == 0) return;
+  if (nt == 0) return;
+  if (!room) {
+    for (int t = base + lane; t < L.cap && t < base + nt; t += G) L.items[2 * t] = -1;
+    return;
+  }
   int done = 0;
   for (int c0 = 0; c0 < ncon; c0 += G) {
     int c = c0 + lane;
@@ -173,30 +173,8 @@ __device__ void learn_features(const Tile<G>& T, const DModel& m, const LearnArg
     int tot;
     int rank = done + T.excl_scan(touch ? 1 : 0, &tot);
     if (touch) {
-      const double* r = con + C_STRIDE * c;
-      int g1 = (int)r[C_G1], g2 = (int)r[C_G2];
-      int b1 = m.geom_body[g1], b2 = m.geom_body[g2];
-      V3 p = ld3(r + C_POS);
-      V3 dir[3] = {ld3(r + C_NORMAL), ld3(r + C_T1), ld3(r + C_T2)};
-      double jv[3] = {0, 0, 0}, ja[3] = {0, 0, 0};
-      for (int k = 0; k < nv; k++)
-        for (int d = 0; d < 3; d++) {
-          double j = pair_jac(m, cdof, b1, b2, p, dir[d], k);
-          jv[d] += j * qvel[k];
-          ja[d] += j * a0[k];
-        }
-      const double* gp1 = e.geo + G_STRIDE * g1 + G_POS;
-      const double* gp2 = e.geo + G_STRIDE * g2 + G_POS;
-      float* f = L.feat + (size_t)(base + rank) * LEARN_NF;
-      double v[LEARN_NF] = {r[C_DEPTH],
-                            fmax(prm[m.p_friction + g1], prm[m.p_friction + g2]),
-                            jv[0], jv[1], jv[2], ja[0], ja[1], ja[2],
-                            prm[m.p_body_invw + 2 * b1] + prm[m.p_body_invw + 2 * b2],
-                            prm[m.p_body_invw + 2 * b1 + 1] + prm[m.p_body_invw + 2 * b2 + 1],
-                            dir[0].x, dir[0].y, dir[0].z, (double)nt, m.timestep,
-                            p.x - gp2[0], p.y - gp2[1], p.z - gp2[2], p.x - gp1[0], p.y - gp1[1], p.z - gp1[2],
-                            (double)m.geom_type[g1], (double)m.geom_type[g2], 1.0};
-      for (int k = 0; k < LEARN_NF; k++) f[k] = (float)v[k];
+      L.items[2 * (base + rank)] = e.env;
+      L.items[2 * (base + rank) + 1] = c;
     }
     done += tot;
   }
@@ -396,45 +374,131 @@ __device__ double cost(const Tile<G>& T, int k, int nr, const double* J, double*
   return c + T.sum(cr);
 }
 
+// Row field the learned start reuses once build_rows has formed aref and D
+// from it: the row's predicted activity (-1: none; set by newton_solve).
+constexpr int R_PRED = R_DIAG;
+
+// The learned candidate on the tile path, as newton_small forms it: the
+// minimiser of the cost with the rows' R_PRED activity held fixed (rows
+// without a prediction take their activity at a0), out = a0 - H^-1 g(a0)
+// with H = M + J_P' D J_P and g = J_P' D (J a0 - aref) over that set P.
+// Uses the Hessian slot, p and grad (free until Newton starts; out must be
+// none of them); leaves the set P in R_ACT. False if H is not positive
+// definite.
+template <int G>
+__device__ bool learned_candidate(const Tile<G>& T, int k, int nr, const double* J, double* R, const double* M,
+                                  const double* a0, const NewtonBufs& B, double* out) {
+  int lane = T.lane();
+  double *grad = B.grad, *p = B.p, *H = B.hess;
+  for (int r = lane; r < nr; r += G) {
+    double* rr = R + R_STRIDE * r;
+    double jar = dot_ref(J + r * k, 1, a0, 1, k) - rr[R_AREF];
+    rr[R_JAR] = jar;
+    rr[R_ACT] = rr[R_PRED] >= 0.0 ? rr[R_PRED] : (row_active(rr, jar) ? 1.0 : 0.0);
+  }
+  T.sync();
+  for (int i = lane; i < k; i += G) {
+    double g = 0.0;
+    for (int r = 0; r < nr; r++) {
+      const double* rr = R + R_STRIDE * r;
+      if (rr[R_ACT] != 0.0) g += (rr[R_D] * rr[R_JAR]) * J[r * k + i];
+    }
+    grad[i] = g;
+  }
+  for (int t = lane; t < k * (k + 1) / 2; t += G) {
+    int i = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+    while ((i + 1) * (i + 2) / 2 <= t) i++;
+    while (i * (i + 1) / 2 > t) i--;
+    int j = t - i * (i + 1) / 2;
+    double h = M[i * k + j];
+    for (int r = 0; r < nr; r++) {
+      const double* rr = R + R_STRIDE * r;
+      if (rr[R_ACT] == 0.0) continue;
+      double ji = J[r * k + i];
+      if (ji == 0.0) continue;
+      h += (rr[R_D] * ji) * J[r * k + j];
+    }
+    H[i * k + j] = h;
+  }
+  T.sync();
+  bool ok = chol_auto(T, H, k, k, 1, nullptr, nullptr, k, B.rinv);
+  if (ok) {
+    for (int i = lane; i < k; i += G) p[i] = -grad[i];
+    T.sync();
+    solve_auto(T, H, k, k, 1, nullptr, nullptr, k, B.rinv, p);
+    for (int i = lane; i < k; i += G) out[i] = a0[i] + p[i];
+  }
+  T.sync();
+  return ok;
+}
+
 // newton.rs:224-358: `a` holds the unconstrained acceleration on entry and
-// the constrained one on exit. Returns the iteration count.
+// the constrained one on exit. Returns the iteration count. With `cand`,
+// the learned candidate (learned_candidate) is the start the cost gate
+// judges against a0.
 template <int G>
 __device__ __noinline__ int newton_dense(const Tile<G>& T, int k, int nr, const double* J, double* R, const double* M,
                                          double* a,
-                            const double* warm, int max_iters, double tol, const NewtonBufs& B) {
+                            const double* warm, int max_iters, double tol, const NewtonBufs& B, bool cand = false) {
   int lane = T.lane();
   double *a0 = B.a0, *grad = B.grad, *p = B.p, *tmp = B.tmp, *tmp2 = B.tmp2, *mp = B.mp, *H = B.hess;
   for (int i = lane; i < k; i += G) a0[i] = a[i];
   T.sync();
+  // (mp is free until the line search, and the gate's cost() leaves it alone)
+  bool cand_kept = cand && learned_candidate(T, k, nr, J, R, M, a0, B, B.mp);
+  if (cand_kept) warm = B.mp;
+  // when the gate keeps the start, its cost evaluation leaves the first
+  // iteration's products there: M (a - a0) in tmp2, J a - aref in R_JAR
+  bool have = false;
   if (warm) {
-    double c0 = cost(T, k, nr, J, R, M, a0, a0, tmp, tmp2);
+    // the quadratic term of the cost is exactly zero at a0
+    double cr0 = 0.0;
+    for (int r = lane; r < nr; r += G) {
+      const double* rr = R + R_STRIDE * r;
+      double jar = dot_ref(J + r * k, 1, a0, 1, k) - rr[R_AREF];
+      if (row_active(rr, jar)) cr0 += 0.5 * rr[R_D] * jar * jar;
+    }
+    double c0 = T.sum(cr0);
     double c1 = cost(T, k, nr, J, R, M, warm, a0, tmp, tmp2);
-    if (c1 < c0)
-      for (int i = lane; i < k; i += G) a[i] = warm[i];
+    if (c1 < c0) {
+      for (int i = lane; i < k; i += G) {
+        a[i] = warm[i];
+        grad[i] = tmp2[i];
+      }
+      have = true;
+    } else {
+      cand_kept = false;
+    }
     T.sync();
   }
+  // a kept learned candidate counts as the first iteration, with R_ACT
+  // holding its active set (as in newton_small); otherwise no previous set
+  if (!cand_kept)
+    for (int r = lane; r < nr; r += G) R[R_STRIDE * r + R_ACT] = -1.0;
+  T.sync();
   mul_m(T, M, k, a0, tmp);
   double ss = 0.0;
   for (int i = lane; i < k; i += G) ss += tmp[i] * tmp[i];
   double scale = 1.0 + sqrt(T.sum(ss));
-  int iters = 0;
+  int iters = cand_kept ? 1 : 0;
   int maxit = max_iters > 1 ? max_iters : 1;
   while (iters < maxit) {
     iters++;
     for (int i = lane; i < k; i += G) tmp[i] = a[i] - a0[i];
     T.sync();
-    mul_m(T, M, k, tmp, grad);
+    if (!have) mul_m(T, M, k, tmp, grad);
     // residuals, active set; R_ACT keeps the previous iteration's set
     bool same = true;
     for (int r = lane; r < nr; r += G) {
       double* rr = R + R_STRIDE * r;
-      double jar = dot_ref(J + r * k, 1, a, 1, k) - rr[R_AREF];
+      double jar = have ? rr[R_JAR] : dot_ref(J + r * k, 1, a, 1, k) - rr[R_AREF];
       rr[R_JAR] = jar;
       double act = row_active(rr, jar) ? 1.0 : 0.0;
       if (act != rr[R_ACT]) same = false;
       rr[R_ACT] = act;
     }
     T.sync();
+    have = false;
     for (int i = lane; i < k; i += G) {
       double g = grad[i];
       for (int r = 0; r < nr; r++) {
@@ -570,11 +634,15 @@ constexpr int SMALL_ROWS = 2 * SMALL_N;  // rows the register Newton takes (two 
 //
 // Learned warm start (lforce != nullptr, lnum touching contacts whose
 // pyramid rows are the first 4 lnum rows): the predicted frame forces
-// (f_n, f_t1, f_t2) become row forces f_n / 4 +- f_tk / (2 mu), so that
-// sum_r f_r J_r = f_n J_n + f_t1 J_t1 + f_t2 J_t2, and the candidate start is
-// a0 + M^-1 sum_r f_r J_r', behind the same cost gate as the previous-step
-// start (newton.rs:238-245). With ldump, the converged forces of those rows
-// are written there (4 per contact) as training targets.
+// (f_n, f_t1, f_t2) become row forces f_n / 4 +- f_tk / (2 mu) (so that
+// sum_r f_r J_r = f_n J_n + f_t1 J_t1 + f_t2 J_t2), and a row is predicted
+// active when its force is positive; every other row takes its activity at
+// a0. The candidate start is the minimiser of the cost with that active set
+// held fixed, a0 - H^-1 g(a0), and it goes behind the same cost gate as the
+// previous-step start (newton.rs:238-245). When the prediction is the
+// solution's active set, the gradient there is zero to rounding and the
+// first iteration ends the solve. With ldump, the converged forces of those
+// rows are written there (4 per contact) as training targets.
 template <int G>
 __device__ inline int newton_small(const Tile<G>& T, int k, int nr, const double* Jsrc, const double* R,
                                          const double* M, double* a, const double* warm, int max_iters, double tol,
@@ -621,58 +689,73 @@ __device__ inline int newton_small(const Tile<G>& T, int k, int nr, const double
     T.sync();
   };
   auto jdot = [&](int s) { return dot_ref_sm(jrow(i + SMALL_N * s), B.x, k); };
-  // newton.rs:96-110
-  auto cost = [&](double xi) -> double {
-    double tmp = xi - a0;
-    publish(tmp);
-    double tmp2 = dof ? dot_ref_sm(mrow, B.x, k) : 0.0;
-    double c = 0.5 * T.sum(dof ? tmp * tmp2 : 0.0);
-    publish(xi);
-    double cr = 0.0;
-#pragma unroll
-    for (int s = 0; s < 2; s++)
-      if (has[s]) {
-        double jar = jdot(s) - aref[s];
-        if (bil[s] || jar < 0.0) cr += 0.5 * dr[s] * jar * jar;
-      }
-    return c + T.sum(cr);
-  };
+
   double ai = a0;
   double wl = wi;
   bool use_warm = warm != nullptr;
+  bool cand = false;                  // wl is the learned candidate
+  double pset[2] = {-1.0, -1.0};      // the activity it was formed with (this lane's rows)
   if (lforce && lnum > 0 && 4 * lnum <= nr) {
-    double cv0[2];
+    // residuals at a0, and each of this lane's rows' predicted activity
+    publish(a0);
+    double jr0[2], on[2];
 #pragma unroll
     for (int s = 0; s < 2; s++) {
       int r = i + SMALL_N * s;
-      cv0[s] = 0.0;
+      jr0[s] = has[s] ? jdot(s) - aref[s] : 0.0;
+      on[s] = (bil[s] || jr0[s] < 0.0) ? 1.0 : 0.0;
       if (has[s] && r < 4 * lnum) {
         int c = r / 4, q = r % 4;
         double mu = lfeat[c * LEARN_NF + 1];
         double fn = lforce[3 * c], ft = lforce[3 * c + 1 + q / 2];
-        cv0[s] = 0.25 * fn + (mu > 0.0 ? ((q & 1) ? -ft : ft) / (2.0 * mu) : 0.0);
+        double f = 0.25 * fn + (mu > 0.0 ? ((q & 1) ? -ft : ft) / (2.0 * mu) : 0.0);
+        on[s] = f > 0.0 ? 1.0 : 0.0;
       }
     }
+    // H = M + J_P' D J_P over the predicted set P, and g(a0) = J_P' D jar0
+    double cv0[2];
+#pragma unroll
+    for (int s = 0; s < 2; s++) cv0[s] = on[s] != 0.0 ? dr[s] : 0.0;
     coeffs(cv0);
-    double x = 0.0;
-    if (dof)
-      for (int r = 0; r < 4 * lnum; r++) {
-        double cf = B.c[r];
-        if (cf != 0.0) x += cf * jrow(r)[i];
-      }
     double hl[SMALL_N];
 #pragma unroll
     for (int q = 0; q < SMALL_N; q++) hl[q] = (dof && q <= i) ? mrow[q] : 0.0;
+    if (dof)
+      for (int r = 0; r < nr; r++) {
+        double d = B.c[r];
+        if (d == 0.0) continue;
+        const double* jr = jrow(r);
+        double ji = jr[i];
+        if (ji == 0.0) continue;
+        double e = d * ji;
+#pragma unroll
+        for (int q = 0; q < SMALL_N; q++)
+          if (q <= i && q < k) hl[q] += e * jr[q];
+      }
+#pragma unroll
+    for (int s = 0; s < 2; s++) cv0[s] = on[s] != 0.0 ? dr[s] * jr0[s] : 0.0;
+    coeffs(cv0);
+    double g0 = 0.0;
+    if (dof)
+      for (int r = 0; r < nr; r++) {
+        double cf = B.c[r];
+        if (cf != 0.0) g0 += cf * jrow(r)[i];
+      }
     double rv = 0.0;
     if (chol_regx(T, hl, k, B.L, &rv)) {
-      wl = a0 + solve_regx(T, hl, k, B.L, rv, dof ? x : 0.0);
+      wl = a0 + solve_regx(T, hl, k, B.L, rv, dof ? -g0 : 0.0);
       use_warm = true;
+      cand = true;
+      pset[0] = on[0];
+      pset[1] = on[1];
     }
   }
   // x = a0 once: M a0 for the scale, and J a0 for the cold cost, whose
   // quadratic term is exactly zero (a - a0 = 0)
   publish(a0);
   double ma0 = dof ? dot_ref_sm(mrow, B.x, k) : 0.0;
+  double gw = 0.0, jw[2] = {0.0, 0.0};
+  bool have = false;
   if (use_warm) {
     double cr = 0.0;
 #pragma unroll
@@ -682,27 +765,64 @@ __device__ inline int newton_small(const Tile<G>& T, int k, int nr, const double
         if (bil[s] || jar < 0.0) cr += 0.5 * dr[s] * jar * jar;
       }
     double c0 = T.sum(cr);
-    double c1 = cost(wl);
-    if (c1 < c0) ai = wl;
+    // the cost at wl (newton.rs:96-110), keeping its products M (wl - a0)
+    // and J wl - aref: the first iteration's when the gate keeps wl
+    double tw = wl - a0;
+    publish(tw);
+    double mw = dof ? dot_ref_sm(mrow, B.x, k) : 0.0;
+    double c = 0.5 * T.sum(dof ? tw * mw : 0.0);
+    publish(wl);
+    double cr1 = 0.0;
+#pragma unroll
+    for (int s = 0; s < 2; s++)
+      if (has[s]) {
+        jw[s] = jdot(s) - aref[s];
+        if (bil[s] || jw[s] < 0.0) cr1 += 0.5 * dr[s] * jw[s] * jw[s];
+      }
+    double c1 = c + T.sum(cr1);
+    if (c1 < c0) {
+      ai = wl;
+      gw = mw;
+      have = true;
+    } else {
+      cand = false;
+    }
   }
   double scale = 1.0 + sqrt(T.sum(ma0 * ma0));
-  int iters = 0;
+  // A kept learned candidate is the Newton step (full length) of the
+  // predicted active set from a0, and counts as the first iteration: the
+  // next one ends the solve by the reference's exit rule when the active set
+  // at the candidate is that set, i.e. when the candidate minimises the cost
+  // on a self-consistent active set, which is the optimality condition of
+  // the piecewise quadratic (newton.rs:273-276)
+  int iters = cand ? 1 : 0;
   int maxit = max_iters > 1 ? max_iters : 1;
-  double prev[2] = {-1.0, -1.0};  // the rows' activity in the previous iteration (none yet)
+  // the rows' activity in the previous iteration (-1: none yet)
+  double prev[2] = {cand ? pset[0] : -1.0, cand ? pset[1] : -1.0};
   double jar[2] = {0.0, 0.0}, act[2] = {0.0, 0.0}, cv[2];
   bool fresh = false;  // left at the convergence check: B.c holds D_r jar_r of the final a
   while (iters < maxit) {
     iters++;
     // gradient M (a - a0) + sum over active rows of D jar J_r (newton.rs:254-270)
     double tmp = ai - a0;
-    publish(tmp);
-    double grad = dof ? dot_ref_sm(mrow, B.x, k) : 0.0;
-    publish(ai);
+    double grad;
+    if (have) {  // the gate's products at the start it kept
+      grad = gw;
+      jar[0] = jw[0];
+      jar[1] = jw[1];
+      have = false;
+    } else {
+      publish(tmp);
+      grad = dof ? dot_ref_sm(mrow, B.x, k) : 0.0;
+      publish(ai);
+#pragma unroll
+      for (int s = 0; s < 2; s++)
+        if (has[s]) jar[s] = jdot(s) - aref[s];
+    }
     bool same = true;
 #pragma unroll
     for (int s = 0; s < 2; s++)
       if (has[s]) {
-        jar[s] = jdot(s) - aref[s];
         act[s] = (bil[s] || jar[s] < 0.0) ? 1.0 : 0.0;
         if (act[s] != prev[s]) same = false;
         prev[s] = act[s];
@@ -829,7 +949,7 @@ __device__ inline int newton_small(const Tile<G>& T, int k, int nr, const double
 template <int G>
 __device__ __noinline__ int newton_islands(const Tile<G>& T, const DModel& m, const WsLayout& w, const ScrLayout& s,
                                            const EnvCtx& e, int nr, double* a, const double* warm,
-                                           const NewtonBufs& B) {
+                                           const NewtonBufs& B, bool cand) {
   int lane = T.lane(), nv = m.nv;
   double* ws = e.ws;
   double* qfrc = ws + w.qfrc_c;
@@ -887,7 +1007,7 @@ __device__ __noinline__ int newton_islands(const Tile<G>& T, const DModel& m, co
   }
   for (int b = 0; b < m.nblock; b++) all_one &= blk_isl[b] == only;
   if (n_isl == 1 && all_one) {
-    int it = newton_dense(T, nv, nr, J, R, e.qm, a, warm, max_iters, tol, B);
+    int it = newton_dense(T, nv, nr, J, R, e.qm, a, warm, max_iters, tol, B, cand);
     add_constraint_force(T, nv, nr, J, R, a, (const int*)nullptr, qfrc);
     return it;
   }
@@ -912,14 +1032,17 @@ __device__ __noinline__ int newton_islands(const Tile<G>& T, const DModel& m, co
     }
     // rows of the island, in row order
     int nri = 0;
+    bool pred = false;  // a row of the island has a learned prediction
     for (int base = 0; base < nr; base += G) {
       int r = base + lane;
       bool in = r < nr && iscr[r] == isl;
       int tot;
       int off = T.excl_scan(in ? 1 : 0, &tot);
       if (in) idx[nv + nri + off] = r;
+      if (in && cand) pred |= R[R_STRIDE * r + R_PRED] >= 0.0;
       nri += tot;
     }
+    pred = T.any(pred);
     T.sync();
     for (int t = lane; t < kk * kk; t += G) subM[t] = e.qm[idx[t / kk] * nv + idx[t % kk]];
     for (int t = lane; t < nri * kk; t += G) subJ[t] = J[idx[nv + t / kk] * nv + idx[t % kk]];
@@ -929,49 +1052,13 @@ __device__ __noinline__ int newton_islands(const Tile<G>& T, const DModel& m, co
       wsub[i] = warm ? warm[idx[i]] : 0.0;
     }
     T.sync();
-    int it = newton_dense(T, kk, nri, subJ, subR, subM, suba, warm ? wsub : nullptr, max_iters, tol, B);
+    int it = newton_dense(T, kk, nri, subJ, subR, subM, suba, warm ? wsub : nullptr, max_iters, tol, B, pred);
     iters = it > iters ? it : iters;
     for (int i = lane; i < kk; i += G) a[idx[i]] = suba[i];
     T.sync();
     add_constraint_force(T, kk, nri, subJ, subR, suba, idx, qfrc);
   }
   return iters;
-}
-
-// The learned warm start on the tile paths (several dof trees, or more dofs
-// or rows than the register Newton takes), as newton_small does it: the
-// predicted frame forces of the lnum touching contacts (whose pyramid rows
-// are the first 4 lnum rows) become row forces f_n / 4 +- f_tk / (2 mu), and
-// out = a + M^-1 sum_r f_r J_r' is the candidate start for the dense
-// solver's cost gate. M is factored per dof block in the Hessian's slot,
-// which is free until Newton starts. Returns false if M is not positive
-// definite (no candidate).
-template <int G>
-__device__ bool learned_start(const Tile<G>& T, const DModel& m, const WsLayout& w, const EnvCtx& e,
-                              const double* J, const double* a, const float* lfeat, const float* lforce, int lnum,
-                              double* out) {
-  int lane = T.lane(), nv = m.nv;
-  double* ws = e.ws;
-  double* F = e.fac;
-  double* rinv = ws + w.rinv;
-  for (int t = lane; t < nv * nv; t += G) F[t] = e.qm[t];
-  for (int i = lane; i < nv; i += G) {
-    double x = 0.0;
-    for (int r = 0; r < 4 * lnum; r++) {
-      int c = r / 4, q = r % 4;
-      double mu = lfeat[c * LEARN_NF + 1];
-      double fn = lforce[3 * c], ft = lforce[3 * c + 1 + q / 2];
-      double f = 0.25 * fn + (mu > 0.0 ? ((q & 1) ? -ft : ft) / (2.0 * mu) : 0.0);
-      if (f != 0.0) x += f * J[r * nv + i];
-    }
-    out[i] = x;
-  }
-  T.sync();
-  if (!chol_auto(T, F, nv, nv, m.nblock, m.block_adr, m.dof_block, m.maxbs, rinv)) return false;
-  solve_auto(T, F, nv, nv, m.nblock, m.block_adr, m.dof_block, m.maxbs, rinv, out);
-  for (int i = lane; i < nv; i += G) out[i] = a[i] + out[i];
-  T.sync();
-  return true;
 }
 
 // The converged forces -D_r (J_r a - aref_r) of rows [0, nrows) (zero where
@@ -1001,15 +1088,28 @@ __device__ int newton_solve(const Tile<G>& T, const DModel& m, const WsLayout& w
   if (nr == 0) return 0;
   double* J = e.scr + s.jac;
   double* R = e.scr + s.rows;
-  for (int r = lane; r < nr; r += G) R[R_STRIDE * r + R_ACT] = -1.0;  // no previous active set
+  bool learned = lnum > 0 && 4 * lnum <= nr;
+  bool cand = learned && lforce;
+  for (int r = lane; r < nr; r += G) {
+    double* rr = R + R_STRIDE * r;
+    rr[R_ACT] = -1.0;  // no previous active set
+    // the learned start's predicted activity of the touching contacts'
+    // pyramid rows (row force f_n / 4 +- f_tk / (2 mu) > 0), as newton_small
+    // forms it; -1 for every other row
+    double pred = -1.0;
+    if (cand && r < 4 * lnum) {
+      int c = r / 4, q = r % 4;
+      double mu = lfeat[c * LEARN_NF + 1];
+      double fn = lforce[3 * c], ft = lforce[3 * c + 1 + q / 2];
+      double f = 0.25 * fn + (mu > 0.0 ? ((q & 1) ? -ft : ft) / (2.0 * mu) : 0.0);
+      pred = f > 0.0 ? 1.0 : 0.0;
+    }
+    rr[R_PRED] = pred;
+  }
   T.sync();
   NewtonBufs B{ws + w.a0, ws + w.grad, ws + w.p, ws + w.tmp, ws + w.tmp2, ws + w.mp, e.fac, ws + w.rinv};
-  bool learned = lnum > 0 && 4 * lnum <= nr;
   if (m.nblock > 1) {
-    // the learned candidate goes over the previous qacc, which the learned
-    // mode does not read and the kernel rewrites after Newton
-    if (learned && lforce && learned_start(T, m, w, e, J, a, lfeat, lforce, lnum, ws + w.qacc)) warm = ws + w.qacc;
-    int it = newton_islands(T, m, w, s, e, nr, a, warm, B);
+    int it = newton_islands(T, m, w, s, e, nr, a, warm, B, cand);
     if (learned && ldump) dump_row_forces(T, nv, J, R, a, 4 * lnum, ldump);
     return it;
   }
@@ -1026,8 +1126,7 @@ __device__ int newton_solve(const Tile<G>& T, const DModel& m, const WsLayout& w
                           lnum, ldump);
     }
   }
-  if (learned && lforce && learned_start(T, m, w, e, J, a, lfeat, lforce, lnum, ws + w.qacc)) warm = ws + w.qacc;
-  int it = newton_dense(T, nv, nr, J, R, e.qm, a, warm, m.iterations, m.tolerance, B);
+  int it = newton_dense(T, nv, nr, J, R, e.qm, a, warm, m.iterations, m.tolerance, B, cand);
   add_constraint_force(T, nv, nr, J, R, a, (const int*)nullptr, qfrc);
   if (learned && ldump) dump_row_forces(T, nv, J, R, a, 4 * lnum, ldump);
   return it;

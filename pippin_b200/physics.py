@@ -268,9 +268,12 @@ class CudaPhysics:
         """Step like step_device, timing each phase kernel with CUDA events;
         returns the summed device milliseconds per phase."""
         s, e = _span(envs)
-        ms = (C.c_float * 3)()
+        ms = (C.c_float * 4)()
         self._check(self._L.pg_time_phases(self._h, s, e, int(nstep), C.c_void_p(ctrl_dev_ptr or None), ms))
-        return {"smooth": ms[0], "collide": ms[1], "newton": ms[2]}
+        out = {"smooth": ms[0], "collide": ms[1], "newton": ms[2]}
+        if ms[3] > 0.0:
+            out["inference"] = ms[3]
+        return out
 
     def reset(self, envs: Sequence[int]):
         ids = np.ascontiguousarray(np.asarray(list(envs), dtype=np.int64))

@@ -378,10 +378,10 @@ TENDON_ARM = (
     '<body name="fore" pos="0.25 0 0"><joint name="el" axis="0 1 0" range="-150 150"/>'
     '<geom type="capsule" fromto="0 0 0 0.22 0 0" size="0.03"/>'
     '<body name="hand" pos="0.22 0 0"><joint name="wr" axis="1 0 0"/>'
-    '<geom type="box" size="0.04 0.03 0.02"/></body></body></body></body></worldbody>'
+    '<geom type="box" size="0.06 0.05 0.04"/></body></body></body></body></worldbody>'
     '<tendon><fixed name="flex"><joint joint="sh" coef="1"/><joint joint="el" coef="-0.5"/></fixed>'
     '<fixed name="twist"><joint joint="yaw" coef="0.3"/><joint joint="wr" coef="1"/></fixed></tendon>'
-    '<actuator><motor tendon="flex" gear="12" ctrlrange="-1 1"/><motor tendon="twist" gear="2"/>'
+    '<actuator><motor tendon="flex" gear="12" ctrlrange="-1 1"/><motor tendon="twist" gear="0.3"/>'
     '<motor joint="el" gear="4"/></actuator></mujoco>')
 
 IMPLICITFAST_ARM = (
