@@ -1856,7 +1856,7 @@ int pg_time_phases(pg_handle* h, int64_t start, int64_t end, int64_t nstep, cons
     for (int p = 0; p < 4 && e == cudaSuccess; p++) {
       float ms = 0.0f;
       e = cudaEventElapsedTime(&ms, ev[p], ev[p + 1]);
-      ms_out[slot[p]] += ms;
+      if (slot[p] != 3 || learned) ms_out[slot[p]] += ms;  // no inference launched: 0
     }
   }
   for (auto& x : ev) cudaEventDestroy(x);

@@ -445,8 +445,7 @@ __device__ __noinline__ int newton_dense(const Tile<G>& T, int k, int nr, const 
   for (int i = lane; i < k; i += G) a0[i] = a[i];
   T.sync();
   // (mp is free until the line search, and the gate's cost() leaves it alone)
-  bool cand_kept = cand && learned_candidate(T, k, nr, J, R, M, a0, B, B.mp);
-  if (cand_kept) warm = B.mp;
+  if (cand && learned_candidate(T, k, nr, J, R, M, a0, B, B.mp)) warm = B.mp;
   // when the gate keeps the start, its cost evaluation leaves the first
   // iteration's products there: M (a - a0) in tmp2, J a - aref in R_JAR
   bool have = false;
@@ -466,21 +465,19 @@ __device__ __noinline__ int newton_dense(const Tile<G>& T, int k, int nr, const 
         grad[i] = tmp2[i];
       }
       have = true;
-    } else {
-      cand_kept = false;
     }
     T.sync();
   }
-  // a kept learned candidate counts as the first iteration, with R_ACT
-  // holding its active set (as in newton_small); otherwise no previous set
-  if (!cand_kept)
+  // no previous iteration's active set (the candidate's stays out of it:
+  // iterations count as the reference counts them, from the kept start)
+  if (cand)
     for (int r = lane; r < nr; r += G) R[R_STRIDE * r + R_ACT] = -1.0;
   T.sync();
   mul_m(T, M, k, a0, tmp);
   double ss = 0.0;
   for (int i = lane; i < k; i += G) ss += tmp[i] * tmp[i];
   double scale = 1.0 + sqrt(T.sum(ss));
-  int iters = cand_kept ? 1 : 0;
+  int iters = 0;
   int maxit = max_iters > 1 ? max_iters : 1;
   while (iters < maxit) {
     iters++;
@@ -693,8 +690,6 @@ __device__ inline int newton_small(const Tile<G>& T, int k, int nr, const double
   double ai = a0;
   double wl = wi;
   bool use_warm = warm != nullptr;
-  bool cand = false;                  // wl is the learned candidate
-  double pset[2] = {-1.0, -1.0};      // the activity it was formed with (this lane's rows)
   if (lforce && lnum > 0 && 4 * lnum <= nr) {
     // residuals at a0, and each of this lane's rows' predicted activity
     publish(a0);
@@ -745,9 +740,6 @@ __device__ inline int newton_small(const Tile<G>& T, int k, int nr, const double
     if (chol_regx(T, hl, k, B.L, &rv)) {
       wl = a0 + solve_regx(T, hl, k, B.L, rv, dof ? -g0 : 0.0);
       use_warm = true;
-      cand = true;
-      pset[0] = on[0];
-      pset[1] = on[1];
     }
   }
   // x = a0 once: M a0 for the scale, and J a0 for the cold cost, whose
@@ -784,21 +776,14 @@ __device__ inline int newton_small(const Tile<G>& T, int k, int nr, const double
       ai = wl;
       gw = mw;
       have = true;
-    } else {
-      cand = false;
     }
   }
   double scale = 1.0 + sqrt(T.sum(ma0 * ma0));
-  // A kept learned candidate is the Newton step (full length) of the
-  // predicted active set from a0, and counts as the first iteration: the
-  // next one ends the solve by the reference's exit rule when the active set
-  // at the candidate is that set, i.e. when the candidate minimises the cost
-  // on a self-consistent active set, which is the optimality condition of
-  // the piecewise quadratic (newton.rs:273-276)
-  int iters = cand ? 1 : 0;
+  // iterations count as the reference counts them, from the start the gate
+  // kept (forming the learned candidate costs one factorisation before them)
+  int iters = 0;
   int maxit = max_iters > 1 ? max_iters : 1;
-  // the rows' activity in the previous iteration (-1: none yet)
-  double prev[2] = {cand ? pset[0] : -1.0, cand ? pset[1] : -1.0};
+  double prev[2] = {-1.0, -1.0};  // the rows' activity in the previous iteration (none yet)
   double jar[2] = {0.0, 0.0}, act[2] = {0.0, 0.0}, cv[2];
   bool fresh = false;  // left at the convergence check: B.c holds D_r jar_r of the final a
   while (iters < maxit) {
