@@ -364,7 +364,8 @@ __device__ __noinline__ void clip_faces(const Poly& r, int rf, const Poly& s, V3
 }
 
 template <int G>
-__device__ void polytope_polytope(const Tile<G>& T, const Poly& a, const Poly& b, double margin, Hits& out) {
+__device__ void polytope_polytope(const Tile<G>& T, const Poly& a, const Poly& b, double margin, Hits& out,
+                                  int owner) {
   int fa, fb, ea, eb;
   V3 axis{0.0, 0.0, 0.0};
   double sa = face_query(T, a, b, &fa);
@@ -376,6 +377,7 @@ __device__ void polytope_polytope(const Tile<G>& T, const Poly& a, const Poly& b
   double oa = -sa, ob = -sb, oe = -se;
   bool face_a = !(ob < oa - GEN_TIE);
   double of = face_a ? oa : ob;
+  if (T.lane() != owner) return;  // the contact points: on the owning lane only
   if (ea >= 0 && oe < of && !(of < oe * 1.05 + 1e-4)) {
     int i0, i1, j0, j1;
     p_edge(a, ea, &i0, &i1);
@@ -480,32 +482,36 @@ __device__ void poly_cache(const Tile<G>& T, Poly& p, double* buf) {
   p.nc = buf + 3 * nv;
 }
 
-// One pair on the whole tile: every lane passes the same pair and ends with
-// the same contacts; the polytope queries share their candidates out over
-// the lanes, the rest runs on every lane alike. With `cache` (6 (gen_vmax +
-// gen_fmax) doubles of the tile's shared memory) the polytopes' world
-// vertices and normals are formed once instead of at every use.
+// One pair on the whole tile: every lane passes the same pair; the polytope
+// queries share their candidates out over the lanes, and the contact points
+// (clipping, closest points) are formed on lane `owner` alone, whose `out`
+// gets them (the other lanes' stays as it was: their clip and point buffers
+// stay untouched, so the tile's local-memory footprint is one lane's). With
+// `cache` (6 (gen_vmax + gen_fmax) doubles of the tile's shared memory) the
+// polytopes' world vertices and normals are formed once instead of at every
+// use.
 template <int G>
 __device__ __noinline__ void collide_general(const Tile<G>& T, const DModel& m, const GPose& a0, const GPose& b0,
-                                             double margin, Hits& out, double* cache) {
+                                             double margin, Hits& out, double* cache, int owner) {
   bool swap = a0.type > b0.type;  // type order, normals flipped back (collision.rs:59-67)
   const GPose& a = swap ? b0 : a0;
   const GPose& b = swap ? a0 : b0;
   int start = out.n;
   Poly pb{b.type, b.pos, b.mat, b.size, &m, b.data};
   if (cache) poly_cache(T, pb, cache);
+  const bool own = T.lane() == owner;
   if (a.type == GEOM_PLANE) {
-    plane_polytope(a, pb, margin, out);
+    if (own) plane_polytope(a, pb, margin, out);
   } else if (a.type == GEOM_SPHERE) {
-    sphere_polytope(a.pos, a.size.x, pb, margin, out);
+    if (own) sphere_polytope(a.pos, a.size.x, pb, margin, out);
   } else if (a.type == GEOM_CAPSULE) {
-    capsule_polytope(a, pb, margin, out);
+    if (own) capsule_polytope(a, pb, margin, out);
   } else {
     Poly pa{a.type, a.pos, a.mat, a.size, &m, a.data};
     if (cache) poly_cache(T, pa, cache + 3 * (m.gen_vmax + m.gen_fmax));
-    polytope_polytope(T, pa, pb, margin, out);
+    polytope_polytope(T, pa, pb, margin, out, owner);
   }
-  if (swap)
+  if (swap && own)
     for (int k = start; k < out.n && k < MAX_HITS; k++) out.h[k].normal = -out.h[k].normal;
 }
 

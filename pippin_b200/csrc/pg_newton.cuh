@@ -50,10 +50,7 @@ __device__ int collide(const Tile<G>& T, const DModel& m, const WsLayout& w, con
     for (unsigned gm = T.ballot(general); gm; gm &= gm - 1) {
       int d = __ffs(gm) - 1;
       int h1 = T.bcast(g1, d), h2 = T.bcast(g2, d);
-      Hits gh;
-      gh.n = 0;
-      collide_general(T, m, pose(h1), pose(h2), m.margin, gh, gcache);
-      if (lane == d) hits = gh;
+      collide_general(T, m, pose(h1), pose(h2), m.margin, hits, gcache, d);
     }
     int nh = hits.n < MAX_HITS ? hits.n : MAX_HITS;
     int tot;
