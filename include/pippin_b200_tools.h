@@ -37,6 +37,15 @@ int pg_phase_launch(const pg_handle* h, int phase, int* lanes_per_env, int* envs
  * when one block does not fit. Pure arithmetic: needs no GPU. */
 int pg_static_tiles(size_t tile_bytes, int tiles_per_block, int64_t* tiles);
 
+/* Support vertices of mesh `mesh`'s convex hull as the collision kernel
+ * finds them: for each of n directions (host memory, [n][3], in the mesh's
+ * own frame) the index of the hull vertex with the largest projection on it
+ * (vertex[n], host memory). Hulls of 64 vertices or more walk their vertex
+ * graph from vertex 0 and 26 seed vertices, smaller ones scan: the support
+ * query of crates/pippin/src/fasthull.rs:76-120. Synchronises the handle's
+ * stream. Returns PG_OK or a PG_ERR_* code. */
+int pg_hull_support(pg_handle* h, int mesh, const double* dirs, int64_t n, int32_t* vertex);
+
 #ifdef __cplusplus
 }
 #endif

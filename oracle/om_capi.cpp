@@ -447,6 +447,18 @@ void om_quat_from_axis_angle(const double* axis, double angle, double* q) {
   Quat r = qaxis_angle(v3(axis[0], axis[1], axis[2]), angle);
   for (int k = 0; k < 4; k++) q[k] = r[k];
 }
+int om_hull_support(const double* verts, int64_t nv, const int32_t* edges, int64_t ne, const double* dirs, int64_t nd,
+                    int32_t* out) {
+  std::vector<Vec3> pts;
+  for (int64_t i = 0; i < nv; i++) pts.push_back(v3(verts[3 * i], verts[3 * i + 1], verts[3 * i + 2]));
+  std::vector<std::array<int, 2>> ed;
+  for (int64_t e = 0; e < ne; e++) {
+    if (edges[2 * e] < 0 || edges[2 * e] >= nv || edges[2 * e + 1] < 0 || edges[2 * e + 1] >= nv) return -1;
+    ed.push_back({edges[2 * e], edges[2 * e + 1]});
+  }
+  for (int64_t k = 0; k < nd; k++) out[k] = hull_support_walk(pts, ed, v3(dirs[3 * k], dirs[3 * k + 1], dirs[3 * k + 2]));
+  return 0;
+}
 void om_quat_to_mat(const double* q, double* m) {
   Mat3 r = qto_mat(Quat{{q[0], q[1], q[2], q[3]}});
   for (int k = 0; k < 9; k++) m[k] = r[k];

@@ -225,6 +225,69 @@ static Real edge_query(const Polytope& a, Vec3 ca, const Polytope& b, int* ea, i
   return best;
 }
 
+// FastHull::support_vertex (fasthull.rs:52-120): hulls under 64 vertices
+// are scanned (the first maximum); larger ones build each vertex's
+// neighbours from the edges and the vertex extreme along each of the 26
+// normalised directions (x, y, z) in {-1, 0, 1}^3 (Iterator::max_by keeps the
+// last maximum), start from the better of vertex 0 (the hint, never written
+// after construction) and the vertex of the seed direction closest to dir,
+// then move to the neighbour with the largest projection while one improves.
+int hull_support_walk(const std::vector<Vec3>& pts, const std::vector<std::array<int, 2>>& edges, Vec3 dir) {
+  const int n = (int)pts.size();
+  if (n < 64) {
+    int v = 0;
+    Real best = -INFINITY;
+    for (int i = 0; i < n; i++) {
+      Real d = dot(pts[i], dir);
+      if (d > best) {
+        best = d;
+        v = i;
+      }
+    }
+    return v;
+  }
+  std::vector<std::vector<int>> nb(n);
+  for (const auto& e : edges) {
+    nb[e[0]].push_back(e[1]);
+    nb[e[1]].push_back(e[0]);
+  }
+  std::vector<std::pair<Vec3, int>> seeds;
+  for (int x = -1; x <= 1; x++)
+    for (int y = -1; y <= 1; y++)
+      for (int z = -1; z <= 1; z++) {
+        Vec3 d = v3(x, y, z);
+        if (dot(d, d) <= 0.0) continue;
+        d = normalized(d);
+        int bi = 0;
+        for (int i = 1; i < n; i++)
+          if (!(dot(pts[i], d) < dot(pts[bi], d))) bi = i;
+        seeds.push_back({d, bi});
+      }
+  int v = 0, seed = 0;
+  Real seed_dot = -INFINITY;
+  for (const auto& sd : seeds) {
+    Real x = dot(sd.first, dir);
+    if (x > seed_dot) {
+      seed_dot = x;
+      seed = sd.second;
+    }
+  }
+  if (dot(pts[seed], dir) > dot(pts[v], dir)) v = seed;
+  Real best = dot(pts[v], dir);
+  for (;;) {
+    int next = v;
+    for (int w : nb[v]) {
+      Real d = dot(pts[w], dir);
+      if (d > best) {
+        best = d;
+        next = w;
+      }
+    }
+    if (next == v) return v;
+    v = next;
+  }
+}
+
 static Vec3 centroid(const Polytope& p) {
   Vec3 c = v3zero();
   for (const Vec3& x : p.v) c += x;

@@ -216,6 +216,7 @@ void reduce_to_four(std::vector<DistPt>& pts);
 void stable_sort_dist(std::vector<DistPt>& v);
 bool needs_general(int a, int b);
 void collide_general(const GeomPose& a, const GeomPose& b, Real margin, std::vector<Hit>& out);
+int hull_support_walk(const std::vector<Vec3>& pts, const std::vector<std::array<int, 2>>& edges, Vec3 dir);
 
 // newton.rs:378-473, solver.rs:63-251
 void newton_solve(const Model& m, Data& d, Real* a);

@@ -68,6 +68,7 @@ def _lib(fast: bool = False):
     L.om_cholesky_solve_block.argtypes = [pd, i64, i64, i64, pd]
     L.om_quat_from_axis_angle.argtypes = [pd, dbl, pd]
     L.om_quat_to_mat.argtypes = [pd, pd]
+    L.om_hull_support.argtypes = [pd, i64, pi32, i64, pd, i64, pi32]
     _LIBS[name] = L
     return L
 
@@ -218,6 +219,18 @@ class Oracle:
 def impedance(solimp, pos):
     s = np.ascontiguousarray(solimp, dtype=np.float64)
     return lib().om_impedance(_p(s), float(pos))
+
+
+def hull_support(verts, edges, dirs):
+    """The reference's hull support walk (fasthull.rs:76-120): for each
+    direction, the index of the vertex it ends at."""
+    v = np.ascontiguousarray(verts, dtype=np.float64).reshape(-1, 3)
+    e = np.ascontiguousarray(edges, dtype=np.int32).reshape(-1, 2)
+    d = np.ascontiguousarray(dirs, dtype=np.float64).reshape(-1, 3)
+    out = np.zeros(len(d), dtype=np.int32)
+    if lib().om_hull_support(_p(v), len(v), _p(e, C.c_int32), len(e), _p(d), len(d), _p(out, C.c_int32)) != 0:
+        raise OracleError("hull_support: edge vertex out of range")
+    return out
 
 
 def vdot(a, b):

@@ -67,6 +67,7 @@ SIGNATURES = [
     ("pg_time_phases", _i32, [_vp, _i64, _i64, _i64, _vp, _pf]),
     ("pg_phase_launch", _i32, [_vp, _i32, _pi32, _pi32, _pi32]),
     ("pg_static_tiles", _i32, [_sz, _i32, _pi64]),
+    ("pg_hull_support", _i32, [_vp, _i32, _pd, _i64, _pi32]),
     ("pg_set_warm_mlp", _i32, [_vp, _pf, _sz]),
     ("pg_warm_samples", _i32, [_vp, _i64, _i64, _pf, _sz, _pf, _sz, _pi64]),
     ("pg_warm_capacity", _i64, [_vp]),

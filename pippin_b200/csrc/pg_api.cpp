@@ -310,14 +310,15 @@ bool load_model(const void* blob, size_t bytes, HostModel& m, std::string* err) 
       if (v < 0 || v >= m.hull_vnum[i]) return bad("hull triangle vertex");
     }
     // polygon faces: every loop within the hull's vertices and at most
-    // HULL_FACE_MAX long (the device clips in fixed buffers); edges likewise
+    // HULL_FACE_LIMIT long (the clip buffers are sized from the longest);
+    // edges likewise
     long nf = (long)m.hull_fvadr.size(), nfv = (long)m.hull_fv.size(), ne = (long)m.hull_edge.size() / 2;
     if ((long)m.hull_fvnum.size() != nf || (long)m.hull_fplane.size() != 4 * nf) return bad("hull faces");
     if (m.hull_fadr[i] < 0 || m.hull_fnum[i] < 4 || (long)m.hull_fadr[i] + m.hull_fnum[i] > nf) return bad("hull faces");
     for (int f = m.hull_fadr[i]; f < m.hull_fadr[i] + m.hull_fnum[i]; f++) {
-      if (m.hull_fvnum[f] < 3 || m.hull_fvnum[f] > HULL_FACE_MAX || m.hull_fvadr[f] < 0 ||
+      if (m.hull_fvnum[f] < 3 || m.hull_fvnum[f] > HULL_FACE_LIMIT || m.hull_fvadr[f] < 0 ||
           (long)m.hull_fvadr[f] + m.hull_fvnum[f] > nfv)
-        return bad("hull face loop (3 to 32 vertices)");
+        return bad("hull face loop (3 to 256 vertices)");
       for (int k = 0; k < m.hull_fvnum[f]; k++) {
         int v = m.hull_fv[m.hull_fvadr[f] + k];
         if (v < 0 || v >= m.hull_vnum[i]) return bad("hull face vertex");
@@ -620,7 +621,7 @@ std::vector<int> dmodel_pointer_fields() {
   PF(act_moment_num); PF(moment_jnt); PF(moment_coef); PF(eq_j1); PF(eq_j2); PF(eq_poly); PF(eq_solref);
   PF(eq_solimp); PF(qpos0); PF(hull_vadr); PF(hull_vnum); PF(hull_vert); PF(hull_fadr); PF(hull_fnum);
   PF(hull_face); PF(hull_fvadr); PF(hull_fvnum); PF(hull_fv); PF(hull_eadr); PF(hull_enum); PF(hull_edge);
-  PF(hull_eface);
+  PF(hull_eface); PF(hull_nbadr); PF(hull_nbnum); PF(hull_nb); PF(hull_seed);
 #undef PF
   return o;
 }
@@ -950,6 +951,46 @@ int build_device_model(Handle* h) {
       }
     }
 
+  // the support walk of large hulls (fasthull.rs:52-75): each vertex's
+  // neighbours along the hull's edges, and the vertex extreme along each of
+  // the 26 seed directions (the first maximum)
+  const int nhv = (int)m.hull_vert.size() / 3;
+  std::vector<std::vector<int>> nbl(nhv);
+  for (int i = 0; i < m.nmesh; i++)
+    for (int e = m.hull_eadr[i]; e < m.hull_eadr[i] + m.hull_enum[i]; e++) {
+      int a = m.hull_edge[2 * e], b = m.hull_edge[2 * e + 1];
+      nbl[m.hull_vadr[i] + a].push_back(b);
+      nbl[m.hull_vadr[i] + b].push_back(a);
+    }
+  std::vector<int> hull_nbadr(nhv + 1, 0), hull_nbnum(nhv + 1, 0), hull_nb;
+  for (int v = 0; v < nhv; v++) {
+    hull_nbadr[v] = (int)hull_nb.size();
+    hull_nbnum[v] = (int)nbl[v].size();
+    hull_nb.insert(hull_nb.end(), nbl[v].begin(), nbl[v].end());
+  }
+  hull_nb.push_back(0);
+  std::vector<int> hull_seed(HULL_SEEDS * std::max(m.nmesh, 1), 0);
+  for (int i = 0; i < m.nmesh; i++) {
+    int k = 0;
+    for (int x = -1; x <= 1; x++)
+      for (int y = -1; y <= 1; y++)
+        for (int z = -1; z <= 1; z++) {
+          if (!x && !y && !z) continue;
+          double inv = 1.0 / std::sqrt((double)(x * x + y * y + z * z));
+          double bd = -INFINITY;
+          int bv = 0;
+          for (int v = 0; v < m.hull_vnum[i]; v++) {
+            const double* p = &m.hull_vert[3 * (m.hull_vadr[i] + v)];
+            double dv = (x * p[0] + y * p[1] + z * p[2]) * inv;
+            if (dv > bd) {
+              bd = dv;
+              bv = v;
+            }
+          }
+          hull_seed[HULL_SEEDS * i + k++] = bv;
+        }
+  }
+
   d.nq = m.nq;
   d.nv = nv;
   d.nu = m.nu;
@@ -969,7 +1010,7 @@ int build_device_model(Handle* h) {
   // polytope sizes of the general pairs (mesh against anything, cylinder
   // against a non-plane): the collide kernel caches their world vertices
   // and face normals per tile
-  d.gen_vmax = d.gen_fmax = 0;
+  d.gen_vmax = d.gen_fmax = d.gen_lmax = 0;
   for (size_t p = 0; p + 1 < m.pairs.size(); p += 2) {
     int ta = m.geom_type[m.pairs[p]], tb = m.geom_type[m.pairs[p + 1]];
     bool general = ta == GEOM_MESH || tb == GEOM_MESH || (ta == GEOM_CYLINDER && tb != GEOM_PLANE) ||
@@ -979,11 +1020,24 @@ int build_device_model(Handle* h) {
       int t = m.geom_type[g], nvx = 0, nfx = 0;
       if (t == GEOM_BOX) nvx = 8, nfx = 6;
       if (t == GEOM_CYLINDER) nvx = 2 * CYL_SIDES, nfx = CYL_SIDES + 2;
-      if (t == GEOM_MESH) nvx = m.hull_vnum[m.geom_dataid[g]], nfx = m.hull_fnum[m.geom_dataid[g]];
+      int lx = t == GEOM_BOX ? 4 : t == GEOM_CYLINDER ? CYL_SIDES : 0;
+      if (t == GEOM_MESH) {
+        int mi = m.geom_dataid[g];
+        nvx = m.hull_vnum[mi], nfx = m.hull_fnum[mi];
+        for (int f = m.hull_fadr[mi]; f < m.hull_fadr[mi] + m.hull_fnum[mi]; f++) lx = std::max(lx, m.hull_fvnum[f]);
+      }
       d.gen_vmax = std::max(d.gen_vmax, nvx);
       d.gen_fmax = std::max(d.gen_fmax, nfx);
+      d.gen_lmax = std::max(d.gen_lmax, lx);
     }
   }
+  // the polytope cache holds both polytopes' world vertices and normals
+  // while it stays small; clip buffers move to shared memory when a face is
+  // longer than a lane's own buffers take (an incident loop plus one vertex
+  // per side plane, for two buffers, then the kept points)
+  d.gen_cache = 6 * (d.gen_vmax + d.gen_fmax);
+  if (d.gen_cache > GEN_CACHE_LIMIT) d.gen_cache = 0;
+  d.gen_clip = d.gen_lmax > HULL_FACE_MAX ? 10 * (2 * d.gen_lmax) : 0;
   d.timestep = m.timestep;
   for (int k = 0; k < 3; k++) d.gravity[k] = m.gravity[k];
   d.integrator = m.integrator;
@@ -1074,6 +1128,10 @@ int build_device_model(Handle* h) {
   ADDI(hull_enum, m.hull_enum);
   ADDI(hull_edge, m.hull_edge);
   ADDI(hull_eface, hull_eface);
+  ADDI(hull_nbadr, hull_nbadr);
+  ADDI(hull_nbnum, hull_nbnum);
+  ADDI(hull_nb, hull_nb);
+  ADDI(hull_seed, hull_seed);
 #undef ADDI
 #undef ADDD
   ar.host.resize((ar.host.size() + 15) & ~size_t(15));  // staged in 16-byte chunks
@@ -1247,6 +1305,12 @@ int pg_create(const void* blob, size_t bytes, int64_t n_envs, int device, pg_han
   int npair = (int)m.pairs.size() / 2;
   int gc = npair > 16 ? 32 : (npair > 8 ? 16 : 8);
   SubstepCfg want{{g, 4, 0}, {gc, 4, 0}, {g, 4, 0}};
+  {
+    StepArgs a = make_args(h.get());
+    while (want.collide.tiles_per_block > 1 && kernel_smem(K_COLLIDE, a, want.collide.tiles_per_block) > h->smem_optin)
+      want.collide.tiles_per_block /= 2;
+    while (want.collide.tiles_per_block * want.collide.G < 32) want.collide.G *= 2;
+  }
   rc = apply_cfg(h.get(), want);
   if (rc) return rc;
   rc = set_const_range(h.get(), 0, n_envs);
@@ -1452,6 +1516,27 @@ int pg_poses_device(pg_handle* h, int64_t start, int64_t end, pg_pose* geoms_dev
   a.start = (int)start;
   a.count = (int)cnt;
   return launch_status(launch_poses(a, fit(h->cfg.smooth, cnt), (float*)geoms_dev, (float*)cams_dev, h->stream));
+}
+
+int pg_hull_support(pg_handle* h, int mesh, const double* dirs, int64_t n, int32_t* vertex) {
+  if (!h) return fail(PG_ERR_INVALID, "NULL handle");
+  if (mesh < 0 || mesh >= h->hm.nmesh) return fail(PG_ERR_INVALID, "hull_support: no mesh " + std::to_string(mesh));
+  if (n < 0 || n > (int64_t)1 << 28) return fail(PG_ERR_INVALID, "hull_support: direction count out of range");
+  if (n == 0) return PG_OK;
+  if (!dirs || !vertex) return fail(PG_ERR_INVALID, "hull_support: NULL buffer");
+  CK(cudaSetDevice(h->device));
+  double* d_dirs = nullptr;
+  int* d_out = nullptr;
+  cudaError_t e = cudaMalloc(&d_dirs, sizeof(double) * 3 * n);
+  if (e == cudaSuccess) e = cudaMalloc(&d_out, sizeof(int) * n);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_dirs, dirs, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess) e = launch_hull_support(h->dm, mesh, d_dirs, (int)n, d_out, h->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(vertex, d_out, sizeof(int) * n, cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  cudaFree(d_dirs);
+  cudaFree(d_out);
+  if (e != cudaSuccess) return cuda_fail(e, "hull_support");
+  return PG_OK;
 }
 
 int pg_param_width(const pg_handle* h, int param) {

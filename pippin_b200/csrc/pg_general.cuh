@@ -6,8 +6,8 @@
 // lanes share out the polytope queries' candidates):
 //   box        8 vertices, 6 faces
 //   cylinder   a 16-sided prism (faces at distance r cos(pi/16) from the axis)
-//   mesh       its convex hull: polygon faces (at most HULL_FACE_MAX long) and
-//              edges from the model, with each edge's two faces
+//   mesh       its convex hull: polygon faces (at most HULL_FACE_LIMIT long)
+//              and edges from the model, with each edge's two faces
 //   sphere     a point of radius r;  capsule  a segment of radius r
 // Polytope pairs: separating axes over both shapes' face normals and the
 // cross products of edge pairs that form a face of the Minkowski difference
@@ -17,6 +17,10 @@
 // reference face's side planes (up to four points kept as reduce_to_four
 // picks them). Spheres and capsules against a polytope use its exact
 // closest point; a plane against a hull takes the four deepest vertices.
+// Two accelerations leave the results as they are: hulls of HULL_SCAN_BELOW
+// vertices or more find support points by walking their vertex graph
+// (fasthull.rs:76-120) instead of scanning, and the edge query skips every
+// edge whose separation bound shows it cannot change the contacts.
 #pragma once
 #include "pg_collide.cuh"
 #include "pg_tile.cuh"
@@ -24,6 +28,16 @@
 namespace pg {
 
 constexpr int GEN_CLIP_CAP = 2 * HULL_FACE_MAX;  // incident loop + one vertex per side plane
+
+// A collide tile's shared scratch for general pairs: the polytope cache
+// (poly_cache), clip buffers for faces longer than HULL_FACE_MAX, and the
+// edge query's two survivor lists (GEN_SURV_CAP ints each). A pointer is
+// nullptr when the model needs none.
+struct GenScratch {
+  double* cache;
+  double* clip;
+  int* surv;
+};
 
 // box faces (outward normals -z, +x, +y, -y, -x, +z), their loops, edges
 // (vertex i to i | bit) and each edge's two faces; vertex i has coordinate
@@ -138,6 +152,71 @@ __device__ inline void p_eface(const Poly& p, int e, int* f1, int* f2) {
   }
 }
 
+// Hull vertex extreme along dl (a direction in the hull's own frame), the
+// support query of fasthull.rs:76-120: a hull under HULL_SCAN_BELOW
+// vertices is scanned (the first maximum); a larger one starts from the
+// better of vertex `hint` and the vertex extreme along the seed direction
+// closest to dl, then moves to the neighbour with the largest projection
+// while one beats the current vertex. On a convex hull that walk ends at a
+// global maximum. Every step raises the projection, so no walk is longer
+// than the hull's vertex count.
+__device__ inline int hull_support(const DModel& m, int mesh, V3 dl, int hint) {
+  const int nv = m.hull_vnum[mesh], base = m.hull_vadr[mesh];
+  const double* vert = m.hull_vert + 3 * base;
+  auto proj = [&](int i) { return dot(ld3(vert + 3 * i), dl); };
+  if (nv < HULL_SCAN_BELOW) {
+    int v = 0;
+    double best = -INFINITY;
+    for (int i = 0; i < nv; i++) {
+      double d = proj(i);
+      if (d > best) {
+        best = d;
+        v = i;
+      }
+    }
+    return v;
+  }
+  // seed directions (x, y, z) / |(x, y, z)| in the order x, y, z from -1 to 1
+  const double inv[4] = {0.0, 1.0, 0.70710678118654752440, 0.57735026918962576451};
+  int seed = 0, k = 0;
+  double sd = -INFINITY;
+  for (int x = -1; x <= 1; x++)
+    for (int y = -1; y <= 1; y++)
+      for (int z = -1; z <= 1; z++) {
+        if (!x && !y && !z) continue;
+        double d = (x * dl.x + y * dl.y + z * dl.z) * inv[x * x + y * y + z * z];
+        if (d > sd) {
+          sd = d;
+          seed = m.hull_seed[HULL_SEEDS * mesh + k];
+        }
+        k++;
+      }
+  int v = hint < 0 ? 0 : (hint >= nv ? nv - 1 : hint);
+  double best = proj(v);
+  double ds = proj(seed);
+  if (ds > best) {
+    best = ds;
+    v = seed;
+  }
+  for (int step = 0; step < nv; step++) {
+    int next = v;
+    const int* nb = m.hull_nb + m.hull_nbadr[base + v];
+    const int nn = m.hull_nbnum[base + v];
+    for (int j = 0; j < nn; j++) {
+      double d = proj(nb[j]);
+      if (d > best) {
+        best = d;
+        next = nb[j];
+      }
+    }
+    if (next == v) break;
+    v = next;
+  }
+  return v;
+}
+
+__device__ inline bool p_walks(const Poly& p) { return p.kind == GEOM_MESH && p.m->hull_vnum[p.mesh] >= HULL_SCAN_BELOW; }
+
 // Point of the polytope closest to x: the signed distance (negative inside,
 // then to the nearest face plane), the point, and the face when inside (-1
 // outside). Outside, the closest point lies on a face (projection inside
@@ -202,14 +281,23 @@ constexpr double GEN_TIE = 1e-10;
 
 // largest separation of b beyond a face of a (first face within GEN_TIE),
 // the faces shared out over the tile's lanes: the maximum, then the lowest
-// face index within GEN_TIE of it, as a loop over the faces in order finds
+// face index within GEN_TIE of it, as a loop over the faces in order finds.
+// b's vertex deepest below a face comes from a scan, or from the support
+// walk when b is a hull of HULL_SCAN_BELOW vertices or more.
 template <int G>
 __device__ double face_query(const Tile<G>& T, const Poly& a, const Poly& b, int* face) {
   int nf = p_nf(a), nv = p_nv(b);
+  const bool walk = p_walks(b);
+  int hint = 0;  // a large hull's walks start from this lane's last answer
   auto sep = [&](int f) {
     V3 n = p_fn(a, f);
     double mn = INFINITY;
-    for (int i = 0; i < nv; i++) mn = fmin(mn, dot(n, p_v(b, i)));
+    if (walk) {
+      hint = hull_support(*b.m, b.mesh, mtv(b.mat, -n), hint);
+      mn = dot(n, p_v(b, hint));
+    } else {
+      for (int i = 0; i < nv; i++) mn = fmin(mn, dot(n, p_v(b, i)));
+    }
     return mn - p_fd(a, f, n);
   };
   double best = -INFINITY;
@@ -234,12 +322,91 @@ __device__ inline bool minkowski_face(V3 a, V3 b, V3 c, V3 d) {
   return cba * dba < 0.0 && adc * bdc < 0.0 && cba * bdc > 0.0;
 }
 
+// Largest u.w over the unit vectors u on the great-circle arc from n1 to n2
+// (the outward normals of an edge's two faces, less than pi apart): the
+// projection of w onto the arc's plane when it points between n1 and n2,
+// else the better end.
+__device__ inline double arc_max(V3 n1, V3 n2, V3 w) {
+  double mx = fmax(dot(n1, w), dot(n2, w));
+  V3 e = cross(n1, n2);
+  double ee = dot(e, e);
+  if (!(ee > 0.0)) return mx;
+  V3 wp = w - e * (dot(e, w) / ee);
+  if (dot(cross(n1, wp), e) > 0.0 && dot(cross(wp, n2), e) > 0.0) mx = fmax(mx, norm(wp));
+  return mx;
+}
+
+// Index of p's vertex with the largest projection on dir: the walk for a
+// large hull (every lane takes the same walk), else a scan shared out over
+// the lanes.
+template <int G>
+__device__ int support_index(const Tile<G>& T, const Poly& p, V3 dir) {
+  if (p_walks(p)) return hull_support(*p.m, p.mesh, mtv(p.mat, dir), 0);
+  double best = -INFINITY;
+  int bi = 0x7fffffff;
+  for (int i = T.lane(); i < p_nv(p); i += G) {
+    double d = dot(dir, p_v(p, i));
+    if (d > best) {
+      best = d;
+      bi = i;
+    }
+  }
+  T.argmax(&best, &bi);
+  return bi == 0x7fffffff ? 0 : bi;
+}
+
+// Edge pruning. For an edge pair that forms a face of the Minkowski
+// difference, its axis u lies on the arc of p's edge e, and the separation
+// along it is -h_p(u) - h_q(-u) with h the support function. h_p(u) = u.x_e
+// for any point x_e of the edge and h_q(-u) >= -u.y for any point y of q, so
+// the separation is at most arc_max(n1, n2, y - x_e) for every y in q (with
+// the roles of a and b swapped for b's edges). The witnesses y are q's
+// vertices on its best face fq (up to eight, evenly spread) and q's vertex
+// deepest below p's best face fp. An edge whose bound is below the pair's
+// threshold cannot take part in the result, and is dropped with every pair
+// it forms.
+__device__ inline double edge_bound(const Poly& p, int e, const Poly& q, int fq, int yq) {
+  int f1, f2, i0, i1;
+  p_eface(p, e, &f1, &f2);
+  if (f2 < 0) return -INFINITY;  // not between two faces: never a candidate
+  p_edge(p, e, &i0, &i1);
+  V3 xe = p_v(p, i0), n1 = p_fn(p, f1), n2 = p_fn(p, f2);
+  double bd = arc_max(n1, n2, p_v(q, yq) - xe);
+  int nl = p_fvn(q, fq), step = (nl + 7) / 8;
+  for (int k = 0; k < nl; k += step) bd = fmin(bd, arc_max(n1, n2, p_v(q, p_fv(q, fq, k)) - xe));
+  return bd;
+}
+
+// Lists p's edges whose bound reaches thr (ascending) in out[0, GEN_SURV_CAP);
+// returns how many there are (past the cap only counted).
+template <int G>
+__device__ int edge_survivors(const Tile<G>& T, const Poly& p, const Poly& q, int fq, int yq, double thr, int* out) {
+  int ne = p_ne(p), cnt = 0;
+  for (int base = 0; base < ne; base += G) {
+    int e = base + T.lane();
+    bool keep = e < ne && !(edge_bound(p, e, q, fq, yq) < thr);
+    unsigned mask = T.ballot(keep);
+    if (keep) {
+      unsigned below = T.lane() == 0 ? 0u : (mask & (0xffffffffu >> (32 - T.lane())));
+      int pos = cnt + __popc(below);
+      if (pos < GEN_SURV_CAP) out[pos] = e;
+    }
+    cnt += __popc(mask);
+  }
+  return cnt;
+}
+
 // largest separation along the cross product of an edge of a and of b; the
 // edge pairs (i, j), in the order i * (edges of b) + j, are shared out over
 // the tile's lanes, and the first pair with the largest separation wins, as
-// a loop over the pairs in order with a strict comparison finds
+// a loop over the pairs in order with a strict comparison finds. With
+// `surv`, only pairs of edges whose bound (edge_bound) reaches thr are
+// visited: fa / fb are a's and b's best faces, and thr lies below every
+// separation that could change the contacts, so the pairs skipped could
+// not have been the winner where the winner matters.
 template <int G>
-__device__ double edge_query(const Tile<G>& T, const Poly& a, V3 ca, const Poly& b, int* ea, int* eb, V3* axis) {
+__device__ double edge_query(const Tile<G>& T, const Poly& a, V3 ca, const Poly& b, int fa, int fb, double thr,
+                             int* surv, int* ea, int* eb, V3* axis) {
   int nea = p_ne(a), neb = p_ne(b);
   // separation along the pair's axis; false when the pair is not a candidate
   auto pair_sep = [&](int i, int j, double* s, V3* n) -> bool {
@@ -263,12 +430,33 @@ __device__ double edge_query(const Tile<G>& T, const Poly& a, V3 ca, const Poly&
   };
   double best = -INFINITY;
   int bidx = 0x7fffffff;
-  for (int k = T.lane(); k < nea * neb; k += G) {
-    double sk;
-    V3 nk;
-    if (pair_sep(k / neb, k % neb, &sk, &nk) && sk > best) {
-      best = sk;
-      bidx = k;
+  int na = -1, nb = -1;
+  if (surv) {
+    int yb = support_index(T, b, -p_fn(a, fa));  // b's vertex deepest below a's best face
+    int ya = support_index(T, a, -p_fn(b, fb));
+    T.sync();  // the lists of the previous pair are read
+    na = edge_survivors(T, a, b, fb, yb, thr, surv);
+    nb = na > 0 ? edge_survivors(T, b, a, fa, ya, thr, surv + GEN_SURV_CAP) : 0;
+    T.sync();
+  }
+  if (na >= 0 && na <= GEN_SURV_CAP && nb <= GEN_SURV_CAP) {
+    for (int k = T.lane(); k < na * nb; k += G) {
+      int i = surv[k / nb], j = surv[GEN_SURV_CAP + k % nb];
+      double sk;
+      V3 nk;
+      if (pair_sep(i, j, &sk, &nk) && sk > best) {
+        best = sk;
+        bidx = i * neb + j;
+      }
+    }
+  } else {
+    for (int k = T.lane(); k < nea * neb; k += G) {
+      double sk;
+      V3 nk;
+      if (pair_sep(k / neb, k % neb, &sk, &nk) && sk > best) {
+        best = sk;
+        bidx = k;
+      }
     }
   }
   T.argmax(&best, &bidx);
@@ -334,26 +522,39 @@ __device__ inline int clip_poly_cap(const V3* in, int n, V3 pn, double off, V3* 
 
 // reference face rf of r (outward normal toward s), incident polytope s:
 // clip s's most anti-parallel face against rf's side planes, keep the points
-// within the margin (up to four); normals along n (first geom to second)
-__device__ __noinline__ void clip_faces(const Poly& r, int rf, const Poly& s, V3 n, double margin, Hits& out) {
+// within the margin (up to four); (first geom to second). The clip runs in `area` (10 cap
+// doubles: two polygon buffers of cap vertices, then cap kept points) when
+// given, else in the lane's own buffers of GEN_CLIP_CAP.
+__device__ __noinline__ void clip_faces(const Poly& r, int rf, const Poly& s, V3 n, double margin, Hits& out,
+                                        double* area, int cap) {
   V3 nref = p_fn(r, rf);
   double dref = p_fd(r, rf, nref);
   int nfs = p_nf(s), inc = 0;
   double mn = INFINITY;
   for (int f = 0; f < nfs; f++) mn = fmin(mn, dot(p_fn(s, f), nref));
   while (inc + 1 < nfs && dot(p_fn(s, inc), nref) > mn + GEN_TIE) inc++;
-  V3 buf[2][GEN_CLIP_CAP];
+  V3 lbuf[2][GEN_CLIP_CAP];
+  DP lpts[GEN_CLIP_CAP];
+  V3* buf[2] = {lbuf[0], lbuf[1]};
+  DP* pts = lpts;
+  if (area) {
+    buf[0] = reinterpret_cast<V3*>(area);
+    buf[1] = buf[0] + cap;
+    pts = reinterpret_cast<DP*>(area + 6 * cap);
+  } else {
+    cap = GEN_CLIP_CAP;
+  }
   int np = p_fvn(s, inc), cur = 0;
-  for (int k = 0; k < np; k++) buf[0][k] = p_v(s, p_fv(s, inc, k));
+  for (int k = 0; k < np && k < cap; k++) buf[0][k] = p_v(s, p_fv(s, inc, k));
+  np = np < cap ? np : cap;
   int nl = p_fvn(r, rf);
   for (int k = 0; k < nl; k++) {
     V3 a = p_v(r, p_fv(r, rf, k)), b = p_v(r, p_fv(r, rf, (k + 1) % nl));
     V3 sn = normalized(cross(b - a, nref));
-    np = clip_poly_cap(buf[cur], np, sn, dot(sn, a), buf[cur ^ 1], GEN_CLIP_CAP);
+    np = clip_poly_cap(buf[cur], np, sn, dot(sn, a), buf[cur ^ 1], cap);
     cur ^= 1;
     if (np == 0) return;
   }
-  DP pts[GEN_CLIP_CAP];
   int n_pts = 0;
   for (int k = 0; k < np; k++) {
     double sep = dot(buf[cur][k], nref) - dref;
@@ -365,14 +566,21 @@ __device__ __noinline__ void clip_faces(const Poly& r, int rf, const Poly& s, V3
 
 template <int G>
 __device__ void polytope_polytope(const Tile<G>& T, const Poly& a, const Poly& b, double margin, Hits& out,
-                                  int owner) {
+                                  int owner, const GenScratch& gs) {
   int fa, fb, ea, eb;
   V3 axis{0.0, 0.0, 0.0};
   double sa = face_query(T, a, b, &fa);
   if (sa > margin) return;
   double sb = face_query(T, b, a, &fb);
   if (sb > margin) return;
-  double se = edge_query(T, a, p_centroid(a), b, &ea, &eb, &axis);
+  // An edge axis changes the contacts only when its separation is above
+  // the margin (no contact) or wins over the face axis below (the edge
+  // contact); the face separation used there is at least max(sa, sb) -
+  // GEN_TIE. Edges bounded below thr are skipped (edge_query); 1e-9 covers
+  // the rounding of the bounds.
+  double sfl = fmax(sa, sb) - GEN_TIE;
+  double thr = fmin(margin, fmax(sfl, (sfl + 1e-4) / 1.05)) - 1e-9;
+  double se = edge_query(T, a, p_centroid(a), b, fa, fb, thr, gs.surv, &ea, &eb, &axis);
   if (se > margin) return;
   double oa = -sa, ob = -sb, oe = -se;
   bool face_a = !(ob < oa - GEN_TIE);
@@ -387,8 +595,9 @@ __device__ void polytope_polytope(const Tile<G>& T, const Poly& a, const Poly& b
     out.push((x + y) * 0.5, axis, oe);
     return;
   }
-  if (face_a) clip_faces(a, fa, b, p_fn(a, fa), margin, out);
-  else clip_faces(b, fb, a, -p_fn(b, fb), margin, out);
+  const int cap = 2 * a.m->gen_lmax;
+  if (face_a) clip_faces(a, fa, b, p_fn(a, fa), margin, out, gs.clip, cap);
+  else clip_faces(b, fb, a, -p_fn(b, fb), margin, out, gs.clip, cap);
 }
 
 // sphere (center c, radius r) against a polytope; normal from the sphere
@@ -487,12 +696,13 @@ __device__ void poly_cache(const Tile<G>& T, Poly& p, double* buf) {
 // (clipping, closest points) are formed on lane `owner` alone, whose `out`
 // gets them (the other lanes' stays as it was: their clip and point buffers
 // stay untouched, so the tile's local-memory footprint is one lane's). With
-// `cache` (6 (gen_vmax + gen_fmax) doubles of the tile's shared memory) the
+// gs.cache (6 (gen_vmax + gen_fmax) doubles of the tile's shared memory) the
 // polytopes' world vertices and normals are formed once instead of at every
 // use.
 template <int G>
 __device__ __noinline__ void collide_general(const Tile<G>& T, const DModel& m, const GPose& a0, const GPose& b0,
-                                             double margin, Hits& out, double* cache, int owner) {
+                                             double margin, Hits& out, const GenScratch& gs, int owner) {
+  double* cache = gs.cache;
   bool swap = a0.type > b0.type;  // type order, normals flipped back (collision.rs:59-67)
   const GPose& a = swap ? b0 : a0;
   const GPose& b = swap ? a0 : b0;
@@ -509,7 +719,7 @@ __device__ __noinline__ void collide_general(const Tile<G>& T, const DModel& m, 
   } else {
     Poly pa{a.type, a.pos, a.mat, a.size, &m, a.data};
     if (cache) poly_cache(T, pa, cache + 3 * (m.gen_vmax + m.gen_fmax));
-    polytope_polytope(T, pa, pb, margin, out, owner);
+    polytope_polytope(T, pa, pb, margin, out, owner, gs);
   }
   if (swap && own)
     for (int k = start; k < out.n && k < MAX_HITS; k++) out.h[k].normal = -out.h[k].normal;

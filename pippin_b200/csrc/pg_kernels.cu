@@ -48,9 +48,14 @@ __device__ inline const DModel& stage_model(const StepArgs& A, unsigned char* sm
   return *dm;
 }
 
-// doubles of polytope cache a collide tile needs: world vertices and face
-// normals of both polytopes of a general pair
-__host__ __device__ inline int collide_cache_doubles(const DModel& m) { return 6 * (m.gen_vmax + m.gen_fmax); }
+// shared memory of a collide tile: its queue of broad-phase survivors, with
+// the edge query's two survivor lists behind it when the model has general
+// pairs (ints); then the polytope cache (world vertices and face normals of
+// both polytopes of a general pair) and the clip buffers (doubles)
+__host__ __device__ inline int collide_tile_ints(const DModel& m) {
+  return COLLIDE_QUEUE + (m.gen_vmax > 0 ? 2 * GEN_SURV_CAP : 0);
+}
+__host__ __device__ inline int collide_cache_doubles(const DModel& m) { return m.gen_cache + m.gen_clip; }
 
 __device__ inline double* tile_workspace(const StepArgs& A, unsigned char* sm, int stride, int tib) {
   int off = A.stage_model ? staged_model_bytes(A.m.arena_bytes) : 0;
@@ -167,13 +172,19 @@ __global__ void __launch_bounds__(256, 2) collide_kernel(const __grid_constant__
   EnvCtx e;
   e.ws = nullptr;
   e.scr = nullptr;
-  // the tile's queue of broad-phase survivors (2G ints), then its polytope cache
+  // the tile's queue of broad-phase survivors (2G ints) and edge lists, then
+  // its polytope cache and clip buffers
   int tpb = blockDim.x / G;
-  int* queue = reinterpret_cast<int*>(tile_workspace(A, smem, 0, 0)) + (threadIdx.x / G) * COLLIDE_QUEUE;
-  double* gcache = nullptr;
-  if (m.gen_vmax > 0)
-    gcache = reinterpret_cast<double*>(reinterpret_cast<int*>(tile_workspace(A, smem, 0, 0)) + tpb * COLLIDE_QUEUE) +
-             (threadIdx.x / G) * collide_cache_doubles(m);
+  int* queue = reinterpret_cast<int*>(tile_workspace(A, smem, 0, 0)) + (threadIdx.x / G) * collide_tile_ints(m);
+  GenScratch gs{nullptr, nullptr, nullptr};
+  if (m.gen_vmax > 0) {
+    double* tile = reinterpret_cast<double*>(reinterpret_cast<int*>(tile_workspace(A, smem, 0, 0)) +
+                                             tpb * collide_tile_ints(m)) +
+                   (threadIdx.x / G) * collide_cache_doubles(m);
+    gs.cache = m.gen_cache ? tile : nullptr;
+    gs.clip = m.gen_clip ? tile + m.gen_cache : nullptr;
+    gs.surv = queue + COLLIDE_QUEUE;
+  }
   for (int item = first_item<G>(); item < A.count; item = next_item(T, A.queue + 1, A.count)) {
     size_t env = (size_t)A.start + item;
     e.env = (int)env;
@@ -184,7 +195,7 @@ __global__ void __launch_bounds__(256, 2) collide_kernel(const __grid_constant__
     prefetch_l1(T, e.prm, sizeof(double) * m.pstride);
     prefetch_l1(T, e.geo, sizeof(double) * G_STRIDE * m.ngeom);
     int status = 0;
-    int ncon = collide(T, m, A.w, A.s, e, &status, queue, gcache);
+    int ncon = collide(T, m, A.w, A.s, e, &status, queue, gs);
     if (T.lane() == 0) {
       wk[A.k.meta + K_META_NCON] = ncon;
       wk[A.k.meta + K_META_STATUS] = (double)((int)wk[A.k.meta + K_META_STATUS] | status);
@@ -596,7 +607,8 @@ size_t kernel_smem(int which, const StepArgs& a, int tiles_per_block) {
   size_t staged = a.stage_model ? (size_t)staged_model_bytes(a.m.arena_bytes) : 0;
   switch (which) {
     case K_COLLIDE:
-      return staged + (size_t)tiles_per_block * (COLLIDE_QUEUE * sizeof(int) + collide_cache_doubles(a.m) * sizeof(double));
+      return staged + (size_t)tiles_per_block *
+                          (collide_tile_ints(a.m) * sizeof(int) + collide_cache_doubles(a.m) * sizeof(double));
     case K_NEWTON: return staged + (size_t)tiles_per_block * a.wn.stride * sizeof(double);
     default: return staged + (size_t)tiles_per_block * a.w.stride * sizeof(double);
   }
@@ -633,6 +645,18 @@ cudaError_t launch_substep(const StepArgs& a, const SubstepCfg& c, cudaStream_t 
   }
   PG_LAUNCH(K_NEWTON, newton_kernel, c.newton, a);
   return cudaSuccess;
+}
+
+__global__ void hull_support_kernel(const __grid_constant__ DModel m, int mesh, const double* dirs, int n,
+                                    int* vertex) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) vertex[i] = hull_support(m, mesh, ld3(dirs + 3 * i), 0);
+}
+
+cudaError_t launch_hull_support(const DModel& m, int mesh, const double* dirs, int n, int* vertex, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  hull_support_kernel<<<(n + 127) / 128, 128, 0, s>>>(m, mesh, dirs, n, vertex);
+  return cudaGetLastError();
 }
 
 cudaError_t reset_queue(const StepArgs& a, cudaStream_t s) { return cudaMemsetAsync(a.queue, 0, 4 * sizeof(int), s); }

@@ -37,7 +37,12 @@ enum { R_AREF = 0, R_D = 1, R_JAR = 2, R_JP = 3, R_POS = 4, R_DIAG = 5, R_FLAGS 
 enum { G_POS = 0, G_MAT = 3, G_AABB = 12, G_STRIDE = 18 };
 
 constexpr int NV_MAX = 64;  // dof-chain masks are 64-bit
-constexpr int HULL_FACE_MAX = 32;  // longest hull face loop the device clips
+constexpr int HULL_FACE_MAX = 32;     // longest face loop a lane clips in its own buffers
+constexpr int HULL_FACE_LIMIT = 256;  // longest hull face loop accepted (past HULL_FACE_MAX: clipped in shared memory)
+constexpr int HULL_SCAN_BELOW = 64;   // hulls with fewer vertices scan for support points (fasthull.rs:23)
+constexpr int HULL_SEEDS = 26;        // seed directions of the support walk: (x, y, z) in {-1, 0, 1}^3, not 0
+constexpr int GEN_SURV_CAP = 64;      // edges per polytope the edge query lists after pruning
+constexpr int GEN_CACHE_LIMIT = 1152; // largest polytope cache of a collide tile (doubles); above: no cache
 constexpr int CYL_SIDES = 16;  // a cylinder in the general narrow phase: a prism of this many sides
 constexpr int COLLIDE_QUEUE = 64;  // broad-phase survivor slots per collide tile (2 x the widest tile)
 
@@ -46,6 +51,9 @@ struct DModel {
   int nq, nv, nu, nbody, njnt, ngeom, ncam, neq, npair, nblock, nlevel, nmesh;
   int maxcon, maxrows, maxbs;
   int gen_vmax, gen_fmax;  // most vertices / faces of a polytope in a general pair (0: no such pair)
+  int gen_lmax;            // longest face loop of a polytope in a general pair
+  int gen_cache;           // doubles of polytope cache per collide tile (0: vertices formed at each use)
+  int gen_clip;            // doubles of shared clip buffers per collide tile (0: the lane's own buffers)
   // ---- options (model.rs:60-100)
   double timestep, gravity[3];
   int integrator, solver, iterations;
@@ -127,6 +135,10 @@ struct DModel {
   const int* hull_enum;
   const int* hull_edge;      // [*][2] vertex pairs
   const int* hull_eface;     // [*][2] the two faces of each edge (mesh-local face index)
+  const int* hull_nbadr;     // per hull vertex (global index): its neighbours in hull_nb, count
+  const int* hull_nbnum;
+  const int* hull_nb;        // neighbour vertices (mesh-local index), from the edges
+  const int* hull_seed;      // [nmesh][HULL_SEEDS] vertex extreme along each seed direction
 
   // ---- per-env parameter block offsets (doubles) and stride
   int p_friction, p_size, p_contype, p_conaff, p_mass, p_inertia, p_ipos, p_damping, p_gain, p_bias, p_qpos_reset,

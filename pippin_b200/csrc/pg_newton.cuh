@@ -19,10 +19,10 @@ namespace pg {
 // (in pair order) in `queue` (2G ints of shared memory); the narrow phase
 // takes them G at a time, one pair per lane, so a batch of narrow-phase
 // work waits for G survivors instead of running once per G candidates.
-// gcache: the tile's polytope cache for general pairs (or nullptr).
+// gs: the tile's shared scratch for general pairs (pointers nullptr when absent).
 template <int G>
 __device__ int collide(const Tile<G>& T, const DModel& m, const WsLayout& w, const ScrLayout& s, const EnvCtx& e,
-                       int* status, int* queue, double* gcache) {
+                       int* status, int* queue, const GenScratch& gs) {
   int lane = T.lane();
   const double* prm = e.prm;
   const double* gr = e.geo;  // poses and boxes from the tree walk
@@ -50,7 +50,7 @@ __device__ int collide(const Tile<G>& T, const DModel& m, const WsLayout& w, con
     for (unsigned gm = T.ballot(general); gm; gm &= gm - 1) {
       int d = __ffs(gm) - 1;
       int h1 = T.bcast(g1, d), h2 = T.bcast(g2, d);
-      collide_general(T, m, pose(h1), pose(h2), m.margin, hits, gcache, d);
+      collide_general(T, m, pose(h1), pose(h2), m.margin, hits, gs, d);
     }
     int nh = hits.n < MAX_HITS ? hits.n : MAX_HITS;
     int tot;

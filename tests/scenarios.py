@@ -401,3 +401,52 @@ IMPLICITFAST_ARM = (
     '<actuator><position joint="a1" kp="40" kv="4"/><velocity joint="a2" kv="3"/>'
     '<position joint="a0" kp="10" kv="1" ctrlrange="-1 1"/><velocity joint="a3" kv="5" forcerange="-2 2"/>'
     '<motor joint="a2" gear="2"/></actuator></mujoco>')
+
+
+# ----------------------------------------------------------------- large hulls
+def lumpy_sphere_points(n=600, scale=1.0):
+    """The point set of the reference's support-walk test
+    (crates/pippin/src/fasthull.rs:221-229): n points on a golden-angle
+    spiral over a sphere whose radius has a lump pattern, squashed to 0.7 in
+    z. Its hull keeps the points outside the dips: 276 of the 600."""
+    i = np.arange(n, dtype=np.float64)
+    t = i * 2.399963
+    p = np.arccos(1.0 - 2.0 * (i + 0.5) / n)
+    r = 1.0 + 0.2 * np.sin(3.0 * t) * np.cos(2.0 * p)
+    pts = np.stack([r * np.sin(p) * np.cos(t), r * np.sin(p) * np.sin(t), 0.7 * r * np.cos(p)], axis=1)
+    return pts * scale
+
+
+def support_directions(n=2000):
+    """The query directions of fasthull.rs:231-233."""
+    a = np.arange(n, dtype=np.float64) * 0.731
+    d = np.stack([np.sin(a) * np.cos(1.3 * a), np.cos(0.7 * a), np.sin(2.1 * a)], axis=1)
+    return d / np.linalg.norm(d, axis=1, keepdims=True)
+
+
+def _verts(pts):
+    return " ".join(repr(float(x)) for x in np.asarray(pts).ravel())
+
+
+def prism_points(sides=48, r=0.05, h=0.03):
+    th = 2.0 * np.pi * np.arange(sides) / sides
+    ring = np.stack([r * np.cos(th), r * np.sin(th)], axis=1)
+    return np.concatenate([np.column_stack([ring, np.full(sides, -h)]), np.column_stack([ring, np.full(sides, h)])])
+
+
+def big_hulls_xml():
+    """Hulls past the scan limit and faces past a lane's clip buffers: two
+    lumpy spheres of 276 hull vertices (the support walk on both sides of a
+    pair), a 48-sided prism (96 vertices, 48-gon caps: clipped in shared
+    memory) and a box, dropped onto a plane and onto each other."""
+    lumpy = _verts(lumpy_sphere_points(600, 0.05))
+    prism = _verts(prism_points())
+    return ('<mujoco><option timestep="0.002"/><asset>'
+            f'<mesh name="lumpy" vertex="{lumpy}"/><mesh name="prism" vertex="{prism}"/></asset><worldbody>'
+            '<geom type="plane" size="5 5 .1"/>'
+            '<body name="l1" pos="0 0 0.06" euler="10 20 30"><freejoint/><geom type="mesh" mesh="lumpy"/></body>'
+            '<body name="l2" pos="0.02 0.01 0.16" euler="40 5 70"><freejoint/><geom type="mesh" mesh="lumpy"/></body>'
+            '<body name="p" pos="0.3 0 0.04"><freejoint/><geom type="mesh" mesh="prism"/></body>'
+            '<body name="b" pos="0.31 0.01 0.1" euler="0 0 20"><freejoint/><geom type="box" size=".03 .03 .02"/></body>'
+            '<body name="p2" pos="0.6 0 0.1" euler="90 0 0"><freejoint/><geom type="mesh" mesh="prism"/></body>'
+            '</worldbody></mujoco>')

@@ -6,11 +6,13 @@ Tolerances (relative to the quantity's scale, max(|ref|_inf, 1)):
   per-step qacc, qvel, qpos        1e-10 (identical input states each step)
   contact-free 1 s trajectories    1e-8
 """
+import ctypes as C
+
 import numpy as np
 import pytest
 
 from oracle.oracle import CTRL, QACC, QPOS, QVEL, Oracle
-from pippin_b200 import CudaPhysics, Field, Param, PhysicsError, mjcf, scenes
+from pippin_b200 import CudaPhysics, Field, Param, PhysicsError, _native, mjcf, scenes
 from tests import scenarios as S
 
 pytestmark = pytest.mark.gpu
@@ -56,6 +58,7 @@ MODELS = {
     "mesh_stack": lambda: S.mesh_stack_xml(),
     "cylinders": lambda: S.CYLINDERS,
     "hull_tumble": scenes.hull_tumble_xml,
+    "big_hulls": lambda: S.big_hulls_xml(),
     # joint equality rows, fixed tendons, implicitfast actuators
     "equality_chain": lambda: S.EQUALITY_CHAIN,
     "equality_chain_solo": lambda: S.EQUALITY_CHAIN.replace(
@@ -196,10 +199,13 @@ def test_general_convex_behaviour(check, solver):
     check(S.CudaSim, solver)
 
 
-@pytest.mark.parametrize("name", ["hull_tumble", "cylinders", "mesh_stack"])
+@pytest.mark.parametrize("name", ["hull_tumble", "cylinders", "mesh_stack", "big_hulls"])
 def test_general_convex_step_parity(name):
     """Per-step Newton output on identical input states while hulls and
-    cylinders fall, collide and settle (tolerance 1e-10)."""
+    cylinders fall, collide and settle (tolerance 1e-10). The oracle scans
+    every vertex and tests every edge pair; the device walks large hulls'
+    vertex graphs and prunes edges (big_hulls: hulls of 276 and 96 vertices,
+    48-gon faces clipped in shared memory)."""
     n = 16
     m, g, o = pair(MODELS[name](), n, tolerance=1e-10)
     T = int(round(0.6 / m.timestep))
@@ -221,6 +227,28 @@ def test_general_convex_step_parity(name):
             for e in range(n):
                 assert rel(a[e], b[e]) < TOL_STEP, (t, e, fg, rel(a[e], b[e]))
     assert contacts_seen > 0
+
+
+def test_hull_support_walk_on_device_matches_brute_force():
+    """fasthull.rs:217-240 on the device: the collision kernel's support walk
+    over the hull of the 600-point lumpy sphere (276 vertices) projects as far
+    as a scan of every hull vertex along each of 2000 directions (1e-12)."""
+    L = _native.load()
+    m = mjcf.load_string(S.big_hulls_xml())
+    g = CudaPhysics(mjcf.to_blob(m), 1)
+    v = np.asarray(m.hull_vert[0], dtype=np.float64)
+    assert len(v) >= 64
+    d = np.ascontiguousarray(S.support_directions())
+    out = np.zeros(len(d), dtype=np.int32)
+    rc = L.pg_hull_support(g._h, 0, d.ctypes.data_as(C.POINTER(C.c_double)), len(d),
+                           out.ctypes.data_as(C.POINTER(C.c_int32)))
+    assert rc == 0, _native.last_error()
+    assert ((out >= 0) & (out < len(v))).all()
+    exact = (v @ d.T).max(axis=0)
+    got = np.einsum("ij,ij->i", v[out], d)
+    assert np.abs(exact - got).max() < 1e-12
+    assert L.pg_hull_support(g._h, 2, d.ctypes.data_as(C.POINTER(C.c_double)), 1,
+                             out.ctypes.data_as(C.POINTER(C.c_int32))) != 0  # no mesh 2
 
 
 @pytest.mark.parametrize("solver", ["newton", "pgs"])

@@ -86,3 +86,22 @@ def test_cube_mass_properties_are_exact():
     for i in range(3):
         assert abs(icom[4 * i] - expected) < k["tol"]
     assert abs(icom[1]) < k["tol"] and abs(icom[2]) < k["tol"] and abs(icom[5]) < k["tol"]
+
+
+def test_hull_support_walk_matches_brute_force():
+    """fasthull.rs:217-240 restated: on the hull of 600 points of a lumpy
+    sphere, the support walk's vertex projects as far as a scan over every
+    hull vertex along each of 2000 directions (1e-12)."""
+    from oracle.oracle import hull_support
+
+    from . import scenarios as S
+
+    verts, tris = mjcf.convex_hull([tuple(p) for p in S.lumpy_sphere_points()])
+    _, edges = mjcf.hull_features(verts, tris)
+    v = np.asarray(verts)
+    assert len(v) >= 64  # the walk, not the scan
+    d = S.support_directions()
+    walked = hull_support(v, edges, d)
+    exact = (v @ d.T).max(axis=0)
+    got = np.einsum("ij,ij->i", v[walked], d)
+    assert np.abs(exact - got).max() < 1e-12
