@@ -220,12 +220,16 @@ __device__ inline bool p_walks(const Poly& p) { return p.kind == GEOM_MESH && p.
 // Point of the polytope closest to x: the signed distance (negative inside,
 // then to the nearest face plane), the point, and the face when inside (-1
 // outside). Outside, the closest point lies on a face (projection inside
-// its loop) or on an edge.
-__device__ __noinline__ double closest_point(const Poly& p, V3 x, V3* q, int* inside_face) {
-  int nf = p_nf(p);
+// its loop) or on an edge. The faces and edges are shared out over the
+// tile's lanes; every choice is the one a loop over the faces, then the
+// edges, in order with strict comparisons makes (the first maximum inside,
+// the first minimum outside), and every lane returns the result.
+template <int G>
+__device__ __noinline__ double closest_point(const Tile<G>& T, const Poly& p, V3 x, V3* q, int* inside_face) {
+  const int nf = p_nf(p), ne = p_ne(p);
   double best = -INFINITY;
-  int bf = 0;
-  for (int f = 0; f < nf; f++) {
+  int bf = 0x7fffffff;
+  for (int f = T.lane(); f < nf; f += G) {
     V3 n = p_fn(p, f);
     double s = dot(n, x) - p_fd(p, f, n);
     if (s > best) {
@@ -233,14 +237,18 @@ __device__ __noinline__ double closest_point(const Poly& p, V3 x, V3* q, int* in
       bf = f;
     }
   }
+  T.argmax(&best, &bf);
+  if (bf == 0x7fffffff) bf = 0;
   if (best <= 0.0) {
     *q = x - p_fn(p, bf) * best;
     *inside_face = bf;
     return best;
   }
   *inside_face = -1;
+  // candidates in the order faces (index f), then edges (index nf + e)
   double bd = INFINITY;
-  for (int f = 0; f < nf; f++) {
+  int bk = 0x7fffffff;
+  for (int f = T.lane(); f < nf; f += G) {
     V3 n = p_fn(p, f);
     double s = dot(n, x) - p_fd(p, f, n);
     if (s <= 0.0) continue;
@@ -254,22 +262,34 @@ __device__ __noinline__ double closest_point(const Poly& p, V3 x, V3* q, int* in
     }
     if (in && s < bd) {
       bd = s;
-      *q = y;
+      bk = f;
     }
   }
-  int ne = p_ne(p);
-  for (int e = 0; e < ne; e++) {
+  for (int e = T.lane(); e < ne; e += G) {
     int ia, ib;
     p_edge(p, e, &ia, &ib);
     V3 a = p_v(p, ia), b = p_v(p, ib);
     V3 ab = b - a;
     double t = clampd(dot(x - a, ab) / fmax(dot(ab, ab), 1e-300), 0.0, 1.0);
-    V3 y = a + ab * t;
-    double d = norm(x - y);
+    double d = norm(x - (a + ab * t));
     if (d < bd) {
       bd = d;
-      *q = y;
+      bk = nf + e;
     }
+  }
+  double nb = -bd;
+  T.argmax(&nb, &bk);
+  bd = -nb;
+  if (bk < nf) {
+    V3 n = p_fn(p, bk);
+    *q = x - n * (dot(n, x) - p_fd(p, bk, n));
+  } else if (bk != 0x7fffffff) {
+    int ia, ib;
+    p_edge(p, bk - nf, &ia, &ib);
+    V3 a = p_v(p, ia), b = p_v(p, ib);
+    V3 ab = b - a;
+    double t = clampd(dot(x - a, ab) / fmax(dot(ab, ab), 1e-300), 0.0, 1.0);
+    *q = a + ab * t;
   }
   return bd;
 }
@@ -600,11 +620,14 @@ __device__ void polytope_polytope(const Tile<G>& T, const Poly& a, const Poly& b
   else clip_faces(b, fb, a, -p_fn(b, fb), margin, out, gs.clip, cap);
 }
 
-// sphere (center c, radius r) against a polytope; normal from the sphere
-__device__ inline void sphere_polytope(V3 c, double r, const Poly& p, double margin, Hits& out) {
+// sphere (center c, radius r) against a polytope; normal from the sphere;
+// the contact on lane `owner`
+template <int G>
+__device__ void sphere_polytope(const Tile<G>& T, V3 c, double r, const Poly& p, double margin, Hits& out, int owner) {
   V3 q{0.0, 0.0, 0.0};
   int face;
-  double dist = closest_point(p, c, &q, &face);
+  double dist = closest_point(T, p, c, &q, &face);
+  if (T.lane() != owner) return;
   if (face < 0) {
     double depth = r - dist;
     if (depth <= -margin || dist <= 1e-12) return;
@@ -619,14 +642,15 @@ __device__ inline void sphere_polytope(V3 c, double r, const Poly& p, double mar
 
 // capsule against a polytope: the deepest point along the axis (golden
 // section on the signed distance) and the ends, as capsule-box does
-__device__ inline void capsule_polytope(const GPose& a, const Poly& p, double margin, Hits& out) {
+template <int G>
+__device__ void capsule_polytope(const Tile<G>& T, const GPose& a, const Poly& p, double margin, Hits& out, int owner) {
   V3 ax = col(a.mat, 2) * a.size.y;
   V3 p0 = a.pos - ax, p1 = a.pos + ax;
   double r = a.size.x;
   auto f = [&](double t) {
     V3 q;
     int face;
-    return closest_point(p, p0 + (p1 - p0) * t, &q, &face);
+    return closest_point(T, p, p0 + (p1 - p0) * t, &q, &face);
   };
   const double g = 0.61803398875;
   double lo = 0.0, hi = 1.0;
@@ -648,33 +672,53 @@ __device__ inline void capsule_polytope(const GPose& a, const Poly& p, double ma
     }
   }
   double tmin = 0.5 * (lo + hi);
-  sphere_polytope(p0 + (p1 - p0) * tmin, r, p, margin, out);
+  sphere_polytope(T, p0 + (p1 - p0) * tmin, r, p, margin, out, owner);
   for (int e = 0; e < 2; e++) {
     double t = e == 0 ? 0.0 : 1.0;
-    if (fabs(t - tmin) > 0.1 && f(t) < r + margin) sphere_polytope(p0 + (p1 - p0) * t, r, p, margin, out);
+    if (fabs(t - tmin) > 0.1 && f(t) < r + margin) sphere_polytope(T, p0 + (p1 - p0) * t, r, p, margin, out, owner);
   }
 }
 
 // plane against a hull: the four deepest vertices within the margin, in
-// the order a stable sort by depth gives
-__device__ inline void plane_polytope(const GPose& pl, const Poly& p, double margin, Hits& out) {
+// the order a stable sort by depth gives (equal depths by vertex index).
+// Each lane keeps the four best of its share of the vertices by (depth,
+// index); four tile-wide minima then pick the result, which lane `owner`
+// records.
+template <int G>
+__device__ void plane_polytope(const Tile<G>& T, const GPose& pl, const Poly& p, double margin, Hits& out, int owner) {
   V3 n = col(pl.mat, 2);
-  DP keep[4];
+  double kd[4];
+  int ki[4];
   int nk = 0;
   int nv = p_nv(p);
-  for (int i = 0; i < nv; i++) {
-    V3 x = p_v(p, i);
-    double d = dot(x - pl.pos, n);
+  for (int i = T.lane(); i < nv; i += G) {
+    double d = dot(p_v(p, i) - pl.pos, n);
     if (!(d < margin)) continue;
-    if (nk == 4 && !(d < keep[3].d)) continue;
+    if (nk == 4 && !(d < kd[3])) continue;
     int j = nk < 4 ? nk++ : 3;
-    while (j > 0 && keep[j - 1].d > d) {
-      keep[j] = keep[j - 1];
+    while (j > 0 && kd[j - 1] > d) {
+      kd[j] = kd[j - 1];
+      ki[j] = ki[j - 1];
       j--;
     }
-    keep[j] = DP{d, x};
+    kd[j] = d;
+    ki[j] = i;
   }
-  for (int k = 0; k < nk; k++) out.push(keep[k].p - n * (keep[k].d * 0.5), n, -keep[k].d);
+  int head = 0, ns = 0, sel[4];
+  for (int r = 0; r < 4; r++) {
+    double v = head < nk ? -kd[head] : -INFINITY;
+    int idx = head < nk ? ki[head] : 0x7fffffff;
+    T.argmax(&v, &idx);
+    if (idx == 0x7fffffff) break;
+    sel[ns++] = idx;
+    if (head < nk && ki[head] == idx) head++;
+  }
+  if (T.lane() != owner) return;
+  for (int k = 0; k < ns; k++) {
+    V3 x = p_v(p, sel[k]);
+    double d = dot(x - pl.pos, n);
+    out.push(x - n * (d * 0.5), n, -d);
+  }
 }
 
 // Fills buf with p's world vertices, then its world face normals (the values
@@ -692,10 +736,11 @@ __device__ void poly_cache(const Tile<G>& T, Poly& p, double* buf) {
 }
 
 // One pair on the whole tile: every lane passes the same pair; the polytope
-// queries share their candidates out over the lanes, and the contact points
-// (clipping, closest points) are formed on lane `owner` alone, whose `out`
-// gets them (the other lanes' stays as it was: their clip and point buffers
-// stay untouched, so the tile's local-memory footprint is one lane's). With
+// queries, closest-point searches and deepest-vertex picks share their
+// candidates out over the lanes, and the contacts are formed (the clipping
+// included) on lane `owner` alone, whose `out` gets them (the other lanes'
+// stays as it was: their clip and point buffers stay untouched, so the
+// tile's local-memory footprint is one lane's). With
 // gs.cache (6 (gen_vmax + gen_fmax) doubles of the tile's shared memory) the
 // polytopes' world vertices and normals are formed once instead of at every
 // use.
@@ -711,11 +756,11 @@ __device__ __noinline__ void collide_general(const Tile<G>& T, const DModel& m, 
   if (cache) poly_cache(T, pb, cache);
   const bool own = T.lane() == owner;
   if (a.type == GEOM_PLANE) {
-    if (own) plane_polytope(a, pb, margin, out);
+    plane_polytope(T, a, pb, margin, out, owner);
   } else if (a.type == GEOM_SPHERE) {
-    if (own) sphere_polytope(a.pos, a.size.x, pb, margin, out);
+    sphere_polytope(T, a.pos, a.size.x, pb, margin, out, owner);
   } else if (a.type == GEOM_CAPSULE) {
-    if (own) capsule_polytope(a, pb, margin, out);
+    capsule_polytope(T, a, pb, margin, out, owner);
   } else {
     Poly pa{a.type, a.pos, a.mat, a.size, &m, a.data};
     if (cache) poly_cache(T, pa, cache + 3 * (m.gen_vmax + m.gen_fmax));

@@ -438,7 +438,8 @@ def big_hulls_xml():
     """Hulls past the scan limit and faces past a lane's clip buffers: two
     lumpy spheres of 276 hull vertices (the support walk on both sides of a
     pair), a 48-sided prism (96 vertices, 48-gon caps: clipped in shared
-    memory) and a box, dropped onto a plane and onto each other."""
+    memory), a box, a sphere and a capsule, dropped onto a plane and onto
+    each other."""
     lumpy = _verts(lumpy_sphere_points(600, 0.05))
     prism = _verts(prism_points())
     return ('<mujoco><option timestep="0.002"/><asset>'
@@ -449,4 +450,6 @@ def big_hulls_xml():
             '<body name="p" pos="0.3 0 0.04"><freejoint/><geom type="mesh" mesh="prism"/></body>'
             '<body name="b" pos="0.31 0.01 0.1" euler="0 0 20"><freejoint/><geom type="box" size=".03 .03 .02"/></body>'
             '<body name="p2" pos="0.6 0 0.1" euler="90 0 0"><freejoint/><geom type="mesh" mesh="prism"/></body>'
+            '<body name="s" pos="0.03 0.01 0.25"><freejoint/><geom type="sphere" size=".02"/></body>'
+            '<body name="c" pos="0.6 0.01 0.22" euler="0 80 10"><freejoint/><geom type="capsule" size=".015 .04"/></body>'
             '</worldbody></mujoco>')
