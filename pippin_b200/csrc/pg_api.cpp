@@ -401,6 +401,7 @@ struct Handle {
   double* prev_con = nullptr;   // [env][maxcon][P_STRIDE] PGS warm start (allocated with PGS)
   int32_t* prev_ncon = nullptr;  // [env]
   int* queue = nullptr;
+  int* order = nullptr;  // [n] Newton-phase order of a substep's envs
   // learned warm start: contact list, network, and whether one is loaded
   LearnArgs learn{};
   bool mlp_loaded = false;
@@ -471,9 +472,10 @@ StepArgs make_args(Handle* h) {
   a.st.prev_ncon = h->prev_ncon;
   a.scratch = h->scratch;
   a.queue = h->queue;
+  a.order = h->order;
   a.warm_mode = h->warm_mode;
   a.learn = h->learn;
-  a.learn.count = h->queue + 3;
+  a.learn.count = h->queue + Q_LEARN;
   a.stage_model = h->dm.arena_bytes <= STAGE_LIMIT ? 1 : 0;
   std::vector<int> po = dmodel_pointer_fields();
   a.n_ptr = (int)std::min<size_t>(po.size(), MAX_PTR_FIELDS);
@@ -1193,7 +1195,7 @@ void destroy(pg_handle* h) {
   cudaSetDevice(h->device);
   clear_graphs(h);
   void* ptrs[] = {h->d_model, h->qpos, h->qvel, h->ctrl, h->qacc, h->applied, h->params, h->iters, h->ncon,
-                  h->nrows, h->status, h->scratch, h->work, h->prev_con, h->prev_ncon, h->queue, h->b_ctrl.p, h->b_qout.p, h->b_poses_g.p,
+                  h->nrows, h->status, h->scratch, h->work, h->prev_con, h->prev_ncon, h->queue, h->order, h->b_ctrl.p, h->b_qout.p, h->b_poses_g.p,
                   h->b_poses_c.p, h->b_dbg.p, h->b_vals.p, h->b_ids.p, h->learn.items, h->learn.feat, h->learn.force,
                   h->learn.rows, (void*)h->learn.mlp_w, (void*)h->learn.mlp_f};
   for (void* p : ptrs)
@@ -1278,7 +1280,8 @@ int pg_create(const void* blob, size_t bytes, int64_t n_envs, int device, pg_han
   CK(cudaMalloc(&h->ncon, sizeof(int32_t) * n));
   CK(cudaMalloc(&h->nrows, sizeof(int32_t) * n));
   CK(cudaMalloc(&h->status, sizeof(int32_t) * n));
-  CK(cudaMalloc(&h->queue, sizeof(int) * 4));
+  CK(cudaMalloc(&h->queue, sizeof(int) * QUEUE_INTS));
+  CK(cudaMalloc(&h->order, sizeof(int) * std::max<int64_t>(n, 1)));
   CK(cudaMalloc(&h->work, sizeof(double) * n * h->k.stride));
   CK(cudaMemsetAsync(h->work, 0, sizeof(double) * n * h->k.stride, h->stream));
   CK(cudaMemsetAsync(h->qvel, 0, sizeof(double) * n * std::max(m.nv, 1), h->stream));
@@ -2018,7 +2021,7 @@ int pg_warm_samples(pg_handle* h, int64_t start, int64_t end, float* X, size_t x
   a.sidx = 0;
   if ((rc = launch_status(launch_substep(a, fit(h->cfg, end - start), h->stream)))) return rc;
   int count = 0;
-  CK(cudaMemcpyAsync(&count, h->queue + 3, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemcpyAsync(&count, h->queue + Q_LEARN, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   int64_t m = std::min(count, h->learn.cap);
   std::vector<float> fx((size_t)m * LEARN_NF), fr((size_t)m * 4);

@@ -185,7 +185,7 @@ __global__ void __launch_bounds__(256, 2) collide_kernel(const __grid_constant__
     gs.clip = m.gen_clip ? tile + m.gen_cache : nullptr;
     gs.surv = queue + COLLIDE_QUEUE;
   }
-  for (int item = first_item<G>(); item < A.count; item = next_item(T, A.queue + 1, A.count)) {
+  for (int item = first_item<G>(); item < A.count; item = next_item(T, A.queue + Q_COLLIDE, A.count)) {
     size_t env = (size_t)A.start + item;
     e.env = (int)env;
     e.prm = A.st.params + env * m.pstride;
@@ -199,6 +199,12 @@ __global__ void __launch_bounds__(256, 2) collide_kernel(const __grid_constant__
     if (T.lane() == 0) {
       wk[A.k.meta + K_META_NCON] = ncon;
       wk[A.k.meta + K_META_STATUS] = (double)((int)wk[A.k.meta + K_META_STATUS] | status);
+      // the Newton phase takes envs with contacts (its long solves) first,
+      // so that the envs left for the end of its queue are short ones
+      if (A.order) {
+        int slot = ncon > 0 ? atomicAdd(A.queue + Q_FRONT, 1) : A.count - 1 - atomicAdd(A.queue + Q_BACK, 1);
+        A.order[slot] = item;
+      }
     }
     T.sync();
     if (A.learn.mode == LEARN_DUMP || (A.learn.mode == LEARN_PREDICT && A.warm_mode == WARM_LEARNED))
@@ -226,8 +232,9 @@ __global__ void __launch_bounds__(256, 2) newton_kernel(const __grid_constant__ 
   e.scr = A.scratch + gtile * (size_t)A.s.stride;
   int nq = m.nq, nv = m.nv;
   double h = m.timestep;
-  for (int item = first_item<G>(); item < A.count; item = next_item(T, A.queue + 2, A.count)) {
-    size_t env = (size_t)A.start + item;
+  for (int item = first_item<G>(); item < A.count; item = next_item(T, A.queue + Q_NEWTON, A.count)) {
+    const int ei = A.order ? A.order[item] : item;  // the env's index in the range
+    size_t env = (size_t)A.start + ei;
     e.env = (int)env;
     e.prm = A.st.params + env * m.pstride;
     double* wk = A.work + env * A.k.stride;
@@ -311,9 +318,9 @@ __global__ void __launch_bounds__(256, 2) newton_kernel(const __grid_constant__ 
       copy_in(T, A.st.qpos + env * nq, ws + w.qpos, nq);
       copy_in(T, A.st.qvel + env * nv, v, nv);
       copy_in(T, A.st.qacc + env * nv, ws + w.qacc, nv);
-      if (A.qpos_out) copy_in(T, A.qpos_out + ((size_t)item * A.nstep + A.sidx) * nq, ws + w.qpos, nq);
+      if (A.qpos_out) copy_in(T, A.qpos_out + ((size_t)ei * A.nstep + A.sidx) * nq, ws + w.qpos, nq);
     } else if (A.qpos_out) {
-      copy_in(T, A.qpos_out + ((size_t)item * A.nstep + A.sidx) * nq, A.st.qpos + env * nq, nq);
+      copy_in(T, A.qpos_out + ((size_t)ei * A.nstep + A.sidx) * nq, A.st.qpos + env * nq, nq);
     }
     if (T.lane() == 0) {
       A.st.iters[env] = iters;
@@ -629,14 +636,25 @@ size_t kernel_smem(int which, const StepArgs& a, int tiles_per_block) {
   } while (0)
 
 cudaError_t launch_smooth_collide(const StepArgs& a, const SubstepCfg& c, cudaStream_t s) {
-  cudaError_t e = cudaMemsetAsync(a.queue, 0, 4 * sizeof(int), s);
+  cudaError_t e = cudaMemsetAsync(a.queue, 0, QUEUE_INTS * sizeof(int), s);
   if (e != cudaSuccess) return e;
   PG_LAUNCH(K_SMOOTH, smooth_kernel, c.smooth, a);
   PG_LAUNCH(K_COLLIDE, collide_kernel, c.collide, a);
   return cudaSuccess;
 }
 
-cudaError_t launch_substep(const StepArgs& a, const SubstepCfg& c, cudaStream_t s) {
+// The Newton phase's order (envs with contacts first) pays only when its
+// grid has fewer tiles than envs, so that tiles pull further envs from the
+// queue; with a tile per env every env starts at once and the order is left
+// out (the collision phase then records none).
+inline StepArgs ordered_for(const StepArgs& a0, const LaunchCfg& newton) {
+  StepArgs a = a0;
+  if ((int64_t)newton.blocks * newton.tiles_per_block >= a.count) a.order = nullptr;
+  return a;
+}
+
+cudaError_t launch_substep(const StepArgs& a0, const SubstepCfg& c, cudaStream_t s) {
+  const StepArgs a = ordered_for(a0, c.newton);
   cudaError_t e = launch_smooth_collide(a, c, s);
   if (e != cudaSuccess) return e;
   if (a.learn.mode == LEARN_DUMP || (a.learn.mode == LEARN_PREDICT && a.warm_mode == WARM_LEARNED)) {
@@ -659,7 +677,7 @@ cudaError_t launch_hull_support(const DModel& m, int mesh, const double* dirs, i
   return cudaGetLastError();
 }
 
-cudaError_t reset_queue(const StepArgs& a, cudaStream_t s) { return cudaMemsetAsync(a.queue, 0, 4 * sizeof(int), s); }
+cudaError_t reset_queue(const StepArgs& a, cudaStream_t s) { return cudaMemsetAsync(a.queue, 0, QUEUE_INTS * sizeof(int), s); }
 
 cudaError_t learn_prepare() {
   return cudaFuncSetAttribute(learn_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MLP_SMEM);
@@ -676,7 +694,10 @@ cudaError_t launch_learn(const StepArgs& a, bool infer, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-cudaError_t launch_phase(int which, const StepArgs& a, const LaunchCfg& c, cudaStream_t s) {
+cudaError_t launch_phase(int which, const StepArgs& a0, const LaunchCfg& c, cudaStream_t s) {
+  // the collision phase always records the order; the Newton phase reads it
+  // when its own grid is smaller than the range (ordered_for)
+  const StepArgs a = which == K_NEWTON ? ordered_for(a0, c) : a0;
   switch (which) {
     case K_SMOOTH: PG_LAUNCH(K_SMOOTH, smooth_kernel, c, a); break;
     case K_COLLIDE: PG_LAUNCH(K_COLLIDE, collide_kernel, c, a); break;
@@ -687,14 +708,14 @@ cudaError_t launch_phase(int which, const StepArgs& a, const LaunchCfg& c, cudaS
 }
 
 cudaError_t launch_set_const(const StepArgs& a, const LaunchCfg& c, const int* envs, int n, cudaStream_t s) {
-  cudaError_t e = cudaMemsetAsync(a.queue, 0, 4 * sizeof(int), s);
+  cudaError_t e = cudaMemsetAsync(a.queue, 0, QUEUE_INTS * sizeof(int), s);
   if (e != cudaSuccess) return e;
   PG_LAUNCH(K_SET_CONST, set_const_kernel, c, a, envs, n);
   return cudaSuccess;
 }
 
 cudaError_t launch_poses(const StepArgs& a, const LaunchCfg& c, float* geoms, float* cams, cudaStream_t s) {
-  cudaError_t e = cudaMemsetAsync(a.queue, 0, 4 * sizeof(int), s);
+  cudaError_t e = cudaMemsetAsync(a.queue, 0, QUEUE_INTS * sizeof(int), s);
   if (e != cudaSuccess) return e;
   PG_LAUNCH(K_POSES, poses_kernel, c, a, geoms, cams);
   return cudaSuccess;

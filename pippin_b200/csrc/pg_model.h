@@ -237,6 +237,10 @@ enum { PK_NORMAL = 0, PK_FRICTION = 1, PK_BILATERAL = 2 };
 
 constexpr int MAX_PTR_FIELDS = 80;
 
+// the work counters of a substep: one per phase kernel, the learned start's
+// contact count, and the two ends of the Newton-phase order
+enum { Q_SMOOTH = 0, Q_COLLIDE = 1, Q_NEWTON = 2, Q_LEARN = 3, Q_FRONT = 4, Q_BACK = 5, QUEUE_INTS = 8 };
+
 struct StepArgs {
   DModel m;
   WsLayout w;   // smooth-dynamics phase (also set_const, poses)
@@ -246,7 +250,8 @@ struct StepArgs {
   EnvState st;
   double* scratch;   // [tiles][s.stride] (the Newton phase's rows and islands)
   double* work;      // [env][k.stride]
-  int* queue;        // work counters, one per phase kernel (reset before each substep)
+  int* queue;        // QUEUE_INTS work counters (reset before each substep): Q_* below
+  int* order;        // [count] Newton-phase order (envs with contacts first), or nullptr: env order
   int start, count, nstep;
   int sidx;          // substep index within the call
   int warm_mode;

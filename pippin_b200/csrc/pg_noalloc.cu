@@ -97,7 +97,8 @@ extern "C" int pg_step_static(pg_handle* h, int64_t start, int64_t end, int64_t 
   if ((rc = pg_static_tiles((size_t)a.s.stride * sizeof(double), nc.tiles_per_block, &tiles)) != PG_OK) return rc;
   nc.blocks = (int)std::min<int64_t>((int64_t)nc.blocks, tiles / nc.tiles_per_block);
   a.queue = reinterpret_cast<int*>(base);
-  a.learn.count = a.queue + 3;
+  a.order = nullptr;  // envs in index order: an order array would need memory per env
+  a.learn.count = a.queue + pg::Q_LEARN;
   a.scratch = reinterpret_cast<double*>(base + PG_STATIC_COUNTER_BYTES);
   // each substep restarts the phase counters before its kernels
   cudaError_t e = cudaSuccess;
