@@ -73,6 +73,8 @@ def parse():
                     "(comma-separated, e.g. 64,128) instead of the headline")
     ap.add_argument("--render-envs", type=int, default=4096, help="envs rendered per frame (the reference's "
                     "render benchmark renders 4096)")
+    ap.add_argument("--aux", action="store_true", help="per-call device time of the auxiliary kernels (set_const, "
+                    "pose export, reset, learned inference, network training, hull support) instead of the headline")
     return ap.parse_args()
 
 
@@ -666,6 +668,112 @@ def run_scene(args):
     print(json.dumps(line), flush=True)
 
 
+def run_aux(args):
+    """Device time per call of the kernels outside the substep's three phases,
+    each on a small workload through the public API (CUDA events on the
+    handle's stream): set_const after a per-env mass change
+    (set_const_kernel), pose export into device buffers (poses_kernel), reset
+    (reset_kernel), a substep with the learned start (learn_kernel, between
+    the collision and Newton phases), the network's forward pass and a
+    training epoch (mlp_forward_kernel; gemm_kernel, gemm_atb_kernel,
+    sum_splits_kernel, colsum_split_kernel, mse_kernel, loss_add_kernel,
+    adam_kernel, gather_kernel) and the hull support walk
+    (hull_support_kernel) over 2000 directions on a 276-vertex hull. Each
+    runs once inside the NVTX range "aux_once" (one launch of each kernel,
+    one training batch, for profilers) before it is timed."""
+    import ctypes as C
+
+    import torch
+    from pippin_b200 import CudaPhysics, Field, Param, _native, mjcf, scenes, warm
+    from pippin_b200.physics import WarmStart
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    n = args.envs
+    m = mjcf.load_string(scenes.ant_xml(tolerance=TOL, iterations=ITERS))
+    p = CudaPhysics(mjcf.to_blob(m), n)
+    stream = torch.cuda.ExternalStream(p.stream(), device=dev)
+    rng = np.random.default_rng(7)
+    L = _native.load()
+    out = {}
+
+    def timed(name, fn, reps=5):
+        p.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        e1.synchronize()
+        out[name] = e0.elapsed_time(e1) / reps
+
+    # states, contacts and a network fitted to them, outside the range
+    q = np.tile(np.array(m.qpos0), (n, 1)) + rng.uniform(-0.1, 0.1, (n, m.nq))
+    p.set(Field.QPOS, range(n), q)
+    p.set(Field.QVEL, range(n), rng.normal(0, 0.1, (n, m.nv)))
+    X, F = warm.collect(p, 120, controls=lambda t: rng.uniform(-1, 1, (n, m.nu)), skip=60)
+    k = min(len(X), 1 << 18)
+    w, _ = warm.train(X[:k], F[:k], epochs=1, batch=8192, lr=1e-3, seed=1)
+    masses = np.array(m.body_mass[1]) * rng.uniform(0.5, 2.0, (n, 1))
+    sc = p.scene()
+    gd = torch.empty(n * len(sc.geoms) * 12, dtype=torch.float32, device=dev)
+    hm = mjcf.load_string(scenes.lumpy_hull_xml())
+    h = CudaPhysics(mjcf.to_blob(hm), 1)
+    d = np.ascontiguousarray(scenes.support_directions())
+    v = np.zeros(len(d), dtype=np.int32)
+
+    def hull_support():
+        rc = L.pg_hull_support(h._h, 0, d.ctypes.data_as(C.POINTER(C.c_double)), len(d),
+                               v.ctypes.data_as(C.POINTER(C.c_int32)))
+        if rc != 0:
+            raise RuntimeError(_native.last_error())
+
+    p.set_warm_mlp(w)
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_push("aux_once")
+    p.set_param(Param.BODY_MASS, 1, range(n), masses)
+    p.poses_device(range(n), gd.data_ptr(), 0)
+    p.reset(range(n))
+    p.synchronize()
+    torch.cuda.nvtx.range_pop()
+    p.set(Field.QPOS, range(n), q)  # the Ant lands: the learned substep has contacts
+    p.step(range(n), 100)
+    p.synchronize()
+    torch.cuda.nvtx.range_push("aux_once")
+    warm.forward(w, X[:8192])
+    warm.train(X[:8192], F[:8192], epochs=1, batch=8192, lr=1e-3, seed=2)
+    p.set_solver(warm=int(WarmStart.LEARNED))
+    p.time_phases(range(n), 1)
+    hull_support()
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
+
+    timed("set_param_body_mass_ms", lambda: p.set_param(Param.BODY_MASS, 1, range(n), masses))
+    timed("poses_device_ms", lambda: p.poses_device(range(n), gd.data_ptr(), 0))
+    timed("reset_ms", lambda: p.reset(range(n)))
+    p.set(Field.QPOS, range(n), q)
+    p.step(range(n), 100)
+    ph = {}
+    for _ in range(5):
+        for name, ms in p.time_phases(range(n), 1).items():
+            ph[name] = ph.get(name, 0.0) + ms / 5
+    out["learned_substep_phase_ms"] = ph
+    t0 = time.perf_counter()
+    warm.forward(w, X[:k])
+    out["mlp_forward_host_s"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    warm.train(X[:k], F[:k], epochs=1, batch=8192, lr=1e-3, seed=3)
+    out["train_epoch_host_s"] = time.perf_counter() - t0
+    out["train_samples"] = int(k)
+    t0 = time.perf_counter()
+    hull_support()
+    out["hull_support_host_s"] = time.perf_counter() - t0
+    hv = np.asarray(hm.hull_vert[0])
+    out["hull_support_exact"] = bool(np.abs((hv @ d.T).max(axis=0) - np.einsum("ij,ij->i", hv[v], d)).max() < 1e-12)
+    h.close()
+    p.close()
+    print(json.dumps({"metric": "auxiliary kernels, time per call", "envs": n, "workload": "ant", **out}), flush=True)
+
+
 def hbm_peak() -> float:
     """Measured HBM copy bandwidth (GB/s) from MEASURED_PEAKS.json, else the
     pool's earlier measurement of 6650 GB/s."""
@@ -805,6 +913,8 @@ def main():
         run_scene(args)
     elif args.render:
         run_render(args)
+    elif args.aux:
+        run_aux(args)
     else:
         run_ours(args)
 

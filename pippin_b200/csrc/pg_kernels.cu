@@ -20,7 +20,7 @@
 #include <algorithm>
 
 #include "pg_kernels.h"
-#include "pg_mlp.cuh"
+#include "pg_mlp.h"
 #include "pg_pgs.cuh"
 
 namespace pg {
@@ -333,16 +333,15 @@ __global__ void __launch_bounds__(256, 2) newton_kernel(const __grid_constant__ 
 }
 
 // ---------------------------------------------------------------- learned start
-// Features of the learned warm start's slots and, with INFER, the network's
-// predicted frame forces, between the collision and Newton phases. A block
-// takes 16 slots at a time: 8 threads share a slot's 3 x nv contact-frame
-// Jacobian entries (thread t takes dofs t, t + 8, ...) and reduce J qvel and
-// J a0 by shuffles, then write its 24 features (in the contact frame n, t1,
-// t2: depth, friction, J qvel (3), J a0 (3), the two bodies' translational
-// and rotational invweight sums, the normal (3), the env's touching-contact
-// count, the timestep, the point relative to each geom's centre (3 + 3),
-// both geom types, and 1) to the list and to shared memory, where the
-// tensor-core forward pass (mlp_group) reads them.
+// Features of the learned warm start's slots, between the collision and
+// Newton phases (the network's forward pass over them follows as its own
+// launch, mlp_forward_counted). A block takes 16 slots at a time: 8 threads
+// share a slot's 3 x nv contact-frame Jacobian entries (thread t takes dofs
+// t, t + 8, ...) and reduce J qvel and J a0 by shuffles, then write its 24
+// features (in the contact frame n, t1, t2: depth, friction, J qvel (3),
+// J a0 (3), the two bodies' translational and rotational invweight sums, the
+// normal (3), the env's touching-contact count, the timestep, the point
+// relative to each geom's centre (3 + 3), both geom types, and 1) to the list.
 __device__ inline double learn_feature(int f, const DModel& m, const double* r, const double* prm, const double* geo,
                                        const double (&jv)[3], const double (&ja)[3], double nt) {
   int g1 = (int)r[C_G1], g2 = (int)r[C_G2];
@@ -365,18 +364,11 @@ __device__ inline double learn_feature(int f, const DModel& m, const double* r, 
   }
 }
 
-template <bool INFER>
-__global__ void __launch_bounds__(32 * MLP_WARPS) learn_kernel(const __grid_constant__ StepArgs A) {
+constexpr int LEARN_THREADS = 128;  // 16 slots of 8 threads
+
+__global__ void __launch_bounds__(LEARN_THREADS) learn_kernel(const __grid_constant__ StepArgs A) {
   const LearnArgs& L = A.learn;
   const int64_t n = min(*L.count, L.cap);
-  if ((int64_t)blockIdx.x * 16 >= n) return;
-  extern __shared__ __align__(16) unsigned char smem[];
-  __shared__ float xs[16 * LEARN_NF];
-  MlpSmem S = mlp_smem_layout(smem);
-  S.X = xs;
-  // the weights arrive while the first group's features are formed
-  if (INFER) stage_weights_begin(MlpDevice{L.mlp_w, L.mlp_f}, S.W, S.F);
-  bool staged = !INFER;
   const DModel& m = A.m;
   const int nv = m.nv;
   const int j = threadIdx.x >> 3, t = threadIdx.x & 7;  // slot of the group, thread of the slot
@@ -412,22 +404,14 @@ __global__ void __launch_bounds__(32 * MLP_WARPS) learn_kernel(const __grid_cons
         jv[d] += __shfl_xor_sync(0xffffffffu, jv[d], o);
         ja[d] += __shfl_xor_sync(0xffffffffu, ja[d], o);
       }
-    for (int f = t; f < LEARN_NF; f += 8) {
-      float v = 0.0f;
-      if (live)
-        v = (float)learn_feature(f, m, r, A.st.params + (size_t)env * m.pstride, wk + A.k.geoms, jv, ja,
-                                 wk[A.k.meta + K_META_LNUM]);
-      xs[j * LEARN_NF + f] = v;
-      if (slot < n) L.feat[slot * LEARN_NF + f] = v;
-    }
-    if (!staged) {
-      stage_weights_end();  // (its block barrier also publishes the features)
-      staged = true;
-    } else {
-      __syncthreads();
-    }
-    if (INFER) mlp_group(S, base, n, L.force);
-    else __syncthreads();
+    if (slot < n)
+      for (int f = t; f < LEARN_NF; f += 8) {
+        float v = 0.0f;
+        if (live)
+          v = (float)learn_feature(f, m, r, A.st.params + (size_t)env * m.pstride, wk + A.k.geoms, jv, ja,
+                                   wk[A.k.meta + K_META_LNUM]);
+        L.feat[slot * LEARN_NF + f] = v;
+      }
   }
 }
 
@@ -679,19 +663,18 @@ cudaError_t launch_hull_support(const DModel& m, int mesh, const double* dirs, i
 
 cudaError_t reset_queue(const StepArgs& a, cudaStream_t s) { return cudaMemsetAsync(a.queue, 0, QUEUE_INTS * sizeof(int), s); }
 
-cudaError_t learn_prepare() {
-  return cudaFuncSetAttribute(learn_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MLP_SMEM);
-}
+cudaError_t learn_prepare() { return mlp_prepare(); }
 
 cudaError_t launch_learn(const StepArgs& a, bool infer, cudaStream_t s) {
-  // the list's slots are counted on the device: the grid covers the
-  // capacity, and blocks past this substep's slots return at once; two
-  // blocks an SM stay resident with the network staged
-  int64_t blocks = std::min<int64_t>((a.learn.cap + 15) / 16, 296);
+  // the list's slots are counted on the device: the grids cover the
+  // capacity, and blocks past this substep's slots return at once
+  int64_t blocks = std::min<int64_t>((a.learn.cap + 15) / 16, 16 * 148);
   if (blocks < 1) return cudaSuccess;
-  if (infer) learn_kernel<true><<<(unsigned)blocks, 32 * MLP_WARPS, MLP_SMEM, s>>>(a);
-  else learn_kernel<false><<<(unsigned)blocks, 32 * MLP_WARPS, 0, s>>>(a);
-  return cudaGetLastError();
+  learn_kernel<<<(unsigned)blocks, LEARN_THREADS, 0, s>>>(a);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || !infer) return e;
+  return mlp_forward_counted(MlpDevice{a.learn.mlp_w, a.learn.mlp_f}, a.learn.feat, a.learn.count, a.learn.cap,
+                             a.learn.force, s);
 }
 
 cudaError_t launch_phase(int which, const StepArgs& a0, const LaunchCfg& c, cudaStream_t s) {

@@ -56,11 +56,10 @@ void mlp_pack(const float* wt, uint16_t* w, float* f) {
 }
 
 // ---------------------------------------------------------------- inference
-// the standalone forward pass (pg_mlp_forward): features from global memory
-__global__ void __launch_bounds__(32 * MLP_WARPS) mlp_forward_kernel(MlpDevice d, const float* X, int64_t n,
-                                                                     float* Y) {
+// Y = net(X) over rows [0, n), 16 rows at a time per block, the weights
+// staged once per block
+__device__ inline void mlp_rows(const MlpDevice& d, const float* X, int64_t n, float* Y, unsigned char* smem) {
   if ((int64_t)blockIdx.x * 16 >= n) return;
-  extern __shared__ __align__(16) unsigned char smem[];
   MlpSmem S = mlp_smem_layout(smem);
   stage_weights(d, S.W, S.F);
   for (int64_t base = (int64_t)blockIdx.x * 16; base < n; base += (int64_t)gridDim.x * 16) {
@@ -73,8 +72,38 @@ __global__ void __launch_bounds__(32 * MLP_WARPS) mlp_forward_kernel(MlpDevice d
   }
 }
 
+// the standalone forward pass (pg_mlp_forward): features from global memory
+__global__ void __launch_bounds__(32 * MLP_WARPS) mlp_forward_kernel(MlpDevice d, const float* X, int64_t n,
+                                                                     float* Y) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  mlp_rows(d, X, n, Y, smem);
+}
+
+// the learned start's forward pass: min(*count, cap) rows, counted on the
+// device by the collision phase
+__global__ void __launch_bounds__(32 * MLP_WARPS) mlp_count_kernel(MlpDevice d, const float* X, const int* count,
+                                                                   int64_t cap, float* Y) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  int64_t n = *count;
+  mlp_rows(d, X, n < cap ? n : cap, Y, smem);
+}
+
 cudaError_t mlp_prepare() {
-  return cudaFuncSetAttribute(mlp_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MLP_SMEM);
+  cudaError_t e = cudaFuncSetAttribute(mlp_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MLP_SMEM);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(mlp_count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MLP_SMEM);
+  return e;
+}
+
+cudaError_t mlp_forward_counted(const MlpDevice& d, const float* X, const int* count, int64_t cap, float* Y,
+                                cudaStream_t s) {
+  // the grid covers the capacity; blocks past the device-side count return
+  // at once
+  int64_t blocks = (cap + 15) / 16;
+  if (blocks > 1184) blocks = 1184;
+  if (blocks < 1) return cudaSuccess;
+  mlp_count_kernel<<<(unsigned)blocks, 32 * MLP_WARPS, MLP_SMEM, s>>>(d, X, count, cap, Y);
+  return cudaGetLastError();
 }
 
 cudaError_t mlp_forward(const MlpDevice& d, const float* X, int64_t n, float* Y, cudaStream_t s) {

@@ -45,5 +45,9 @@ void mlp_pack(const float* weights, uint16_t* w_bf16, float* f32);
 cudaError_t mlp_prepare();
 // Y[n][3] = net(X[n][24]) on the tensor cores, on stream s
 cudaError_t mlp_forward(const MlpDevice& d, const float* X, int64_t n, float* Y, cudaStream_t s);
+// the same over min(*count, cap) rows, count read on the device (for launches
+// whose row count the host does not know)
+cudaError_t mlp_forward_counted(const MlpDevice& d, const float* X, const int* count, int64_t cap, float* Y,
+                                cudaStream_t s);
 
 }  // namespace pg

@@ -301,3 +301,36 @@ def tabletop(num_envs: int, seed: int = 0, slots: int = 6, count=(2, 6), timeste
         b = 2 + s
         params += [(5, b, mass[s]), (9, b, inertia[s])]  # mass first: it rescales inertia (params.rs:145-156)
     return TabletopPlan(xml, nq, params, qpos0)
+
+
+def lumpy_sphere_points(n: int = 600, scale: float = 1.0):
+    """The point set of the reference's support-walk test
+    (crates/pippin/src/fasthull.rs:221-229): n points on a golden-angle
+    spiral over a sphere whose radius has a lump pattern, squashed to 0.7 in
+    z. Its hull keeps the points outside the dips: 276 of the 600."""
+    import numpy as np
+
+    i = np.arange(n, dtype=np.float64)
+    t = i * 2.399963
+    p = np.arccos(1.0 - 2.0 * (i + 0.5) / n)
+    r = 1.0 + 0.2 * np.sin(3.0 * t) * np.cos(2.0 * p)
+    pts = np.stack([r * np.sin(p) * np.cos(t), r * np.sin(p) * np.sin(t), 0.7 * r * np.cos(p)], axis=1)
+    return pts * scale
+
+
+def support_directions(n: int = 2000):
+    """The query directions of fasthull.rs:231-233 (unit vectors)."""
+    import numpy as np
+
+    a = np.arange(n, dtype=np.float64) * 0.731
+    d = np.stack([np.sin(a) * np.cos(1.3 * a), np.cos(0.7 * a), np.sin(2.1 * a)], axis=1)
+    return d / np.linalg.norm(d, axis=1, keepdims=True)
+
+
+def lumpy_hull_xml(scale: float = 0.05) -> str:
+    """One free body whose geom is the hull of the 600-point lumpy sphere
+    (276 vertices: its support points come from the walk)."""
+    pts = " ".join(repr(float(x)) for x in lumpy_sphere_points(600, scale).ravel())
+    return ('<mujoco><asset><mesh name="lumpy" vertex="' + pts + '"/></asset><worldbody>'
+            '<geom type="plane" size="5 5 .1"/><body name="l" pos="0 0 0.1"><freejoint/>'
+            '<geom type="mesh" mesh="lumpy"/></body></worldbody></mujoco>')

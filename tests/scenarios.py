@@ -9,7 +9,7 @@ import math
 
 import numpy as np
 
-from pippin_b200 import mjcf
+from pippin_b200 import mjcf, scenes
 
 NEWTON, PGS = 0, 1
 
@@ -404,26 +404,6 @@ IMPLICITFAST_ARM = (
 
 
 # ----------------------------------------------------------------- large hulls
-def lumpy_sphere_points(n=600, scale=1.0):
-    """The point set of the reference's support-walk test
-    (crates/pippin/src/fasthull.rs:221-229): n points on a golden-angle
-    spiral over a sphere whose radius has a lump pattern, squashed to 0.7 in
-    z. Its hull keeps the points outside the dips: 276 of the 600."""
-    i = np.arange(n, dtype=np.float64)
-    t = i * 2.399963
-    p = np.arccos(1.0 - 2.0 * (i + 0.5) / n)
-    r = 1.0 + 0.2 * np.sin(3.0 * t) * np.cos(2.0 * p)
-    pts = np.stack([r * np.sin(p) * np.cos(t), r * np.sin(p) * np.sin(t), 0.7 * r * np.cos(p)], axis=1)
-    return pts * scale
-
-
-def support_directions(n=2000):
-    """The query directions of fasthull.rs:231-233."""
-    a = np.arange(n, dtype=np.float64) * 0.731
-    d = np.stack([np.sin(a) * np.cos(1.3 * a), np.cos(0.7 * a), np.sin(2.1 * a)], axis=1)
-    return d / np.linalg.norm(d, axis=1, keepdims=True)
-
-
 def _verts(pts):
     return " ".join(repr(float(x)) for x in np.asarray(pts).ravel())
 
@@ -440,7 +420,7 @@ def big_hulls_xml():
     pair), a 48-sided prism (96 vertices, 48-gon caps: clipped in shared
     memory), a box, a sphere and a capsule, dropped onto a plane and onto
     each other."""
-    lumpy = _verts(lumpy_sphere_points(600, 0.05))
+    lumpy = _verts(scenes.lumpy_sphere_points(600, 0.05))
     prism = _verts(prism_points())
     return ('<mujoco><option timestep="0.002"/><asset>'
             f'<mesh name="lumpy" vertex="{lumpy}"/><mesh name="prism" vertex="{prism}"/></asset><worldbody>'
@@ -453,3 +433,8 @@ def big_hulls_xml():
             '<body name="s" pos="0.03 0.01 0.25"><freejoint/><geom type="sphere" size=".02"/></body>'
             '<body name="c" pos="0.6 0.01 0.22" euler="0 80 10"><freejoint/><geom type="capsule" size=".015 .04"/></body>'
             '</worldbody></mujoco>')
+
+
+# the reference's support-walk test inputs, kept in the package for the bench
+lumpy_sphere_points = scenes.lumpy_sphere_points
+support_directions = scenes.support_directions
