@@ -38,11 +38,13 @@ ITERS = 30
 PHASE_STAGES = {"smooth": ("kinematics", "crba", "vel_rne", "passive_act", "factor_solve"),
                 "collide": ("collide",),
                 "newton": ("rows", "newton", "pgs", "integrate")}
-# DRAM bytes (read + write) per env of each phase kernel, from one ncu capture
-# of the phase kernels on the Ant workload at 4096 envs after 100 steps (ncu
-# flushes L2 before the captured launch, so the work record the phases hand
-# each other counts here although it stays in L2 between the phases)
-NCU_TRAFFIC_PER_ENV = {"smooth": 4047.0, "collide": 6373.0, "newton": 8510.0}
+# DRAM bytes (read + write) per env of each phase kernel, from one in-situ ncu
+# capture (--cache-control none: the caches hold what the previous launches
+# left) of the headline's phase kernels at 16384 Ant envs after 100 substeps:
+# smooth 65.3 + 93.8 MB, collide 98.0 + 53.2 MB, Newton 132.5 + 49.9 MB per
+# launch. The work record the phases hand each other (12 KB per env, 200 MB
+# at 16384 envs) is larger than the 126 MB L2, so most of it reaches HBM.
+NCU_TRAFFIC_PER_ENV = {"smooth": 9711.0, "collide": 9227.0, "newton": 11132.0}
 
 
 def parse():
@@ -424,7 +426,7 @@ def run_ours(args):
                          "note": f"{phase_flops[top]:.0f} algorithmic FP64 ops per env in the {top} phase (oracle "
                                  f"counters, {flops_step:.0f} per whole env-step) x {n} envs per launch / that "
                                  "kernel's mean event-timed duration; peak = live DFMA microbenchmark (pg_fp64_peak); "
-                                 "traffic = ncu DRAM bytes per env of that kernel x envs",
+                                 "traffic = in-situ ncu DRAM bytes per env of that kernel x envs",
                          "hbm_achieved_gbs": bytes_step * n / (ms_ref / K * 1e-3) / 1e9},
             "phases": {ph: {"ms_per_launch": phase_ms[ph] / K, "share": phase_ms[ph] / phase_total,
                             "fp64_ops_per_env": phase_flops.get(ph),

@@ -828,36 +828,6 @@ bool validate_param(const HostModel& m, int p, int64_t id, const double* v, std:
   return true;
 }
 
-// apply one env's new values to its parameter block (params.rs:121-176)
-void apply_param(const DModel& d, double* prm, int p, int64_t id, const double* v, int nq) {
-  switch (p) {
-    case PG_PARAM_GEOM_FRICTION: prm[d.p_friction + id] = std::fmax(v[0], 0.0); break;
-    case PG_PARAM_GEOM_SIZE: for (int k = 0; k < 3; k++) prm[d.p_size + 3 * id + k] = v[k]; break;
-    case PG_PARAM_GEOM_RGBA: for (int k = 0; k < 4; k++) prm[d.p_rgba + 4 * id + k] = (double)(float)v[k]; break;
-    case PG_PARAM_GEOM_CONTYPE:
-    case PG_PARAM_GEOM_CONAFFINITY: {
-      double bits = std::floor(std::fmin(std::fmax(v[0], 0.0), 4294967295.0));
-      prm[(p == PG_PARAM_GEOM_CONTYPE ? d.p_contype : d.p_conaff) + id] = bits;
-      break;
-    }
-    case PG_PARAM_BODY_MASS: {
-      double old = prm[d.p_mass + id];
-      double scale = old > 0.0 ? v[0] / old : 1.0;
-      prm[d.p_mass + id] = v[0];
-      for (int k = 0; k < 9; k++) prm[d.p_inertia + 9 * id + k] *= scale;
-      break;
-    }
-    case PG_PARAM_DOF_DAMPING: prm[d.p_damping + id] = std::fmax(v[0], 0.0); break;
-    case PG_PARAM_ACTUATOR_GAIN: prm[d.p_gain + id] = v[0]; break;
-    case PG_PARAM_ACTUATOR_BIAS: for (int k = 0; k < 3; k++) prm[d.p_bias + 3 * id + k] = v[k]; break;
-    case PG_PARAM_BODY_INERTIA:
-      for (int k = 0; k < 9; k++) prm[d.p_inertia + 9 * id + k] = 0.0;
-      for (int k = 0; k < 3; k++) prm[d.p_inertia + 9 * id + 4 * k] = v[k];
-      break;
-    case PG_PARAM_BODY_IPOS: for (int k = 0; k < 3; k++) prm[d.p_ipos + 3 * id + k] = v[k]; break;
-    case PG_PARAM_QPOS0: for (int k = 0; k < nq; k++) prm[d.p_qpos_reset + k] = v[k]; break;
-  }
-}
 
 void read_param(const DModel& d, const double* prm, int p, int64_t id, double* o, int nq) {
   switch (p) {
@@ -1565,11 +1535,11 @@ int pg_set_param(pg_handle* h, int param, int64_t id, int64_t start, int64_t end
     if (!validate_param(m, param, id, values + k * w, &err)) return fail(PG_ERR_INVALID, err);
   if (end == start) return PG_OK;
   CK(cudaSetDevice(h->device));
-  std::vector<double> blk;
-  if ((rc = read_params(h, start, end, blk))) return rc;
-  for (int64_t k = 0; k < end - start; k++) apply_param(h->dm, blk.data() + k * h->dm.pstride, param, id, values + k * w, m.nq);
-  CK(cudaMemcpyAsync(h->params + start * h->dm.pstride, blk.data(), sizeof(double) * blk.size(), cudaMemcpyHostToDevice,
-                     h->stream));
+  // the values go to the device, where each env's parameter block takes them
+  if ((rc = grow(h, h->b_vals, sizeof(double) * len))) return rc;
+  CK(cudaMemcpyAsync(h->b_vals.p, values, sizeof(double) * len, cudaMemcpyHostToDevice, h->stream));
+  CK(launch_apply_param(h->dm, h->params + start * h->dm.pstride, end - start, param, id, (const double*)h->b_vals.p, w,
+                        m.nq, h->stream));
   if (param == PG_PARAM_BODY_MASS || param == PG_PARAM_BODY_INERTIA || param == PG_PARAM_BODY_IPOS) {
     if ((rc = set_const_range(h, start, end))) return rc;
   }

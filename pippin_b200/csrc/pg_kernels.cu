@@ -415,6 +415,53 @@ __global__ void __launch_bounds__(LEARN_THREADS) learn_kernel(const __grid_const
   }
 }
 
+// row' M^-1 row for set_const's right-hand sides (one per lane, r < nrhs):
+// the unit vectors, then per body 3 axes x (translation, rotation) rows of
+// its Jacobian at the inertial frame. With M = L L', row' M^-1 row is
+// |L^-1 row|^2: one forward substitution, the vector in registers (NB >= nv;
+// larger models solve in scratch below).
+template <int NB, int G>
+__device__ void invweight_quads(const Tile<G>& T, const DModel& m, const WsLayout& w, const EnvCtx& e,
+                                const double* prm, const double* L, int nv, int nrhs, double* quad) {
+  for (int r = T.lane(); r < nrhs; r += G) {
+    double y[NB];
+    if (r < nv) {
+#pragma unroll
+      for (int k = 0; k < NB; k++) y[k] = k == r ? 1.0 : 0.0;
+    } else {
+      int q = r - nv;
+      int b = q / 6, axis = (q % 6) / 2, kind = q % 2;
+      if (b == 0) {
+        quad[r] = 0.0;
+        continue;
+      }
+      V3 dir{axis == 0 ? 1.0 : 0.0, axis == 1 ? 1.0 : 0.0, axis == 2 ? 1.0 : 0.0};
+      V3 xip = ld3(e.ws + w.xpos + 3 * b) + mv(q_mat(ld4(e.ws + w.xquat + 4 * b)), ld3(prm + m.p_ipos + 3 * b));
+      unsigned long long chain = m.body_dofmask[b];
+#pragma unroll
+      for (int k = 0; k < NB; k++) {
+        y[k] = 0.0;
+        if (k < nv && ((chain >> k) & 1ull)) {
+          Sp c = ld6(e.ws + w.cdof + 6 * k);
+          y[k] = kind == 0 ? dot(dir, point_vel(c, xip)) : dot(dir, c.ang);
+        }
+      }
+    }
+    double sq = 0.0;
+#pragma unroll
+    for (int i = 0; i < NB; i++) {
+      if (i < nv) {
+        double v = y[i];
+#pragma unroll
+        for (int k = 0; k < i; k++) v -= L[i * nv + k] * y[k];
+        y[i] = v / L[i * nv + i];
+        sq += y[i] * y[i];
+      }
+    }
+    quad[r] = sq;
+  }
+}
+
 // forward.rs:275-333: invweight0 of each env's model at its reset state
 template <int G>
 __global__ void __launch_bounds__(256) set_const_kernel(const __grid_constant__ StepArgs A, const int* envs, int n) {
@@ -449,7 +496,9 @@ __global__ void __launch_bounds__(256) set_const_kernel(const __grid_constant__ 
     double* xs = e.scr + A.s.jac;  // [rhs][nv]
     int nrhs = nv + 6 * m.nbody;
     double* quad = e.scr + A.s.rows;  // [nrhs]
-    if (ok) {
+    if (ok && nv <= 16) {
+      invweight_quads<16>(T, m, w, e, prm, L, nv, nrhs, quad);
+    } else if (ok) {
       for (int r = T.lane(); r < nrhs; r += G) {
         double* x = xs + (size_t)r * nv;
         double* row = xs + (size_t)(nrhs + (r % G)) * nv;  // per-lane copy of the row
@@ -647,6 +696,19 @@ cudaError_t launch_substep(const StepArgs& a0, const SubstepCfg& c, cudaStream_t
   }
   PG_LAUNCH(K_NEWTON, newton_kernel, c.newton, a);
   return cudaSuccess;
+}
+
+__global__ void apply_param_kernel(const __grid_constant__ DModel d, double* params, int64_t count, int p, int64_t id,
+                                   const double* v, int w, int nq) {
+  int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < count) apply_param(d, params + e * d.pstride, p, id, v + e * w, nq);
+}
+
+cudaError_t launch_apply_param(const DModel& d, double* params, int64_t count, int p, int64_t id, const double* v, int w,
+                               int nq, cudaStream_t s) {
+  if (count <= 0) return cudaSuccess;
+  apply_param_kernel<<<(unsigned)((count + 127) / 128), 128, 0, s>>>(d, params, count, p, id, v, w, nq);
+  return cudaGetLastError();
 }
 
 __global__ void hull_support_kernel(const __grid_constant__ DModel m, int mesh, const double* dirs, int n,

@@ -39,6 +39,9 @@ cudaError_t launch_phase(int which, const StepArgs& a, const LaunchCfg& c, cudaS
 cudaError_t launch_set_const(const StepArgs& a, const LaunchCfg& c, const int* envs, int n, cudaStream_t s);
 cudaError_t launch_poses(const StepArgs& a, const LaunchCfg& c, float* geoms, float* cams, cudaStream_t s);
 cudaError_t launch_reset(const StepArgs& a, const int64_t* ids, int n, cudaStream_t s);
+// params[e * pstride ..] takes values v[e][w] of parameter p, element id, for e < count
+cudaError_t launch_apply_param(const DModel& d, double* params, int64_t count, int p, int64_t id, const double* v, int w,
+                               int nq, cudaStream_t s);
 // vertex[i] = the hull support walk of mesh `mesh` along dirs[i] (mesh frame; device memory)
 cudaError_t launch_hull_support(const DModel& m, int mesh, const double* dirs, int n, int* vertex, cudaStream_t s);
 

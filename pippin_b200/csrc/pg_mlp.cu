@@ -232,10 +232,15 @@ static cudaError_t gemm_atb(int M, int N, int K, const float* A, int lda, const 
   return cudaGetLastError();
 }
 
+// the bias gradients' row splits: short column runs per thread (32 rows of a
+// batch of 8192), so that the first pass has a block per split
+constexpr int COLSUM_SPLITS = 256;
+static_assert(COLSUM_SPLITS * MLP_H <= SPLITS * MLP_H * MLP_H, "colsum partial sums fit the split-K buffer");
+
 static cudaError_t colsum(const float* dY, int M, int N, float* db, float* part, cudaStream_t s) {
-  int rc = (M + SPLITS - 1) / SPLITS;
-  colsum_split_kernel<<<dim3((N + 127) / 128, SPLITS), 128, 0, s>>>(dY, M, N, rc, part);
-  sum_splits_kernel<<<(N + 255) / 256, 256, 0, s>>>(part, SPLITS, N, db);
+  int rc = (M + COLSUM_SPLITS - 1) / COLSUM_SPLITS;
+  colsum_split_kernel<<<dim3((N + 127) / 128, COLSUM_SPLITS), 128, 0, s>>>(dY, M, N, rc, part);
+  sum_splits_kernel<<<(N + 255) / 256, 256, 0, s>>>(part, COLSUM_SPLITS, N, db);
   return cudaGetLastError();
 }
 

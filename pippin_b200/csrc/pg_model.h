@@ -16,7 +16,12 @@
 //                     workspaces (state, M, cdof, and one region used first
 //                     by the tree walks, then by the factorisations/Newton)
 #pragma once
+#include <cuda_runtime.h>
+
+#include <cmath>
 #include <cstdint>
+
+#include "../../include/pippin_b200.h"
 
 namespace pg {
 
@@ -149,6 +154,38 @@ struct DModel {
   const unsigned char* arena;
   int arena_bytes;
 };
+
+// One env's new values of one parameter into its parameter block
+// (params.rs:121-176); pg_set_param runs it on the device, one env a thread.
+__host__ __device__ inline void apply_param(const DModel& d, double* prm, int p, int64_t id, const double* v, int nq) {
+  switch (p) {
+    case PG_PARAM_GEOM_FRICTION: prm[d.p_friction + id] = ::fmax(v[0], 0.0); break;
+    case PG_PARAM_GEOM_SIZE: for (int k = 0; k < 3; k++) prm[d.p_size + 3 * id + k] = v[k]; break;
+    case PG_PARAM_GEOM_RGBA: for (int k = 0; k < 4; k++) prm[d.p_rgba + 4 * id + k] = (double)(float)v[k]; break;
+    case PG_PARAM_GEOM_CONTYPE:
+    case PG_PARAM_GEOM_CONAFFINITY: {
+      double bits = ::floor(::fmin(::fmax(v[0], 0.0), 4294967295.0));
+      prm[(p == PG_PARAM_GEOM_CONTYPE ? d.p_contype : d.p_conaff) + id] = bits;
+      break;
+    }
+    case PG_PARAM_BODY_MASS: {
+      double old = prm[d.p_mass + id];
+      double scale = old > 0.0 ? v[0] / old : 1.0;
+      prm[d.p_mass + id] = v[0];
+      for (int k = 0; k < 9; k++) prm[d.p_inertia + 9 * id + k] *= scale;
+      break;
+    }
+    case PG_PARAM_DOF_DAMPING: prm[d.p_damping + id] = ::fmax(v[0], 0.0); break;
+    case PG_PARAM_ACTUATOR_GAIN: prm[d.p_gain + id] = v[0]; break;
+    case PG_PARAM_ACTUATOR_BIAS: for (int k = 0; k < 3; k++) prm[d.p_bias + 3 * id + k] = v[k]; break;
+    case PG_PARAM_BODY_INERTIA:
+      for (int k = 0; k < 9; k++) prm[d.p_inertia + 9 * id + k] = 0.0;
+      for (int k = 0; k < 3; k++) prm[d.p_inertia + 9 * id + 4 * k] = v[k];
+      break;
+    case PG_PARAM_BODY_IPOS: for (int k = 0; k < 3; k++) prm[d.p_ipos + 3 * id + k] = v[k]; break;
+    case PG_PARAM_QPOS0: for (int k = 0; k < nq; k++) prm[d.p_qpos_reset + k] = v[k]; break;
+  }
+}
 
 // Per-tile shared-memory workspace (offsets in doubles). The `tree` region
 // (poses, inertias, velocities, forces) is dead once the contacts are built
