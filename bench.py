@@ -69,8 +69,9 @@ def parse():
                     help="skip configs 2-5 (tabletop, hull tumble, contact-free, learned evaluation) in the line")
     ap.add_argument("--extras-steps", type=int, default=50, help="timed substeps of each extra config")
     ap.add_argument("--learned-envs", type=int, default=16384)
-    ap.add_argument("--scene", default="", choices=["", "tabletop", "hull_tumble", "cartpole", "arm3hinge"],
-                    help="phase timing of another workload (configs 2-4) beside the oracle, instead of the headline")
+    ap.add_argument("--scene", default="", choices=["", "tabletop", "hull_tumble", "cartpole", "arm3hinge", "big_hulls"],
+                    help="phase timing of another workload (configs 2-4; big_hulls: hulls of 96 and 276 vertices) "
+                    "beside the oracle, instead of the headline")
     ap.add_argument("--render", default="", help="batched rendering of Ant poses at these square resolutions "
                     "(comma-separated, e.g. 64,128) instead of the headline")
     ap.add_argument("--render-envs", type=int, default=4096, help="envs rendered per frame (the reference's "
@@ -560,7 +561,8 @@ def run_learned_eval(args):
 
 def scene_measure(scene, n, K, W, cpu=True):
     """Device env-steps/s and per-phase time of the tabletop (config 3), the
-    hull tumble (config 4) or a contact-free model (config 2: random states
+    hull tumble (config 4), the large-hull scene (scenes.big_hulls_xml, with
+    the hull tumble's initial velocities) or a contact-free model (config 2: random states
     over the joint ranges, qvel N(0, 1), per-env masses x U[0.5, 2], random
     controls held) after W settling substeps, with the oracle's rate on a
     bounded sample of the same workload on the host cores beside it. Returns
@@ -578,6 +580,11 @@ def scene_measure(scene, n, K, W, cpu=True):
         m = mjcf.load_string(scenes.cartpole_xml() if scene == "cartpole" else scenes.arm3hinge_xml())
         desc = (f"{scene}: {n} envs, qpos uniform over the joint ranges (hinges [-pi, pi], slides +-0.5), "
                 f"qvel N(0,1), per-env masses x U[0.5,2], controls U[-1,1] held; timed after {W} substeps")
+    elif scene == "big_hulls":
+        m = mjcf.load_string(scenes.big_hulls_xml())
+        desc = (f"big hulls: {n} envs of two 276-vertex hulls, two 96-vertex prisms (48-gon faces), a box, a sphere "
+                f"and a capsule, v N(0,0.5^2), w N(0,3^2), dt 0.002, Newton tol 1e-10 cap {ITERS}; timed after {W} "
+                "substeps")
     else:
         m = mjcf.load_string(scenes.hull_tumble_xml())
         desc = (f"hull tumble: {n} envs of 8 hulls (8-32 vertices), v N(0,0.5^2), w N(0,3^2), dt 0.002, "
@@ -639,7 +646,8 @@ def scene_measure(scene, n, K, W, cpu=True):
     launch = p.phase_launch()
     p.close()
     # the oracle on a sample of the same workload (same settling, then timed)
-    cn = 4096 if scene in ("cartpole", "arm3hinge") else 256
+    # (the oracle tests every edge pair of the 276-vertex hulls: a small sample)
+    cn = 4096 if scene in ("cartpole", "arm3hinge") else (16 if scene == "big_hulls" else 256)
     line = {"metric": f"{scene} env-steps/s", "value": n * K / (ms * 1e-3), "unit": "env-steps/s",
             "n_gpus": 1, "steps": K, "warmup": W, "ms_per_step": ms / K, "higher_is_better": True, "dtype": "f64",
             "data": "synthetic", "config": {"workload": desc, "envs": n},

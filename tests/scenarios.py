@@ -404,37 +404,8 @@ IMPLICITFAST_ARM = (
 
 
 # ----------------------------------------------------------------- large hulls
-def _verts(pts):
-    return " ".join(repr(float(x)) for x in np.asarray(pts).ravel())
-
-
-def prism_points(sides=48, r=0.05, h=0.03):
-    th = 2.0 * np.pi * np.arange(sides) / sides
-    ring = np.stack([r * np.cos(th), r * np.sin(th)], axis=1)
-    return np.concatenate([np.column_stack([ring, np.full(sides, -h)]), np.column_stack([ring, np.full(sides, h)])])
-
-
-def big_hulls_xml():
-    """Hulls past the scan limit and faces past a lane's clip buffers: two
-    lumpy spheres of 276 hull vertices (the support walk on both sides of a
-    pair), a 48-sided prism (96 vertices, 48-gon caps: clipped in shared
-    memory), a box, a sphere and a capsule, dropped onto a plane and onto
-    each other."""
-    lumpy = _verts(scenes.lumpy_sphere_points(600, 0.05))
-    prism = _verts(prism_points())
-    return ('<mujoco><option timestep="0.002"/><asset>'
-            f'<mesh name="lumpy" vertex="{lumpy}"/><mesh name="prism" vertex="{prism}"/></asset><worldbody>'
-            '<geom type="plane" size="5 5 .1"/>'
-            '<body name="l1" pos="0 0 0.06" euler="10 20 30"><freejoint/><geom type="mesh" mesh="lumpy"/></body>'
-            '<body name="l2" pos="0.02 0.01 0.16" euler="40 5 70"><freejoint/><geom type="mesh" mesh="lumpy"/></body>'
-            '<body name="p" pos="0.3 0 0.04"><freejoint/><geom type="mesh" mesh="prism"/></body>'
-            '<body name="b" pos="0.31 0.01 0.1" euler="0 0 20"><freejoint/><geom type="box" size=".03 .03 .02"/></body>'
-            '<body name="p2" pos="0.6 0 0.1" euler="90 0 0"><freejoint/><geom type="mesh" mesh="prism"/></body>'
-            '<body name="s" pos="0.03 0.01 0.25"><freejoint/><geom type="sphere" size=".02"/></body>'
-            '<body name="c" pos="0.6 0.01 0.22" euler="0 80 10"><freejoint/><geom type="capsule" size=".015 .04"/></body>'
-            '</worldbody></mujoco>')
-
-
-# the reference's support-walk test inputs, kept in the package for the bench
+# the reference's support-walk test inputs and the large-hull scene, kept in
+# the package for the bench
 lumpy_sphere_points = scenes.lumpy_sphere_points
 support_directions = scenes.support_directions
+big_hulls_xml = scenes.big_hulls_xml
