@@ -476,6 +476,39 @@ def test_subranges_step_like_the_whole():
     np.testing.assert_array_equal(a.get(Field.QPOS, range(n)), b.get(Field.QPOS, range(n)))
 
 
+def test_queued_newton_order_steps_like_one_wave():
+    """With more envs than the Newton grid has tiles, the Newton phase takes
+    envs in the order the collision phase wrote (envs with contacts first);
+    with a tile per env it takes them in index order. Both must give every
+    env the same bits: all 12000 envs at once against ranges of 2000 (one
+    wave each), for pg_step and for pg_rollout (whose per-substep qpos goes
+    to the env's own row of the output)."""
+    n, t = 12000, 6
+    m = mjcf.load_string(scenes.ant_xml(tolerance=1e-10))
+    blob = mjcf.to_blob(m)
+    a, b = CudaPhysics(blob, n), CudaPhysics(blob, n)
+    lanes, per_block, blocks = a.phase_launch()["newton"]
+    assert per_block * blocks < n  # the queued, ordered path
+    rng = np.random.default_rng(12)
+    q, v = random_state(m, n, rng, qnoise=0.3, vscale=0.5)
+    q[:, 2] = rng.uniform(0.2, 0.9, n)  # torso heights: some envs touch the floor, others fly
+    for p in (a, b):
+        p.set(Field.QPOS, range(n), q)
+        p.set(Field.QVEL, range(n), v)
+    a.step(range(n), 30)
+    for s0 in range(0, n, 2000):
+        b.step(range(s0, min(n, s0 + 2000)), 30)
+    assert a.stats()["ncon"].any() and not a.stats()["ncon"].all()
+    for f in (Field.QPOS, Field.QVEL, Field.QACC):
+        np.testing.assert_array_equal(a.get(f, range(n)), b.get(f, range(n)))
+    np.testing.assert_array_equal(a.stats()["iters"], b.stats()["iters"])
+    ctrl = rng.uniform(-1, 1, (n, t, m.nu))
+    out_a = a.rollout(ctrl)
+    out_b = np.concatenate([b.rollout(ctrl[s0:s0 + 2000], range(s0, min(n, s0 + 2000)))
+                            for s0 in range(0, n, 2000)])
+    np.testing.assert_array_equal(out_a, out_b)
+
+
 def test_rollout_matches_step_loop():
     n, t = 8, 30
     m = mjcf.load_string(scenes.ant_xml())
