@@ -1167,7 +1167,7 @@ void destroy(pg_handle* h) {
   void* ptrs[] = {h->d_model, h->qpos, h->qvel, h->ctrl, h->qacc, h->applied, h->params, h->iters, h->ncon,
                   h->nrows, h->status, h->scratch, h->work, h->prev_con, h->prev_ncon, h->queue, h->order, h->b_ctrl.p, h->b_qout.p, h->b_poses_g.p,
                   h->b_poses_c.p, h->b_dbg.p, h->b_vals.p, h->b_ids.p, h->learn.items, h->learn.feat, h->learn.force,
-                  h->learn.rows, (void*)h->learn.mlp_w, (void*)h->learn.mlp_f};
+                  h->learn.rows, (void*)h->learn.mlp_w, (void*)h->learn.mlp_f, (void*)h->learn.mlp_err};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -1950,10 +1950,14 @@ int pg_set_warm_mlp(pg_handle* h, const float* weights, size_t len) {
   if (!h->learn.mlp_w) {
     uint16_t* w = nullptr;
     float* f = nullptr;
+    int* err = nullptr;
     CK(cudaMalloc(&w, sizeof(uint16_t) * MLP_BF16_ELEMS));
     CK(cudaMalloc(&f, sizeof(float) * MLP_F32_ELEMS));
+    CK(cudaMalloc(&err, sizeof(int)));
+    CK(cudaMemset(err, 0, sizeof(int)));
     h->learn.mlp_w = w;
     h->learn.mlp_f = f;
+    h->learn.mlp_err = err;
   }
   std::vector<uint16_t> wb(MLP_BF16_ELEMS);
   std::vector<float> fb(MLP_F32_ELEMS);

@@ -735,7 +735,7 @@ cudaError_t launch_learn(const StepArgs& a, bool infer, cudaStream_t s) {
   learn_kernel<<<(unsigned)blocks, LEARN_THREADS, 0, s>>>(a);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess || !infer) return e;
-  return mlp_forward_counted(MlpDevice{a.learn.mlp_w, a.learn.mlp_f}, a.learn.feat, a.learn.count, a.learn.cap,
+  return mlp_forward_counted(MlpDevice{a.learn.mlp_w, a.learn.mlp_f, a.learn.mlp_err}, a.learn.feat, a.learn.count, a.learn.cap,
                              a.learn.force, s);
 }
 

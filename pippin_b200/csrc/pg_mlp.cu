@@ -1,12 +1,10 @@
 // The learned warm start's network: inference on the tensor cores and
 // training kernels.
 //
-// Inference (mlp_forward_kernel): one warp per 16 samples, mma.sync
-// m16n8k16 with BF16 operands and FP32 accumulation. The BF16 weights (84 KB
-// with row padding) are staged in shared memory once per block; a layer's
-// FP32 accumulator fragments become the next layer's BF16 A fragments in
-// registers (the C layout of one n8 tile pair is the A layout of one k16
-// tile), so activations never leave the warp.
+// Inference (mlp_forward_kernel, mlp_count_kernel; device side in
+// pg_mlp.cuh): tcgen05.mma with BF16 operands in shared memory and FP32
+// accumulators in tensor memory, 128 samples a block, the 76 KB of BF16
+// weights staged once per block in the operands' canonical layout.
 //
 // Training (mlp_train_*): FP32 throughout (master weights, activations,
 // gradients, Adam moments), simple tiled kernels: the network is small
@@ -34,19 +32,15 @@ static uint16_t to_bf16(float x) {
 void mlp_pack(const float* wt, uint16_t* w, float* f) {
   std::fill(w, w + MLP_BF16_ELEMS, to_bf16(0.0f));
   std::fill(f, f + MLP_F32_ELEMS, 0.0f);
-  uint16_t* w1 = w;
-  uint16_t* w2 = w1 + MLP_H * MLP_LD1;
-  uint16_t* w3 = w2 + MLP_H * MLP_LDH;
-  uint16_t* w4 = w3 + MLP_H * MLP_LDH;
-  for (int n = 0; n < MLP_H; n++)
-    for (int k = 0; k < MLP_IN; k++) w1[n * MLP_LD1 + k] = to_bf16(wt[MLP_W1 + n * MLP_IN + k]);
-  for (int n = 0; n < MLP_H; n++)
-    for (int k = 0; k < MLP_H; k++) {
-      w2[n * MLP_LDH + k] = to_bf16(wt[MLP_W2 + n * MLP_H + k]);
-      w3[n * MLP_LDH + k] = to_bf16(wt[MLP_W3 + n * MLP_H + k]);
-    }
-  for (int n = 0; n < MLP_OUT; n++)
-    for (int k = 0; k < MLP_H; k++) w4[n * MLP_LDH + k] = to_bf16(wt[MLP_W4 + n * MLP_H + k]);
+  // W[out][in] of each layer into its canonical operand layout (pg_mlp.h)
+  auto put = [&](int base, int rows, int K, int src, int in) {
+    for (int n = 0; n < rows; n++)
+      for (int k = 0; k < in; k++) w[base + umma_offset(n, k, K) / 2] = to_bf16(wt[src + n * in + k]);
+  };
+  put(MLP_WU1, MLP_H, MLP_K1, MLP_W1, MLP_IN);
+  put(MLP_WU2, MLP_H, MLP_H, MLP_W2, MLP_H);
+  put(MLP_WU3, MLP_H, MLP_H, MLP_W3, MLP_H);
+  put(MLP_WU4, MLP_OUT, MLP_H, MLP_W4, MLP_H);
   std::memcpy(f, wt + MLP_IN_MEAN, sizeof(float) * (2 * MLP_IN + MLP_OUT));
   float* b = f + 2 * MLP_IN + MLP_OUT;
   std::memcpy(b, wt + MLP_B1, sizeof(float) * MLP_H);
@@ -56,36 +50,19 @@ void mlp_pack(const float* wt, uint16_t* w, float* f) {
 }
 
 // ---------------------------------------------------------------- inference
-// Y = net(X) over rows [0, n), 16 rows at a time per block, the weights
-// staged once per block
-__device__ inline void mlp_rows(const MlpDevice& d, const float* X, int64_t n, float* Y, unsigned char* smem) {
-  if ((int64_t)blockIdx.x * 16 >= n) return;
-  MlpSmem S = mlp_smem_layout(smem);
-  stage_weights(d, S.W, S.F);
-  for (int64_t base = (int64_t)blockIdx.x * 16; base < n; base += (int64_t)gridDim.x * 16) {
-    for (int t = threadIdx.x; t < 16 * MLP_IN; t += blockDim.x) {
-      int64_t r = base + t / MLP_IN;
-      S.X[t] = r < n ? X[r * MLP_IN + t % MLP_IN] : 0.f;
-    }
-    __syncthreads();
-    mlp_group(S, base, n, Y);
-  }
-}
-
 // the standalone forward pass (pg_mlp_forward): features from global memory
-__global__ void __launch_bounds__(32 * MLP_WARPS) mlp_forward_kernel(MlpDevice d, const float* X, int64_t n,
-                                                                     float* Y) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  mlp_rows(d, X, n, Y, smem);
+__global__ void __launch_bounds__(MLP_TC_THREADS) mlp_forward_kernel(MlpDevice d, const float* X, int64_t n, float* Y) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  mlp_tc_rows(d, X, n, Y, smem);
 }
 
 // the learned start's forward pass: min(*count, cap) rows, counted on the
 // device by the collision phase
-__global__ void __launch_bounds__(32 * MLP_WARPS) mlp_count_kernel(MlpDevice d, const float* X, const int* count,
+__global__ void __launch_bounds__(MLP_TC_THREADS) mlp_count_kernel(MlpDevice d, const float* X, const int* count,
                                                                    int64_t cap, float* Y) {
-  extern __shared__ __align__(16) unsigned char smem[];
+  extern __shared__ __align__(128) unsigned char smem[];
   int64_t n = *count;
-  mlp_rows(d, X, n < cap ? n : cap, Y, smem);
+  mlp_tc_rows(d, X, n < cap ? n : cap, Y, smem);
 }
 
 cudaError_t mlp_prepare() {
@@ -95,22 +72,24 @@ cudaError_t mlp_prepare() {
   return e;
 }
 
+// blocks of 128 rows: one resident an SM (its shared memory), at most two
+// waves of a 148-SM GPU; each block stages the weights once and loops
+static unsigned mlp_blocks(int64_t rows) {
+  int64_t b = (rows + MLP_TC_ROWS - 1) / MLP_TC_ROWS;
+  return (unsigned)std::max<int64_t>(1, std::min<int64_t>(b, 296));
+}
+
 cudaError_t mlp_forward_counted(const MlpDevice& d, const float* X, const int* count, int64_t cap, float* Y,
                                 cudaStream_t s) {
-  // the grid covers the capacity; blocks past the device-side count return
-  // at once
-  int64_t blocks = (cap + 15) / 16;
-  if (blocks > 1184) blocks = 1184;
-  if (blocks < 1) return cudaSuccess;
-  mlp_count_kernel<<<(unsigned)blocks, 32 * MLP_WARPS, MLP_SMEM, s>>>(d, X, count, cap, Y);
+  // the grid covers the capacity; blocks past the device-side count return at once
+  if (cap <= 0) return cudaSuccess;
+  mlp_count_kernel<<<mlp_blocks(cap), MLP_TC_THREADS, MLP_SMEM, s>>>(d, X, count, cap, Y);
   return cudaGetLastError();
 }
 
 cudaError_t mlp_forward(const MlpDevice& d, const float* X, int64_t n, float* Y, cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
-  int64_t blocks = (n + 15) / 16;
-  if (blocks > 2048) blocks = 2048;
-  mlp_forward_kernel<<<(unsigned)blocks, 32 * MLP_WARPS, MLP_SMEM, s>>>(d, X, n, Y);
+  mlp_forward_kernel<<<mlp_blocks(n), MLP_TC_THREADS, MLP_SMEM, s>>>(d, X, n, Y);
   return cudaGetLastError();
 }
 
@@ -414,16 +393,22 @@ int pg_mlp_forward(const float* weights, size_t wlen, const float* X, int64_t n,
   DevBufs d;
   uint16_t* dw;
   float *df, *dx, *dy;
+  int* derr;
   MCK(d.alloc(&dw, MLP_BF16_ELEMS));
   MCK(d.alloc(&df, MLP_F32_ELEMS));
   MCK(d.alloc(&dx, (size_t)n * MLP_IN));
   MCK(d.alloc(&dy, (size_t)n * MLP_OUT));
+  MCK(d.alloc(&derr, 1));
+  MCK(cudaMemset(derr, 0, sizeof(int)));
   MCK(cudaMemcpy(dw, wb.data(), sizeof(uint16_t) * MLP_BF16_ELEMS, cudaMemcpyHostToDevice));
   MCK(cudaMemcpy(df, fb.data(), sizeof(float) * MLP_F32_ELEMS, cudaMemcpyHostToDevice));
   MCK(cudaMemcpy(dx, X, sizeof(float) * n * MLP_IN, cudaMemcpyHostToDevice));
   MCK(mlp_prepare());
-  MCK(mlp_forward(MlpDevice{dw, df}, dx, n, dy, 0));
+  MCK(mlp_forward(MlpDevice{dw, df, derr}, dx, n, dy, 0));
   MCK(cudaMemcpy(Y, dy, sizeof(float) * n * MLP_OUT, cudaMemcpyDeviceToHost));
+  int err = 0;
+  MCK(cudaMemcpy(&err, derr, sizeof(int), cudaMemcpyDeviceToHost));
+  if (err) return mlp_fail(PG_ERR_CUDA, "mlp_forward: a wait on the tensor cores ran out");
   return PG_OK;
 }
 

@@ -244,6 +244,7 @@ struct LearnArgs {
   float* rows;      // [cap][4]  converged pyramid row forces (LEARN_DUMP)
   const uint16_t* mlp_w;  // the network (pg_mlp.h MlpDevice)
   const float* mlp_f;
+  int* mlp_err;           // set when a wait of the forward pass on the tensor cores ran out
 };
 struct WorkLayout {
   int qm, cdof, a0, smooth, bias, lh, rinvh, geoms, contacts, meta;
