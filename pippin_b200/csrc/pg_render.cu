@@ -6,7 +6,8 @@
 // go to the earlier triangle, as a depth test `Less` over triangles drawn in
 // order does. Triangles are transformed, clipped at the near plane and set
 // up one per thread; small ones are scanned by their thread, large ones are
-// queued and scanned by the whole block. A resolve pass then recomputes the
+// queued and scanned by the whole block once every triangle is set up (no
+// thread waits for another while drawing). A resolve pass then recomputes the
 // winning triangle at each pixel, interpolates its attributes with
 // perspective correction and shades it (render.metal:67-128), writing
 // RGBA8, linear depth and segmentation in (image, y, x) order (:130-145).
@@ -242,11 +243,22 @@ __device__ __forceinline__ bool in_front(const PV* v, float near_) {
   return (-v[0].a[2]) - near_ >= 0.0f && (-v[1].a[2]) - near_ >= 0.0f && (-v[2].a[2]) - near_ >= 0.0f;
 }
 
+// A large sub-triangle that found the block's queue full: its warp scans it
+// (warp_scan) instead of its thread alone.
+struct Pend {
+  float x[3], y[3], z[3];
+  unsigned id;
+  int b[4];
+  bool on;
+};
+
 // one sub-triangle into the tile's visibility buffer: scanned by its own
-// thread when its bounding box is small, else queued for the whole block
+// thread when its bounding box is small, else queued for the whole block to
+// scan after every triangle has been set up, or, with the queue of qcap
+// entries full, left in *pend for the thread's warp
 template <int RT>
 __device__ __forceinline__ void raster_sub(SV s0, SV s1, SV s2, unsigned id, int tx0, int ty0, int tx1, int ty1,
-                                           unsigned long long* keys, float* queue, int* qn) {
+                                           unsigned long long* keys, float* queue, int* qn, int qcap, Pend* pend) {
   SV s[3] = {s0, s1, s2};
   int ord[3] = {0, 1, 2};
   const float area = orient(s, ord);
@@ -256,16 +268,29 @@ __device__ __forceinline__ void raster_sub(SV s0, SV s1, SV s2, unsigned id, int
   if (b[0] > b[2] || b[1] > b[3]) return;
   const int bw = b[2] - b[0] + 1, npix = bw * (b[3] - b[1] + 1);
   if (npix > BIG_PIX) {
-    float* q = queue + QWORDS * atomicAdd(qn, 1);
+    const int slot = atomicAdd(qn, 1);
+    float* q = queue + QWORDS * (slot < qcap ? slot : 0);
 #pragma unroll
     for (int k = 0; k < 3; k++) {
-      q[k] = s[k].x;
-      q[3 + k] = s[k].y;
-      q[6 + k] = s[k].z;
+      if (slot < qcap) {
+        q[k] = s[k].x;
+        q[3 + k] = s[k].y;
+        q[6 + k] = s[k].z;
+      }
+      pend->x[k] = s[k].x;
+      pend->y[k] = s[k].y;
+      pend->z[k] = s[k].z;
     }
-    q[9] = __uint_as_float(id);
+    if (slot < qcap) {
+      q[9] = __uint_as_float(id);
 #pragma unroll
-    for (int k = 0; k < 4; k++) q[10 + k] = __int_as_float(b[k]);
+      for (int k = 0; k < 4; k++) q[10 + k] = __int_as_float(b[k]);
+      return;
+    }
+    pend->id = id;
+#pragma unroll
+    for (int k = 0; k < 4; k++) pend->b[k] = b[k];
+    pend->on = true;
     return;
   }
   for (int p = 0; p < npix; p++) {
@@ -275,9 +300,37 @@ __device__ __forceinline__ void raster_sub(SV s0, SV s1, SV s2, unsigned id, int
   }
 }
 
+// every lane of the warp calls it: the lanes' pending sub-triangles, one
+// after another, each scanned by the 32 lanes together
+template <int RT>
+__device__ __forceinline__ void warp_scan(const Pend& pd, int ty0, int tx0, unsigned long long* keys) {
+  unsigned m = __ballot_sync(0xffffffffu, pd.on);
+  const int lane = threadIdx.x & 31;
+  while (m) {
+    const int src = __ffs(m) - 1;
+    m &= m - 1;
+    SV s[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+      s[k] = SV{__shfl_sync(0xffffffffu, pd.x[k], src), __shfl_sync(0xffffffffu, pd.y[k], src),
+                __shfl_sync(0xffffffffu, pd.z[k], src), 0.0f};
+    const unsigned id = __shfl_sync(0xffffffffu, pd.id, src);
+    int b[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) b[k] = __shfl_sync(0xffffffffu, pd.b[k], src);
+    const float area = edge(s[0].x, s[0].y, s[1].x, s[1].y, s[2].x, s[2].y);
+    const int bw = b[2] - b[0] + 1, npix = bw * (b[3] - b[1] + 1);
+    for (int p = lane; p < npix; p += 32) {
+      const int px = b[0] + p % bw, py = b[1] + p / bw;
+      const unsigned long long k = frag_key(s, area, px, py, id);
+      if (k != EMPTY) atomicMin(&keys[(py - ty0) * RT + (px - tx0)], k);
+    }
+  }
+}
+
 template <int RT, int NT>
 __global__ void __launch_bounds__(NT, RT == 64 ? 3 : 1) render_kernel(RArgs A) {
-  constexpr int QCAP = 2 * NT;  // queue entries: at most two sub-triangles per thread per round
+  constexpr int QCAP = 2 * NT;  // queue entries for the image's large sub-triangles
   extern __shared__ __align__(16) unsigned char smem[];
   unsigned long long* keys = (unsigned long long*)smem;
   float* queue = (float*)(keys + RT * RT);
@@ -307,48 +360,64 @@ __global__ void __launch_bounds__(NT, RT == 64 ? 3 : 1) render_kernel(RArgs A) {
     for (int g = tid; g < A.ngeom; g += NT) seen[g] = geom_seen(A, g, sg, sa, cp, fx, fy, tx0, ty0, tx1, ty1);
     __syncthreads();
 
-    // ---- visibility
+    // ---- visibility: no thread waits for another while the triangles are
+    // set up and the small ones scanned; the large ones, queued meanwhile,
+    // are scanned by the whole block afterwards (the visibility keys are a
+    // minimum: the order of the updates does not matter)
     for (int base = 0; base < A.ntri; base += NT) {
       const int t = base + tid;
+      // the triangle's one or two sub-triangles (two when the near plane clips it to a quad)
+      SV a[3], c[3];
+      int nsub = 0;
       PV v[3];
       int geom;
       if (t < A.ntri && tri_verts<3>(A, t, sg, sa, cp, v, &geom, seen)) {
         if (in_front(v, A.near_)) {
-          raster_sub<RT>(project(v[0], fx, fy, A), project(v[1], fx, fy, A), project(v[2], fx, fy, A), 2u * t, tx0,
-                         ty0, tx1, ty1, keys, queue, &qn);
+#pragma unroll
+          for (int k = 0; k < 3; k++) a[k] = project(v[k], fx, fy, A);
+          nsub = 1;
         } else {
           PV poly[4];
           const int n = clip_near<3>(v, poly, A.near_);
           if (n >= 3) {
-            const SV p0 = project(poly[0], fx, fy, A), p2 = project(poly[2], fx, fy, A);
-            raster_sub<RT>(p0, project(poly[1], fx, fy, A), p2, 2u * t, tx0, ty0, tx1, ty1, keys, queue, &qn);
-            if (n == 4)
-              raster_sub<RT>(p0, p2, project(poly[3], fx, fy, A), 2u * t + 1u, tx0, ty0, tx1, ty1, keys, queue, &qn);
+            a[0] = project(poly[0], fx, fy, A);
+            a[1] = project(poly[1], fx, fy, A);
+            a[2] = project(poly[2], fx, fy, A);
+            nsub = 1;
+            if (n == 4) {
+              c[0] = a[0];
+              c[1] = a[2];
+              c[2] = project(poly[3], fx, fy, A);
+              nsub = 2;
+            }
           }
         }
       }
-      __syncthreads();
-      const int nq = qn;  // the same value in every thread: the branch below is uniform
-      if (nq > 0) {
-        for (int e = 0; e < nq; e++) {
-          const float* q = queue + QWORDS * e;
-          SV s[3];
-          for (int k = 0; k < 3; k++) s[k] = SV{q[k], q[3 + k], q[6 + k], 0.0f};
-          const float area = edge(s[0].x, s[0].y, s[1].x, s[1].y, s[2].x, s[2].y);
-          const unsigned id = __float_as_uint(q[9]);
-          const int bx0 = __float_as_int(q[10]), by0 = __float_as_int(q[11]);
-          const int bw = __float_as_int(q[12]) - bx0 + 1, npix = bw * (__float_as_int(q[13]) - by0 + 1);
-          for (int p = tid; p < npix; p += NT) {
-            const int px = bx0 + p % bw, py = by0 + p / bw;
-            const unsigned long long k = frag_key(s, area, px, py, id);
-            if (k != EMPTY) atomicMin(&keys[(py - ty0) * RT + (px - tx0)], k);
-          }
-        }
-        __syncthreads();
-        if (tid == 0) qn = 0;
-        __syncthreads();
+      Pend pd;
+      pd.on = false;
+      if (nsub >= 1) raster_sub<RT>(a[0], a[1], a[2], 2u * t, tx0, ty0, tx1, ty1, keys, queue, &qn, QCAP, &pd);
+      warp_scan<RT>(pd, ty0, tx0, keys);
+      pd.on = false;
+      if (nsub >= 2) raster_sub<RT>(c[0], c[1], c[2], 2u * t + 1u, tx0, ty0, tx1, ty1, keys, queue, &qn, QCAP, &pd);
+      warp_scan<RT>(pd, ty0, tx0, keys);
+    }
+    __syncthreads();
+    const int nq = min(qn, QCAP);
+    for (int e = 0; e < nq; e++) {
+      const float* q = queue + QWORDS * e;
+      SV s[3];
+      for (int k = 0; k < 3; k++) s[k] = SV{q[k], q[3 + k], q[6 + k], 0.0f};
+      const float area = edge(s[0].x, s[0].y, s[1].x, s[1].y, s[2].x, s[2].y);
+      const unsigned id = __float_as_uint(q[9]);
+      const int bx0 = __float_as_int(q[10]), by0 = __float_as_int(q[11]);
+      const int bw = __float_as_int(q[12]) - bx0 + 1, npix = bw * (__float_as_int(q[13]) - by0 + 1);
+      for (int p = tid; p < npix; p += NT) {
+        const int px = bx0 + p % bw, py = by0 + p / bw;
+        const unsigned long long k = frag_key(s, area, px, py, id);
+        if (k != EMPTY) atomicMin(&keys[(py - ty0) * RT + (px - tx0)], k);
       }
     }
+    __syncthreads();  // every fragment is in before the resolve reads the keys
 
     // ---- resolve and shade
     const int tw = tx1 - tx0, npx = tw * (ty1 - ty0);
