@@ -69,6 +69,7 @@ def parse():
                     help="skip configs 2-5 (tabletop, hull tumble, contact-free, learned evaluation) in the line")
     ap.add_argument("--extras-steps", type=int, default=50, help="timed substeps of each extra config")
     ap.add_argument("--learned-envs", type=int, default=16384)
+    ap.add_argument("--solver", default="newton", choices=["newton", "pgs"], help="solver of --scene")
     ap.add_argument("--scene", default="", choices=["", "tabletop", "hull_tumble", "cartpole", "arm3hinge", "big_hulls"],
                     help="phase timing of another workload (configs 2-4; big_hulls: hulls of 96 and 276 vertices) "
                     "beside the oracle, instead of the headline")
@@ -446,6 +447,7 @@ def run_ours(args):
         E = args.extras_steps
         extras["tabletop"] = scene_measure("tabletop", 8192, E, 300)
         extras["hull_tumble"] = scene_measure("hull_tumble", 4096, E, 250)
+        extras["hull_tumble_pgs"] = scene_measure("hull_tumble", 4096, E, 250, solver=1)
         extras["cartpole"] = scene_measure("cartpole", 16384, 4 * E, 50)
         extras["arm3hinge"] = scene_measure("arm3hinge", 16384, 4 * E, 50)
         if not args.no_learned:
@@ -559,14 +561,15 @@ def run_learned_eval(args):
         print(json.dumps(line), flush=True)
 
 
-def scene_measure(scene, n, K, W, cpu=True):
+def scene_measure(scene, n, K, W, cpu=True, solver=0):
     """Device env-steps/s and per-phase time of the tabletop (config 3), the
     hull tumble (config 4), the large-hull scene (scenes.big_hulls_xml, with
     the hull tumble's initial velocities) or a contact-free model (config 2: random states
     over the joint ranges, qvel N(0, 1), per-env masses x U[0.5, 2], random
     controls held) after W settling substeps, with the oracle's rate on a
-    bounded sample of the same workload on the host cores beside it. Returns
-    the JSON line as a dict (one GPU)."""
+    bounded sample of the same workload on the host cores beside it; solver
+    0 is Newton, 1 PGS (both sides). Returns the JSON line as a dict (one
+    GPU)."""
     import torch
     from oracle.oracle import CTRL, QPOS, QVEL, Oracle
     from pippin_b200 import CudaPhysics, Field, Param, mjcf, scenes
@@ -622,7 +625,7 @@ def scene_measure(scene, n, K, W, cpu=True):
             set_v(v)
 
     p = CudaPhysics(blob, n)
-    p.set_solver(tolerance=TOL, iterations=ITERS)
+    p.set_solver(kind=solver, tolerance=TOL, iterations=ITERS)
     setup(p, n, lambda pid, elem, vals: p.set_param(Param(pid), elem, range(n), vals), lambda: p.reset(range(n)),
           lambda q: p.set(Field.QPOS, range(n), q), lambda v: p.set(Field.QVEL, range(n), v),
           lambda c: p.set(Field.CTRL, range(n), c))
@@ -650,7 +653,10 @@ def scene_measure(scene, n, K, W, cpu=True):
     # the oracle on a sample of the same workload (same settling, then timed)
     # (the oracle tests every edge pair of the 276-vertex hulls: a small sample)
     cn = 4096 if scene in ("cartpole", "arm3hinge") else (16 if scene == "big_hulls" else 256)
-    line = {"metric": f"{scene} env-steps/s", "value": n * K / (ms * 1e-3), "unit": "env-steps/s",
+    if solver == 1:
+        desc = desc.replace("Newton tol 1e-10 cap", "PGS cap")
+    line = {"metric": f"{scene}{' (PGS)' if solver == 1 else ''} env-steps/s", "value": n * K / (ms * 1e-3),
+            "unit": "env-steps/s",
             "n_gpus": 1, "steps": K, "warmup": W, "ms_per_step": ms / K, "higher_is_better": True, "dtype": "f64",
             "data": "synthetic", "config": {"workload": desc, "envs": n},
             "phases": {k: {"ms_per_launch": v / K, "launch": dict(zip(("lanes_per_env", "envs_per_block", "blocks"),
@@ -660,7 +666,7 @@ def scene_measure(scene, n, K, W, cpu=True):
     if not cpu:
         return line
     o = Oracle(blob, cn, threads=0, fast=True)
-    o.set_solver(tolerance=TOL, iterations=ITERS)
+    o.set_solver(kind=solver, tolerance=TOL, iterations=ITERS)
     setup(o, cn, lambda pid, elem, vals: o.set_param(pid, elem, np.asarray(vals), 0, cn),
           lambda: o.reset(list(range(cn))), lambda q: o.set(QPOS, q), lambda v: o.set(QVEL, v),
           lambda c: o.set(CTRL, c))
@@ -676,7 +682,8 @@ def scene_measure(scene, n, K, W, cpu=True):
 
 
 def run_scene(args):
-    line = scene_measure(args.scene, args.envs, args.steps, max(args.warmup, 3))
+    line = scene_measure(args.scene, args.envs, args.steps, max(args.warmup, 3),
+                         solver=1 if args.solver == "pgs" else 0)
     print(json.dumps(line), flush=True)
 
 
