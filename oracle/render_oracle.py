@@ -149,7 +149,7 @@ def render_image(verts, tris, view, uni, W, H, geoms, app, cams):
             inside = (_owns(e0, x[:, 1], y[:, 1], x[:, 2], y[:, 2]) & _owns(e1, x[:, 2], y[:, 2], x[:, 0], y[:, 0])
                       & _owns(e2, x[:, 0], y[:, 0], x[:, 1], y[:, 1]))
             with np.errstate(all="ignore"):
-                zz = ((e0 * z[:, 0] + e1 * z[:, 1]) + e2 * z[:, 2]) / area
+                zz = ((e0 * z[:, 0] + e1 * z[:, 1]) + e2 * z[:, 2]) * (f32(1) / area)
             inside &= (zz >= 0) & (zz <= 1)
             ids = (2 * tid[r] + sub).astype(np.uint64)[:, None]
             key = (zz.astype(f32).view(np.uint32).astype(np.uint64) << np.uint64(32)) | ids
@@ -173,21 +173,22 @@ def render_image(verts, tris, view, uni, W, H, geoms, app, cams):
         e0 = _edge(x[:, 1], y[:, 1], x[:, 2], y[:, 2], Xh[m], Yh[m])
         e1 = _edge(x[:, 2], y[:, 2], x[:, 0], y[:, 0], Xh[m], Yh[m])
         e2 = _edge(x[:, 0], y[:, 0], x[:, 1], y[:, 1], Xh[m], Yh[m])
-        l = [e0 / area, e1 / area, e2 / area]
-        q = [l[k] / w[:, k] for k in range(3)]
-        Q = (q[0] + q[1]) + q[2]
+        # perspective-correct weights: e_k * (1 / area) * (1 / w_k), normalised by their sum
+        ia = f32(1) / area
+        q = [(e0, e1, e2)[k] * (ia * (f32(1) / w[:, k])) for k in range(3)]
+        iQ = f32(1) / ((q[0] + q[1]) + q[2])
         att = np.take_along_axis(poly[r], S["order"][r][:, :, None], axis=1)  # (n, 3, 8)
-        at = [((q[0] * att[:, 0, 3 + j] + q[1] * att[:, 1, 3 + j]) + q[2] * att[:, 2, 3 + j]) / Q for j in range(5)]
-        d = ((q[0] * w[:, 0] + q[1] * w[:, 1]) + q[2] * w[:, 2]) / Q
-        ln = np.sqrt((at[0] * at[0] + at[1] * at[1]) + at[2] * at[2])
-        n0, n1, n2 = at[0] / ln, at[1] / ln, at[2] / ln
+        at = [((q[0] * att[:, 0, 3 + j] + q[1] * att[:, 1, 3 + j]) + q[2] * att[:, 2, 3 + j]) * iQ for j in range(5)]
+        d = ((q[0] * w[:, 0] + q[1] * w[:, 1]) + q[2] * w[:, 2]) * iQ
+        il = f32(1) / np.sqrt((at[0] * at[0] + at[1] * at[1]) + at[2] * at[2])
+        n0, n1, n2 = at[0] * il, at[1] * il, at[2] * il
         head = np.abs(n2)
         keyl = np.fmax((n0 * L0 + n1 * L1) + n2 * L2, f32(0))
         shade = (f32(0.25) + f32(0.5) * head) + f32(0.35) * keyl
         tg_hit = tg[t_glob[m]]
         flags = vb[tris[t_glob[m], 0], 7]
-        cx = np.floor(at[3] / f32(0.25)).astype(np.int64)
-        cy = np.floor(at[4] / f32(0.25)).astype(np.int64)
+        cx = np.floor(at[3] * f32(4)).astype(np.int64)  # checker squares of 0.25
+        cy = np.floor(at[4] * f32(4)).astype(np.int64)
         checker = np.where(((cx + cy) & 1) == 1, f32(0.8), f32(1.05))
         shade = np.where((flags & 1) == 1, shade * checker, shade)
         col = np.fmin(np.fmax(app[tg_hit, 0:3].astype(f32) * shade[:, None], f32(0)), f32(1))

@@ -160,16 +160,17 @@ __device__ __forceinline__ bool cover(const SV* s, int px, int py, float* e) {
          owns(e[2], s[0].x, s[0].y, s[1].x, s[1].y);
 }
 
-// NDC depth of a covered pixel, interpolated linearly in screen space
-__device__ __forceinline__ float ndc_depth(const SV* s, float area, const float* e) {
-  return ((e[0] * s[0].z + e[1] * s[1].z) + e[2] * s[2].z) / area;
+// NDC depth of a covered pixel, interpolated linearly in screen space (ia:
+// the reciprocal of the sub-triangle's doubled area)
+__device__ __forceinline__ float ndc_depth(const SV* s, float ia, const float* e) {
+  return ((e[0] * s[0].z + e[1] * s[1].z) + e[2] * s[2].z) * ia;
 }
 
 // visibility key of pixel (px, py), or EMPTY
-__device__ __forceinline__ unsigned long long frag_key(const SV* s, float area, int px, int py, unsigned id) {
+__device__ __forceinline__ unsigned long long frag_key(const SV* s, float ia, int px, int py, unsigned id) {
   float e[3];
   if (!cover(s, px, py, e)) return EMPTY;
-  const float z = ndc_depth(s, area, e);
+  const float z = ndc_depth(s, ia, e);
   if (!(z >= 0.0f && z <= 1.0f)) return EMPTY;
   return ((unsigned long long)__float_as_uint(z) << 32) | id;
 }
@@ -293,11 +294,12 @@ __device__ __forceinline__ void raster_sub(SV s0, SV s1, SV s2, unsigned id, int
     pend->on = true;
     return;
   }
-  for (int p = 0; p < npix; p++) {
-    const int px = b[0] + p % bw, py = b[1] + p / bw;
-    const unsigned long long k = frag_key(s, area, px, py, id);
-    if (k != EMPTY) atomicMin(&keys[(py - ty0) * RT + (px - tx0)], k);
-  }
+  const float ia = 1.0f / area;
+  for (int py = b[1]; py <= b[3]; py++)
+    for (int px = b[0]; px <= b[2]; px++) {
+      const unsigned long long k = frag_key(s, ia, px, py, id);
+      if (k != EMPTY) atomicMin(&keys[(py - ty0) * RT + (px - tx0)], k);
+    }
 }
 
 // every lane of the warp calls it: the lanes' pending sub-triangles, one
@@ -318,14 +320,70 @@ __device__ __forceinline__ void warp_scan(const Pend& pd, int ty0, int tx0, unsi
     int b[4];
 #pragma unroll
     for (int k = 0; k < 4; k++) b[k] = __shfl_sync(0xffffffffu, pd.b[k], src);
-    const float area = edge(s[0].x, s[0].y, s[1].x, s[1].y, s[2].x, s[2].y);
+    const float ia = 1.0f / edge(s[0].x, s[0].y, s[1].x, s[1].y, s[2].x, s[2].y);
     const int bw = b[2] - b[0] + 1, npix = bw * (b[3] - b[1] + 1);
     for (int p = lane; p < npix; p += 32) {
       const int px = b[0] + p % bw, py = b[1] + p / bw;
-      const unsigned long long k = frag_key(s, area, px, py, id);
+      const unsigned long long k = frag_key(s, ia, px, py, id);
       if (k != EMPTY) atomicMin(&keys[(py - ty0) * RT + (px - tx0)], k);
     }
   }
+}
+
+// what the resolve needs of the sub-triangle that won a pixel: its screen
+// vertices in the orientation the visibility pass used, their normal and
+// local xy, the weights c[k] = (1 / doubled area) * (1 / w[k]) that turn edge
+// functions into perspective-correct barycentric weights, its geom and flags
+struct Resolved {
+  float x[3], y[3], w[3], c[3], at[15];
+  int geom;
+  uint32_t flags;
+};
+
+__device__ __forceinline__ void resolve_setup(const RArgs& A, unsigned id, const float* sg, const float* sa,
+                                              const float* cp, float fx, float fy, Resolved& R) {
+  const int t = (int)(id >> 1), sub = (int)(id & 1u);
+  PV v[3];
+  tri_verts<8>(A, t, sg, sa, cp, v, &R.geom);
+  PV a0, a1, a2;
+  if (in_front(v, A.near_)) {
+    a0 = v[0];
+    a1 = v[1];
+    a2 = v[2];
+  } else {
+    PV poly[4];
+    clip_near<8>(v, poly, A.near_);
+    a0 = poly[0];
+    a1 = sub ? poly[2] : poly[1];
+    a2 = sub ? poly[3] : poly[2];
+  }
+  SV s[3] = {project(a0, fx, fy, A), project(a1, fx, fy, A), project(a2, fx, fy, A)};
+  float area = edge(s[0].x, s[0].y, s[1].x, s[1].y, s[2].x, s[2].y);
+  if (area < 0.0f) {  // the orientation the visibility pass used
+    const SV ts = s[1];
+    s[1] = s[2];
+    s[2] = ts;
+    const PV ta = a1;
+    a1 = a2;
+    a2 = ta;
+    area = edge(s[0].x, s[0].y, s[1].x, s[1].y, s[2].x, s[2].y);
+  }
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    R.x[k] = s[k].x;
+    R.y[k] = s[k].y;
+    R.w[k] = s[k].w;
+  }
+#pragma unroll
+  for (int j = 0; j < 5; j++) {
+    R.at[j] = a0.a[3 + j];
+    R.at[5 + j] = a1.a[3 + j];
+    R.at[10 + j] = a2.a[3 + j];
+  }
+  const float ia = 1.0f / area;
+#pragma unroll
+  for (int k = 0; k < 3; k++) R.c[k] = ia * (1.0f / s[k].w);
+  R.flags = __float_as_uint(A.verts[8 * (size_t)A.tris[3 * (size_t)t] + 7]);
 }
 
 template <int RT, int NT>
@@ -402,24 +460,37 @@ __global__ void __launch_bounds__(NT, RT == 64 ? 3 : 1) render_kernel(RArgs A) {
       warp_scan<RT>(pd, ty0, tx0, keys);
     }
     __syncthreads();
+    // each queued sub-triangle by the whole block, pixel p of its box to
+    // thread p mod NT; a thread steps its pixel's coordinates by NT pixels
+    // at a time (one division a triangle, none a pixel)
     const int nq = min(qn, QCAP);
     for (int e = 0; e < nq; e++) {
       const float* q = queue + QWORDS * e;
       SV s[3];
       for (int k = 0; k < 3; k++) s[k] = SV{q[k], q[3 + k], q[6 + k], 0.0f};
-      const float area = edge(s[0].x, s[0].y, s[1].x, s[1].y, s[2].x, s[2].y);
+      const float ia = 1.0f / edge(s[0].x, s[0].y, s[1].x, s[1].y, s[2].x, s[2].y);
       const unsigned id = __float_as_uint(q[9]);
       const int bx0 = __float_as_int(q[10]), by0 = __float_as_int(q[11]);
-      const int bw = __float_as_int(q[12]) - bx0 + 1, npix = bw * (__float_as_int(q[13]) - by0 + 1);
-      for (int p = tid; p < npix; p += NT) {
-        const int px = bx0 + p % bw, py = by0 + p / bw;
-        const unsigned long long k = frag_key(s, area, px, py, id);
+      const int bx1 = __float_as_int(q[12]), by1 = __float_as_int(q[13]);
+      const int bw = bx1 - bx0 + 1, dy = NT / bw, dx = NT - dy * bw;
+      int py = by0 + tid / bw, px = bx0 + (tid - (tid / bw) * bw);
+      while (py <= by1) {
+        const unsigned long long k = frag_key(s, ia, px, py, id);
         if (k != EMPTY) atomicMin(&keys[(py - ty0) * RT + (px - tx0)], k);
+        px += dx;
+        py += dy;
+        if (px > bx1) {
+          px -= bw;
+          py++;
+        }
       }
     }
     __syncthreads();  // every fragment is in before the resolve reads the keys
 
-    // ---- resolve and shade
+    // ---- resolve and shade: a thread keeps the set-up of the last triangle
+    // it resolved, which the next pixels it visits mostly share
+    Resolved R;
+    unsigned rid = ~0u;  // no sub-triangle id: ids are 2 * triangle + sub with fewer than 2^30 triangles
     const int tw = tx1 - tx0, npx = tw * (ty1 - ty0);
     for (int p = tid; p < npx; p += NT) {
       const int px = tx0 + p % tw, py = ty0 + p / tw;
@@ -430,53 +501,32 @@ __global__ void __launch_bounds__(NT, RT == 64 ? 3 : 1) render_kernel(RArgs A) {
       int sgid = -1;
       if (key != EMPTY) {
         const unsigned id = (unsigned)(key & 0xffffffffu);
-        const int t = (int)(id >> 1), sub = (int)(id & 1u);
-        PV v[3];
-        int geom;
-        tri_verts<8>(A, t, sg, sa, cp, v, &geom);
-        PV a0, a1, a2;
-        if (in_front(v, A.near_)) {
-          a0 = v[0];
-          a1 = v[1];
-          a2 = v[2];
-        } else {
-          PV poly[4];
-          clip_near<8>(v, poly, A.near_);
-          a0 = poly[0];
-          a1 = sub ? poly[2] : poly[1];
-          a2 = sub ? poly[3] : poly[2];
+        if (id != rid) {
+          rid = id;
+          resolve_setup(A, id, sg, sa, cp, fx, fy, R);
         }
-        SV s[3] = {project(a0, fx, fy, A), project(a1, fx, fy, A), project(a2, fx, fy, A)};
-        float area = edge(s[0].x, s[0].y, s[1].x, s[1].y, s[2].x, s[2].y);
-        if (area < 0.0f) {  // the orientation the visibility pass used
-          const SV ts = s[1];
-          s[1] = s[2];
-          s[2] = ts;
-          const PV ta = a1;
-          a1 = a2;
-          a2 = ta;
-          area = edge(s[0].x, s[0].y, s[1].x, s[1].y, s[2].x, s[2].y);
-        }
+        const SV s[3] = {{R.x[0], R.y[0], 0.0f, R.w[0]}, {R.x[1], R.y[1], 0.0f, R.w[1]},
+                         {R.x[2], R.y[2], 0.0f, R.w[2]}};
         float e[3];
         cover(s, px, py, e);
         float q[3];
 #pragma unroll
-        for (int k = 0; k < 3; k++) q[k] = (e[k] / area) / s[k].w;
-        const float Q = (q[0] + q[1]) + q[2];
+        for (int k = 0; k < 3; k++) q[k] = e[k] * R.c[k];
+        const float iQ = 1.0f / ((q[0] + q[1]) + q[2]);
         float at[6];  // normal xyz, local xy, linear depth
 #pragma unroll
-        for (int j = 0; j < 5; j++) at[j] = ((q[0] * a0.a[3 + j] + q[1] * a1.a[3 + j]) + q[2] * a2.a[3 + j]) / Q;
-        at[5] = ((q[0] * s[0].w + q[1] * s[1].w) + q[2] * s[2].w) / Q;
-        const float len = sqrtf((at[0] * at[0] + at[1] * at[1]) + at[2] * at[2]);
-        const float n0 = at[0] / len, n1 = at[1] / len, n2 = at[2] / len;
+        for (int j = 0; j < 5; j++) at[j] = ((q[0] * R.at[j] + q[1] * R.at[5 + j]) + q[2] * R.at[10 + j]) * iQ;
+        at[5] = ((q[0] * s[0].w + q[1] * s[1].w) + q[2] * s[2].w) * iQ;
+        const float il = 1.0f / sqrtf((at[0] * at[0] + at[1] * at[1]) + at[2] * at[2]);
+        const float n0 = at[0] * il, n1 = at[1] * il, n2 = at[2] * il;
         const float head = fabsf(n2);
         const float keyl = fmaxf((n0 * A.L0 + n1 * A.L1) + n2 * A.L2, 0.0f);
         float shade = (0.25f + 0.5f * head) + 0.35f * keyl;
-        const uint32_t flags = __float_as_uint(A.verts[8 * (size_t)A.tris[3 * (size_t)t] + 7]);
-        if (flags & 1u) {
-          const int cx = (int)floorf(at[3] / 0.25f), cy = (int)floorf(at[4] / 0.25f);
+        if (R.flags & 1u) {
+          const int cx = (int)floorf(at[3] * 4.0f), cy = (int)floorf(at[4] * 4.0f);  // checker squares of 0.25
           shade = shade * (((cx + cy) & 1) ? 0.8f : 1.05f);
         }
+        const int geom = R.geom;
         const float* ap = sa + 8 * geom;
         unsigned char u[3];
 #pragma unroll
