@@ -186,6 +186,38 @@ __device__ __forceinline__ void bbox(const SV* s, int tx0, int ty0, int tx1, int
   b[3] = min(ty1 - 1, (int)floorf(fminf(mxy, 1.0e6f) - 0.25f));
 }
 
+// Blocks of BLK x BLK pixels that a queued sub-triangle cannot cover are
+// skipped as a whole. An edge function as `edge` evaluates it,
+// fl(fl(A * fl(Y - ay)) - fl(B * fl(X - ax))) with A = fl(bx - ax) and
+// B = fl(by - ay), is monotonic in X along a row (non-increasing for B > 0)
+// and in Y along a column (non-decreasing for A > 0), since every rounding
+// in it is monotonic; `owns` is a threshold on it. So over a rectangle of
+// pixel centres the edge is largest at one corner picked by the signs of A
+// and B, and a rectangle whose corner fails an edge has no centre that
+// passes it: the test drops exactly pixels the per-pixel test rejects. It
+// is applied only when every coordinate is below 1e18 in magnitude, where no
+// product overflows.
+constexpr int BLK = 4;  // blocks of 4 x 4 pixels: a half warp scans one
+
+__device__ __forceinline__ bool edge_may_own(const SV& a, const SV& b, int x0, int x1, int y0, int y1) {
+  const int x = (b.y - a.y) > 0.0f ? x0 : x1;
+  const int y = (b.x - a.x) > 0.0f ? y1 : y0;
+  return owns(edge(a.x, a.y, b.x, b.y, (float)x + 0.5f, (float)y + 0.5f), a.x, a.y, b.x, b.y);
+}
+
+// false when no pixel centre of [x0, x1] x [y0, y1] is covered (edges in `cover`'s order)
+__device__ __forceinline__ bool rect_may_cover(const SV* s, bool tame, int x0, int x1, int y0, int y1) {
+  return !tame || (edge_may_own(s[1], s[2], x0, x1, y0, y1) && edge_may_own(s[2], s[0], x0, x1, y0, y1) &&
+                   edge_may_own(s[0], s[1], x0, x1, y0, y1));
+}
+
+__device__ __forceinline__ bool tame_coords(const SV* s) {
+  bool ok = true;
+#pragma unroll
+  for (int k = 0; k < 3; k++) ok = ok && fabsf(s[k].x) < 1e18f && fabsf(s[k].y) < 1e18f;
+  return ok;
+}
+
 // triangle t's vertices in camera space (K = 3: position only; K = 8: with
 // normal and local xy); false when its geom is hidden in this environment
 template <int K>
@@ -330,6 +362,51 @@ __device__ __forceinline__ void warp_scan(const Pend& pd, int ty0, int tx0, unsi
   }
 }
 
+// A queued sub-triangle whose box has at most HUGE_PIX pixels, scanned by
+// one warp (every lane calls it): the lanes first test the box's 4 x 4
+// blocks, 32 at a time, with rect_may_cover, then scan the blocks kept, two
+// at a time, a half warp each.
+constexpr int HUGE_PIX = 1024;
+
+template <int RT>
+__device__ __forceinline__ void warp_blocks(const float* q, int tx0, int ty0, unsigned long long* keys) {
+  const int bx0 = __float_as_int(q[10]), by0 = __float_as_int(q[11]);
+  const int bx1 = __float_as_int(q[12]), by1 = __float_as_int(q[13]);
+  if ((bx1 - bx0 + 1) * (by1 - by0 + 1) > HUGE_PIX) return;
+  SV s[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) s[k] = SV{q[k], q[3 + k], q[6 + k], 0.0f};
+  const float ia = 1.0f / edge(s[0].x, s[0].y, s[1].x, s[1].y, s[2].x, s[2].y);
+  const unsigned id = __float_as_uint(q[9]);
+  const bool tame = tame_coords(s);
+  const int lane = threadIdx.x & 31;
+  const int ncx = (bx1 - bx0) / BLK + 1, nb = ncx * ((by1 - by0) / BLK + 1);
+  for (int base = 0; base < nb; base += 32) {
+    const int j = base + lane;
+    bool keep = false;
+    if (j < nb) {
+      const int x0 = bx0 + BLK * (j % ncx), y0 = by0 + BLK * (j / ncx);
+      keep = rect_may_cover(s, tame, x0, min(x0 + BLK - 1, bx1), y0, min(y0 + BLK - 1, by1));
+    }
+    unsigned m = __ballot_sync(0xffffffffu, keep);
+    while (m) {
+      const int a = __ffs(m) - 1;
+      m &= m - 1;
+      const int b = m ? __ffs(m) - 1 : -1;
+      if (m) m &= m - 1;
+      const int mine = lane < 16 ? a : b;
+      if (mine >= 0) {
+        const int jj = base + mine;
+        const int px = bx0 + BLK * (jj % ncx) + (lane & 3), py = by0 + BLK * (jj / ncx) + ((lane >> 2) & 3);
+        if (px <= bx1 && py <= by1) {
+          const unsigned long long k = frag_key(s, ia, px, py, id);
+          if (k != EMPTY) atomicMin(&keys[(py - ty0) * RT + (px - tx0)], k);
+        }
+      }
+    }
+  }
+}
+
 // what the resolve needs of the sub-triangle that won a pixel: its screen
 // vertices in the orientation the visibility pass used, their normal and
 // local xy, the weights c[k] = (1 / doubled area) * (1 / w[k]) that turn edge
@@ -460,19 +537,22 @@ __global__ void __launch_bounds__(NT, RT == 64 ? 3 : 1) render_kernel(RArgs A) {
       warp_scan<RT>(pd, ty0, tx0, keys);
     }
     __syncthreads();
-    // each queued sub-triangle by the whole block, pixel p of its box to
-    // thread p mod NT; a thread steps its pixel's coordinates by NT pixels
-    // at a time (one division a triangle, none a pixel)
+    // the queued sub-triangles: those with boxes over HUGE_PIX pixels (a plane
+    // crossing the view) by the whole block, pixel p of the box to thread
+    // p mod NT, stepping coordinates by NT pixels at a time; the others (long
+    // thin sides of capsules and cylinders, mostly) a warp each (warp_blocks)
     const int nq = min(qn, QCAP);
     for (int e = 0; e < nq; e++) {
       const float* q = queue + QWORDS * e;
+      const int bx0 = __float_as_int(q[10]), by0 = __float_as_int(q[11]);
+      const int bx1 = __float_as_int(q[12]), by1 = __float_as_int(q[13]);
+      const int bw = bx1 - bx0 + 1;
+      if (bw * (by1 - by0 + 1) <= HUGE_PIX) continue;
       SV s[3];
       for (int k = 0; k < 3; k++) s[k] = SV{q[k], q[3 + k], q[6 + k], 0.0f};
       const float ia = 1.0f / edge(s[0].x, s[0].y, s[1].x, s[1].y, s[2].x, s[2].y);
       const unsigned id = __float_as_uint(q[9]);
-      const int bx0 = __float_as_int(q[10]), by0 = __float_as_int(q[11]);
-      const int bx1 = __float_as_int(q[12]), by1 = __float_as_int(q[13]);
-      const int bw = bx1 - bx0 + 1, dy = NT / bw, dx = NT - dy * bw;
+      const int dy = NT / bw, dx = NT - dy * bw;
       int py = by0 + tid / bw, px = bx0 + (tid - (tid / bw) * bw);
       while (py <= by1) {
         const unsigned long long k = frag_key(s, ia, px, py, id);
@@ -485,6 +565,7 @@ __global__ void __launch_bounds__(NT, RT == 64 ? 3 : 1) render_kernel(RArgs A) {
         }
       }
     }
+    for (int e = tid >> 5; e < nq; e += NT / 32) warp_blocks<RT>(queue + QWORDS * e, tx0, ty0, keys);
     __syncthreads();  // every fragment is in before the resolve reads the keys
 
     // ---- resolve and shade: a thread keeps the set-up of the last triangle
