@@ -42,9 +42,10 @@ def _vertex_stage(V, geom_pose, app, cam):
     w = [((g[:, 3 + 3 * i] * p[0] + g[:, 4 + 3 * i] * p[1]) + g[:, 5 + 3 * i] * p[2]) + g[:, i] for i in range(3)]
     d = [w[i] - c[i] for i in range(3)]
     pc = [(c[3 + i] * d[0] + c[6 + i] * d[1]) + c[9 + i] * d[2] for i in range(3)]
-    n = [V[:, 4 + k] / np.fmax(a[:, 4 + k], f32(1e-6)) for k in range(3)]
-    ln = np.sqrt((n[0] * n[0] + n[1] * n[1]) + n[2] * n[2])
-    n = [n[k] / ln for k in range(3)]
+    # normals: times the reciprocal scale (the inverse transpose of a diagonal scale), then unit length
+    n = [V[:, 4 + k] * (f32(1) / np.fmax(a[:, 4 + k], f32(1e-6))) for k in range(3)]
+    il = f32(1) / np.sqrt((n[0] * n[0] + n[1] * n[1]) + n[2] * n[2])
+    n = [n[k] * il for k in range(3)]
     nw = [(g[:, 3 + 3 * i] * n[0] + g[:, 4 + 3 * i] * n[1]) + g[:, 5 + 3 * i] * n[2] for i in range(3)]
     nc = [(c[3 + i] * nw[0] + c[6 + i] * nw[1]) + c[9 + i] * nw[2] for i in range(3)]
     return np.stack(pc + nc + [V[:, 0], V[:, 1]], axis=1).astype(f32)

@@ -74,12 +74,13 @@ __device__ __forceinline__ void cam_xform(const float* v, const float* g, const 
   for (int i = 0; i < 3; i++) pc[i] = (c[3 + i] * d0 + c[6 + i] * d1) + c[9 + i] * d2;
 }
 
-__device__ __forceinline__ void cam_normal(const float* v, const float* g, const float* ap, const float* c, float* nc) {
-  float n0 = v[4] / fmaxf(ap[4], 1e-6f), n1 = v[5] / fmaxf(ap[5], 1e-6f), n2 = v[6] / fmaxf(ap[6], 1e-6f);
-  float len = sqrtf((n0 * n0 + n1 * n1) + n2 * n2);
-  n0 = n0 / len;
-  n1 = n1 / len;
-  n2 = n2 / len;
+// is[k] = 1 / max(scale[k], 1e-6): the inverse transpose of the geom's scale
+__device__ __forceinline__ void cam_normal(const float* v, const float* g, const float* is, const float* c, float* nc) {
+  float n0 = v[4] * is[0], n1 = v[5] * is[1], n2 = v[6] * is[2];
+  const float il = 1.0f / sqrtf((n0 * n0 + n1 * n1) + n2 * n2);
+  n0 = n0 * il;
+  n1 = n1 * il;
+  n2 = n2 * il;
   float w[3];
 #pragma unroll
   for (int i = 0; i < 3; i++) w[i] = (g[3 + 3 * i] * n0 + g[4 + 3 * i] * n1) + g[5 + 3 * i] * n2;
@@ -231,12 +232,17 @@ __device__ __forceinline__ bool tri_verts(const RArgs& A, int t, const float* sg
   const float* ap = sa + 8 * g;
   if (!(ap[3] > 0.0f)) return false;
   if (seen && seen[g] == 0.0f) return false;
+  float is[3];
+  if (K == 8) {
+#pragma unroll
+    for (int k = 0; k < 3; k++) is[k] = 1.0f / fmaxf(ap[4 + k], 1e-6f);
+  }
 #pragma unroll
   for (int k = 0; k < 3; k++) {
     const float* vv = A.verts + 8 * (size_t)ix[k];
     cam_xform(vv, gp, ap, cp, v[k].a);
     if (K == 8) {
-      cam_normal(vv, gp, ap, cp, v[k].a + 3);
+      cam_normal(vv, gp, is, cp, v[k].a + 3);
       v[k].a[6] = vv[0];
       v[k].a[7] = vv[1];
     }
