@@ -203,7 +203,12 @@ def run_reference(args):
 
 # ------------------------------------------------------------------ clocks
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms. start()
+    returns once the first sample is in (nvidia-smi's own start-up, which
+    briefly disturbs the GPU, then falls before the timed region); stop()
+    waits for the next sample and reports those taken from the return of
+    start() to that one, so a region shorter than the period still has the
+    sample that closes it."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -213,6 +218,7 @@ class ClockSampler:
         self.index = index
         self.proc = None
         self.lines = []
+        self.skip = 0
 
     def start(self):
         try:
@@ -223,6 +229,11 @@ class ClockSampler:
             self.thread.start()
         except FileNotFoundError:
             self.proc = None
+            return
+        t0 = time.perf_counter()
+        while not self.lines and self.proc.poll() is None and time.perf_counter() - t0 < 10.0:
+            time.sleep(0.01)
+        self.skip = len(self.lines)
 
     def _read(self):
         for line in self.proc.stdout:
@@ -231,6 +242,10 @@ class ClockSampler:
     def stop(self):
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        n_end, t0 = len(self.lines), time.perf_counter()
+        while len(self.lines) <= n_end and self.proc.poll() is None and time.perf_counter() - t0 < 1.0:
+            time.sleep(0.01)
+        n_end = min(len(self.lines), n_end + 1)
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
@@ -238,7 +253,7 @@ class ClockSampler:
             self.proc.kill()
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for ln in self.lines[self.skip:n_end] or self.lines[-1:]:
             p = [x.strip() for x in ln.split(",")]
             if len(p) < 9:
                 continue

@@ -479,7 +479,7 @@ __global__ void __launch_bounds__(NT, RT == 64 ? 3 : 1) render_kernel(RArgs A) {
   float* sa = sg + 12 * A.ngeom;      // and appearance
   float* cp = sa + 8 * A.ngeom;       // the view's camera pose
   float* seen = cp + 12;              // per geom: may reach this tile
-  __shared__ int qn;
+  __shared__ int qn, tri_next, q_next;  // queue length; next triangle and next queue entry to hand out
   const int tid = threadIdx.x;
   const int tiles = A.tiles_x * A.tiles_y;
   const long long items = (long long)A.nenv * A.nview * tiles;
@@ -496,7 +496,11 @@ __global__ void __launch_bounds__(NT, RT == 64 ? 3 : 1) render_kernel(RArgs A) {
     for (int i = tid; i < 8 * A.ngeom; i += NT) sa[i] = A.app[(size_t)env * A.ngeom * 8 + i];
     if (tid < 12) cp[tid] = cam >= 0 ? A.cams[((size_t)env * A.ncam + cam) * 12 + tid] : vw[4 + tid];
     for (int i = tid; i < RT * RT; i += NT) keys[i] = EMPTY;
-    if (tid == 0) qn = 0;
+    if (tid == 0) {
+      qn = 0;
+      tri_next = 0;
+      q_next = 0;
+    }
     __syncthreads();
     for (int g = tid; g < A.ngeom; g += NT) seen[g] = geom_seen(A, g, sg, sa, cp, fx, fy, tx0, ty0, tx1, ty1);
     __syncthreads();
@@ -505,8 +509,15 @@ __global__ void __launch_bounds__(NT, RT == 64 ? 3 : 1) render_kernel(RArgs A) {
     // set up and the small ones scanned; the large ones, queued meanwhile,
     // are scanned by the whole block afterwards (the visibility keys are a
     // minimum: the order of the updates does not matter)
-    for (int base = 0; base < A.ntri; base += NT) {
-      const int t = base + tid;
+    // warps take 32 consecutive triangles at a time, so that none waits at
+    // the barrier below while others still have triangles left
+    const int lane = tid & 31;
+    for (;;) {
+      int base = 0;
+      if (lane == 0) base = atomicAdd(&tri_next, 32);
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (base >= A.ntri) break;
+      const int t = base + lane;
       // the triangle's one or two sub-triangles (two when the near plane clips it to a quad)
       SV a[3], c[3];
       int nsub = 0;
@@ -571,7 +582,13 @@ __global__ void __launch_bounds__(NT, RT == 64 ? 3 : 1) render_kernel(RArgs A) {
         }
       }
     }
-    for (int e = tid >> 5; e < nq; e += NT / 32) warp_blocks<RT>(queue + QWORDS * e, tx0, ty0, keys);
+    for (;;) {  // the other entries, a warp each, handed out one at a time
+      int e = 0;
+      if (lane == 0) e = atomicAdd(&q_next, 1);
+      e = __shfl_sync(0xffffffffu, e, 0);
+      if (e >= nq) break;
+      warp_blocks<RT>(queue + QWORDS * e, tx0, ty0, keys);
+    }
     __syncthreads();  // every fragment is in before the resolve reads the keys
 
     // ---- resolve and shade: a thread keeps the set-up of the last triangle
