@@ -35,9 +35,9 @@ void internal_set_error(const std::string& msg);
 namespace {
 
 // Tiles of RT x RT pixels with NT threads: 64 x 64 with 256 threads (three
-// blocks an SM), or 128 x 128 with 512 threads (one block an SM) for images
-// that fit in one such tile, so that they set up their triangles once. Each
-// tile first culls the geoms whose bounding spheres cannot reach it.
+// blocks an SM) for images up to 64 pixels, else 128 x 128 with 512 threads
+// (one block an SM). Each tile first culls the geoms whose bounding spheres
+// cannot reach it.
 constexpr int BIG_PIX = 64;       // bounding boxes above this many pixels are scanned by the whole block
 constexpr int QWORDS = 14;        // x[3], y[3], z[3], id, x0, y0, x1, y1
 constexpr unsigned long long EMPTY = ~0ull;
@@ -772,14 +772,12 @@ int pg_render_create(const float* vertices, int64_t nvert, const uint32_t* trian
   }
   if (!(uniforms[0] > 0.0f) || !(uniforms[1] > uniforms[0])) return rfail(PG_ERR_INVALID, "need 0 < near < far");
   const size_t smem_limit = 227 * 1024;
-  // One 128 x 128 tile for images above 64 pixels that fit in it (the image's
-  // triangles are set up once instead of once per 64 x 64 tile); 64 x 64 tiles
-  // otherwise, where the per-tile geom culling skips most triangles (Ant at
-  // 256 x 256: 88k frames/s against 69k with 128 x 128 tiles).
+  // 128 x 128 tiles for images above 64 pixels (fewer tiles set up the same
+  // triangles: Ant at 256 x 256, 139k frames/s against 117k with 64 x 64
+  // tiles), 64 x 64 tiles, three blocks an SM, for images up to 64 pixels.
   // PIPPIN_RENDER_TILE=64 or 128 overrides the choice.
   const char* tile_env = std::getenv("PIPPIN_RENDER_TILE");
-  const bool fits128 = width <= 128 && height <= 128 && (width > 64 || height > 64);
-  const int want = tile_env ? std::atoi(tile_env) : (fits128 ? 128 : 64);
+  const int want = tile_env ? std::atoi(tile_env) : (width > 64 || height > 64 ? 128 : 64);
   const bool large = want == 128 && render_smem(128, 512, (int)ngeom) <= smem_limit;
   const size_t smem = large ? render_smem(128, 512, (int)ngeom) : render_smem(64, 256, (int)ngeom);
   if (smem > smem_limit) return rfail(PG_ERR_UNSUPPORTED, "too many geoms for the renderer's shared memory");

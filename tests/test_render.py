@@ -218,8 +218,12 @@ def test_cuda_renderer_passes_the_reference_analytic_tests(check):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("w,h,seed", [(48, 40, 0), (96, 80, 1), (130, 70, 2), (200, 150, 3)])
-def test_cuda_renderer_matches_the_oracle_bit_for_bit(w, h, seed):
+@pytest.mark.parametrize("w,h,seed,tile", [(48, 40, 0, None), (96, 80, 1, None), (130, 70, 2, None), (200, 150, 3, None),
+                                          (48, 40, 0, "128"), (130, 70, 2, "64"), (200, 150, 3, "64")])
+def test_cuda_renderer_matches_the_oracle_bit_for_bit(w, h, seed, tile, monkeypatch):
+    # tile: the renderer's tile edge when not its default (64 up to 64 pixels, else 128)
+    if tile is not None:
+        monkeypatch.setenv("PIPPIN_RENDER_TILE", tile)
     rng = np.random.default_rng(seed)
     sc = random_scene(rng)
     nenv, ng = 3, len(sc.geoms)
