@@ -6,11 +6,12 @@
 // go to the earlier triangle, as a depth test `Less` over triangles drawn in
 // order does. Triangles are transformed, clipped at the near plane and set
 // up one per thread; small ones are scanned by their thread, large ones are
-// queued and scanned by the whole block once every triangle is set up (no
-// thread waits for another while drawing). A resolve pass then recomputes the
-// winning triangle at each pixel, interpolates its attributes with
-// perspective correction and shades it (render.metal:67-128), writing
-// RGBA8, linear depth and segmentation in (image, y, x) order (:130-145).
+// queued and scanned once every triangle is set up (no thread waits for
+// another while drawing): planes by the whole block, thin sides a warp each.
+// A resolve pass then recomputes the winning triangle at each pixel,
+// interpolates its attributes with perspective correction and shades it
+// (render.metal:67-128), writing RGBA8, linear depth and segmentation in
+// (image, y, x) order (:130-145).
 //
 // The file is compiled without FMA contraction: every product and sum is
 // rounded on its own, in the order written, so that a CPU evaluation of the
@@ -38,7 +39,7 @@ namespace {
 // blocks an SM) for images up to 64 pixels, else 128 x 128 with 512 threads
 // (one block an SM). Each tile first culls the geoms whose bounding spheres
 // cannot reach it.
-constexpr int BIG_PIX = 64;       // bounding boxes above this many pixels are scanned by the whole block
+constexpr int BIG_PIX = 64;       // bounding boxes above this many pixels are queued (scanned by a warp or the block)
 constexpr int QWORDS = 14;        // x[3], y[3], z[3], id, x0, y0, x1, y1
 constexpr unsigned long long EMPTY = ~0ull;
 
@@ -507,10 +508,10 @@ __global__ void __launch_bounds__(NT, RT == 64 ? 3 : 1) render_kernel(RArgs A) {
 
     // ---- visibility: no thread waits for another while the triangles are
     // set up and the small ones scanned; the large ones, queued meanwhile,
-    // are scanned by the whole block afterwards (the visibility keys are a
-    // minimum: the order of the updates does not matter)
-    // warps take 32 consecutive triangles at a time, so that none waits at
-    // the barrier below while others still have triangles left
+    // are scanned afterwards (the visibility keys are a minimum: the order of
+    // the updates does not matter). Warps take 32 consecutive triangles at a
+    // time, so that none waits at the barrier below while others still have
+    // triangles left.
     const int lane = tid & 31;
     for (;;) {
       int base = 0;
