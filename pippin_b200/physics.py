@@ -151,6 +151,16 @@ def _pd(a):
     return a.ctypes.data_as(C.POINTER(C.c_double))
 
 
+class _DeviceArray:
+    """__cuda_array_interface__ over FP64 device memory a CudaPhysics owns
+    (it holds the owner, so torch's reference to it keeps the handle alive)."""
+
+    def __init__(self, ptr: int, shape, owner):
+        self.owner = owner
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": "<f8", "data": (int(ptr), False),
+                                         "strides": None, "version": 2}
+
+
 class CudaPhysics:
     """A batch of environments stepped on one GPU by the sm_100a kernels."""
 
@@ -170,6 +180,7 @@ class CudaPhysics:
         self._dims = Dims(d.nq, d.nv, d.nu, d.ngeom, d.ncam)
         self.nbody, self.njnt = d.nbody, d.njnt
         self._n = int(num_envs)
+        self._device = int(device)
 
     # ---- plumbing
     def _check(self, rc: int):
@@ -401,6 +412,23 @@ class CudaPhysics:
         p = C.POINTER(C.c_double)()
         self._check(self._L.pg_field_device_ptr(self._h, int(f), C.byref(p)))
         return C.cast(p, C.c_void_p).value
+
+    def device_view(self, f: Field):
+        """A zero-copy torch tensor (num_envs, width) float64 over this
+        handle's device state for field f: the observation and action buffers
+        an on-GPU policy works on, in place of the host copies of
+        crates/pippin-env/src/pipeline.rs:65-72. The memory stays the handle's:
+        the view keeps this object alive, but close() frees it all the same.
+        The physics writes it on stream(): wait for that stream (or call
+        synchronize()) before reading, and finish writes before the next step.
+        A write through the view is a plain store: set(QPOS) also refreshes the
+        kinematics that poses() reports, a write to the QPOS view does not
+        until the next step. CTRL and QFRC_APPLIED are plain inputs."""
+        import torch
+
+        shape = (self._n, self._dims.width(f))
+        return torch.as_tensor(_DeviceArray(self.device_ptr(f), shape, self),
+                               device=torch.device("cuda", self._device))
 
     def stream(self) -> int:
         return self._L.pg_stream(self._h) or 0

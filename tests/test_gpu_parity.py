@@ -442,6 +442,50 @@ def test_device_poses_equal_host_poses():
     g.close()
 
 
+def test_device_views_are_the_state_in_place():
+    """device_view gives zero-copy torch tensors over the handle's device
+    state: they read what get() returns after each step, and controls written
+    through the CTRL view drive the next steps exactly as set() does."""
+    import torch
+    n = 48
+    m = mjcf.load_string(scenes.ant_xml())
+    rng = np.random.default_rng(6)
+    q, v = random_state(m, n, rng)
+    ctrl = rng.uniform(-1, 1, (n, m.nu))
+    a, b = CudaPhysics(mjcf.to_blob(m), n), CudaPhysics(mjcf.to_blob(m), n)
+    for g in (a, b):
+        g.set(Field.QPOS, range(n), q)
+        g.set(Field.QVEL, range(n), v)
+    qv, cv = b.device_view(Field.QPOS), b.device_view(Field.CTRL)
+    assert qv.shape == (n, m.nq) and cv.shape == (n, m.nu) and qv.dtype == torch.float64 and qv.is_cuda
+    assert qv.data_ptr() == b.device_ptr(Field.QPOS) and cv.data_ptr() == b.device_ptr(Field.CTRL)
+    for k in range(3):
+        a.set(Field.CTRL, range(n), ctrl * (k + 1) / 3)
+        b.synchronize()
+        cv.copy_(torch.from_numpy(ctrl * (k + 1) / 3).to(cv.device))
+        torch.cuda.synchronize()
+        a.step(range(n), 4)
+        b.step(range(n), 4)
+        b.synchronize()
+        np.testing.assert_array_equal(qv.cpu().numpy(), b.get(Field.QPOS, range(n)))
+        np.testing.assert_array_equal(b.get(Field.QPOS, range(n)), a.get(Field.QPOS, range(n)))
+        np.testing.assert_array_equal(b.device_view(Field.QVEL).cpu().numpy(), a.get(Field.QVEL, range(n)))
+    # a policy on the physics stream: the controls are computed from the
+    # viewed qpos and stored in place, in stream order, with no host sync
+    stream = torch.cuda.ExternalStream(b.stream(), device=qv.device)
+    for _ in range(3):
+        # (a halving and a clamp: exact on both sides, so both handles see the same controls)
+        a.set(Field.CTRL, range(n), np.clip(0.5 * a.get(Field.QPOS, range(n))[:, 7:7 + m.nu], -1.0, 1.0))
+        a.step(range(n), 2)
+        with torch.cuda.stream(stream):
+            cv.copy_(torch.clamp(0.5 * qv[:, 7:7 + m.nu], -1.0, 1.0))
+            b.step(range(n), 2)
+    b.synchronize()
+    np.testing.assert_array_equal(qv.cpu().numpy(), a.get(Field.QPOS, range(n)))
+    a.close()
+    b.close()
+
+
 def test_reset_keeps_qacc_and_restores_state():
     n = 4
     m, g, o = pair(scenes.ant_xml(), n)
