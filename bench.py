@@ -45,6 +45,11 @@ PHASE_STAGES = {"smooth": ("kinematics", "crba", "vel_rne", "passive_act", "fact
 # launch. The work record the phases hand each other (12 KB per env, 200 MB
 # at 16384 envs) is larger than the 126 MB L2, so most of it reaches HBM.
 NCU_TRAFFIC_PER_ENV = {"smooth": 9711.0, "collide": 9227.0, "newton": 11132.0}
+# DRAM bytes (read + write) per image of render_kernel, from one ncu capture of a
+# whole frame of 4096 Ant images (the render benchmark's view): 8.2 + 274.0 MB
+# at 64 x 64, 6.8 + 787.6 MB at 128 x 128 (the images written are 12 B a pixel:
+# 49152 and 196608 B an image).
+NCU_RENDER_TRAFFIC_PER_IMAGE = {64: 68894.0, 128: 193948.0}
 
 
 def parse():
@@ -929,9 +934,10 @@ def run_render(args):
                 "gpu_launches": K, "clocks": clock_info,
                 "roofline": {"bound": "hbm", "kernel": "render_kernel", "achieved": out_bytes / (ms * 1e-3) / 1e9,
                              "peak": hbm_peak(), "unit": "GB/s", "frac": out_bytes / (ms * 1e-3) / 1e9 / hbm_peak(),
-                             "traffic": None,
+                             "traffic": NCU_RENDER_TRAFFIC_PER_IMAGE.get(res, 0.0) * n or None,
                              "note": "algorithmic bytes = the images written (12 B a pixel); the poses read are "
-                                     "48 B a geom"}}
+                                     "48 B a geom; traffic = ncu DRAM bytes per image of one frame's capture x "
+                                     "images"}}
         print(json.dumps(line), flush=True)
         r.close()
     phys.close()
