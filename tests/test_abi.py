@@ -68,3 +68,16 @@ def test_static_scratch_capacity_and_rejection():
     msg = _native.last_error()
     assert "bytes of scratch per block" in msg and "use pg_step" in msg
     assert L.pg_static_tiles(0, 8, ctypes.byref(tiles)) == _native.PG_ERR_INVALID
+
+
+def test_device_view_describes_the_state_buffer():
+    """The array interface behind CudaPhysics.device_view: the field's device
+    address, (num_envs, width) float64, row-major, and a reference to the
+    owner that keeps the handle alive while a view exists."""
+    from pippin_b200.physics import _DeviceArray
+    owner = object()
+    a = _DeviceArray(0x7F0000001000, (16384, 15), owner)
+    cai = a.__cuda_array_interface__
+    assert cai["shape"] == (16384, 15) and cai["typestr"] == "<f8" and cai["strides"] is None
+    assert cai["data"] == (0x7F0000001000, False) and cai["version"] == 2
+    assert a.owner is owner
