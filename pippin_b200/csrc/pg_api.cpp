@@ -651,6 +651,7 @@ int choose_grid(Handle* h, int phase, const LaunchCfg& want, LaunchCfg* out) {
   StepArgs a = make_args(h);
   std::vector<int> kinds = {phase};
   if (phase == K_SMOOTH) kinds = {K_SMOOTH, K_SET_CONST, K_POSES};
+  if (phase == K_NEWTON) kinds = {K_NEWTON, K_NEWTON_PLAIN};  // with and without the learned start's code
   int per_sm = 0;
   for (int k : kinds) {
     size_t smem = kernel_smem(k, a, c.tiles_per_block);

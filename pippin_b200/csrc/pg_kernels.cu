@@ -217,9 +217,11 @@ __global__ void __launch_bounds__(256, 2) collide_kernel(const __grid_constant__
 // newton.rs:113-473 and forward.rs:359-389: rows, Newton, the damped
 // solve qacc = (M + hD)^-1 (f + qfrc_constraint), integration.
 // two blocks of 256 threads an SM (128 registers a thread): 28 tiles of 16
-// lanes an SM, one wave for 4096 Ant envs
-template <int G>
-__global__ void __launch_bounds__(256, 2) newton_kernel(const __grid_constant__ StepArgs A) {
+// lanes an SM, one wave for 4096 Ant envs. LEARN = false (newton_plain_kernel,
+// launched when the learned start neither predicts nor collects) leaves the
+// learned start's code out of the kernel.
+template <int G, bool LEARN>
+__device__ __forceinline__ void newton_phase(const StepArgs& A) {
   extern __shared__ __align__(16) unsigned char smem[];
   const DModel& m = stage_model(A, smem);
   cg::thread_block block = cg::this_thread_block();
@@ -288,7 +290,7 @@ __global__ void __launch_bounds__(256, 2) newton_kernel(const __grid_constant__ 
         const float *lfeat = nullptr, *lforce = nullptr;
         float* ldump = nullptr;
         int lnum = 0;
-        if (A.learn.mode == LEARN_DUMP || (A.learn.mode == LEARN_PREDICT && A.warm_mode == WARM_LEARNED)) {
+        if (LEARN && (A.learn.mode == LEARN_DUMP || (A.learn.mode == LEARN_PREDICT && A.warm_mode == WARM_LEARNED))) {
           int lbase = (int)wk[A.k.meta + K_META_LBASE];
           lnum = (int)wk[A.k.meta + K_META_LNUM];
           if (lnum > 0) {
@@ -297,7 +299,7 @@ __global__ void __launch_bounds__(256, 2) newton_kernel(const __grid_constant__ 
             if (A.learn.mode == LEARN_DUMP) ldump = A.learn.rows + (size_t)lbase * 4;
           }
         }
-        iters = newton_solve(T, m, w, A.s, e, nr, acc, warm, lfeat, lforce, lnum, ldump);
+        iters = newton_solve<G, LEARN>(T, m, w, A.s, e, nr, acc, warm, lfeat, lforce, lnum, ldump);
         if (wk[A.k.meta + K_META_DAMPED] != 0.0) {
           const double* lh = w.fac >= 0 ? ws + w.fac : wk + A.k.lh;
           if (w.fac >= 0) load_async(T, ws + w.fac, wk + A.k.lh, nv * nv);
@@ -330,6 +332,20 @@ __global__ void __launch_bounds__(256, 2) newton_kernel(const __grid_constant__ 
     }
     T.sync();
   }
+}
+
+template <int G>
+__global__ void __launch_bounds__(256, 2) newton_kernel(const __grid_constant__ StepArgs A) {
+  newton_phase<G, true>(A);
+}
+template <int G>
+__global__ void __launch_bounds__(256, 2) newton_plain_kernel(const __grid_constant__ StepArgs A) {
+  newton_phase<G, false>(A);
+}
+
+// whether a substep's Newton phase needs the learned start's code
+inline bool newton_learns(const StepArgs& a) {
+  return a.learn.mode == LEARN_DUMP || (a.learn.mode == LEARN_PREDICT && a.warm_mode == WARM_LEARNED);
 }
 
 // ---------------------------------------------------------------- learned start
@@ -628,6 +644,7 @@ static const void* kernel_ptr(int which) {
     case K_SMOOTH: return (const void*)smooth_kernel<G>;
     case K_COLLIDE: return (const void*)collide_kernel<G>;
     case K_NEWTON: return (const void*)newton_kernel<G>;
+    case K_NEWTON_PLAIN: return (const void*)newton_plain_kernel<G>;
     case K_SET_CONST: return (const void*)set_const_kernel<G>;
     case K_POSES: return (const void*)poses_kernel<G>;
   }
@@ -649,7 +666,8 @@ size_t kernel_smem(int which, const StepArgs& a, int tiles_per_block) {
     case K_COLLIDE:
       return staged + (size_t)tiles_per_block *
                           (collide_tile_ints(a.m) * sizeof(int) + collide_cache_doubles(a.m) * sizeof(double));
-    case K_NEWTON: return staged + (size_t)tiles_per_block * a.wn.stride * sizeof(double);
+    case K_NEWTON:
+    case K_NEWTON_PLAIN: return staged + (size_t)tiles_per_block * a.wn.stride * sizeof(double);
     default: return staged + (size_t)tiles_per_block * a.w.stride * sizeof(double);
   }
 }
@@ -694,7 +712,8 @@ cudaError_t launch_substep(const StepArgs& a0, const SubstepCfg& c, cudaStream_t
     e = launch_learn(a, a.learn.mode == LEARN_PREDICT, s);
     if (e != cudaSuccess) return e;
   }
-  PG_LAUNCH(K_NEWTON, newton_kernel, c.newton, a);
+  if (newton_learns(a)) PG_LAUNCH(K_NEWTON, newton_kernel, c.newton, a);
+  else PG_LAUNCH(K_NEWTON_PLAIN, newton_plain_kernel, c.newton, a);
   return cudaSuccess;
 }
 
@@ -746,7 +765,10 @@ cudaError_t launch_phase(int which, const StepArgs& a0, const LaunchCfg& c, cuda
   switch (which) {
     case K_SMOOTH: PG_LAUNCH(K_SMOOTH, smooth_kernel, c, a); break;
     case K_COLLIDE: PG_LAUNCH(K_COLLIDE, collide_kernel, c, a); break;
-    case K_NEWTON: PG_LAUNCH(K_NEWTON, newton_kernel, c, a); break;
+    case K_NEWTON:
+      if (newton_learns(a)) PG_LAUNCH(K_NEWTON, newton_kernel, c, a);
+      else PG_LAUNCH(K_NEWTON_PLAIN, newton_plain_kernel, c, a);
+      break;
     default: return cudaErrorInvalidValue;
   }
   return cudaSuccess;

@@ -7,7 +7,7 @@
 namespace pg {
 
 // tile kernels (one env per tile of G lanes, persistent over a work counter)
-enum { K_SMOOTH = 0, K_COLLIDE = 1, K_NEWTON = 2, K_SET_CONST = 3, K_POSES = 4, K_COUNT = 5 };
+enum { K_SMOOTH = 0, K_COLLIDE = 1, K_NEWTON = 2, K_SET_CONST = 3, K_POSES = 4, K_NEWTON_PLAIN = 5, K_COUNT = 6 };
 
 struct LaunchCfg {
   int G;                // lanes per environment (8, 16, 32)

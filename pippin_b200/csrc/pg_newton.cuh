@@ -1057,11 +1057,18 @@ __device__ void dump_row_forces(const Tile<G>& T, int nv, const double* J, const
   T.sync();
 }
 
-// newton.rs:378-473
-template <int G>
+// newton.rs:378-473. LEARN = false compiles the learned start's inputs out
+// (a kernel for the other warm-start modes carries none of its code).
+template <int G, bool LEARN = true>
 __device__ int newton_solve(const Tile<G>& T, const DModel& m, const WsLayout& w, const ScrLayout& s,
                             const EnvCtx& e, int nr, double* a, const double* warm, const float* lfeat = nullptr,
                             const float* lforce = nullptr, int lnum = 0, float* ldump = nullptr) {
+  if constexpr (!LEARN) {
+    lfeat = nullptr;
+    lforce = nullptr;
+    lnum = 0;
+    ldump = nullptr;
+  }
   int lane = T.lane(), nv = m.nv;
   double* ws = e.ws;
   double* qfrc = ws + w.qfrc_c;
