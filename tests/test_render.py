@@ -117,6 +117,53 @@ def test_oracle_matches_the_reference_analytic_tests(check):
 
 
 # ------------------------------------------------------------- host side
+def test_block_corner_test_never_drops_a_covered_pixel():
+    """The renderer skips a 4 x 4 block of a queued sub-triangle when, for some
+    edge, the ownership test fails at one corner of the block chosen by the
+    signs of A = bx - ax and B = by - ay (pg_render.cu: edge_may_own). That is
+    exact because the IEEE single-precision edge function
+    fl(fl(A * fl(Y - ay)) - fl(B * fl(X - ax))) is monotonic in X along a row
+    and in Y along a column. Checked here with the oracle's own float32 edge
+    and ownership functions on random triangles, small and huge, thin and
+    axis-aligned: no skipped block holds a pixel centre the per-pixel test
+    accepts."""
+    rng = np.random.default_rng(11)
+    px, py = np.meshgrid(np.arange(64), np.arange(64))
+    X, Y = px.astype(f32) + f32(0.5), py.astype(f32) + f32(0.5)
+    checked = skipped = 0
+    for trial in range(600):
+        scale = f32(10.0 ** rng.uniform(-0.5, 7))
+        c = rng.uniform(0, 64, 2)
+        v = (rng.uniform(-1, 1, (3, 2)) * scale + c).astype(f32)
+        if trial % 5 == 0:
+            v[1] = v[0] + (v[1] - v[0]) * f32(1e-3)  # a sliver
+        if trial % 7 == 0:
+            v[2, 1] = v[1, 1]  # a horizontal edge
+        area = O._edge(v[0, 0], v[0, 1], v[1, 0], v[1, 1], v[2, 0], v[2, 1])
+        if not area > 0:
+            v = v[[0, 2, 1]]
+            area = O._edge(v[0, 0], v[0, 1], v[1, 0], v[1, 1], v[2, 0], v[2, 1])
+        if not area > 0 or np.abs(v).max() >= 1e18:
+            continue
+        edges = [(v[1], v[2]), (v[2], v[0]), (v[0], v[1])]  # cover()'s order
+        inside = np.ones_like(X, dtype=bool)
+        for a, b in edges:
+            inside &= O._owns(O._edge(a[0], a[1], b[0], b[1], X, Y), a[0], a[1], b[0], b[1])
+        for by in range(0, 64, 4):
+            for bx in range(0, 64, 4):
+                keep = True
+                for a, b in edges:
+                    x = bx if (b[1] - a[1]) > 0 else bx + 3
+                    y = by + 3 if (b[0] - a[0]) > 0 else by
+                    e = O._edge(a[0], a[1], b[0], b[1], f32(x) + f32(0.5), f32(y) + f32(0.5))
+                    keep &= bool(O._owns(e, a[0], a[1], b[0], b[1]))
+                checked += 1
+                if not keep:
+                    skipped += 1
+                    assert not inside[by:by + 4, bx:bx + 4].any(), (trial, bx, by, v.tolist())
+    assert checked > 50000 and skipped > checked // 4
+
+
 def test_mesh_triangle_counts_and_welding():
     sc = Scene([], [geom(Shape.PLANE, (0, 0, 0.1)), geom(Shape.SPHERE, (0.1, 0, 0)), geom(Shape.CAPSULE, (0.05, 0.2, 0)),
                     geom(Shape.CYLINDER, (0.05, 0.1, 0)), geom(Shape.BOX, (0.1, 0.2, 0.3)),
