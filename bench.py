@@ -38,13 +38,13 @@ ITERS = 30
 PHASE_STAGES = {"smooth": ("kinematics", "crba", "vel_rne", "passive_act", "factor_solve"),
                 "collide": ("collide",),
                 "newton": ("rows", "newton", "pgs", "integrate")}
-# DRAM bytes (read + write) per env of each phase kernel, from one in-situ ncu
-# capture (--cache-control none: the caches hold what the previous launches
+# DRAM bytes (read + write) per env of each phase kernel, from in-situ ncu
+# captures (--cache-control none: the caches hold what the previous launches
 # left) of the headline's phase kernels at 16384 Ant envs after 100 substeps:
-# smooth 65.3 + 93.8 MB, collide 98.0 + 53.2 MB, Newton 132.5 + 49.9 MB per
-# launch. The work record the phases hand each other (12 KB per env, 200 MB
+# smooth 65.3 + 93.8 MB, collide 98.0 + 53.2 MB, Newton (newton_plain_kernel)
+# 131.7 + 48.6 MB per launch. The work record the phases hand each other (12 KB per env, 200 MB
 # at 16384 envs) is larger than the 126 MB L2, so most of it reaches HBM.
-NCU_TRAFFIC_PER_ENV = {"smooth": 9711.0, "collide": 9227.0, "newton": 11132.0}
+NCU_TRAFFIC_PER_ENV = {"smooth": 9711.0, "collide": 9227.0, "newton": 11004.0}
 # DRAM bytes (read + write) per image of render_kernel, from one ncu capture of a
 # whole frame of 4096 Ant images (the render benchmark's view): 8.2 + 274.0 MB
 # at 64 x 64, 6.8 + 787.6 MB at 128 x 128 (the images written are 12 B a pixel:
